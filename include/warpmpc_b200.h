@@ -1,0 +1,225 @@
+/*
+ * warpmpc_b200.h -- C ABI of the B200-native batched fixed-pattern
+ * QDLDL (LDL^T) / OSQP-ADMM library (libwarpmpc_b200.so, sm_100a).
+ *
+ * Every entry point returns an int status (WMPC_OK = 0) and never throws.
+ * wmpc_last_error_string() returns a thread-local message for the last
+ * failure on the calling thread.  All device pointers are caller-owned
+ * (inputs, outputs and workspace); a plan owns only its uploaded pattern
+ * tables.  Compute entry points are stream-ordered and launch-only: they
+ * allocate nothing and do not synchronize the host.
+ *
+ * Layouts.  "Symbolic-major" arrays hold element (i, b) at [i * ld + b]
+ * (rows = KKT / L / value index, columns = instance b), exactly the
+ * (nnz, batch) / (n, batch) layout of the reference's Warp backend
+ * (values_layout="original_symbolic", rhs_layout="symbolic",
+ * warpmpc/jax_qdldl/warp_backend.py:1302-1408).  A "batch stride" of 0
+ * broadcasts one instance over the batch.  "Batch-major" arrays hold
+ * (b, i) at [b * ld + i], the layout of the reference's OSQP API
+ * (warpmpc/jax_osqp/solver.py:934-982).
+ *
+ * Floating point: float32 throughout, the reference's operation order with
+ * separately rounded products and sums (no multiply-add contraction).
+ */
+#ifndef WARPMPC_B200_H
+#define WARPMPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* wmpc_stream_t; /* cudaStream_t */
+
+enum {
+  WMPC_OK = 0,
+  WMPC_ERR_INVALID_ARGUMENT = 1,
+  WMPC_ERR_CUDA = 2,
+  WMPC_ERR_UNSUPPORTED = 3,
+  WMPC_ERR_WORKSPACE = 4,
+  WMPC_ERR_OUT_OF_MEMORY = 5
+};
+
+/* Per-instance status words written by the OSQP entry points. */
+enum {
+  WMPC_STATUS_MAX_ITER = 0,      /* ran max_iter iterations (reference behaviour) */
+  WMPC_STATUS_SOLVED = 1,        /* met the eps_abs/eps_rel termination test */
+  WMPC_STATUS_NONFINITE = 2,     /* a non-finite iterate or residual appeared */
+  WMPC_STATUS_ZERO_PIVOT = 4     /* D had an exact zero or non-finite pivot */
+};
+
+/* ------------------------------------------------------------------ */
+/* Pattern (QDLDL plan) tables, host pointers, int32.                  */
+/* Produced by the host planner (build_qdldl_plan), ragged form of      */
+/* QDLDLPlan: warpmpc/jax_qdldl/types.py:11-53, core.py:147-256.        */
+/* ------------------------------------------------------------------ */
+typedef struct wmpc_pattern_desc {
+  int32_t n;       /* KKT dimension                                   */
+  int32_t nnz_a;   /* stored upper-triangle entries (original order)  */
+  int32_t nnz_l;   /* strictly-lower entries of L                     */
+  const int32_t* perm_to_orig; /* [nnz_a] permuted slot -> original slot */
+  const int32_t* diag_pos;     /* [n] permuted slot of diagonal k        */
+  const int32_t* init_ptr;     /* [n+1] off-diagonal entries of column k */
+  const int32_t* init_rows;    /* [init_ptr[n]]                          */
+  const int32_t* init_pos;     /* [init_ptr[n]] permuted slots           */
+  const int32_t* proc_ptr;     /* [n+1] row program of row k             */
+  const int32_t* proc_cols;    /* [nnz_l] column cidx visited            */
+  const int32_t* proc_lidx;    /* [nnz_l] L slot written                 */
+  const int32_t* proc_offsets; /* [nnz_l] entries of cidx already set    */
+  const int32_t* lp;           /* [n+1] CSC column pointers of L         */
+  const int32_t* li;           /* [nnz_l] CSC row indices of L           */
+  const int32_t* p;            /* [n] permutation (new -> old)           */
+  const int32_t* pinv;         /* [n] inverse permutation                */
+} wmpc_pattern_desc;
+
+typedef struct wmpc_plan wmpc_plan;
+
+/* Upload a pattern to `device`.  Replaces the host plan the reference
+ * builds in build_qdldl_plan (warpmpc/jax_qdldl/core.py:259-311) and the
+ * jnp.asarray uploads of compile_qdldl_warp (warp_backend.py:1230-1286). */
+int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out);
+int wmpc_plan_destroy(wmpc_plan* plan);
+/* Number of int32 table entries resident on the device (diagnostics). */
+int wmpc_plan_info(const wmpc_plan* plan, int32_t* n, int32_t* nnz_a, int32_t* nnz_l,
+                   int32_t* max_row_nnz, int32_t* max_col_nnz);
+
+/* ------------------------------------------------------------------ */
+/* Batched LDL^T factor / solve.                                       */
+/* ------------------------------------------------------------------ */
+
+/* Bytes of device workspace wmpc_factor / wmpc_solve / wmpc_factor_solve
+ * need for `batch` instances (0 when the kernels stage everything in
+ * shared memory). */
+size_t wmpc_factor_workspace_bytes(const wmpc_plan* plan, int32_t batch);
+size_t wmpc_solve_workspace_bytes(const wmpc_plan* plan, int32_t batch);
+
+/* Numeric factorization.  Replaces CompiledQDLDL.factor of the Warp
+ * backend (warp_backend.py:1302-1349 -> _qdldl_factor[_segmented]_transpose_kernel
+ * 41-173).  values: [nnz_a x batch] symbolic-major, original (un-permuted)
+ * upper-CSC order, batch stride values_bstride (0 = one shared matrix).
+ * Outputs lx [nnz_l x batch], d, dinv [n x batch] (ld = batch). */
+int wmpc_factor(const wmpc_plan* plan, const float* values, int64_t values_ld,
+                int32_t values_bstride, float* lx, float* d, float* dinv, int32_t batch,
+                void* workspace, size_t workspace_bytes, wmpc_stream_t stream);
+
+/* Triangular solve x = P^T L^-T D^-1 L^-1 P rhs.  Replaces CompiledQDLDL.solve
+ * (warp_backend.py:1351-1402 -> serial/segmented/level kernels 176-454).
+ * lx [nnz_l x *], dinv [n x *] with batch stride factor_bstride (0 = one
+ * factor shared by every right-hand side); rhs, x [n x batch] (ld = batch);
+ * x may alias rhs. */
+int wmpc_solve(const wmpc_plan* plan, const float* lx, const float* dinv,
+               int32_t factor_bstride, const float* rhs, float* x, int32_t batch,
+               void* workspace, size_t workspace_bytes, wmpc_stream_t stream);
+
+/* factor then solve.  Replaces CompiledQDLDL.factor_and_solve
+ * (warp_backend.py:1404-1408). */
+int wmpc_factor_solve(const wmpc_plan* plan, const float* values, int64_t values_ld,
+                      int32_t values_bstride, const float* rhs, float* x, float* lx, float* d,
+                      float* dinv, int32_t batch, void* workspace, size_t workspace_bytes,
+                      wmpc_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* OSQP problem (FixedOSQPPlan: warpmpc/jax_osqp/types.py:86-132).     */
+/* ------------------------------------------------------------------ */
+typedef struct wmpc_osqp_desc {
+  int32_t n;        /* variables                                      */
+  int32_t m;        /* constraints                                    */
+  int32_t nnz_p;    /* stored upper entries of P                      */
+  int32_t nnz_a;    /* stored entries of A                            */
+  int32_t nnz_kkt;  /* stored upper entries of the KKT matrix         */
+  float sigma, alpha;
+  const float* kkt_base;      /* [nnz_kkt] KKT values (fp32 of the plan's) */
+  const int32_t* p_to_kkt;    /* [nnz_p]  */
+  const float* p_diag_sigma;  /* [nnz_p]  */
+  const int32_t* a_to_kkt;    /* [nnz_a]  */
+  const float* p_scale;       /* [nnz_p]  */
+  const float* a_scale;       /* [nnz_a]  */
+  const int32_t* a_rows;      /* [nnz_a] CSC entry rows of A */
+  const int32_t* a_cols;      /* [nnz_a] */
+  const int32_t* p_full_rows; /* [nnz_pf] both triangles of P, reference order */
+  const int32_t* p_full_cols;
+  const int32_t* p_full_value_map;
+  int32_t nnz_p_full;
+  const float* rho_vec;       /* [m] */
+  const float* rho_inv_vec;   /* [m] */
+  const float* q_scale;       /* [n] c*D        */
+  const float* scaling_d;     /* [n] D          */
+  const float* scaling_dinv;  /* [n] 1/D        */
+  const float* scaling_e;     /* [m] E          */
+  const float* scaling_einv;  /* [m] 1/E        */
+  const float* y_scale;       /* [m] c/E        */
+  const float* y_unscale;     /* [m] E/c        */
+} wmpc_osqp_desc;
+
+typedef struct wmpc_osqp wmpc_osqp;
+
+/* Upload an OSQP problem bound to a KKT plan (same device). */
+int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc_osqp** out);
+int wmpc_osqp_destroy(wmpc_osqp* osqp);
+
+/* Solve options (OSQPSettings subset, warpmpc/jax_osqp/types.py:60-75). */
+typedef struct wmpc_osqp_options {
+  int32_t max_iter;
+  int32_t check_termination; /* 0: exactly max_iter iterations (reference)  */
+  float eps_abs, eps_rel;
+  int32_t warm_start;        /* 1: x0/z0/y0 given (unscaled), 0: zeros       */
+} wmpc_osqp_options;
+
+/* Batched problem data, batch-major.  p_values [pb x nnz_p], a_values
+ * [ab x nnz_a] with pb, ab in {1, batch}; q [batch x n]; l, u [batch x m];
+ * warm start x0 [batch x n], z0, y0 [batch x m] (ignored unless
+ * options.warm_start).  Outputs x [batch x n], z, y [batch x m],
+ * prim_res, dual_res, obj [batch]; iters and status [batch] (int32, may be
+ * NULL). */
+typedef struct wmpc_osqp_batch {
+  int32_t batch;
+  const float* p_values; int32_t p_batch;
+  const float* a_values; int32_t a_batch;
+  const float* q; const float* l; const float* u;
+  const float* x0; const float* z0; const float* y0;
+  float* x; float* z; float* y;
+  float* prim_res; float* dual_res; float* obj;
+  int32_t* iters; int32_t* status;
+} wmpc_osqp_batch;
+
+/* Device workspace bytes for `batch` instances.  mode: WMPC_OSQP_PLAIN or
+ * WMPC_OSQP_PERSISTENT; external_factor: 1 when the caller passes lx/dinv
+ * (solve_with_factor), 0 when the call factors. */
+size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t mode, int32_t external_factor);
+
+enum { WMPC_OSQP_PLAIN = 0, WMPC_OSQP_PERSISTENT = 1 };
+
+/* KKT assembly + numeric factorization.  Replaces CompiledOSQP.factor
+ * (solver.py:799-804: assemble_kkt_values -> transpose -> qdldl.factor).
+ * Factor batch fb = max(p_batch, a_batch); lx [nnz_l x fb], d, dinv
+ * [n+m x fb] symbolic-major. */
+int wmpc_osqp_factor(const wmpc_osqp* osqp, const float* p_values, int32_t p_batch, const float* a_values,
+                     int32_t a_batch, float* lx, float* d, float* dinv, void* workspace,
+                     size_t workspace_bytes, wmpc_stream_t stream);
+
+/* mode WMPC_OSQP_PLAIN: the reference's loop structure with the CUDA
+ * factor/solve as drop-in (solver.py:799-872: one factor, then max_iter x
+ * {wmpc_solve, ADMM update + next right-hand side} as separate launches).
+ * mode WMPC_OSQP_PERSISTENT: one fused launch per instance tile: KKT
+ * assembly + factor + all ADMM iterations + residual epilogue, with an
+ * optional termination test.  Replaces CompiledOSQP.solve /
+ * solve_warm_start (solver.py:934-982).  When lx/dinv are non-NULL the
+ * factorization is taken from them (factor_batch 1 = shared by all
+ * instances, or batch): CompiledOSQP.solve_with_factor[_warm_start]
+ * (solver.py:881-932). */
+int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
+                    const wmpc_osqp_batch* data, const float* lx, const float* dinv,
+                    int32_t factor_batch, int32_t mode, void* workspace, size_t workspace_bytes,
+                    wmpc_stream_t stream);
+
+const char* wmpc_last_error_string(void);
+/* Library version string, e.g. "0.1.0 sm_100a". */
+const char* wmpc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARPMPC_B200_H */

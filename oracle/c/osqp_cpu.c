@@ -1,0 +1,195 @@
+/*
+ * CPU restatement (C, OpenMP over instances) of the reference's batched
+ * fixed-iteration OSQP-ADMM over QDLDL, float32.
+ *
+ * TEST INFRASTRUCTURE ONLY (oracle): the CPU baseline timed by bench.py and
+ * a cross-check of oracle/osqp_ref.py.  Never linked into the product.
+ *
+ * Restates, per instance:
+ *   - KKT value assembly            warpmpc/jax_osqp/solver.py:764-776
+ *   - numeric LDL^T factorization   warpmpc/jax_qdldl/warp_backend.py:41-101
+ *   - triangular solve              warpmpc/jax_qdldl/warp_backend.py:176-218
+ *   - ADMM iteration                warpmpc/jax_osqp/solver.py:806-820
+ *   - scaling, unscaling, residuals warpmpc/jax_osqp/solver.py:842-871
+ * with every product and sum rounded separately (build with
+ * -ffp-contract=off), in the reference's operation order.
+ *
+ * Data layout: batch-major (instance b row of width w at b*w), P/A values
+ * with batch 1 broadcast.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  int n, nnz_a, nnz_l;
+  const int32_t *perm_to_orig, *diag_pos, *init_ptr, *init_rows, *init_pos;
+  const int32_t *proc_ptr, *proc_cols, *proc_lidx, *proc_offsets, *lp, *li, *p, *pinv;
+} oc_pattern;
+
+typedef struct {
+  int n, m, nnz_p, nnz_a, nnz_kkt, nnz_pf;
+  float sigma, alpha;
+  const float* kkt_base;
+  const int32_t* kkt_src; /* -1 base, j P entry, nnz_p+j A entry */
+  const float *p_scale, *p_diag_sigma, *a_scale;
+  const int32_t *a_row_ptr, *a_row_ent, *a_rows, *a_cols, *a_col_ptr;
+  const int32_t *pf_row_ptr, *pf_val, *pf_col;
+  const float *rho, *rho_inv, *q_scale, *scaling_d, *scaling_dinv, *scaling_e, *scaling_einv, *y_scale, *y_unscale;
+} oc_osqp;
+
+static void factor_one(const oc_pattern* pat, const float* kkt /* original order */, float* lx, float* d,
+                       float* dinv, float* y) {
+  const int n = pat->n;
+  for (int i = 0; i < n; ++i) y[i] = 0.0f;
+  for (int k = 0; k < n; ++k) {
+    float dk = kkt[pat->perm_to_orig[pat->diag_pos[k]]];
+    for (int e = pat->init_ptr[k]; e < pat->init_ptr[k + 1]; ++e) {
+      const int row = pat->init_rows[e];
+      y[row] = y[row] + kkt[pat->perm_to_orig[pat->init_pos[e]]];
+    }
+    for (int e = pat->proc_ptr[k]; e < pat->proc_ptr[k + 1]; ++e) {
+      const int cidx = pat->proc_cols[e];
+      const int off = pat->proc_offsets[e];
+      const int base = pat->lp[cidx];
+      const float val = y[cidx];
+      for (int q = 0; q < off; ++q) {
+        const int r = pat->li[base + q];
+        y[r] = y[r] - lx[base + q] * val;
+      }
+      const float lval = val * dinv[cidx];
+      lx[pat->proc_lidx[e]] = lval;
+      dk = dk - val * lval;
+    }
+    d[k] = dk;
+    dinv[k] = 1.0f / dk;
+    for (int e = pat->proc_ptr[k]; e < pat->proc_ptr[k + 1]; ++e) y[pat->proc_cols[e]] = 0.0f;
+  }
+}
+
+/* in-place solve in the permuted space */
+static void solve_permuted(const oc_pattern* pat, const float* lx, const float* dinv, float* x) {
+  const int n = pat->n;
+  for (int col = 0; col < n; ++col) {
+    const float val = x[col];
+    for (int e = pat->lp[col]; e < pat->lp[col + 1]; ++e) {
+      const int r = pat->li[e];
+      x[r] = x[r] - lx[e] * val;
+    }
+  }
+  for (int i = 0; i < n; ++i) x[i] = x[i] * dinv[i];
+  for (int col = n - 1; col >= 0; --col) {
+    float corr = 0.0f;
+    for (int e = pat->lp[col]; e < pat->lp[col + 1]; ++e) corr = corr + lx[e] * x[pat->li[e]];
+    x[col] = x[col] - corr;
+  }
+}
+
+static float clip_nan(float v, float lo, float hi) {
+  float t = (v < lo) ? lo : v;
+  return (t > hi) ? hi : t;
+}
+
+/* Solve `batch` instances; returns 0.  Outputs batch-major. */
+int oc_osqp_solve(const oc_pattern* pat, const oc_osqp* o, int batch, int max_iter, const float* p_values,
+                  int p_batch, const float* a_values, int a_batch, const float* q, const float* l, const float* u,
+                  const float* x0, const float* z0, const float* y0, float* x_out, float* z_out, float* y_out,
+                  float* prim_out, float* dual_out, float* obj_out) {
+  const int n = o->n, m = o->m, nk = n + m;
+#pragma omp parallel
+  {
+    float* kkt = (float*)malloc(sizeof(float) * (size_t)o->nnz_kkt);
+    float* lx = (float*)malloc(sizeof(float) * (size_t)(pat->nnz_l > 0 ? pat->nnz_l : 1));
+    float* d = (float*)malloc(sizeof(float) * (size_t)nk);
+    float* dinv = (float*)malloc(sizeof(float) * (size_t)nk);
+    float* w = (float*)malloc(sizeof(float) * (size_t)nk);
+    float* xs = (float*)malloc(sizeof(float) * (size_t)n);
+    float* zs = (float*)malloc(sizeof(float) * (size_t)m);
+    float* ys = (float*)malloc(sizeof(float) * (size_t)m);
+    float* qs = (float*)malloc(sizeof(float) * (size_t)n);
+    float* ls = (float*)malloc(sizeof(float) * (size_t)m);
+    float* us = (float*)malloc(sizeof(float) * (size_t)m);
+    const float one_minus = 1.0f - o->alpha;
+#pragma omp for schedule(dynamic, 4)
+    for (int b = 0; b < batch; ++b) {
+      const float* pv = p_values + (size_t)(p_batch > 1 ? b : 0) * o->nnz_p;
+      const float* av = a_values + (size_t)(a_batch > 1 ? b : 0) * o->nnz_a;
+      for (int s = 0; s < o->nnz_kkt; ++s) {
+        const int src = o->kkt_src[s];
+        if (src < 0) kkt[s] = o->kkt_base[s];
+        else if (src < o->nnz_p) kkt[s] = pv[src] * o->p_scale[src] + o->p_diag_sigma[src];
+        else kkt[s] = av[src - o->nnz_p] * o->a_scale[src - o->nnz_p];
+      }
+      factor_one(pat, kkt, lx, d, dinv, w);
+      const float* qb = q + (size_t)b * n;
+      const float* lb = l + (size_t)b * m;
+      const float* ub = u + (size_t)b * m;
+      for (int j = 0; j < n; ++j) {
+        qs[j] = qb[j] * o->q_scale[j];
+        xs[j] = x0 ? x0[(size_t)b * n + j] * o->scaling_dinv[j] : 0.0f;
+      }
+      for (int r = 0; r < m; ++r) {
+        ls[r] = lb[r] * o->scaling_e[r];
+        us[r] = ub[r] * o->scaling_e[r];
+        zs[r] = z0 ? z0[(size_t)b * m + r] * o->scaling_e[r] : 0.0f;
+        ys[r] = y0 ? y0[(size_t)b * m + r] * o->y_scale[r] : 0.0f;
+      }
+      for (int it = 0; it < max_iter; ++it) {
+        for (int i = 0; i < nk; ++i) {
+          const int orig = pat->p[i];
+          if (orig < n) w[i] = o->sigma * xs[orig] - qs[orig];
+          else w[i] = zs[orig - n] - o->rho_inv[orig - n] * ys[orig - n];
+        }
+        solve_permuted(pat, lx, dinv, w);
+        for (int i = 0; i < nk; ++i) {
+          const int orig = pat->p[i];
+          const float sol = w[i];
+          if (orig < n) {
+            xs[orig] = o->alpha * sol + one_minus * xs[orig];
+          } else {
+            const int r = orig - n;
+            const float rinv = o->rho_inv[r];
+            const float rz = zs[r] - rinv * ys[r];
+            const float zt = rz + rinv * sol;
+            const float zr = o->alpha * zt + one_minus * zs[r];
+            const float zn = clip_nan(zr + rinv * ys[r], ls[r], us[r]);
+            ys[r] = ys[r] + o->rho[r] * (zr - zn);
+            zs[r] = zn;
+          }
+        }
+      }
+      float* xb = x_out + (size_t)b * n;
+      float* zb = z_out + (size_t)b * m;
+      float* yb = y_out + (size_t)b * m;
+      for (int j = 0; j < n; ++j) xb[j] = xs[j] * o->scaling_d[j];
+      for (int r = 0; r < m; ++r) {
+        zb[r] = zs[r] * o->scaling_einv[r];
+        yb[r] = ys[r] * o->y_unscale[r];
+      }
+      float prim = 0.0f, dual = 0.0f, quad = 0.0f, lin = 0.0f;
+      for (int r = 0; r < m; ++r) {
+        float ax = 0.0f;
+        for (int t = o->a_row_ptr[r]; t < o->a_row_ptr[r + 1]; ++t) {
+          const int e = o->a_row_ent[t];
+          ax = ax + av[e] * xb[o->a_cols[e]];
+        }
+        prim = fmaxf(prim, fabsf(ax - zb[r]));
+      }
+      for (int j = 0; j < n; ++j) {
+        float px = 0.0f;
+        for (int t = o->pf_row_ptr[j]; t < o->pf_row_ptr[j + 1]; ++t) px = px + pv[o->pf_val[t]] * xb[o->pf_col[t]];
+        float aty = 0.0f;
+        for (int e = o->a_col_ptr[j]; e < o->a_col_ptr[j + 1]; ++e) aty = aty + av[e] * yb[o->a_rows[e]];
+        dual = fmaxf(dual, fabsf(px + qb[j] + aty));
+        quad = quad + xb[j] * px;
+        lin = lin + qb[j] * xb[j];
+      }
+      prim_out[b] = prim;
+      dual_out[b] = dual;
+      obj_out[b] = 0.5f * quad + lin;
+    }
+    free(kkt); free(lx); free(d); free(dinv); free(w); free(xs); free(zs); free(ys); free(qs); free(ls); free(us);
+  }
+  return 0;
+}

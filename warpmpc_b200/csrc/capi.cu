@@ -1,0 +1,412 @@
+// extern "C" entry points of libwarpmpc_b200.so (declared in
+// include/warpmpc_b200.h).  Argument validation, table upload, error
+// reporting; all numerics live in qdldl.cu / osqp.cu.
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "osqp.cuh"
+#include "qdldl.cuh"
+
+namespace wmpc {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+size_t osqp_workspace_bytes(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external);
+size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, int ab);
+int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
+                float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s);
+int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+               const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
+               cudaStream_t s);
+
+namespace {
+
+// Scoped device switch: compute entry points run on the plan's device.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) { ok = false; return; }
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) ok = false;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+bool valid_perm(const int32_t* p, int n) {
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; ++i) {
+    if (p[i] < 0 || p[i] >= n || seen[p[i]]) return false;
+    seen[p[i]] = 1;
+  }
+  return true;
+}
+
+bool in_range(const int32_t* v, size_t count, int lo, int hi) {
+  for (size_t i = 0; i < count; ++i)
+    if (v[i] < lo || v[i] >= hi) return false;
+  return true;
+}
+
+bool monotone_ptr(const int32_t* ptr, int n, int total) {
+  if (ptr[0] != 0 || ptr[n] != total) return false;
+  for (int i = 0; i < n; ++i)
+    if (ptr[i + 1] < ptr[i]) return false;
+  return true;
+}
+
+// Pack host arrays into one pinned-free staging vector and upload once.
+struct Packer {
+  std::vector<int32_t> ints;
+  std::vector<std::pair<size_t, const int**>> fixups;
+  void add(const int32_t* src, size_t count, const int** dst) {
+    size_t off = (ints.size() + 31) / 32 * 32;  // 128-byte aligned sub-arrays
+    ints.resize(off + count);
+    if (count) std::memcpy(ints.data() + off, src, count * sizeof(int32_t));
+    fixups.push_back({off, dst});
+  }
+  void addf(const float* src, size_t count, const float** dst) {
+    static_assert(sizeof(float) == sizeof(int32_t), "float size");
+    add(reinterpret_cast<const int32_t*>(src), count, reinterpret_cast<const int**>(dst));
+  }
+  int upload(int** block) {
+    const size_t bytes = (ints.size() ? ints.size() : 1) * sizeof(int32_t);
+    WMPC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(block), bytes));
+    if (!ints.empty()) {
+      cudaError_t e = cudaMemcpy(*block, ints.data(), ints.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        cudaFree(*block);
+        *block = nullptr;
+        return fail(WMPC_ERR_CUDA, "table upload failed: %s", cudaGetErrorString(e));
+      }
+    }
+    for (auto& f : fixups) *f.second = *block + f.first;
+    return WMPC_OK;
+  }
+};
+
+}  // namespace
+}  // namespace wmpc
+
+using namespace wmpc;
+
+extern "C" {
+
+const char* wmpc_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* wmpc_version(void) { return "0.1.0 sm_100a"; }
+
+int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out) {
+  if (!desc || !out) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  const int n = desc->n, nnz_a = desc->nnz_a, nnz_l = desc->nnz_l;
+  if (n <= 0 || nnz_a < n || nnz_l < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "bad sizes n=%d nnz_a=%d nnz_l=%d", n, nnz_a, nnz_l);
+  if (!desc->perm_to_orig || !desc->diag_pos || !desc->init_ptr || !desc->proc_ptr || !desc->lp || !desc->p ||
+      !desc->pinv || (nnz_l && (!desc->proc_cols || !desc->proc_lidx || !desc->proc_offsets || !desc->li)))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "null table pointer");
+  const int n_init = desc->init_ptr[n];
+  // structural validation: every index the kernels dereference is in range
+  if (!valid_perm(desc->p, n) || !valid_perm(desc->pinv, n)) return fail(WMPC_ERR_INVALID_ARGUMENT, "p/pinv are not permutations");
+  for (int i = 0; i < n; ++i)
+    if (desc->pinv[desc->p[i]] != i) return fail(WMPC_ERR_INVALID_ARGUMENT, "pinv is not the inverse of p");
+  if (!valid_perm(desc->perm_to_orig, nnz_a)) return fail(WMPC_ERR_INVALID_ARGUMENT, "perm_to_orig is not a permutation");
+  if (!in_range(desc->diag_pos, n, 0, nnz_a)) return fail(WMPC_ERR_INVALID_ARGUMENT, "diag_pos out of range");
+  if (!monotone_ptr(desc->init_ptr, n, n_init) || n_init > nnz_a) return fail(WMPC_ERR_INVALID_ARGUMENT, "bad init_ptr");
+  if (n_init && (!desc->init_rows || !desc->init_pos)) return fail(WMPC_ERR_INVALID_ARGUMENT, "null init tables");
+  if (!in_range(desc->init_rows, n_init, 0, n) || !in_range(desc->init_pos, n_init, 0, nnz_a))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "init tables out of range");
+  if (!monotone_ptr(desc->proc_ptr, n, nnz_l) || !monotone_ptr(desc->lp, n, nnz_l))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "bad proc_ptr/lp");
+  if (!in_range(desc->proc_cols, nnz_l, 0, n) || !in_range(desc->proc_lidx, nnz_l, 0, nnz_l) ||
+      !in_range(desc->li, nnz_l, 0, n))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "L tables out of range");
+  int max_row = 0, max_col = 0;
+  for (int k = 0; k < n; ++k) {
+    max_row = std::max(max_row, desc->proc_ptr[k + 1] - desc->proc_ptr[k]);
+    max_col = std::max(max_col, desc->lp[k + 1] - desc->lp[k]);
+    for (int e = desc->proc_ptr[k]; e < desc->proc_ptr[k + 1]; ++e) {
+      const int c = desc->proc_cols[e];
+      if (c >= k || desc->proc_offsets[e] < 0 || desc->proc_offsets[e] > desc->lp[c + 1] - desc->lp[c] ||
+          desc->proc_lidx[e] != desc->lp[c] + desc->proc_offsets[e])
+        return fail(WMPC_ERR_INVALID_ARGUMENT, "inconsistent row program at row %d", k);
+    }
+    for (int e = desc->lp[k]; e < desc->lp[k + 1]; ++e)
+      if (desc->li[e] <= k) return fail(WMPC_ERR_INVALID_ARGUMENT, "L is not strictly lower triangular");
+  }
+  DeviceGuard guard(device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", device);
+  auto* plan = new wmpc_plan();
+  plan->device = device;
+  Pattern& pat = plan->pat;
+  pat.n = n;
+  pat.nnz_a = nnz_a;
+  pat.nnz_l = nnz_l;
+  pat.max_row_nnz = max_row;
+  pat.max_col_nnz = max_col;
+  Packer pk;
+  pk.add(desc->perm_to_orig, nnz_a, &pat.perm_to_orig);
+  pk.add(desc->diag_pos, n, &pat.diag_pos);
+  pk.add(desc->init_ptr, n + 1, &pat.init_ptr);
+  pk.add(desc->init_rows, n_init, &pat.init_rows);
+  pk.add(desc->init_pos, n_init, &pat.init_pos);
+  pk.add(desc->proc_ptr, n + 1, &pat.proc_ptr);
+  pk.add(desc->proc_cols, nnz_l, &pat.proc_cols);
+  pk.add(desc->proc_lidx, nnz_l, &pat.proc_lidx);
+  pk.add(desc->proc_offsets, nnz_l, &pat.proc_offsets);
+  pk.add(desc->lp, n + 1, &pat.lp);
+  pk.add(desc->li, nnz_l, &pat.li);
+  pk.add(desc->p, n, &pat.p);
+  pk.add(desc->pinv, n, &pat.pinv);
+  int rc = pk.upload(&plan->table_block);
+  if (rc) {
+    delete plan;
+    return rc;
+  }
+  plan->table_ints = pk.ints.size();
+  *out = plan;
+  return WMPC_OK;
+}
+
+int wmpc_plan_destroy(wmpc_plan* plan) {
+  if (!plan) return WMPC_OK;
+  DeviceGuard guard(plan->device);
+  if (plan->table_block) cudaFree(plan->table_block);
+  delete plan;
+  return WMPC_OK;
+}
+
+int wmpc_plan_info(const wmpc_plan* plan, int32_t* n, int32_t* nnz_a, int32_t* nnz_l, int32_t* max_row_nnz,
+                   int32_t* max_col_nnz) {
+  if (!plan) return fail(WMPC_ERR_INVALID_ARGUMENT, "null plan");
+  if (n) *n = plan->pat.n;
+  if (nnz_a) *nnz_a = plan->pat.nnz_a;
+  if (nnz_l) *nnz_l = plan->pat.nnz_l;
+  if (max_row_nnz) *max_row_nnz = plan->pat.max_row_nnz;
+  if (max_col_nnz) *max_col_nnz = plan->pat.max_col_nnz;
+  return WMPC_OK;
+}
+
+size_t wmpc_factor_workspace_bytes(const wmpc_plan* plan, int32_t batch) {
+  return plan ? factor_workspace_bytes(plan->pat, batch) : 0;
+}
+
+size_t wmpc_solve_workspace_bytes(const wmpc_plan* plan, int32_t batch) {
+  return plan ? solve_workspace_bytes(plan->pat, batch) : 0;
+}
+
+int wmpc_factor(const wmpc_plan* plan, const float* values, int64_t values_ld, int32_t values_bstride, float* lx,
+                float* d, float* dinv, int32_t batch, void* workspace, size_t workspace_bytes,
+                wmpc_stream_t stream) {
+  if (!plan || batch < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "bad plan or batch");
+  if (batch == 0) return WMPC_OK;
+  if (!values || (!lx && plan->pat.nnz_l > 0) || !d || !dinv) return fail(WMPC_ERR_INVALID_ARGUMENT, "null buffer");
+  if ((values_bstride != 0 && values_bstride != 1) || (values_bstride == 1 && values_ld < batch))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "values_ld/values_bstride inconsistent with batch");
+  DeviceGuard guard(plan->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", plan->device);
+  return launch_factor(plan->pat, values, values_ld, values_bstride, lx, d, dinv, batch, workspace,
+                       workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int wmpc_solve(const wmpc_plan* plan, const float* lx, const float* dinv, int32_t factor_bstride,
+               const float* rhs, float* x, int32_t batch, void* workspace, size_t workspace_bytes,
+               wmpc_stream_t stream) {
+  if (!plan || batch < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "bad plan or batch");
+  if (batch == 0) return WMPC_OK;
+  if ((!lx && plan->pat.nnz_l > 0) || !dinv || !rhs || !x) return fail(WMPC_ERR_INVALID_ARGUMENT, "null buffer");
+  if (factor_bstride != 0 && factor_bstride != 1) return fail(WMPC_ERR_INVALID_ARGUMENT, "factor_bstride must be 0 or 1");
+  DeviceGuard guard(plan->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", plan->device);
+  return launch_solve(plan->pat, lx, dinv, factor_bstride, rhs, x, batch, workspace, workspace_bytes,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int wmpc_factor_solve(const wmpc_plan* plan, const float* values, int64_t values_ld, int32_t values_bstride,
+                      const float* rhs, float* x, float* lx, float* d, float* dinv, int32_t batch, void* workspace,
+                      size_t workspace_bytes, wmpc_stream_t stream) {
+  const int kb = values_bstride ? batch : 1;
+  int rc = wmpc_factor(plan, values, values_ld, values_bstride, lx, d, dinv, kb, workspace, workspace_bytes, stream);
+  if (rc) return rc;
+  return wmpc_solve(plan, lx, dinv, values_bstride ? 1 : 0, rhs, x, batch, workspace, workspace_bytes, stream);
+}
+
+int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc_osqp** out) {
+  if (!desc || !kkt_plan || !out) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  const int n = desc->n, m = desc->m, np = desc->nnz_p, na = desc->nnz_a, nk = desc->nnz_kkt, npf = desc->nnz_p_full;
+  if (n <= 0 || m < 0 || np < 0 || na < 0 || nk <= 0 || npf < 0)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "bad OSQP sizes");
+  if (kkt_plan->pat.n != n + m || kkt_plan->pat.nnz_a != nk)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "KKT plan (n=%d nnz=%d) does not match OSQP problem (n+m=%d nnz_kkt=%d)",
+                kkt_plan->pat.n, kkt_plan->pat.nnz_a, n + m, nk);
+  if (!in_range(desc->p_to_kkt, np, 0, nk) || !in_range(desc->a_to_kkt, na, 0, nk) ||
+      !in_range(desc->a_rows, na, 0, m) || !in_range(desc->a_cols, na, 0, n) ||
+      !in_range(desc->p_full_rows, npf, 0, n) || !in_range(desc->p_full_cols, npf, 0, n) ||
+      !in_range(desc->p_full_value_map, npf, 0, np > 0 ? np : 1))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "OSQP index tables out of range");
+  for (int e = 1; e < na; ++e)
+    if (desc->a_cols[e] < desc->a_cols[e - 1]) return fail(WMPC_ERR_INVALID_ARGUMENT, "A entries must be in CSC order");
+
+  // KKT slot sources
+  std::vector<int32_t> kkt_src(nk, -1);
+  for (int j = 0; j < np; ++j) {
+    if (kkt_src[desc->p_to_kkt[j]] != -1) return fail(WMPC_ERR_INVALID_ARGUMENT, "duplicate KKT slot");
+    kkt_src[desc->p_to_kkt[j]] = j;
+  }
+  for (int j = 0; j < na; ++j) {
+    if (kkt_src[desc->a_to_kkt[j]] != -1) return fail(WMPC_ERR_INVALID_ARGUMENT, "duplicate KKT slot");
+    kkt_src[desc->a_to_kkt[j]] = np + j;
+  }
+  // A by rows (stable: ascending entry index within each row)
+  std::vector<int32_t> a_row_ptr(m + 1, 0), a_row_ent(na), a_col_ptr(n + 1, 0);
+  for (int e = 0; e < na; ++e) a_row_ptr[desc->a_rows[e] + 1]++;
+  for (int r = 0; r < m; ++r) a_row_ptr[r + 1] += a_row_ptr[r];
+  {
+    std::vector<int32_t> fillp(a_row_ptr.begin(), a_row_ptr.end() - 1);
+    for (int e = 0; e < na; ++e) a_row_ent[fillp[desc->a_rows[e]]++] = e;
+  }
+  for (int e = 0; e < na; ++e) a_col_ptr[desc->a_cols[e] + 1]++;
+  for (int j = 0; j < n; ++j) a_col_ptr[j + 1] += a_col_ptr[j];
+  // both triangles of P grouped by row, stable in the reference's entry order
+  std::vector<int32_t> pf_row_ptr(n + 1, 0), pf_val(npf), pf_col(npf);
+  for (int t = 0; t < npf; ++t) pf_row_ptr[desc->p_full_rows[t] + 1]++;
+  for (int j = 0; j < n; ++j) pf_row_ptr[j + 1] += pf_row_ptr[j];
+  {
+    std::vector<int32_t> fillp(pf_row_ptr.begin(), pf_row_ptr.end() - 1);
+    for (int t = 0; t < npf; ++t) {
+      const int pos = fillp[desc->p_full_rows[t]]++;
+      pf_val[pos] = desc->p_full_value_map[t];
+      pf_col[pos] = desc->p_full_cols[t];
+    }
+  }
+
+  DeviceGuard guard(kkt_plan->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", kkt_plan->device);
+  auto* q = new wmpc_osqp();
+  q->device = kkt_plan->device;
+  q->kkt_plan = kkt_plan;
+  Osqp& o = q->dev;
+  o.n = n;
+  o.m = m;
+  o.nk = n + m;
+  o.nnz_p = np;
+  o.nnz_a = na;
+  o.nnz_kkt = nk;
+  o.nnz_pf = npf;
+  o.sigma = desc->sigma;
+  o.alpha = desc->alpha;
+  o.one_minus_alpha = 1.0f - desc->alpha;
+  Packer pk;
+  pk.addf(desc->kkt_base, nk, &o.kkt_base);
+  pk.add(kkt_src.data(), nk, &o.kkt_src);
+  pk.addf(desc->p_scale, np, &o.p_scale);
+  pk.addf(desc->p_diag_sigma, np, &o.p_diag_sigma);
+  pk.addf(desc->a_scale, na, &o.a_scale);
+  pk.add(a_row_ptr.data(), m + 1, &o.a_row_ptr);
+  pk.add(a_row_ent.data(), na, &o.a_row_ent);
+  pk.add(desc->a_cols, na, &o.a_cols);
+  pk.add(desc->a_rows, na, &o.a_rows);
+  pk.add(a_col_ptr.data(), n + 1, &o.a_col_ptr);
+  pk.add(pf_row_ptr.data(), n + 1, &o.pf_row_ptr);
+  pk.add(pf_val.data(), npf, &o.pf_val);
+  pk.add(pf_col.data(), npf, &o.pf_col);
+  pk.addf(desc->rho_vec, m, &o.rho);
+  pk.addf(desc->rho_inv_vec, m, &o.rho_inv);
+  pk.addf(desc->q_scale, n, &o.q_scale);
+  pk.addf(desc->scaling_d, n, &o.scaling_d);
+  pk.addf(desc->scaling_dinv, n, &o.scaling_dinv);
+  pk.addf(desc->scaling_e, m, &o.scaling_e);
+  pk.addf(desc->scaling_einv, m, &o.scaling_einv);
+  pk.addf(desc->y_scale, m, &o.y_scale);
+  pk.addf(desc->y_unscale, m, &o.y_unscale);
+  int* block = nullptr;
+  int rc = pk.upload(&block);
+  if (rc) {
+    delete q;
+    return rc;
+  }
+  q->block = block;
+  *out = q;
+  return WMPC_OK;
+}
+
+int wmpc_osqp_destroy(wmpc_osqp* osqp) {
+  if (!osqp) return WMPC_OK;
+  DeviceGuard guard(osqp->device);
+  if (osqp->block) cudaFree(osqp->block);
+  delete osqp;
+  return WMPC_OK;
+}
+
+size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t mode, int32_t external_factor) {
+  if (!osqp || batch <= 0) return 0;
+  // P/A value batches may be 1 or `batch`; size for the larger case, and
+  // for the factorization-only call as well
+  const size_t solve = osqp_workspace_bytes(osqp->dev, osqp->kkt_plan->pat, batch, batch, batch, mode,
+                                            external_factor != 0);
+  const size_t fac = osqp_factor_workspace_bytes(osqp->dev, osqp->kkt_plan->pat, batch, batch);
+  return solve > fac ? solve : fac;
+}
+
+int wmpc_osqp_factor(const wmpc_osqp* osqp, const float* p_values, int32_t p_batch, const float* a_values,
+                     int32_t a_batch, float* lx, float* d, float* dinv, void* workspace, size_t workspace_bytes,
+                     wmpc_stream_t stream) {
+  if (!osqp || !p_values || !a_values || (!lx && osqp->kkt_plan->pat.nnz_l > 0) || !d || !dinv)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  if (p_batch <= 0 || a_batch <= 0 || (p_batch != 1 && a_batch != 1 && p_batch != a_batch))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "p_batch/a_batch must be positive and equal unless one is 1");
+  DeviceGuard guard(osqp->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
+  return osqp_factor(osqp->dev, osqp->kkt_plan->pat, p_values, p_batch, a_values, a_batch, lx, d, dinv, workspace,
+                     workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options, const wmpc_osqp_batch* data,
+                    const float* lx, const float* dinv, int32_t factor_batch, int32_t mode, void* workspace,
+                    size_t workspace_bytes, wmpc_stream_t stream) {
+  if (!osqp || !options || !data) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  if (mode != WMPC_OSQP_PLAIN && mode != WMPC_OSQP_PERSISTENT) return fail(WMPC_ERR_INVALID_ARGUMENT, "unknown mode %d", mode);
+  const wmpc_osqp_batch& d = *data;
+  if (d.batch < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "negative batch");
+  if (d.batch == 0) return WMPC_OK;
+  if ((d.p_batch != 1 && d.p_batch != d.batch) || (d.a_batch != 1 && d.a_batch != d.batch))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "p_batch/a_batch must be 1 or batch");
+  if (!d.p_values || !d.a_values || !d.q || !d.l || !d.u || !d.x || !d.z || !d.y || !d.prim_res || !d.dual_res || !d.obj)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "null buffer");
+  if ((lx == nullptr) != (dinv == nullptr)) return fail(WMPC_ERR_INVALID_ARGUMENT, "lx and dinv go together");
+  if (lx && factor_batch != 1 && factor_batch != d.batch)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "factor_batch must be 1 or batch");
+  if (options->max_iter < 0 || options->check_termination < 0)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "max_iter and check_termination must be nonnegative");
+  if (mode == WMPC_OSQP_PLAIN && options->check_termination > 0)
+    return fail(WMPC_ERR_UNSUPPORTED, "the per-call path runs exactly max_iter iterations (check_termination=0)");
+  DeviceGuard guard(osqp->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
+  return osqp_solve(osqp->dev, osqp->kkt_plan->pat, *options, d, lx, dinv, factor_batch, mode, workspace,
+                    workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,543 @@
+// Batched fixed-pattern OSQP-ADMM (sm_100a): layout transposes, KKT
+// assembly, the per-call ("plain") ADMM loop pieces, the fused persistent
+// solve, and the residual epilogue.
+//
+// Arithmetic follows warpmpc/jax_osqp/solver.py operation by operation
+// (assemble_kkt_values 764-776, _iterate 806-820, scaling/unscaling 842-865,
+// residuals 866-871); -fmad=false keeps every product and sum separately
+// rounded.
+#include "common.cuh"
+#include "osqp.cuh"
+#include "qdldl.cuh"
+
+namespace wmpc {
+
+// ---------------------------------------------------------------------------
+// layout transposes (batch-major API <-> symbolic-major kernels)
+// ---------------------------------------------------------------------------
+
+// dst[j, b] = src[b, j] * scale[j]   (scale may be null)
+__global__ void transpose_in_kernel(const float* __restrict__ src, long long lds, int rows, int cols,
+                                    const float* __restrict__ scale, float* __restrict__ dst, long long ldd) {
+  __shared__ float tile[32][33];
+  const int j0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int b = b0 + k, j = j0 + threadIdx.x;
+    if (b < rows && j < cols) tile[k][threadIdx.x] = src[(long long)b * lds + j];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int j = j0 + k, b = b0 + threadIdx.x;
+    if (b < rows && j < cols) {
+      float v = tile[threadIdx.x][k];
+      if (scale) v = v * scale[j];
+      dst[(long long)j * ldd + b] = v;
+    }
+  }
+}
+
+// dst[b, j] = src[j, b]
+__global__ void transpose_out_kernel(const float* __restrict__ src, long long lds, int rows, int cols,
+                                     float* __restrict__ dst, long long ldd) {
+  __shared__ float tile[32][33];
+  const int j0 = blockIdx.y * 32, b0 = blockIdx.x * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int j = j0 + k, b = b0 + threadIdx.x;
+    if (b < rows && j < cols) tile[k][threadIdx.x] = src[(long long)j * lds + b];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int b = b0 + k, j = j0 + threadIdx.x;
+    if (b < rows && j < cols) dst[(long long)b * ldd + j] = tile[threadIdx.x][k];
+  }
+}
+
+static int transpose_in(const float* src, long long lds, int rows, int cols, const float* scale, float* dst,
+                        long long ldd, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return WMPC_OK;
+  dim3 grid(ceil_div(cols, 32), ceil_div(rows, 32));
+  transpose_in_kernel<<<grid, dim3(32, 8), 0, s>>>(src, lds, rows, cols, scale, dst, ldd);
+  WMPC_LAUNCH_CHECK();
+  return WMPC_OK;
+}
+
+static int transpose_out(const float* src, long long lds, int rows, int cols, float* dst, long long ldd,
+                         cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return WMPC_OK;
+  dim3 grid(ceil_div(rows, 32), ceil_div(cols, 32));
+  transpose_out_kernel<<<grid, dim3(32, 8), 0, s>>>(src, lds, rows, cols, dst, ldd);
+  WMPC_LAUNCH_CHECK();
+  return WMPC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// per-instance views of the problem data (symbolic-major)
+// ---------------------------------------------------------------------------
+
+struct InstanceData {
+  const float* pT;  // P values of this instance: pT[j * ldp]
+  long long ldp;
+  const float* aT;
+  long long lda;
+  __device__ __forceinline__ float p(int j) const { return pT[(long long)j * ldp]; }
+  __device__ __forceinline__ float a(int j) const { return aT[(long long)j * lda]; }
+};
+
+// KKT value of original KKT slot s (solver.py:764-776).
+__device__ __forceinline__ float kkt_value(const Osqp& o, const InstanceData& in, int s) {
+  const int src = __ldg(o.kkt_src + s);
+  if (src < 0) return __ldg(o.kkt_base + s);
+  if (src < o.nnz_p) return in.p(src) * __ldg(o.p_scale + src) + __ldg(o.p_diag_sigma + src);
+  const int j = src - o.nnz_p;
+  return in.a(j) * __ldg(o.a_scale + j);
+}
+
+__global__ void assemble_kkt_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
+                                    const float* __restrict__ aT, long long lda, int sba, float* __restrict__ kkt,
+                                    int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
+  for (int s = blockIdx.y; s < o.nnz_kkt; s += gridDim.y) kkt[(long long)s * batch + b] = kkt_value(o, in, s);
+}
+
+// ---------------------------------------------------------------------------
+// ADMM pieces (scaled space, symbolic-major state)
+// ---------------------------------------------------------------------------
+
+struct State {
+  float* x;  // [n, batch]
+  float* z;  // [m, batch]
+  float* y;  // [m, batch]
+  const float* qs;  // scaled q [n, batch]
+  const float* ls;  // scaled l [m, batch]
+  const float* us;  // scaled u [m, batch]
+  long long ld;     // = batch
+};
+
+__device__ __forceinline__ float clip_nan(float v, float lo, float hi) {
+  // jnp.minimum(jnp.maximum(v, lo), hi) with NaN propagation
+  float t = (v < lo) ? lo : v;
+  return (t > hi) ? hi : t;
+}
+
+// rhs entry of KKT index `orig` (original, un-permuted numbering)
+__device__ __forceinline__ float rhs_entry(const Osqp& o, const State& st, int orig, int b) {
+  if (orig < o.n) {
+    const long long k = (long long)orig * st.ld + b;
+    return o.sigma * st.x[k] - st.qs[k];
+  }
+  const int r = orig - o.n;
+  const long long k = (long long)r * st.ld + b;
+  return st.z[k] - __ldg(o.rho_inv + r) * st.y[k];
+}
+
+// ADMM update of KKT index `orig` given the solve output `sol`
+// (solver.py:813-819); returns the next iteration's rhs entry.
+__device__ __forceinline__ float admm_update(const Osqp& o, const State& st, int orig, int b, float sol) {
+  if (orig < o.n) {
+    const long long k = (long long)orig * st.ld + b;
+    const float x = st.x[k];
+    const float xn = o.alpha * sol + o.one_minus_alpha * x;
+    st.x[k] = xn;
+    return o.sigma * xn - st.qs[k];
+  }
+  const int r = orig - o.n;
+  const long long k = (long long)r * st.ld + b;
+  const float rinv = __ldg(o.rho_inv + r);
+  const float z = st.z[k], y = st.y[k];
+  const float rz = z - rinv * y;
+  const float zt = rz + rinv * sol;
+  const float zr = o.alpha * zt + o.one_minus_alpha * z;
+  const float zn = clip_nan(zr + rinv * y, st.ls[k], st.us[k]);
+  const float yn = y + __ldg(o.rho + r) * (zr - zn);
+  st.z[k] = zn;
+  st.y[k] = yn;
+  return zn - rinv * yn;
+}
+
+__global__ void admm_first_rhs_kernel(Osqp o, State st, float* __restrict__ rhs, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  for (int i = blockIdx.y; i < o.nk; i += gridDim.y) rhs[(long long)i * batch + b] = rhs_entry(o, st, i, b);
+}
+
+__global__ void admm_update_kernel(Osqp o, State st, float* __restrict__ rhs, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  for (int i = blockIdx.y; i < o.nk; i += gridDim.y) {
+    const long long k = (long long)i * batch + b;
+    rhs[k] = admm_update(o, st, i, b, rhs[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// residuals (solver.py:863-871) -- unscaled, one lane per instance
+// ---------------------------------------------------------------------------
+
+struct Residuals {
+  float prim, dual, obj;
+  float ax_norm, z_norm, px_norm, aty_norm, q_norm;
+};
+
+// q is the unscaled linear term: q[j * ldq]
+__device__ Residuals residuals(const Osqp& o, const InstanceData& in, const State& st, int b,
+                               const float* __restrict__ q, long long ldq) {
+  Residuals r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  auto xu = [&](int j) { return st.x[(long long)j * st.ld + b] * __ldg(o.scaling_d + j); };
+  for (int row = 0; row < o.m; ++row) {
+    float ax = 0.0f;
+    const int e0 = __ldg(o.a_row_ptr + row), e1 = __ldg(o.a_row_ptr + row + 1);
+    for (int t = e0; t < e1; ++t) {
+      const int e = __ldg(o.a_row_ent + t);
+      ax = ax + in.a(e) * xu(__ldg(o.a_cols + e));
+    }
+    const float zu = st.z[(long long)row * st.ld + b] * __ldg(o.scaling_einv + row);
+    r.prim = fmaxf(r.prim, fabsf(ax - zu));
+    r.ax_norm = fmaxf(r.ax_norm, fabsf(ax));
+    r.z_norm = fmaxf(r.z_norm, fabsf(zu));
+  }
+  float quad = 0.0f, lin = 0.0f;
+  for (int j = 0; j < o.n; ++j) {
+    float px = 0.0f;
+    const int f0 = __ldg(o.pf_row_ptr + j), f1 = __ldg(o.pf_row_ptr + j + 1);
+    for (int t = f0; t < f1; ++t) px = px + in.p(__ldg(o.pf_val + t)) * xu(__ldg(o.pf_col + t));
+    float aty = 0.0f;
+    const int c0 = __ldg(o.a_col_ptr + j), c1 = __ldg(o.a_col_ptr + j + 1);
+    for (int e = c0; e < c1; ++e) {
+      const int row = __ldg(o.a_rows + e);
+      aty = aty + in.a(e) * (st.y[(long long)row * st.ld + b] * __ldg(o.y_unscale + row));
+    }
+    const float qj = q[(long long)j * ldq];
+    const float xj = xu(j);
+    r.dual = fmaxf(r.dual, fabsf(px + qj + aty));
+    r.px_norm = fmaxf(r.px_norm, fabsf(px));
+    r.aty_norm = fmaxf(r.aty_norm, fabsf(aty));
+    r.q_norm = fmaxf(r.q_norm, fabsf(qj));
+    quad = quad + xj * px;
+    lin = lin + qj * xj;
+  }
+  r.obj = 0.5f * quad + lin;
+  return r;
+}
+
+__device__ __forceinline__ void unscale_in_place(const Osqp& o, const State& st, int b) {
+  for (int j = 0; j < o.n; ++j) {
+    const long long k = (long long)j * st.ld + b;
+    st.x[k] = st.x[k] * __ldg(o.scaling_d + j);
+  }
+  for (int r = 0; r < o.m; ++r) {
+    const long long k = (long long)r * st.ld + b;
+    st.z[k] = st.z[k] * __ldg(o.scaling_einv + r);
+    st.y[k] = st.y[k] * __ldg(o.y_unscale + r);
+  }
+}
+
+__device__ __forceinline__ bool finite_res(const Residuals& r) {
+  return isfinite(r.prim) && isfinite(r.dual) && isfinite(r.obj);
+}
+
+__global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
+                                const float* __restrict__ aT, long long lda, int sba, State st,
+                                const float* __restrict__ qT, float* prim, float* dual, float* obj,
+                                int* status, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
+  const Residuals r = residuals(o, in, st, b, qT + b, batch);
+  prim[b] = r.prim;
+  dual[b] = r.dual;
+  obj[b] = r.obj;
+  if (status) status[b] = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
+  unscale_in_place(o, st, b);
+}
+
+__global__ void fill_int_kernel(int* out, int value, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) out[i] = value;
+}
+
+// ---------------------------------------------------------------------------
+// persistent fused solve: assembly + factor + all iterations + epilogue
+// ---------------------------------------------------------------------------
+
+struct PersistentArgs {
+  Pattern pat;
+  Osqp o;
+  const float* pT; long long ldp; int sbp;
+  const float* aT; long long lda; int sba;
+  const float* qT;  // unscaled q [n, batch]
+  State st;
+  float* lx;    // [nnz_l, fld] factor (written here when fused_factor)
+  float* dinv;  // [nk, fld]
+  float* d;     // [nk, fld] (fused_factor only)
+  int fstride;  // 0: one factor shared by all instances, 1: per instance
+  long long fld;
+  int fused_factor;
+  float* wglob; // [nk, batch] when the work vector does not fit in shared memory
+  float* prim; float* dual; float* obj;
+  int* iters; int* status;
+  int batch, max_iter, check_every;
+  float eps_abs, eps_rel;
+};
+
+template <bool kSmem>
+__global__ void __launch_bounds__(256) persistent_kernel(PersistentArgs a) {
+  extern __shared__ float smem[];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.batch) return;
+  const Pattern& pat = a.pat;
+  const Osqp& o = a.o;
+  LaneVec w = kSmem ? LaneVec{smem + threadIdx.x, (long long)blockDim.x}
+                    : LaneVec{a.wglob + b, (long long)a.batch};
+  InstanceData in{a.pT + (long long)b * a.sbp, a.ldp, a.aT + (long long)b * a.sba, a.lda};
+  if (a.fused_factor) {
+    auto val_at = [&](int slot) -> float { return kkt_value(o, in, __ldg(pat.perm_to_orig + slot)); };
+    factor_instance(pat, val_at, w, a.lx, a.fld, a.d, a.dinv, a.fld, b);
+  }
+  const long long fo = (long long)b * a.fstride;
+  const float* lx = a.lx + fo;
+  const float* dinv = a.dinv + fo;
+
+  int status = WMPC_STATUS_MAX_ITER;
+  for (int k = 0; k < pat.n; ++k) {
+    const float di = dinv[(long long)k * a.fld];
+    if (di == 0.0f || !isfinite(di)) status |= WMPC_STATUS_ZERO_PIVOT;
+  }
+  int it = 0;
+  for (; it < a.max_iter; ++it) {
+    for (int i = 0; i < pat.n; ++i) w(i) = rhs_entry(o, a.st, __ldg(pat.p + i), b);
+    ldl_solve_permuted(pat, lx, a.fld, dinv, a.fld, w);
+    for (int i = 0; i < pat.n; ++i) admm_update(o, a.st, __ldg(pat.p + i), b, w(i));
+    if (a.check_every > 0 && ((it + 1) % a.check_every == 0) && it + 1 < a.max_iter) {
+      const Residuals r = residuals(o, in, a.st, b, a.qT + b, a.batch);
+      if (!finite_res(r)) { status |= WMPC_STATUS_NONFINITE; ++it; break; }
+      const float eps_p = a.eps_abs + a.eps_rel * fmaxf(r.ax_norm, r.z_norm);
+      const float eps_d = a.eps_abs + a.eps_rel * fmaxf(fmaxf(r.px_norm, r.aty_norm), r.q_norm);
+      if (r.prim <= eps_p && r.dual <= eps_d) { status |= WMPC_STATUS_SOLVED; ++it; break; }
+    }
+  }
+  const Residuals r = residuals(o, in, a.st, b, a.qT + b, a.batch);
+  a.prim[b] = r.prim;
+  a.dual[b] = r.dual;
+  a.obj[b] = r.obj;
+  if (!finite_res(r)) status |= WMPC_STATUS_NONFINITE;
+  if (a.iters) a.iters[b] = it;
+  if (a.status) a.status[b] = status;
+  unscale_in_place(o, a.st, b);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Carve {
+  char* base;
+  size_t used = 0;
+  float* take(size_t floats) {
+    size_t bytes = ((floats * 4 + 255) / 256) * 256;
+    float* out = reinterpret_cast<float*>(base ? base + used : nullptr);
+    used += bytes;
+    return out;
+  }
+};
+
+struct Layout {
+  float *pT, *aT, *qs, *ls, *us, *qT, *x, *z, *y, *kkt, *lx, *d, *dinv, *rhs, *scratch;
+  size_t scratch_bytes;
+  bool factor_separately;  // factor with the per-call kernels before iterating
+};
+
+// Workspace carve-up.  `external`: the caller supplies the factorization.
+Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external, char* base,
+             size_t* total) {
+  Carve c{base};
+  Layout L{};
+  const int kb = pb > ab ? pb : ab;  // KKT (factor) batch
+  L.pT = c.take((size_t)o.nnz_p * pb);
+  L.aT = c.take((size_t)o.nnz_a * ab);
+  L.qT = c.take((size_t)o.n * batch);
+  L.qs = c.take((size_t)o.n * batch);
+  L.ls = c.take((size_t)o.m * batch);
+  L.us = c.take((size_t)o.m * batch);
+  L.x = c.take((size_t)o.n * batch);
+  L.z = c.take((size_t)o.m * batch);
+  L.y = c.take((size_t)o.m * batch);
+  L.factor_separately = !external && (mode == WMPC_OSQP_PLAIN || kb == 1);
+  size_t scratch = 0;
+  if (!external) {
+    const int fb = L.factor_separately ? kb : batch;
+    if (L.factor_separately) {
+      L.kkt = c.take((size_t)o.nnz_kkt * kb);
+      scratch = factor_workspace_bytes(pat, kb);
+    }
+    L.lx = c.take((size_t)pat.nnz_l * fb);
+    L.d = c.take((size_t)pat.n * fb);
+    L.dinv = c.take((size_t)pat.n * fb);
+  }
+  if (mode == WMPC_OSQP_PLAIN) {
+    L.rhs = c.take((size_t)o.nk * batch);
+    size_t s2 = solve_workspace_bytes(pat, batch);
+    scratch = scratch > s2 ? scratch : s2;
+  } else {
+    size_t s2 = smem_lanes_for_rows(pat.n) >= 32 ? 0 : (size_t)4 * pat.n * batch;
+    scratch = scratch > s2 ? scratch : s2;
+  }
+  L.scratch_bytes = scratch;
+  L.scratch = scratch ? c.take(scratch / 4 + 1) : nullptr;
+  *total = c.used;
+  return L;
+}
+
+int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int pb, const float* aT, int ab,
+                        float* kkt, float* lx, float* d, float* dinv, void* scratch, size_t scratch_bytes,
+                        cudaStream_t s) {
+  const int kb = pb > ab ? pb : ab;
+  dim3 grid(ceil_div(kb, 128), o.nnz_kkt < 4096 ? o.nnz_kkt : 4096);
+  assemble_kkt_kernel<<<grid, 128, 0, s>>>(o, pT, pb, pb > 1 ? 1 : 0, aT, ab, ab > 1 ? 1 : 0, kkt, kb);
+  WMPC_LAUNCH_CHECK();
+  return launch_factor(pat, kkt, kb, 1, lx, d, dinv, kb, scratch, scratch_bytes, s);
+}
+
+}  // namespace
+
+size_t osqp_workspace_bytes(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external) {
+  size_t total = 0;
+  carve(o, pat, batch, pb, ab, mode, external, nullptr, &total);
+  return total;
+}
+
+size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, int ab) {
+  const int kb = pb > ab ? pb : ab;
+  Carve c{nullptr};
+  c.take((size_t)o.nnz_p * pb);
+  c.take((size_t)o.nnz_a * ab);
+  c.take((size_t)o.nnz_kkt * kb);
+  const size_t f = factor_workspace_bytes(pat, kb);
+  if (f) c.take(f / 4 + 1);
+  return c.used;
+}
+
+int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
+                float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s) {
+  const int kb = pb > ab ? pb : ab;
+  const size_t need = osqp_factor_workspace_bytes(o, pat, pb, ab);
+  if (ws == nullptr || ws_bytes < need)
+    return fail(WMPC_ERR_WORKSPACE, "OSQP factor needs %zu workspace bytes, got %zu", need, ws_bytes);
+  Carve c{static_cast<char*>(ws)};
+  float* pT = c.take((size_t)o.nnz_p * pb);
+  float* aT = c.take((size_t)o.nnz_a * ab);
+  float* kkt = c.take((size_t)o.nnz_kkt * kb);
+  const size_t f = factor_workspace_bytes(pat, kb);
+  float* scratch = f ? c.take(f / 4 + 1) : nullptr;
+  int rc;
+  if ((rc = transpose_in(p_values, o.nnz_p, pb, o.nnz_p, nullptr, pT, pb, s))) return rc;
+  if ((rc = transpose_in(a_values, o.nnz_a, ab, o.nnz_a, nullptr, aT, ab, s))) return rc;
+  return assemble_and_factor(o, pat, pT, pb, aT, ab, kkt, lx, d, dinv, scratch, f, s);
+}
+
+int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+               const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
+               cudaStream_t s) {
+  const int B = d.batch;
+  if (B <= 0) return WMPC_OK;
+  const int pb = d.p_batch, ab = d.a_batch;
+  const bool external = lx_ext != nullptr;
+  size_t need = 0;
+  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need);
+  if (ws == nullptr || ws_bytes < need)
+    return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
+  int rc;
+  // batch-major inputs -> symbolic-major, scaled where the reference scales
+  if ((rc = transpose_in(d.p_values, o.nnz_p, pb, o.nnz_p, nullptr, L.pT, pb, s))) return rc;
+  if ((rc = transpose_in(d.a_values, o.nnz_a, ab, o.nnz_a, nullptr, L.aT, ab, s))) return rc;
+  if ((rc = transpose_in(d.q, o.n, B, o.n, nullptr, L.qT, B, s))) return rc;
+  if ((rc = transpose_in(d.q, o.n, B, o.n, o.q_scale, L.qs, B, s))) return rc;
+  if ((rc = transpose_in(d.l, o.m, B, o.m, o.scaling_e, L.ls, B, s))) return rc;
+  if ((rc = transpose_in(d.u, o.m, B, o.m, o.scaling_e, L.us, B, s))) return rc;
+  if (opt.warm_start) {
+    if (!d.x0 || !d.z0 || !d.y0) return fail(WMPC_ERR_INVALID_ARGUMENT, "warm start needs x0, z0 and y0");
+    if ((rc = transpose_in(d.x0, o.n, B, o.n, o.scaling_dinv, L.x, B, s))) return rc;
+    if ((rc = transpose_in(d.z0, o.m, B, o.m, o.scaling_e, L.z, B, s))) return rc;
+    if ((rc = transpose_in(d.y0, o.m, B, o.m, o.y_scale, L.y, B, s))) return rc;
+  } else {
+    WMPC_CUDA_TRY(cudaMemsetAsync(L.x, 0, sizeof(float) * (size_t)o.n * B, s));
+    WMPC_CUDA_TRY(cudaMemsetAsync(L.z, 0, sizeof(float) * (size_t)o.m * B, s));
+    WMPC_CUDA_TRY(cudaMemsetAsync(L.y, 0, sizeof(float) * (size_t)o.m * B, s));
+  }
+  State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
+  const int sbp = pb > 1 ? 1 : 0, sba = ab > 1 ? 1 : 0;
+  const long long ldp = pb, lda = ab;
+  const int kb = pb > ab ? pb : ab;
+
+  // the factorization the iterations use
+  const float* lx = lx_ext;
+  const float* dinv = dinv_ext;
+  int fb = fb_ext;
+  if (!external && L.factor_separately) {
+    if ((rc = assemble_and_factor(o, pat, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch, L.scratch_bytes, s)))
+      return rc;
+    lx = L.lx;
+    dinv = L.dinv;
+    fb = kb;
+  }
+  if (external && fb != 1 && fb != B) return fail(WMPC_ERR_INVALID_ARGUMENT, "factor_batch must be 1 or batch");
+
+  if (mode == WMPC_OSQP_PLAIN) {
+    const int fstride = fb > 1 ? 1 : 0;
+    dim3 egrid(ceil_div(B, 128), o.nk < 2048 ? o.nk : 2048);
+    admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
+    WMPC_LAUNCH_CHECK();
+    for (int it = 0; it < opt.max_iter; ++it) {
+      if ((rc = launch_solve(pat, lx, dinv, fstride, L.rhs, L.rhs, B, L.scratch, L.scratch_bytes, s))) return rc;
+      admm_update_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
+      WMPC_LAUNCH_CHECK();
+    }
+    residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
+                                                     d.dual_res, d.obj, d.status, B);
+    WMPC_LAUNCH_CHECK();
+    if (d.iters) {
+      fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
+      WMPC_LAUNCH_CHECK();
+    }
+  } else {
+    const bool fused = !external && !L.factor_separately;
+    PersistentArgs pa{};
+    pa.pat = pat;
+    pa.o = o;
+    pa.pT = L.pT; pa.ldp = ldp; pa.sbp = sbp;
+    pa.aT = L.aT; pa.lda = lda; pa.sba = sba;
+    pa.qT = L.qT;
+    pa.st = st;
+    pa.lx = fused ? L.lx : const_cast<float*>(lx);
+    pa.dinv = fused ? L.dinv : const_cast<float*>(dinv);
+    pa.d = fused ? L.d : nullptr;
+    pa.fstride = fused ? 1 : (fb > 1 ? 1 : 0);
+    pa.fld = fused ? B : fb;
+    pa.fused_factor = fused ? 1 : 0;
+    pa.wglob = L.scratch;
+    pa.prim = d.prim_res; pa.dual = d.dual_res; pa.obj = d.obj;
+    pa.iters = d.iters; pa.status = d.status;
+    pa.batch = B; pa.max_iter = opt.max_iter; pa.check_every = opt.check_termination;
+    pa.eps_abs = opt.eps_abs; pa.eps_rel = opt.eps_rel;
+    const int lanes = smem_lanes_for_rows(pat.n);
+    if (lanes >= 32) {
+      const int threads = lanes < 128 ? lanes : 128;
+      const size_t smem = (size_t)4 * pat.n * threads;
+      WMPC_CUDA_TRY(cudaFuncSetAttribute(persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      persistent_kernel<true><<<ceil_div(B, threads), threads, smem, s>>>(pa);
+    } else {
+      persistent_kernel<false><<<ceil_div(B, 128), 128, 0, s>>>(pa);
+    }
+    WMPC_LAUNCH_CHECK();
+  }
+  if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
+  if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
+  if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
+  return WMPC_OK;
+}
+
+}  // namespace wmpc

@@ -1,0 +1,47 @@
+// Device-side OSQP problem description (one FixedOSQPPlan) and launchers.
+#pragma once
+
+#include "common.cuh"
+
+namespace wmpc {
+
+struct Osqp {
+  int n, m, nk;          // variables, constraints, KKT dimension (n + m)
+  int nnz_p, nnz_a, nnz_kkt, nnz_pf;
+  float sigma, alpha, one_minus_alpha;
+  // KKT value assembly: slot s takes kkt_base[s], or P entry / A entry j
+  // scaled: kkt_src[s] = -1 (base), j (P entry j) or nnz_p + j (A entry j).
+  const float* kkt_base;
+  const int* kkt_src;
+  const float* p_scale;       // [nnz_p]
+  const float* p_diag_sigma;  // [nnz_p]
+  const float* a_scale;       // [nnz_a]
+  // A by rows (entries of row r in storage order = ascending column)
+  const int* a_row_ptr;       // [m+1]
+  const int* a_row_ent;       // [nnz_a] A entry index
+  const int* a_cols;          // [nnz_a]
+  const int* a_rows;          // [nnz_a]
+  const int* a_col_ptr;       // [n+1] CSC pointers of A
+  // both triangles of P grouped by row, in the reference's entry order
+  const int* pf_row_ptr;      // [n+1]
+  const int* pf_val;          // [nnz_pf] P upper entry index
+  const int* pf_col;          // [nnz_pf]
+  const float* rho;           // [m]
+  const float* rho_inv;       // [m]
+  const float* q_scale;       // [n]
+  const float* scaling_d;     // [n]
+  const float* scaling_dinv;  // [n]
+  const float* scaling_e;     // [m]
+  const float* scaling_einv;  // [m]
+  const float* y_scale;       // [m]
+  const float* y_unscale;     // [m]
+};
+
+}  // namespace wmpc
+
+struct wmpc_osqp {
+  int device = 0;
+  wmpc::Osqp dev{};
+  const wmpc_plan* kkt_plan = nullptr;
+  void* block = nullptr;  // single device allocation holding every table
+};

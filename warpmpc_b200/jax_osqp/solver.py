@@ -1,0 +1,324 @@
+"""Compiled batched OSQP-ADMM on the CUDA library.
+
+Mirror of ``compile_osqp`` (``warpmpc/jax_osqp/solver.py:685-1492``) with
+``qdldl_backend="cuda"``.  All callables take and return ``torch`` tensors
+(batch-major ``(B, .)`` like the reference; P/A value batches of one are
+broadcast).  Two execution modes share one C-ABI call:
+
+* ``mode="persistent"`` (default): one fused launch per instance tile --
+  KKT assembly, factorization, all ``max_iter`` ADMM iterations (optionally
+  with OSQP's termination test every ``check_termination`` iterations) and
+  the residual epilogue;
+* ``mode="plain"``: the reference's loop structure with the CUDA factor and
+  solve as drop-in kernels (one factor, then per iteration one solve launch
+  and one ADMM-update launch), i.e. what ``qdldl_backend="cuda"`` gives the
+  unchanged reference ADMM loop.
+
+Arithmetic is float32 in the reference's operation order.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .. import native
+from ..jax_qdldl.core import DevicePlan, _as_f32, _workspace, compile_qdldl_variant
+from .types import CompiledOSQP, FixedOSQPPlan, OSQPWarmStart
+
+
+def values_for_compiled_qdldl(compiled, kkt_values):
+    """(B, nnz) -> the compiled QDLDL's values layout (solver.py:665-670)."""
+    if compiled.values_layout == "original_batch":
+        return kkt_values
+    if compiled.values_layout == "original_symbolic":
+        return kkt_values.T
+    raise ValueError(f"unknown QDLDL values layout {compiled.values_layout}")
+
+
+def rhs_for_compiled_qdldl(compiled, rhs):
+    """(B, n) -> the compiled QDLDL's rhs layout (solver.py:673-678)."""
+    if compiled.rhs_layout == "batch":
+        return rhs
+    if compiled.rhs_layout == "symbolic":
+        return rhs.T
+    raise ValueError(f"unknown QDLDL rhs layout {compiled.rhs_layout}")
+
+
+def batch_from_compiled_qdldl(compiled, values):
+    return values.T if compiled.rhs_layout == "symbolic" else values
+
+
+class DeviceOSQP:
+    """A FixedOSQPPlan uploaded to one device (``wmpc_osqp``) plus its KKT plan."""
+
+    def __init__(self, plan: FixedOSQPPlan, device=None, kkt_plan: DevicePlan | None = None):
+        self.plan = plan
+        self.kkt = kkt_plan if kkt_plan is not None else DevicePlan(plan.qdldl_plan, device)
+        self.device_index = self.kkt.device_index
+        s = plan.settings
+        keep = {
+            "kkt_base": native.f32(plan.kkt_upper.data),
+            "p_to_kkt": native.i32(plan.p_to_kkt),
+            "p_diag_sigma": native.f32(plan.p_diag_sigma),
+            "a_to_kkt": native.i32(plan.a_to_kkt),
+            "p_scale": native.f32(plan.p_scale),
+            "a_scale": native.f32(plan.a_scale),
+            "a_rows": native.i32(plan.a_rows),
+            "a_cols": native.i32(plan.a_cols),
+            "p_full_rows": native.i32(plan.p_full_rows),
+            "p_full_cols": native.i32(plan.p_full_cols),
+            "p_full_value_map": native.i32(plan.p_full_value_map),
+            "rho_vec": native.f32(plan.rho_vec),
+            "rho_inv_vec": native.f32(plan.rho_inv_vec),
+            "q_scale": native.f32(plan.q_scale),
+            "scaling_d": native.f32(plan.scaling_d),
+            "scaling_dinv": native.f32(plan.scaling_dinv),
+            "scaling_e": native.f32(plan.scaling_e),
+            "scaling_einv": native.f32(plan.scaling_einv),
+            "y_scale": native.f32(plan.y_scale),
+            "y_unscale": native.f32(plan.y_unscale),
+        }
+        kw = {}
+        for k, v in keep.items():
+            kw[k] = native.ptr_f32(v) if v.dtype == np.float32 else native.ptr_i32(v)
+        desc = native.OsqpDesc(
+            n=plan.n, m=plan.m, nnz_p=plan.nnz_p, nnz_a=plan.nnz_a, nnz_kkt=plan.nnz_kkt,
+            sigma=np.float32(s.sigma), alpha=np.float32(s.alpha),
+            nnz_p_full=int(plan.p_full_rows.size), **kw,
+        )
+        handle = ctypes.c_void_p()
+        native.check(native.lib().wmpc_osqp_create(ctypes.byref(desc), self.kkt.handle, ctypes.byref(handle)))
+        self.handle = handle
+
+    @property
+    def torch_device(self):
+        return self.kkt.torch_device
+
+    def __del__(self):
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            try:
+                native.lib().wmpc_osqp_destroy(handle)
+            except Exception:  # pragma: no cover
+                pass
+            self.handle = None
+
+
+_MODES = {"plain": native.WMPC_OSQP_PLAIN, "persistent": native.WMPC_OSQP_PERSISTENT}
+
+
+class OSQPEngine:
+    """Host-side driver of ``wmpc_osqp_factor`` / ``wmpc_osqp_solve``."""
+
+    def __init__(self, plan: FixedOSQPPlan, device=None, mode: str = "persistent", kkt_plan: DevicePlan | None = None):
+        if mode not in _MODES:
+            raise ValueError(f"unknown mode {mode!r}; expected one of {sorted(_MODES)}")
+        self.plan = plan
+        self.mode = mode
+        self.dev = DeviceOSQP(plan, device, kkt_plan=kkt_plan)
+        self.device = self.dev.torch_device
+        self.last_iters = None
+        self.last_status = None
+
+    # -- argument normalisation -------------------------------------------------
+    def _mat(self, values, width, name):
+        t = _as_f32(values, self.device, name)
+        if t.dim() == 1:
+            t = t[None, :]
+        if t.dim() != 2 or t.shape[1] != width:
+            raise ValueError(f"{name} must have shape (batch, {width}) or ({width},)")
+        return t.contiguous()
+
+    def _vec(self, values, width, batch, name):
+        t = self._mat(values, width, name)
+        if t.shape[0] == 1 and batch > 1:
+            t = t.expand(batch, width).contiguous()
+        if t.shape[0] != batch:
+            raise ValueError(f"{name} has batch {t.shape[0]}, expected {batch}")
+        return t
+
+    def factor(self, p_values, a_values):
+        import torch
+
+        pl = self.plan
+        p = self._mat(p_values, pl.nnz_p, "p_values")
+        a = self._mat(a_values, pl.nnz_a, "a_values")
+        pb, ab = int(p.shape[0]), int(a.shape[0])
+        if pb != 1 and ab != 1 and pb != ab:
+            raise ValueError("p_values and a_values batches must match (or be 1)")
+        fb = max(pb, ab)
+        nk = pl.qdldl_plan.n
+        lx = torch.empty((pl.qdldl_plan.nnz_l, fb), dtype=torch.float32, device=self.device)
+        d = torch.empty((nk, fb), dtype=torch.float32, device=self.device)
+        dinv = torch.empty((nk, fb), dtype=torch.float32, device=self.device)
+        lib = native.lib()
+        ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, fb, _MODES[self.mode], 0), self.device)
+        native.check(lib.wmpc_osqp_factor(self.dev.handle, p.data_ptr(), pb, a.data_ptr(), ab, lx.data_ptr(),
+                                          d.data_ptr(), dinv.data_ptr(), native.tensor_ptr(ws), wsb,
+                                          native.current_stream_handle(self.device)))
+        return lx, dinv
+
+    def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
+              mode=None):
+        import torch
+
+        pl = self.plan
+        s = pl.settings
+        p = self._mat(p_values, pl.nnz_p, "p_values")
+        a = self._mat(a_values, pl.nnz_a, "a_values")
+        qm = self._mat(q, pl.n, "q")
+        batch = max(int(qm.shape[0]), int(p.shape[0]), int(a.shape[0]))
+        for t, name in ((p, "p_values"), (a, "a_values")):
+            if t.shape[0] not in (1, batch):
+                raise ValueError(f"{name} batch must be 1 or {batch}")
+        qm = self._vec(qm, pl.n, batch, "q")
+        lm = self._vec(l, pl.m, batch, "l")
+        um = self._vec(u, pl.m, batch, "u")
+        dev = self.device
+        x = torch.empty((batch, pl.n), dtype=torch.float32, device=dev)
+        z = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+        y = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+        prim = torch.empty(batch, dtype=torch.float32, device=dev)
+        dual = torch.empty(batch, dtype=torch.float32, device=dev)
+        obj = torch.empty(batch, dtype=torch.float32, device=dev)
+        iters = torch.empty(batch, dtype=torch.int32, device=dev)
+        status = torch.empty(batch, dtype=torch.int32, device=dev)
+        keep = []
+        if warm is not None:
+            wx = self._vec(warm[0], pl.n, batch, "warm_start_x")
+            wz = self._vec(warm[1], pl.m, batch, "warm_start_z")
+            wy = self._vec(warm[2], pl.m, batch, "warm_start_y")
+            keep += [wx, wz, wy]
+            x0, z0, y0 = wx.data_ptr(), wz.data_ptr(), wy.data_ptr()
+        else:
+            x0 = z0 = y0 = None
+        data = native.OsqpBatch(
+            batch=batch, p_values=p.data_ptr(), p_batch=int(p.shape[0]), a_values=a.data_ptr(),
+            a_batch=int(a.shape[0]), q=qm.data_ptr(), l=lm.data_ptr(), u=um.data_ptr(), x0=x0, z0=z0, y0=y0,
+            x=x.data_ptr(), z=z.data_ptr(), y=y.data_ptr(), prim_res=prim.data_ptr(), dual_res=dual.data_ptr(),
+            obj=obj.data_ptr(), iters=iters.data_ptr(), status=status.data_ptr(),
+        )
+        opts = native.OsqpOptions(
+            max_iter=int(s.max_iter if max_iter is None else max_iter),
+            check_termination=int(s.check_termination if check_termination is None else check_termination),
+            eps_abs=np.float32(s.eps_abs), eps_rel=np.float32(s.eps_rel), warm_start=1 if warm is not None else 0,
+        )
+        mode_id = _MODES[self.mode if mode is None else mode]
+        lib = native.lib()
+        if factor is not None:
+            lx, dinv = factor
+            lx = _as_f32(lx, dev, "lx")
+            dinv = _as_f32(dinv, dev, "dinv")
+            fb = int(lx.shape[1])
+            if lx.shape[0] != pl.qdldl_plan.nnz_l or dinv.shape != (pl.qdldl_plan.n, fb) or fb not in (1, batch):
+                raise ValueError("lx/dinv do not match the plan or the batch")
+            lx_p, dinv_p, ext = lx.data_ptr(), dinv.data_ptr(), 1
+            keep += [lx, dinv]
+        else:
+            lx_p = dinv_p = None
+            fb, ext = 0, 0
+        ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext), dev)
+        native.check(lib.wmpc_osqp_solve(self.dev.handle, ctypes.byref(opts), ctypes.byref(data), lx_p, dinv_p, fb,
+                                         mode_id, native.tensor_ptr(ws), wsb, native.current_stream_handle(dev)))
+        self.last_iters = iters
+        self.last_status = status
+        return x, z, y, prim, dual, obj
+
+
+def compile_osqp(
+    plan: FixedOSQPPlan,
+    dtype=np.float64,
+    *,
+    qdldl_backend: str = "jax",
+    qdldl_factor_backend: str | None = None,
+    qdldl_solve_backend: str | None = None,
+    transpose_work: bool = False,
+    segmented: bool = False,
+    segment_budget: int = 64,
+    segment_strategy: str = "optimal",
+    level_scheduled_solve: bool = False,
+    level_scheduled_solve_threshold: int = 1,
+    derivatives: bool = False,
+    derivative_refinement_iters: int = 100,
+    mode: str = "persistent",
+    device=None,
+) -> CompiledOSQP:
+    """Compile fixed-pattern batched OSQP iterations (solver.py:685-1492)."""
+
+    import torch
+
+    qdldl = compile_qdldl_variant(
+        plan.qdldl_plan,
+        dtype=dtype,
+        backend=qdldl_backend,
+        factor_backend=qdldl_factor_backend,
+        solve_backend=qdldl_solve_backend,
+        transpose_work=transpose_work,
+        segmented=segmented,
+        segment_budget=segment_budget,
+        segment_strategy=segment_strategy,
+        level_scheduled_solve=level_scheduled_solve,
+        level_scheduled_solve_threshold=level_scheduled_solve_threshold,
+        device=device,
+    )
+    engine = OSQPEngine(plan, device=device, mode=mode, kkt_plan=qdldl.device_plan)
+    settings = plan.settings
+    dev = engine.device
+
+    def factor(p_values, a_values):
+        return engine.factor(p_values, a_values)
+
+    def solve(p_values, a_values, q, l, u):
+        return engine.solve(p_values, a_values, q, l, u)
+
+    def solve_warm_start(p_values, a_values, q, l, u, warm_start_x, warm_start_z, warm_start_y):
+        return engine.solve(p_values, a_values, q, l, u, warm=(warm_start_x, warm_start_z, warm_start_y))
+
+    def solve_with_factor(lx, dinv, p_values, a_values, q, l, u):
+        return engine.solve(p_values, a_values, q, l, u, factor=(lx, dinv))
+
+    def solve_with_factor_warm_start(lx, dinv, p_values, a_values, q, l, u, warm_start_x, warm_start_z, warm_start_y):
+        return engine.solve(p_values, a_values, q, l, u, warm=(warm_start_x, warm_start_z, warm_start_y),
+                            factor=(lx, dinv))
+
+    def linear_solve_loop(lx, dinv, rhs):
+        sol = rhs_for_compiled_qdldl(qdldl, _as_f32(rhs, dev, "rhs")).contiguous()
+        for _ in range(settings.max_iter):
+            sol = qdldl.solve(lx, dinv, sol)
+        return batch_from_compiled_qdldl(qdldl, sol)
+
+    def init_warm_start(batch_size: int) -> OSQPWarmStart:
+        return OSQPWarmStart(
+            x=torch.zeros((batch_size, plan.n), dtype=torch.float32, device=dev),
+            z=torch.zeros((batch_size, plan.m), dtype=torch.float32, device=dev),
+            y=torch.zeros((batch_size, plan.m), dtype=torch.float32, device=dev),
+        )
+
+    extra = {}
+    if derivatives:
+        from .adjoint import make_derivative_callables
+
+        extra = make_derivative_callables(plan, engine, qdldl, derivative_refinement_iters)
+
+    return CompiledOSQP(
+        plan=plan,
+        settings=settings,
+        qdldl=qdldl,
+        solve=extra.get("solve", solve),
+        factor=factor,
+        solve_with_factor=solve_with_factor,
+        variant=qdldl.variant + f"+{mode}",
+        dtype=qdldl.dtype,
+        linear_solve_loop=linear_solve_loop,
+        init_warm_start=init_warm_start,
+        solve_warm_start=extra.get("solve_warm_start", solve_warm_start),
+        solve_with_factor_warm_start=solve_with_factor_warm_start,
+        adjoint_derivative_compute=extra.get("adjoint_derivative_compute"),
+        adjoint_derivative_get_mat=extra.get("adjoint_derivative_get_mat"),
+        adjoint_derivative_get_vec=extra.get("adjoint_derivative_get_vec"),
+        solve_primal=extra.get("solve_primal"),
+        solve_xy=extra.get("solve_xy"),
+        engine=engine,
+    )
