@@ -214,6 +214,17 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
                     int32_t factor_batch, int32_t mode, void* workspace, size_t workspace_bytes,
                     wmpc_stream_t stream);
 
+/* Profiling (no counterpart in the reference, which times with wall
+ * clocks around jax.block_until_ready).  Between begin and end the library
+ * records a CUDA event pair on the launching stream around every launch of
+ * the dominant kernel (the persistent solve kernel, or the per-call solve
+ * kernel of the plain path) and counts every kernel it launches.  end()
+ * waits for the recorded events and returns the summed device time. */
+int wmpc_profile_begin(void);
+int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* total_launches);
+/* Kernels launched by this library since load (or the last profile_begin). */
+int64_t wmpc_launch_count(void);
+
 const char* wmpc_last_error_string(void);
 /* Library version string, e.g. "0.1.0 sm_100a". */
 const char* wmpc_version(void);

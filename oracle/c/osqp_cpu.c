@@ -1,5 +1,5 @@
 /*
- * CPU restatement (C, OpenMP over instances) of the reference's batched
+ * CPU restatement (C; callers split the batch across threads) of the reference's batched
  * fixed-iteration OSQP-ADMM over QDLDL, float32.
  *
  * TEST INFRASTRUCTURE ONLY (oracle): the CPU baseline timed by bench.py and
@@ -91,13 +91,13 @@ static float clip_nan(float v, float lo, float hi) {
   return (t > hi) ? hi : t;
 }
 
-/* Solve `batch` instances; returns 0.  Outputs batch-major. */
-int oc_osqp_solve(const oc_pattern* pat, const oc_osqp* o, int batch, int max_iter, const float* p_values,
+/* Solve instances [b_begin, b_end) of the batch; returns 0 (1 on allocation
+ * failure).  Outputs batch-major.  Thread-safe for disjoint ranges. */
+int oc_osqp_solve(const oc_pattern* pat, const oc_osqp* o, int b_begin, int b_end, int max_iter, const float* p_values,
                   int p_batch, const float* a_values, int a_batch, const float* q, const float* l, const float* u,
                   const float* x0, const float* z0, const float* y0, float* x_out, float* z_out, float* y_out,
                   float* prim_out, float* dual_out, float* obj_out) {
   const int n = o->n, m = o->m, nk = n + m;
-#pragma omp parallel
   {
     float* kkt = (float*)malloc(sizeof(float) * (size_t)o->nnz_kkt);
     float* lx = (float*)malloc(sizeof(float) * (size_t)(pat->nnz_l > 0 ? pat->nnz_l : 1));
@@ -111,8 +111,11 @@ int oc_osqp_solve(const oc_pattern* pat, const oc_osqp* o, int batch, int max_it
     float* ls = (float*)malloc(sizeof(float) * (size_t)m);
     float* us = (float*)malloc(sizeof(float) * (size_t)m);
     const float one_minus = 1.0f - o->alpha;
-#pragma omp for schedule(dynamic, 4)
-    for (int b = 0; b < batch; ++b) {
+    if (!kkt || !lx || !d || !dinv || !w || !xs || !zs || !ys || !qs || !ls || !us) {
+      free(kkt); free(lx); free(d); free(dinv); free(w); free(xs); free(zs); free(ys); free(qs); free(ls); free(us);
+      return 1;
+    }
+    for (int b = b_begin; b < b_end; ++b) {
       const float* pv = p_values + (size_t)(p_batch > 1 ? b : 0) * o->nnz_p;
       const float* av = a_values + (size_t)(a_batch > 1 ? b : 0) * o->nnz_a;
       for (int s = 0; s < o->nnz_kkt; ++s) {

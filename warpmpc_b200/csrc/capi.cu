@@ -1,7 +1,9 @@
 // extern "C" entry points of libwarpmpc_b200.so (declared in
 // include/warpmpc_b200.h).  Argument validation, table upload, error
 // reporting; all numerics live in qdldl.cu / osqp.cu.
+#include <atomic>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -31,6 +33,39 @@ int fail(int code, const char* fmt, ...) {
   va_end(ap);
   g_last_error = buf;
   return code;
+}
+
+// ---- profiling ------------------------------------------------------------
+namespace {
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::atomic<long long> g_launches{0};
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+size_t g_prof_used = 0;
+bool g_prof_open = false;
+}  // namespace
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void profile_mark_begin(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return;
+  if (g_prof_used == g_prof_events.size()) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+    g_prof_events.push_back({a, b});
+  }
+  cudaEventRecord(g_prof_events[g_prof_used].first, s);
+  g_prof_open = true;
+}
+
+void profile_mark_end(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on || !g_prof_open) return;
+  cudaEventRecord(g_prof_events[g_prof_used].second, s);
+  ++g_prof_used;
+  g_prof_open = false;
 }
 
 size_t osqp_workspace_bytes(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external);
@@ -118,6 +153,38 @@ extern "C" {
 const char* wmpc_last_error_string(void) { return g_last_error.c_str(); }
 
 const char* wmpc_version(void) { return "0.1.0 sm_100a"; }
+
+int wmpc_profile_begin(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = true;
+  g_prof_used = 0;
+  g_prof_open = false;
+  g_launches.store(0);
+  return WMPC_OK;
+}
+
+int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* total_launches) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  double total = 0.0;
+  for (size_t i = 0; i < g_prof_used; ++i) {
+    cudaError_t e = cudaEventSynchronize(g_prof_events[i].second);
+    if (e != cudaSuccess) {
+      g_prof_on = false;
+      return fail(WMPC_ERR_CUDA, "profile event sync failed: %s", cudaGetErrorString(e));
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g_prof_events[i].first, g_prof_events[i].second);
+    total += ms;
+  }
+  if (dominant_ms) *dominant_ms = static_cast<float>(total);
+  if (dominant_launches) *dominant_launches = static_cast<int32_t>(g_prof_used);
+  if (total_launches) *total_launches = g_launches.load();
+  g_prof_on = false;
+  g_prof_used = 0;
+  return WMPC_OK;
+}
+
+int64_t wmpc_launch_count(void) { return g_launches.load(); }
 
 int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out) {
   if (!desc || !out) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");

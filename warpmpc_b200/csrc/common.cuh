@@ -23,6 +23,11 @@ namespace wmpc {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 
+// Launch accounting and dominant-kernel timing (wmpc_profile_begin/end).
+void count_launch();
+void profile_mark_begin(cudaStream_t s);
+void profile_mark_end(cudaStream_t s);
+
 #define WMPC_CUDA_TRY(expr)                                                              \
   do {                                                                                   \
     cudaError_t err__ = (expr);                                                          \
@@ -33,6 +38,7 @@ int fail(int code, const char* fmt, ...);
 
 #define WMPC_LAUNCH_CHECK()                                                              \
   do {                                                                                   \
+    ::wmpc::count_launch();                                                              \
     cudaError_t err__ = cudaGetLastError();                                              \
     if (err__ != cudaSuccess)                                                            \
       return ::wmpc::fail(WMPC_ERR_CUDA, "kernel launch failed: %s (%s:%d)",              \

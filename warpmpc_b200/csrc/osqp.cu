@@ -491,7 +491,10 @@ int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, 
     admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
     WMPC_LAUNCH_CHECK();
     for (int it = 0; it < opt.max_iter; ++it) {
-      if ((rc = launch_solve(pat, lx, dinv, fstride, L.rhs, L.rhs, B, L.scratch, L.scratch_bytes, s))) return rc;
+      profile_mark_begin(s);
+      rc = launch_solve(pat, lx, dinv, fstride, L.rhs, L.rhs, B, L.scratch, L.scratch_bytes, s);
+      profile_mark_end(s);
+      if (rc) return rc;
       admm_update_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
       WMPC_LAUNCH_CHECK();
     }
@@ -528,10 +531,13 @@ int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, 
       const size_t smem = (size_t)4 * pat.n * threads;
       WMPC_CUDA_TRY(cudaFuncSetAttribute(persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
+      profile_mark_begin(s);
       persistent_kernel<true><<<ceil_div(B, threads), threads, smem, s>>>(pa);
     } else {
+      profile_mark_begin(s);
       persistent_kernel<false><<<ceil_div(B, 128), 128, 0, s>>>(pa);
     }
+    profile_mark_end(s);
     WMPC_LAUNCH_CHECK();
   }
   if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;

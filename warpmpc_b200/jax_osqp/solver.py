@@ -161,7 +161,14 @@ class OSQPEngine:
         return lx, dinv
 
     def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
-              mode=None):
+              mode=None, out=None):
+        """Batched solve; returns ``(x, z, y, prim_res, dual_res, obj_val)``.
+
+        ``out`` optionally supplies those six output tensors (plus ``iters``,
+        ``status`` int32) to write into; warm-start inputs may alias ``out``
+        (they are consumed before the outputs are written), which lets a CUDA
+        graph chain solves without copies.
+        """
         import torch
 
         pl = self.plan
@@ -177,14 +184,21 @@ class OSQPEngine:
         lm = self._vec(l, pl.m, batch, "l")
         um = self._vec(u, pl.m, batch, "u")
         dev = self.device
-        x = torch.empty((batch, pl.n), dtype=torch.float32, device=dev)
-        z = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
-        y = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
-        prim = torch.empty(batch, dtype=torch.float32, device=dev)
-        dual = torch.empty(batch, dtype=torch.float32, device=dev)
-        obj = torch.empty(batch, dtype=torch.float32, device=dev)
-        iters = torch.empty(batch, dtype=torch.int32, device=dev)
-        status = torch.empty(batch, dtype=torch.int32, device=dev)
+        if out is None:
+            x = torch.empty((batch, pl.n), dtype=torch.float32, device=dev)
+            z = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+            y = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+            prim = torch.empty(batch, dtype=torch.float32, device=dev)
+            dual = torch.empty(batch, dtype=torch.float32, device=dev)
+            obj = torch.empty(batch, dtype=torch.float32, device=dev)
+            iters = torch.empty(batch, dtype=torch.int32, device=dev)
+            status = torch.empty(batch, dtype=torch.int32, device=dev)
+        else:
+            x, z, y, prim, dual, obj, iters, status = out
+            shapes = [(batch, pl.n), (batch, pl.m), (batch, pl.m), (batch,), (batch,), (batch,), (batch,), (batch,)]
+            for t, shp in zip(out, shapes):
+                if tuple(t.shape) != shp or not t.is_contiguous() or t.device != dev:
+                    raise ValueError("out tensors have the wrong shape, layout or device")
         keep = []
         if warm is not None:
             wx = self._vec(warm[0], pl.n, batch, "warm_start_x")

@@ -161,6 +161,9 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpBatch), ctypes.c_void_p, ctypes.c_void_p,
          ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
+    "wmpc_profile_begin": (ctypes.c_int, []),
+    "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
+    "wmpc_launch_count": (ctypes.c_int64, []),
     "wmpc_last_error_string": (ctypes.c_char_p, []),
     "wmpc_version": (ctypes.c_char_p, []),
 }
@@ -265,3 +268,16 @@ def version() -> str:
 
 def env_flag(name: str, default: str = "0") -> bool:
     return os.environ.get(name, default) not in ("0", "", "false", "False")
+
+
+def profile_begin() -> None:
+    check(lib().wmpc_profile_begin())
+
+
+def profile_end() -> tuple[float, int, int]:
+    """(dominant kernel ms summed, dominant launches, all launches) since profile_begin."""
+    ms = ctypes.c_float()
+    n = ctypes.c_int32()
+    total = ctypes.c_int64()
+    check(lib().wmpc_profile_end(ctypes.byref(ms), ctypes.byref(n), ctypes.byref(total)))
+    return float(ms.value), int(n.value), int(total.value)
