@@ -110,3 +110,31 @@ def test_termination_and_status(cuda_device):
     status2 = comp.engine.last_status.cpu().numpy()
     assert status2[3] & 2
     np.testing.assert_array_equal(np.delete(x2, 3, 0), np.delete(x, 3, 0))
+
+
+@pytest.mark.parametrize("cls,batch", [(problems.SMALL, 10003), (problems.QUADROTOR, 4801)], ids=["small", "quad"])
+def test_persistent_many_tiles_bitexact(cuda_device, cls, batch):
+    """More instance tiles than SMs, a partial last tile; checked against the C oracle."""
+    from oracle.cpu_baseline import CpuOSQP
+
+    b = problems.make_batch(cls, batch, seed=21)
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    got = _run(comp, b)
+    ref = CpuOSQP(plan).solve(b.p_values, b.a_values, b.q, b.l, b.u)
+    for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r, err_msg=name)
+    for g, r in zip(got[3:], ref[3:]):
+        _close(g, r)
+    assert not np.any(comp.engine.last_status.cpu().numpy() & 8)
+
+
+def test_streaming_and_fallback_agree(cuda_device, monkeypatch):
+    b = problems.make_batch(problems.CARTPOLE, 70, seed=8)
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    fast = _run(comp, b)
+    monkeypatch.setenv("WMPC_DISABLE_STREAM", "1")
+    slow = _run(comp, b)
+    for f, s in zip(fast[:3], slow[:3]):
+        np.testing.assert_array_equal(f, s)

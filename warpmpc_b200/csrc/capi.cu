@@ -68,11 +68,11 @@ void profile_mark_end(cudaStream_t s) {
   g_prof_open = false;
 }
 
-size_t osqp_workspace_bytes(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external);
+size_t osqp_workspace_bytes(const wmpc_osqp& q, int batch, int pb, int ab, int mode, bool external);
 size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, int ab);
 int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
                 float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s);
-int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
                const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
                cudaStream_t s);
 
@@ -186,6 +186,56 @@ int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* to
 
 int64_t wmpc_launch_count(void) { return g_launches.load(); }
 
+int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv, int32_t n_primal,
+                              int32_t ent, int32_t cols, int32_t rel, int32_t* out, int64_t out_capacity,
+                              int64_t* out_words) {
+  if (!desc || !out_words) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  const int n = desc->n, nnz_l = desc->nnz_l;
+  if (n <= 0 || nnz_l < 0 || n_primal < 0 || n_primal > n || ent <= 0 || cols <= 0 || rel <= 0)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "bad sizes");
+  HostPattern hp;
+  hp.n = n;
+  hp.nnz_a = desc->nnz_a;
+  hp.nnz_l = nnz_l;
+  hp.init_ptr.assign(desc->init_ptr, desc->init_ptr + n + 1);
+  const int n_init = desc->init_ptr[n];
+  hp.init_rows.assign(desc->init_rows, desc->init_rows + n_init);
+  hp.proc_ptr.assign(desc->proc_ptr, desc->proc_ptr + n + 1);
+  hp.proc_cols.assign(desc->proc_cols, desc->proc_cols + nnz_l);
+  hp.proc_offsets.assign(desc->proc_offsets, desc->proc_offsets + nnz_l);
+  hp.proc_lidx.assign(desc->proc_lidx, desc->proc_lidx + nnz_l);
+  hp.lp.assign(desc->lp, desc->lp + n + 1);
+  hp.li.assign(desc->li, desc->li + nnz_l);
+  hp.p.assign(desc->p, desc->p + n);
+  std::string why;
+  std::vector<int> init_slot, upd_ptr;
+  std::vector<unsigned short> upd_slot;
+  int max_row = 0;
+  HostStream hs;
+  StreamTargets t;
+  t.ent = ent;
+  t.cols = cols;
+  t.rel = rel;
+  if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
+      !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
+    return fail(WMPC_ERR_UNSUPPORTED, "%s", why.c_str());
+  std::vector<int> w{hs.n_chunks, hs.stream_len, hs.max_ent, hs.max_cols, hs.max_rel, hs.max_meta_words, max_row,
+                     static_cast<int>(hs.meta.size())};
+  auto app = [&](const std::vector<int>& v) { w.insert(w.end(), v.begin(), v.end()); };
+  app(hs.chunk_pos); app(hs.chunk_ent); app(hs.chunk_cols); app(hs.meta_off); app(hs.meta_words); app(hs.meta);
+  app(hs.col_spos); app(hs.dinv_spos); app(hs.proc_spos); app(hs.u_perm); app(hs.u_orig);
+  app(init_slot); app(upd_ptr);
+  for (unsigned short v : upd_slot) w.push_back(v);
+  w.push_back(hs.n_fchunks); w.push_back(hs.max_fent); w.push_back(hs.max_frows); w.push_back(hs.max_fmeta_words);
+  w.push_back(static_cast<int>(hs.fmeta.size()));
+  app(hs.fchunk_pos); app(hs.fmeta_off); app(hs.fmeta_words); app(hs.fmeta); app(hs.proc_fpos);
+  *out_words = static_cast<int64_t>(w.size());
+  if (!out) return WMPC_OK;
+  if (out_capacity < static_cast<int64_t>(w.size())) return fail(WMPC_ERR_INVALID_ARGUMENT, "output buffer too small");
+  std::memcpy(out, w.data(), w.size() * sizeof(int32_t));
+  return WMPC_OK;
+}
+
 int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out) {
   if (!desc || !out) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
@@ -253,6 +303,15 @@ int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out)
     return rc;
   }
   plan->table_ints = pk.ints.size();
+  plan->h_init_ptr.assign(desc->init_ptr, desc->init_ptr + n + 1);
+  plan->h_init_rows.assign(desc->init_rows, desc->init_rows + n_init);
+  plan->h_proc_ptr.assign(desc->proc_ptr, desc->proc_ptr + n + 1);
+  plan->h_proc_cols.assign(desc->proc_cols, desc->proc_cols + nnz_l);
+  plan->h_proc_offsets.assign(desc->proc_offsets, desc->proc_offsets + nnz_l);
+  plan->h_proc_lidx.assign(desc->proc_lidx, desc->proc_lidx + nnz_l);
+  plan->h_lp.assign(desc->lp, desc->lp + n + 1);
+  plan->h_li.assign(desc->li, desc->li + nnz_l);
+  plan->h_p.assign(desc->p, desc->p + n);
   *out = plan;
   return WMPC_OK;
 }
@@ -416,6 +475,88 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     return rc;
   }
   q->block = block;
+  cudaDeviceGetAttribute(&q->num_sms, cudaDevAttrMultiProcessorCount, kkt_plan->device);
+  // streaming persistent path: schedule + compact factor tables
+  {
+    HostPattern hp;
+    hp.n = kkt_plan->pat.n;
+    hp.nnz_a = kkt_plan->pat.nnz_a;
+    hp.nnz_l = kkt_plan->pat.nnz_l;
+    hp.init_ptr = kkt_plan->h_init_ptr;
+    hp.init_rows = kkt_plan->h_init_rows;
+    hp.proc_ptr = kkt_plan->h_proc_ptr;
+    hp.proc_cols = kkt_plan->h_proc_cols;
+    hp.proc_offsets = kkt_plan->h_proc_offsets;
+    hp.proc_lidx = kkt_plan->h_proc_lidx;
+    hp.lp = kkt_plan->h_lp;
+    hp.li = kkt_plan->h_li;
+    hp.p = kkt_plan->h_p;
+    HostStream hs;
+    std::vector<int> init_slot, upd_ptr;
+    std::vector<unsigned short> upd_slot16;
+    int max_row = 0;
+    StreamTargets targets;
+    if (const char* v = getenv("WMPC_STREAM_ENT")) targets.ent = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_COLS")) targets.cols = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_REL")) targets.rel = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_FENT")) targets.fent = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_FROWS")) targets.frows = atoi(v);
+    if (targets.ent <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.fent <= 0 || targets.frows <= 0)
+      targets = StreamTargets();
+    bool ok = build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, &q->stream_why) &&
+              build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why);
+    StreamPlan& sp = q->sp;
+    if (ok) {
+      sp.n = hp.n;
+      sp.nnz_l = hp.nnz_l;
+      sp.n_chunks = hs.n_chunks;
+      sp.stream_len = hs.stream_len;
+      sp.max_ent = hs.max_ent;
+      sp.max_cols = hs.max_cols;
+      sp.max_rel = hs.max_rel;
+      sp.max_meta_words = hs.max_meta_words;
+      sp.max_row_nnz = max_row;
+      sp.n_fchunks = hs.n_fchunks;
+      sp.max_fent = hs.max_fent;
+      sp.max_frows = hs.max_frows;
+      sp.max_fmeta_words = hs.max_fmeta_words;
+      StreamLaunch cfg;
+      if (!stream_launch_config(sp, &cfg)) {
+        ok = false;
+        q->stream_why = "work vector and ring do not fit in shared memory";
+      }
+    }
+    if (ok) {
+      std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
+      Packer sk;
+      sk.add(hs.chunk_pos.data(), hs.chunk_pos.size(), &sp.chunk_pos);
+      sk.add(hs.chunk_ent.data(), hs.chunk_ent.size(), &sp.chunk_ent);
+      sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
+      sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
+      sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
+      sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);
+      sk.add(init_slot.data(), init_slot.size(), &sp.init_slot);
+      sk.add(upd_ptr.data(), upd_ptr.size(), &sp.upd_ptr);
+      sk.add(upd_slot.data(), upd_slot.size(), &sp.upd_slot);
+      sk.add(hs.col_spos.data(), hs.col_spos.size(), &sp.col_spos);
+      sk.add(hs.dinv_spos.data(), hs.dinv_spos.size(), &sp.dinv_spos);
+      sk.add(hs.proc_spos.data(), hs.proc_spos.size(), &sp.proc_spos);
+      sk.add(hs.u_perm.data(), hs.u_perm.size(), &sp.u_perm);
+      sk.add(hs.u_orig.data(), hs.u_orig.size(), &sp.u_orig);
+      sk.add(hs.fchunk_pos.data(), hs.fchunk_pos.size(), &sp.fchunk_pos);
+      sk.add(hs.fmeta_off.data(), hs.fmeta_off.size(), &sp.fmeta_off);
+      sk.add(hs.fmeta_words.data(), hs.fmeta_words.size(), &sp.fmeta_words);
+      sk.add(hs.fmeta.data(), hs.fmeta.size(), &sp.fmeta);
+      sk.add(hs.proc_fpos.data(), hs.proc_fpos.size(), &sp.proc_fpos);
+      int* sblock = nullptr;
+      if (sk.upload(&sblock) == WMPC_OK) {
+        q->stream_block = sblock;
+        q->has_stream = true;
+      } else {
+        q->stream_why = g_last_error;
+      }
+    }
+  }
   *out = q;
   return WMPC_OK;
 }
@@ -424,6 +565,7 @@ int wmpc_osqp_destroy(wmpc_osqp* osqp) {
   if (!osqp) return WMPC_OK;
   DeviceGuard guard(osqp->device);
   if (osqp->block) cudaFree(osqp->block);
+  if (osqp->stream_block) cudaFree(osqp->stream_block);
   delete osqp;
   return WMPC_OK;
 }
@@ -432,8 +574,7 @@ size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t m
   if (!osqp || batch <= 0) return 0;
   // P/A value batches may be 1 or `batch`; size for the larger case, and
   // for the factorization-only call as well
-  const size_t solve = osqp_workspace_bytes(osqp->dev, osqp->kkt_plan->pat, batch, batch, batch, mode,
-                                            external_factor != 0);
+  const size_t solve = osqp_workspace_bytes(*osqp, batch, batch, batch, mode, external_factor != 0);
   const size_t fac = osqp_factor_workspace_bytes(osqp->dev, osqp->kkt_plan->pat, batch, batch);
   return solve > fac ? solve : fac;
 }
@@ -472,8 +613,8 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options, con
     return fail(WMPC_ERR_UNSUPPORTED, "the per-call path runs exactly max_iter iterations (check_termination=0)");
   DeviceGuard guard(osqp->device);
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
-  return osqp_solve(osqp->dev, osqp->kkt_plan->pat, *options, d, lx, dinv, factor_batch, mode, workspace,
-                    workspace_bytes, static_cast<cudaStream_t>(stream));
+  return osqp_solve(*osqp, *options, d, lx, dinv, factor_batch, mode, workspace, workspace_bytes,
+                    static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

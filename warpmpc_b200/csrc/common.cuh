@@ -12,6 +12,7 @@
 #include <stdint.h>
 
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <string>
 
@@ -88,11 +89,21 @@ struct LaneVec {
 
 inline unsigned ceil_div(long long a, long long b) { return static_cast<unsigned>((a + b - 1) / b); }
 
+// Environment switch (testing/diagnostics): "1" disables a code path.
+inline bool env_disabled(const char* name) {
+  const char* v = getenv(name);
+  return v && v[0] == '1';
+}
+
 }  // namespace wmpc
+
+#include <vector>
 
 struct wmpc_plan {
   int device = 0;
   wmpc::Pattern pat{};
   int* table_block = nullptr;  // single device allocation holding every table
   size_t table_ints = 0;
+  // host copies of the ragged program (inputs of the streaming schedule)
+  std::vector<int> h_init_ptr, h_init_rows, h_proc_ptr, h_proc_cols, h_proc_offsets, h_proc_lidx, h_lp, h_li, h_p;
 };

@@ -240,7 +240,7 @@ __device__ __forceinline__ bool finite_res(const Residuals& r) {
 __global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
                                 const float* __restrict__ aT, long long lda, int sba, State st,
                                 const float* __restrict__ qT, float* prim, float* dual, float* obj,
-                                int* status, int batch) {
+                                int* status, int batch, const int* status_in, const int* abort_word) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
   InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
@@ -248,7 +248,12 @@ __global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long 
   prim[b] = r.prim;
   dual[b] = r.dual;
   obj[b] = r.obj;
-  if (status) status[b] = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
+  if (status) {
+    int v = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
+    if (status_in) v |= status_in[b];
+    if (abort_word && *abort_word) v |= WMPC_STATUS_KERNEL_ABORT;
+    status[b] = v;
+  }
   unscale_in_place(o, st, b);
 }
 
@@ -348,13 +353,34 @@ struct Layout {
   float *pT, *aT, *qs, *ls, *us, *qT, *x, *z, *y, *kkt, *lx, *d, *dinv, *rhs, *scratch;
   size_t scratch_bytes;
   bool factor_separately;  // factor with the per-call kernels before iterating
+  bool streaming;          // persistent mode on the TMA-fed streaming kernel
+  float* stream_ws;
+  int* stream_status;
+  int* error_word;
 };
 
 // Workspace carve-up.  `external`: the caller supplies the factorization.
 Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external, char* base,
-             size_t* total) {
+             size_t* total, const wmpc_osqp* q = nullptr, bool use_stream = false) {
   Carve c{base};
   Layout L{};
+  if (use_stream && q && q->has_stream && mode == WMPC_OSQP_PERSISTENT && !external) {
+    L.streaming = true;
+    L.pT = c.take((size_t)o.nnz_p * pb);
+    L.aT = c.take((size_t)o.nnz_a * ab);
+    L.qT = c.take((size_t)o.n * batch);
+    L.qs = c.take((size_t)o.n * batch);
+    L.ls = c.take((size_t)o.m * batch);
+    L.us = c.take((size_t)o.m * batch);
+    L.x = c.take((size_t)o.n * batch);
+    L.z = c.take((size_t)o.m * batch);
+    L.y = c.take((size_t)o.m * batch);
+    L.stream_ws = c.take(stream_workspace_floats(q->sp, batch));
+    L.stream_status = reinterpret_cast<int*>(c.take((size_t)((batch + 31) / 32) * 32));
+    L.error_word = reinterpret_cast<int*>(c.take(4));
+    *total = c.used;
+    return L;
+  }
   const int kb = pb > ab ? pb : ab;  // KKT (factor) batch
   L.pT = c.take((size_t)o.nnz_p * pb);
   L.aT = c.take((size_t)o.nnz_a * ab);
@@ -403,10 +429,21 @@ int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int 
 
 }  // namespace
 
-size_t osqp_workspace_bytes(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external) {
-  size_t total = 0;
-  carve(o, pat, batch, pb, ab, mode, external, nullptr, &total);
-  return total;
+int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
+                        int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
+                        const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
+                        int batch, int max_iter, int num_sms, cudaStream_t s);
+
+static bool stream_eligible(const wmpc_osqp& q, const wmpc_osqp_options* opt) {
+  return q.has_stream && (opt == nullptr || opt->check_termination == 0) && !env_disabled("WMPC_DISABLE_STREAM");
+}
+
+size_t osqp_workspace_bytes(const wmpc_osqp& q, int batch, int pb, int ab, int mode, bool external) {
+  size_t total = 0, total2 = 0;
+  carve(q.dev, q.kkt_plan->pat, batch, pb, ab, mode, external, nullptr, &total);
+  // a workspace sized here must serve both the streaming and the fallback kernels
+  carve(q.dev, q.kkt_plan->pat, batch, pb, ab, mode, external, nullptr, &total2, &q, stream_eligible(q, nullptr));
+  return total > total2 ? total : total2;
 }
 
 size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, int ab) {
@@ -438,15 +475,17 @@ int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb
   return assemble_and_factor(o, pat, pT, pb, aT, ab, kkt, lx, d, dinv, scratch, f, s);
 }
 
-int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
                const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
                cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const Pattern& pat = q.kkt_plan->pat;
   const int B = d.batch;
   if (B <= 0) return WMPC_OK;
   const int pb = d.p_batch, ab = d.a_batch;
   const bool external = lx_ext != nullptr;
   size_t need = 0;
-  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need);
+  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need, &q, stream_eligible(q, &opt));
   if (ws == nullptr || ws_bytes < need)
     return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
   int rc;
@@ -471,6 +510,24 @@ int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, 
   const int sbp = pb > 1 ? 1 : 0, sba = ab > 1 ? 1 : 0;
   const long long ldp = pb, lda = ab;
   const int kb = pb > ab ? pb : ab;
+
+  if (L.streaming) {
+    WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
+    if ((rc = launch_stream_solve(pat, q.sp, o, L.pT, ldp, sbp, L.aT, lda, sba, L.x, L.z, L.y, L.qs, L.ls, L.us,
+                                  L.stream_ws, L.stream_status, L.error_word, B, opt.max_iter, q.num_sms, s)))
+      return rc;
+    residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
+                                                     d.dual_res, d.obj, d.status, B, L.stream_status, L.error_word);
+    WMPC_LAUNCH_CHECK();
+    if (d.iters) {
+      fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
+      WMPC_LAUNCH_CHECK();
+    }
+    if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
+    if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
+    if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
+    return WMPC_OK;
+  }
 
   // the factorization the iterations use
   const float* lx = lx_ext;
@@ -499,7 +556,7 @@ int osqp_solve(const Osqp& o, const Pattern& pat, const wmpc_osqp_options& opt, 
       WMPC_LAUNCH_CHECK();
     }
     residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
-                                                     d.dual_res, d.obj, d.status, B);
+                                                     d.dual_res, d.obj, d.status, B, nullptr, nullptr);
     WMPC_LAUNCH_CHECK();
     if (d.iters) {
       fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);

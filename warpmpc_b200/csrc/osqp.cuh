@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "stream.cuh"
 
 namespace wmpc {
 
@@ -41,7 +42,12 @@ struct Osqp {
 
 struct wmpc_osqp {
   int device = 0;
+  int num_sms = 0;
   wmpc::Osqp dev{};
   const wmpc_plan* kkt_plan = nullptr;
   void* block = nullptr;  // single device allocation holding every table
+  bool has_stream = false;
+  wmpc::StreamPlan sp{};
+  void* stream_block = nullptr;
+  std::string stream_why;  // why the streaming path is unavailable (diagnostics)
 };

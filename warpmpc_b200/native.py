@@ -161,6 +161,11 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpBatch), ctypes.c_void_p, ctypes.c_void_p,
          ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
+    "wmpc_stream_schedule_host": (
+        ctypes.c_int,
+        [ctypes.POINTER(PatternDesc), _f32p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+         _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+    ),
     "wmpc_profile_begin": (ctypes.c_int, []),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
     "wmpc_launch_count": (ctypes.c_int64, []),
