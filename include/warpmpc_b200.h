@@ -166,6 +166,9 @@ typedef struct wmpc_osqp_options {
   int32_t check_termination; /* 0: exactly max_iter iterations (reference)  */
   float eps_abs, eps_rel;
   int32_t warm_start;        /* 1: x0/z0/y0 given (unscaled), 0: zeros       */
+  int32_t reuse_factor;      /* 1: the workspace already holds the factor of
+                                these P/A values from a previous call with the
+                                same workspace, batch and mode: skip it       */
 } wmpc_osqp_options;
 
 /* Batched problem data, batch-major.  p_values [pb x nnz_p], a_values
@@ -243,6 +246,40 @@ int wmpc_profile_begin(void);
 int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* total_launches);
 /* Kernels launched by this library since load (or the last profile_begin). */
 int64_t wmpc_launch_count(void);
+
+/* ------------------------------------------------------------------ */
+/* Adjoint (reverse-mode derivatives of the solution).                 */
+/* Replaces CompiledOSQP.adjoint_derivative_compute/get_mat/get_vec    */
+/* (solver.py:1046-1192) and the custom_vjp backward rules             */
+/* (solver.py:1252-1465).  Instead of the reference's separate adjoint */
+/* KKT factorization + refinement, it solves the active-set adjoint    */
+/* system  [P A_C^T; A_C 0] [w; mu] = [-dx; t]  (t_r = -tau_r dy_r,    */
+/* tau = +1 upper-active / -1 lower-active, equality rows by sign(y))  */
+/* as an equality-constrained QP with the forward's ADMM, re-using the */
+/* forward's LDL^T factor still held in the workspace.  Outputs follow */
+/* the reference's formulas: dq = w, du = -mu (upper rows), dl = -mu   */
+/* (lower rows), dP = (w x^T + x w^T)/2 on P's upper pattern,          */
+/* dA = y w^T + mu x^T on A's pattern (per instance).                  */
+/* ------------------------------------------------------------------ */
+typedef struct wmpc_osqp_adjoint_batch {
+  int32_t batch;
+  const float* p_values; int32_t p_batch;   /* the forward's P/A values   */
+  const float* a_values; int32_t a_batch;
+  const float* l; const float* u;           /* forward bounds [batch x m] */
+  const float* x; const float* z; const float* y; /* forward solution     */
+  const float* dx; const float* dy;         /* cotangents; dy may be NULL */
+  float* dq; float* dl; float* du;          /* [batch x n], [batch x m]   */
+  float* dp; float* da;                     /* [batch x nnz_p], [batch x nnz_a] */
+  float* adj_prim_res;                      /* optional [batch]           */
+} wmpc_osqp_adjoint_batch;
+
+/* Workspace for a forward solve that keeps its factor for the adjoint
+ * (pass the same buffer to wmpc_osqp_solve and wmpc_osqp_adjoint). */
+size_t wmpc_osqp_adjoint_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t mode);
+/* options->max_iter: ADMM iterations of the adjoint solve. */
+int wmpc_osqp_adjoint(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
+                      const wmpc_osqp_adjoint_batch* data, int32_t mode, void* workspace,
+                      size_t workspace_bytes, wmpc_stream_t stream);
 
 const char* wmpc_last_error_string(void);
 /* Library version string, e.g. "0.1.0 sm_100a". */

@@ -16,9 +16,13 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 LIB = HERE / "_build" / "libosqp_cpu.so"
+LIB64 = HERE / "_build" / "libosqp_cpu_f64.so"
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _f32p = ctypes.POINTER(ctypes.c_float)
+
+
+_rp = _f32p  # rebound per precision below
 
 
 class _Pattern(ctypes.Structure):
@@ -29,21 +33,30 @@ class _Pattern(ctypes.Structure):
     ]
 
 
-class _Osqp(ctypes.Structure):
-    _fields_ = [
-        ("n", ctypes.c_int), ("m", ctypes.c_int), ("nnz_p", ctypes.c_int), ("nnz_a", ctypes.c_int),
-        ("nnz_kkt", ctypes.c_int), ("nnz_pf", ctypes.c_int), ("sigma", ctypes.c_float), ("alpha", ctypes.c_float),
-        ("kkt_base", _f32p), ("kkt_src", _i32p), ("p_scale", _f32p), ("p_diag_sigma", _f32p), ("a_scale", _f32p),
-        ("a_row_ptr", _i32p), ("a_row_ent", _i32p), ("a_rows", _i32p), ("a_cols", _i32p), ("a_col_ptr", _i32p),
-        ("pf_row_ptr", _i32p), ("pf_val", _i32p), ("pf_col", _i32p),
-        ("rho", _f32p), ("rho_inv", _f32p), ("q_scale", _f32p), ("scaling_d", _f32p), ("scaling_dinv", _f32p),
-        ("scaling_e", _f32p), ("scaling_einv", _f32p), ("y_scale", _f32p), ("y_unscale", _f32p),
-    ]
+def _osqp_struct(real, rp):
+    class _Osqp(ctypes.Structure):
+        _fields_ = [
+            ("n", ctypes.c_int), ("m", ctypes.c_int), ("nnz_p", ctypes.c_int), ("nnz_a", ctypes.c_int),
+            ("nnz_kkt", ctypes.c_int), ("nnz_pf", ctypes.c_int), ("sigma", real), ("alpha", real),
+            ("kkt_base", rp), ("kkt_src", _i32p), ("p_scale", rp), ("p_diag_sigma", rp), ("a_scale", rp),
+            ("a_row_ptr", _i32p), ("a_row_ent", _i32p), ("a_rows", _i32p), ("a_cols", _i32p), ("a_col_ptr", _i32p),
+            ("pf_row_ptr", _i32p), ("pf_val", _i32p), ("pf_col", _i32p),
+            ("rho", rp), ("rho_inv", rp), ("q_scale", rp), ("scaling_d", rp), ("scaling_dinv", rp),
+            ("scaling_e", rp), ("scaling_einv", rp), ("y_scale", rp), ("y_unscale", rp),
+        ]
+
+    return _Osqp
+
+
+_f64p = ctypes.POINTER(ctypes.c_double)
+_Osqp32 = _osqp_struct(ctypes.c_float, _f32p)
+_Osqp64 = _osqp_struct(ctypes.c_double, _f64p)
 
 
 def build(force: bool = False) -> pathlib.Path:
     src = HERE / "c" / "osqp_cpu.c"
-    if force or not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    stale = lambda p: not p.exists() or p.stat().st_mtime < src.stat().st_mtime  # noqa: E731
+    if force or stale(LIB) or stale(LIB64):
         subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
     return LIB
 
@@ -51,10 +64,14 @@ def build(force: bool = False) -> pathlib.Path:
 class CpuOSQP:
     """The C restatement bound to one FixedOSQPPlan."""
 
-    def __init__(self, plan):
+    def __init__(self, plan, dtype=np.float32):
         build()
-        self.lib = ctypes.CDLL(str(LIB))
-        self.lib.oc_osqp_solve.restype = ctypes.c_int
+        self.dtype = np.dtype(dtype)
+        double = self.dtype == np.float64
+        self.lib = ctypes.CDLL(str(LIB64 if double else LIB))
+        self._fn = self.lib.oc_osqp_solve_f64 if double else self.lib.oc_osqp_solve
+        self._fn.restype = ctypes.c_int
+        self._rp = _f64p if double else _f32p
         self.plan = plan
         from warpmpc_b200.jax_qdldl.planning import plan_ragged_program
 
@@ -68,9 +85,9 @@ class CpuOSQP:
             return a.ctypes.data_as(_i32p)
 
         def f(a):
-            a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+            a = np.ascontiguousarray(np.asarray(a, dtype=self.dtype))
             keep.append(a)
-            return a.ctypes.data_as(_f32p)
+            return a.ctypes.data_as(self._rp)
 
         self.pat = _Pattern(qp.n, qp.nnz_a, qp.nnz_l, i(qp.perm_to_orig), i(qp.diag_pos), i(rg["init_ptr"]),
                             i(rg["init_rows"]), i(rg["init_pos"]), i(rg["proc_ptr"]), i(rg["proc_cols"]),
@@ -85,9 +102,10 @@ class CpuOSQP:
         pf_order = np.argsort(plan.p_full_rows, kind="stable")
         pf_row_ptr = np.concatenate([[0], np.cumsum(np.bincount(plan.p_full_rows, minlength=n))]).astype(np.int32)
         s = plan.settings
-        self.osqp = _Osqp(
-            n, m, plan.nnz_p, plan.nnz_a, plan.nnz_kkt, int(plan.p_full_rows.size), np.float32(s.sigma),
-            np.float32(s.alpha), f(plan.kkt_upper.data), i(kkt_src), f(plan.p_scale), f(plan.p_diag_sigma),
+        osqp_cls = _Osqp64 if double else _Osqp32
+        self.osqp = osqp_cls(
+            n, m, plan.nnz_p, plan.nnz_a, plan.nnz_kkt, int(plan.p_full_rows.size), self.dtype.type(s.sigma),
+            self.dtype.type(s.alpha), f(plan.kkt_upper.data), i(kkt_src), f(plan.p_scale), f(plan.p_diag_sigma),
             f(plan.a_scale), i(a_row_ptr), i(a_row_ent), i(plan.a_rows), i(plan.a_cols), i(a_col_ptr),
             i(pf_row_ptr), i(plan.p_full_value_map[pf_order]), i(plan.p_full_cols[pf_order]),
             f(plan.rho_vec), f(plan.rho_inv_vec), f(plan.q_scale), f(plan.scaling_d), f(plan.scaling_dinv),
@@ -96,23 +114,24 @@ class CpuOSQP:
 
     def solve(self, p_values, a_values, q, l, u, warm=None, max_iter=None, threads: int | None = None):
         plan = self.plan
-        c = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float32))  # noqa: E731
+        c = lambda a: np.ascontiguousarray(np.asarray(a, dtype=self.dtype))  # noqa: E731
         p_values, a_values, q, l, u = (np.atleast_2d(c(v)) for v in (p_values, a_values, q, l, u))
         batch = q.shape[0]
-        x = np.empty((batch, plan.n), np.float32)
-        z = np.empty((batch, plan.m), np.float32)
-        y = np.empty((batch, plan.m), np.float32)
-        prim = np.empty(batch, np.float32)
-        dual = np.empty(batch, np.float32)
-        obj = np.empty(batch, np.float32)
-        fp = lambda a: None if a is None else a.ctypes.data_as(_f32p)  # noqa: E731
+        dt = self.dtype
+        x = np.empty((batch, plan.n), dt)
+        z = np.empty((batch, plan.m), dt)
+        y = np.empty((batch, plan.m), dt)
+        prim = np.empty(batch, dt)
+        dual = np.empty(batch, dt)
+        obj = np.empty(batch, dt)
+        fp = lambda a: None if a is None else a.ctypes.data_as(self._rp)  # noqa: E731
         w = [None, None, None] if warm is None else [c(v) for v in warm]
         threads = threads or os.cpu_count() or 1
         iters = int(plan.settings.max_iter if max_iter is None else max_iter)
 
         def run(lo, hi):
             # ctypes releases the GIL for the duration of the call
-            return self.lib.oc_osqp_solve(
+            return self._fn(
                 ctypes.byref(self.pat), ctypes.byref(self.osqp), lo, hi, iters,
                 fp(p_values), p_values.shape[0], fp(a_values), a_values.shape[0], fp(q), fp(l), fp(u),
                 fp(w[0]), fp(w[1]), fp(w[2]), fp(x), fp(z), fp(y), fp(prim), fp(dual), fp(obj),

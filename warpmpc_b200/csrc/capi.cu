@@ -70,6 +70,9 @@ void profile_mark_end(cudaStream_t s) {
 
 size_t osqp_workspace_bytes(const wmpc_osqp& q, int batch, int pb, int ab, int mode, bool external);
 size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, int ab);
+size_t osqp_adjoint_extra_bytes(const Osqp& o, int batch);
+int osqp_adjoint(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_adjoint_batch& a, int mode,
+                 void* ws, size_t ws_bytes, cudaStream_t s);
 int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
                 float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s);
 int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
@@ -416,6 +419,19 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
   }
   for (int e = 0; e < na; ++e) a_col_ptr[desc->a_cols[e] + 1]++;
   for (int j = 0; j < n; ++j) a_col_ptr[j + 1] += a_col_ptr[j];
+  // upper entries of P: first occurrence of each entry in the full pattern
+  std::vector<int32_t> p_up_rows(np, 0), p_up_cols(np, 0);
+  {
+    std::vector<char> seen(np, 0);
+    for (int t = 0; t < npf; ++t) {
+      const int k = desc->p_full_value_map[t];
+      if (!seen[k]) {
+        seen[k] = 1;
+        p_up_rows[k] = desc->p_full_rows[t];
+        p_up_cols[k] = desc->p_full_cols[t];
+      }
+    }
+  }
   // both triangles of P grouped by row, stable in the reference's entry order
   std::vector<int32_t> pf_row_ptr(n + 1, 0), pf_val(npf), pf_col(npf);
   for (int t = 0; t < npf; ++t) pf_row_ptr[desc->p_full_rows[t] + 1]++;
@@ -468,6 +484,8 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
   pk.addf(desc->scaling_einv, m, &o.scaling_einv);
   pk.addf(desc->y_scale, m, &o.y_scale);
   pk.addf(desc->y_unscale, m, &o.y_unscale);
+  pk.add(p_up_rows.data(), np, &q->p_upper_rows);
+  pk.add(p_up_cols.data(), np, &q->p_upper_cols);
   int* block = nullptr;
   int rc = pk.upload(&block);
   if (rc) {
@@ -577,6 +595,28 @@ size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t m
   const size_t solve = osqp_workspace_bytes(*osqp, batch, batch, batch, mode, external_factor != 0);
   const size_t fac = osqp_factor_workspace_bytes(osqp->dev, osqp->kkt_plan->pat, batch, batch);
   return solve > fac ? solve : fac;
+}
+
+size_t wmpc_osqp_adjoint_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t mode) {
+  if (!osqp || batch <= 0) return 0;
+  return osqp_workspace_bytes(*osqp, batch, batch, batch, mode, false) + osqp_adjoint_extra_bytes(osqp->dev, batch);
+}
+
+int wmpc_osqp_adjoint(const wmpc_osqp* osqp, const wmpc_osqp_options* options, const wmpc_osqp_adjoint_batch* data,
+                      int32_t mode, void* workspace, size_t workspace_bytes, wmpc_stream_t stream) {
+  if (!osqp || !options || !data) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  if (mode != WMPC_OSQP_PLAIN && mode != WMPC_OSQP_PERSISTENT) return fail(WMPC_ERR_INVALID_ARGUMENT, "unknown mode %d", mode);
+  const wmpc_osqp_adjoint_batch& a = *data;
+  if (a.batch < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "negative batch");
+  if (a.batch == 0) return WMPC_OK;
+  if ((a.p_batch != 1 && a.p_batch != a.batch) || (a.a_batch != 1 && a.a_batch != a.batch))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "p_batch/a_batch must be 1 or batch");
+  if (!a.p_values || !a.a_values || !a.l || !a.u || !a.x || !a.z || !a.y || !a.dx || !a.dq || !a.dl || !a.du)
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "null buffer");
+  if (options->max_iter < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "max_iter must be nonnegative");
+  DeviceGuard guard(osqp->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
+  return osqp_adjoint(*osqp, *options, a, mode, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
 int wmpc_osqp_factor(const wmpc_osqp* osqp, const float* p_values, int32_t p_batch, const float* a_values,

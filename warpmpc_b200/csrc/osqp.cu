@@ -432,7 +432,7 @@ int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int 
 int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
                         int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
                         const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int batch, int max_iter, int num_sms, cudaStream_t s);
+                        int batch, int max_iter, int num_sms, bool reuse_factor, cudaStream_t s);
 
 static bool stream_eligible(const wmpc_osqp& q, const wmpc_osqp_options* opt) {
   return q.has_stream && (opt == nullptr || opt->check_termination == 0) && !env_disabled("WMPC_DISABLE_STREAM");
@@ -514,7 +514,8 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if (L.streaming) {
     WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
     if ((rc = launch_stream_solve(pat, q.sp, o, L.pT, ldp, sbp, L.aT, lda, sba, L.x, L.z, L.y, L.qs, L.ls, L.us,
-                                  L.stream_ws, L.stream_status, L.error_word, B, opt.max_iter, q.num_sms, s)))
+                                  L.stream_ws, L.stream_status, L.error_word, B, opt.max_iter, q.num_sms,
+                                  opt.reuse_factor != 0, s)))
       return rc;
     residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
                                                      d.dual_res, d.obj, d.status, B, L.stream_status, L.error_word);
@@ -534,7 +535,8 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   const float* dinv = dinv_ext;
   int fb = fb_ext;
   if (!external && L.factor_separately) {
-    if ((rc = assemble_and_factor(o, pat, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch, L.scratch_bytes, s)))
+    if (!opt.reuse_factor &&
+        (rc = assemble_and_factor(o, pat, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch, L.scratch_bytes, s)))
       return rc;
     lx = L.lx;
     dinv = L.dinv;
@@ -564,6 +566,7 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
     }
   } else {
     const bool fused = !external && !L.factor_separately;
+    const bool refactor = fused && !opt.reuse_factor;
     PersistentArgs pa{};
     pa.pat = pat;
     pa.o = o;
@@ -576,7 +579,7 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
     pa.d = fused ? L.d : nullptr;
     pa.fstride = fused ? 1 : (fb > 1 ? 1 : 0);
     pa.fld = fused ? B : fb;
-    pa.fused_factor = fused ? 1 : 0;
+    pa.fused_factor = refactor ? 1 : 0;
     pa.wglob = L.scratch;
     pa.prim = d.prim_res; pa.dual = d.dual_res; pa.obj = d.obj;
     pa.iters = d.iters; pa.status = d.status;
@@ -600,6 +603,141 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
   if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
   if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
+  return WMPC_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// adjoint: active-set differential QP on the forward's factorization
+// ---------------------------------------------------------------------------
+
+// Per (instance, constraint): activity tau (+1 upper / -1 lower / 0 free) and
+// the differential QP's bounds (t = -tau * dy on active rows, free otherwise).
+__global__ void adjoint_prep_kernel(const float* __restrict__ l, const float* __restrict__ u,
+                                    const float* __restrict__ z, const float* __restrict__ y,
+                                    const float* __restrict__ dy, float* __restrict__ ld, float* __restrict__ ud,
+                                    int* __restrict__ tau, long long count) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const float lk = l[k], uk = u[k], zk = z[k], yk = y[k];
+  int t = 0;
+  if (lk == uk) t = (yk >= 0.0f) ? 1 : -1;
+  else if (zk >= uk) t = 1;
+  else if (zk <= lk) t = -1;
+  const float dyk = dy ? dy[k] : 0.0f;
+  if (t != 0) {
+    const float target = -(float)t * dyk;
+    ld[k] = target;
+    ud[k] = target;
+  } else {
+    ld[k] = -1e30f;
+    ud[k] = 1e30f;
+  }
+  tau[k] = t;
+}
+
+// dl/du from the differential QP's multipliers mu (dq = w is written by the solve)
+__global__ void adjoint_bounds_kernel(const int* __restrict__ tau, const float* __restrict__ mu,
+                                      float* __restrict__ dl, float* __restrict__ du, long long count) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int t = tau[k];
+  const float g = -mu[k];
+  dl[k] = t < 0 ? g : 0.0f;
+  du[k] = t > 0 ? g : 0.0f;
+}
+
+// dP on P's upper pattern and dA on A's pattern, per instance (batch-major):
+// dP_k = 0.5 * (w_i x_j + w_j x_i), dA_k = y_r w_c + nu_r x_c (nu = mu on
+// active rows, 0 on free rows) -- solver.py:1184-1191.
+__global__ void adjoint_matrix_kernel(Osqp o, const int* __restrict__ p_rows, const int* __restrict__ p_cols,
+                                      const float* __restrict__ w, const float* __restrict__ x,
+                                      const float* __restrict__ y, const float* __restrict__ mu,
+                                      const int* __restrict__ tau, float* __restrict__ dp, float* __restrict__ da,
+                                      int batch) {
+  const int b = blockIdx.y;
+  if (b >= batch) return;
+  const float* wb = w + (size_t)b * o.n;
+  const float* xb = x + (size_t)b * o.n;
+  const float* yb = y + (size_t)b * o.m;
+  const float* mb = mu + (size_t)b * o.m;
+  const int* tb = tau + (size_t)b * o.m;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < o.nnz_p + o.nnz_a; k += gridDim.x * blockDim.x) {
+    if (k < o.nnz_p) {
+      const int i = __ldg(p_rows + k), j = __ldg(p_cols + k);
+      dp[(size_t)b * o.nnz_p + k] = 0.5f * (wb[i] * xb[j] + wb[j] * xb[i]);
+    } else {
+      const int e = k - o.nnz_p;
+      const int r = __ldg(o.a_rows + e), c = __ldg(o.a_cols + e);
+      const float nu = tb[r] != 0 ? mb[r] : 0.0f;
+      da[(size_t)b * o.nnz_a + e] = yb[r] * wb[c] + nu * xb[c];
+    }
+  }
+}
+
+size_t osqp_adjoint_extra_bytes(const Osqp& o, int batch) {
+  Carve c{nullptr};
+  c.take((size_t)o.m * batch);       // tau
+  c.take((size_t)o.m * batch);       // mu
+  c.take((size_t)o.m * batch);       // z of the differential QP
+  c.take((size_t)o.m * batch);       // ld
+  c.take((size_t)o.m * batch);       // ud
+  c.take(5 * (size_t)batch);         // prim, dual, obj, iters, status
+  return c.used;
+}
+
+int osqp_adjoint(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_adjoint_batch& a, int mode,
+                 void* ws, size_t ws_bytes, cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const int B = a.batch;
+  if (B <= 0) return WMPC_OK;
+  size_t solve_bytes = 0;
+  carve(o, q.kkt_plan->pat, B, a.p_batch, a.a_batch, mode, false, nullptr, &solve_bytes, &q,
+        stream_eligible(q, &opt) && mode == WMPC_OSQP_PERSISTENT);
+  const size_t extra = osqp_adjoint_extra_bytes(o, B);
+  if (ws == nullptr || ws_bytes < solve_bytes + extra)
+    return fail(WMPC_ERR_WORKSPACE, "OSQP adjoint needs %zu workspace bytes, got %zu", solve_bytes + extra, ws_bytes);
+  Carve c{static_cast<char*>(ws) + solve_bytes};
+  int* tau = reinterpret_cast<int*>(c.take((size_t)o.m * B));
+  float* mu = c.take((size_t)o.m * B);
+  float* zd = c.take((size_t)o.m * B);
+  float* ld = c.take((size_t)o.m * B);
+  float* ud = c.take((size_t)o.m * B);
+  float* misc = c.take(5 * (size_t)B);
+  const long long cm = (long long)o.m * B;
+  adjoint_prep_kernel<<<ceil_div(cm, 256), 256, 0, s>>>(a.l, a.u, a.z, a.y, a.dy, ld, ud, tau, cm);
+  WMPC_LAUNCH_CHECK();
+  wmpc_osqp_batch d{};
+  d.batch = B;
+  d.p_values = a.p_values;
+  d.p_batch = a.p_batch;
+  d.a_values = a.a_values;
+  d.a_batch = a.a_batch;
+  d.q = a.dx;
+  d.l = ld;
+  d.u = ud;
+  d.x = a.dq;  // w
+  d.z = zd;
+  d.y = mu;
+  d.prim_res = a.adj_prim_res ? a.adj_prim_res : misc;
+  d.dual_res = misc + B;
+  d.obj = misc + 2 * B;
+  d.iters = reinterpret_cast<int*>(misc + 3 * B);
+  d.status = reinterpret_cast<int*>(misc + 4 * B);
+  wmpc_osqp_options ao = opt;
+  ao.warm_start = 0;
+  ao.reuse_factor = 1;  // same carve as the forward: check_termination and mode must match it
+  int rc = osqp_solve(q, ao, d, nullptr, nullptr, 0, mode, ws, solve_bytes, s);
+  if (rc) return rc;
+  adjoint_bounds_kernel<<<ceil_div(cm, 256), 256, 0, s>>>(tau, mu, a.dl, a.du, cm);
+  WMPC_LAUNCH_CHECK();
+  if (a.dp || a.da) {
+    if (!a.dp || !a.da) return fail(WMPC_ERR_INVALID_ARGUMENT, "dp and da go together");
+    dim3 grid(ceil_div(o.nnz_p + o.nnz_a, 256) < 64 ? ceil_div(o.nnz_p + o.nnz_a, 256) : 64, B);
+    adjoint_matrix_kernel<<<grid, 256, 0, s>>>(o, q.p_upper_rows, q.p_upper_cols, a.dq, a.x, a.y, mu, tau, a.dp,
+                                               a.da, B);
+    WMPC_LAUNCH_CHECK();
+  }
   return WMPC_OK;
 }
 

@@ -46,6 +46,8 @@ struct wmpc_osqp {
   wmpc::Osqp dev{};
   const wmpc_plan* kkt_plan = nullptr;
   void* block = nullptr;  // single device allocation holding every table
+  const int* p_upper_rows = nullptr;  // [nnz_p] row of every stored upper entry of P
+  const int* p_upper_cols = nullptr;  // [nnz_p]
   bool has_stream = false;
   wmpc::StreamPlan sp{};
   void* stream_block = nullptr;

@@ -535,7 +535,7 @@ size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
 int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
                         int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
                         const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int batch, int max_iter, int num_sms, cudaStream_t s) {
+                        int batch, int max_iter, int num_sms, bool reuse_factor, cudaStream_t s) {
   StreamLaunch cfg;
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
@@ -547,7 +547,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   float* p0 = s1 + tl * sp.n;
   float* p1 = p0 + tl * sp.n;
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
-  {
+  if (!reuse_factor) {
     const int warps = 4;
     const size_t smem = (size_t)warps * (sp.max_row_nnz > 0 ? sp.max_row_nnz : 1) * 32 * sizeof(float);
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

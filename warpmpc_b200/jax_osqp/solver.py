@@ -161,7 +161,7 @@ class OSQPEngine:
         return lx, dinv
 
     def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
-              mode=None, out=None):
+              mode=None, out=None, keep_factor=False):
         """Batched solve; returns ``(x, z, y, prim_res, dual_res, obj_val)``.
 
         ``out`` optionally supplies those six output tensors (plus ``iters``,
@@ -233,12 +233,60 @@ class OSQPEngine:
         else:
             lx_p = dinv_p = None
             fb, ext = 0, 0
-        ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext), dev)
+        if keep_factor:
+            if factor is not None:
+                raise ValueError("keep_factor needs the solve to factor (no external factor)")
+            ws, wsb = _workspace(lib.wmpc_osqp_adjoint_workspace_bytes(self.dev.handle, batch, mode_id), dev)
+        else:
+            ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext), dev)
         native.check(lib.wmpc_osqp_solve(self.dev.handle, ctypes.byref(opts), ctypes.byref(data), lx_p, dinv_p, fb,
                                          mode_id, native.tensor_ptr(ws), wsb, native.current_stream_handle(dev)))
         self.last_iters = iters
         self.last_status = status
+        self.last_workspace = (ws, wsb, mode_id, int(opts.check_termination)) if keep_factor else None
         return x, z, y, prim, dual, obj
+
+    def adjoint(self, workspace, p_values, a_values, l, u, x, z, y, dx, dy=None, max_iter=None):
+        """Reverse-mode derivatives on the factor kept by ``solve(keep_factor=True)``.
+
+        Returns ``(dq, dl, du, dp, da)`` per instance (``dp``/``da`` batch-major
+        on P's upper pattern and A's pattern).
+        """
+        import torch
+
+        ws, wsb, mode_id, check = workspace
+        pl = self.plan
+        p = self._mat(p_values, pl.nnz_p, "p_values")
+        a = self._mat(a_values, pl.nnz_a, "a_values")
+        x = self._mat(x, pl.n, "x")
+        batch = int(x.shape[0])
+        z = self._vec(z, pl.m, batch, "z")
+        y = self._vec(y, pl.m, batch, "y")
+        lm = self._vec(l, pl.m, batch, "l")
+        um = self._vec(u, pl.m, batch, "u")
+        dxm = self._vec(dx, pl.n, batch, "dx")
+        dym = None if dy is None else self._vec(dy, pl.m, batch, "dy")
+        dev = self.device
+        dq = torch.empty((batch, pl.n), dtype=torch.float32, device=dev)
+        dl = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+        du = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
+        dp = torch.empty((batch, pl.nnz_p), dtype=torch.float32, device=dev)
+        da = torch.empty((batch, pl.nnz_a), dtype=torch.float32, device=dev)
+        res = torch.empty(batch, dtype=torch.float32, device=dev)
+        s = pl.settings
+        opts = native.OsqpOptions(max_iter=int(s.max_iter if max_iter is None else max_iter), check_termination=check,
+                                  eps_abs=np.float32(s.eps_abs), eps_rel=np.float32(s.eps_rel), warm_start=0,
+                                  reuse_factor=1)
+        data = native.OsqpAdjointBatch(
+            batch=batch, p_values=p.data_ptr(), p_batch=int(p.shape[0]), a_values=a.data_ptr(),
+            a_batch=int(a.shape[0]), l=lm.data_ptr(), u=um.data_ptr(), x=x.data_ptr(), z=z.data_ptr(),
+            y=y.data_ptr(), dx=dxm.data_ptr(), dy=None if dym is None else dym.data_ptr(), dq=dq.data_ptr(),
+            dl=dl.data_ptr(), du=du.data_ptr(), dp=dp.data_ptr(), da=da.data_ptr(), adj_prim_res=res.data_ptr(),
+        )
+        native.check(native.lib().wmpc_osqp_adjoint(self.dev.handle, ctypes.byref(opts), ctypes.byref(data), mode_id,
+                                                    native.tensor_ptr(ws), wsb, native.current_stream_handle(dev)))
+        self.last_adjoint_residual = res
+        return dq, dl, du, dp, da
 
 
 def compile_osqp(
@@ -258,8 +306,17 @@ def compile_osqp(
     derivative_refinement_iters: int = 100,
     mode: str = "persistent",
     device=None,
+    adjoint_iters: int | None = None,
 ) -> CompiledOSQP:
-    """Compile fixed-pattern batched OSQP iterations (solver.py:685-1492)."""
+    """Compile fixed-pattern batched OSQP iterations (solver.py:685-1492).
+
+    ``derivatives=True`` adds the reverse-mode callables (``solve_xy``,
+    ``solve_primal``, and ``solve``/``solve_warm_start`` with gradients) on the
+    adjoint that re-uses the forward factor; ``adjoint_iters`` sets its ADMM
+    iterations (default ``settings.max_iter``).  ``derivative_refinement_iters``
+    is accepted for signature compatibility (the reference's refinement of a
+    separately factored adjoint system does not exist here).
+    """
 
     import torch
 
@@ -314,7 +371,7 @@ def compile_osqp(
     if derivatives:
         from .adjoint import make_derivative_callables
 
-        extra = make_derivative_callables(plan, engine, qdldl, derivative_refinement_iters)
+        extra = make_derivative_callables(plan, engine, adjoint_iters)
 
     return CompiledOSQP(
         plan=plan,

@@ -97,6 +97,30 @@ class OsqpOptions(ctypes.Structure):
         ("eps_abs", ctypes.c_float),
         ("eps_rel", ctypes.c_float),
         ("warm_start", ctypes.c_int32),
+        ("reuse_factor", ctypes.c_int32),
+    ]
+
+
+class OsqpAdjointBatch(ctypes.Structure):
+    _fields_ = [
+        ("batch", ctypes.c_int32),
+        ("p_values", ctypes.c_void_p),
+        ("p_batch", ctypes.c_int32),
+        ("a_values", ctypes.c_void_p),
+        ("a_batch", ctypes.c_int32),
+        ("l", ctypes.c_void_p),
+        ("u", ctypes.c_void_p),
+        ("x", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("y", ctypes.c_void_p),
+        ("dx", ctypes.c_void_p),
+        ("dy", ctypes.c_void_p),
+        ("dq", ctypes.c_void_p),
+        ("dl", ctypes.c_void_p),
+        ("du", ctypes.c_void_p),
+        ("dp", ctypes.c_void_p),
+        ("da", ctypes.c_void_p),
+        ("adj_prim_res", ctypes.c_void_p),
     ]
 
 
@@ -160,6 +184,12 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpBatch), ctypes.c_void_p, ctypes.c_void_p,
          ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
+    ),
+    "wmpc_osqp_adjoint_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]),
+    "wmpc_osqp_adjoint": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpAdjointBatch), ctypes.c_int32,
+         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
     "wmpc_stream_schedule_host": (
         ctypes.c_int,
