@@ -114,6 +114,22 @@ int wmpc_solve(const wmpc_plan* plan, const float* lx, const float* dinv,
                int32_t factor_bstride, const float* rhs, float* x, int32_t batch,
                void* workspace, size_t workspace_bytes, wmpc_stream_t stream);
 
+/* Allocation-free variant of wmpc_solve (no counterpart in the reference).
+ * For callers that cannot allocate device memory when they solve -- a
+ * real-time control loop that must stay out of the CUDA allocator, or a
+ * framework custom-call handler with no slot for an extra workspace: the
+ * work vectors live in a fixed 32 MiB array of device memory inside this
+ * library, so only inputs and outputs are passed.  Same arguments and
+ * results as wmpc_solve.  Limit: n * batch <= 8,388,608 floats (larger
+ * requests return WMPC_ERR_WORKSPACE and launch nothing).  All calls on a
+ * device share the array: calls whose kernels may overlap on the GPU race
+ * and must be ordered (same stream, or events).  The first call on a device
+ * looks up the array's device address, so make it before any stream
+ * capture that contains the call.  Allocates nothing. */
+int wmpc_solve_noalloc(const wmpc_plan* plan, const float* lx, const float* dinv,
+                       int32_t factor_bstride, const float* rhs, float* x, int32_t batch,
+                       wmpc_stream_t stream);
+
 /* factor then solve.  Replaces CompiledQDLDL.factor_and_solve
  * (warp_backend.py:1404-1408). */
 int wmpc_factor_solve(const wmpc_plan* plan, const float* values, int64_t values_ld,

@@ -166,6 +166,11 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
          ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
+    "wmpc_solve_noalloc": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_int32, ctypes.c_void_p],
+    ),
     "wmpc_factor_solve": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
