@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample duration")
+    ap.add_argument("--no-grad", action="store_true", help="skip the forward+adjoint timing")
+    ap.add_argument("--grad-batch", type=int, default=16384)
     return ap.parse_args()
 
 
@@ -135,39 +137,38 @@ def algorithmic_bytes_per_instance(plan, max_iter):
 
 
 def dist_setup(args):
-    import torch
+    from warpmpc_b200 import multirank
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    env = multirank.rank_env()
+    if env.world > 1:
+        multirank.init(env, "nccl", timeout_s=120.0)
+    else:
+        import torch
 
-        import torch.distributed as dist
+        if torch.cuda.is_available():
+            torch.cuda.set_device(0)
+    return env.world, env.rank, env.local
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return world, rank, local
+
+def _env(world):
+    from warpmpc_b200 import multirank
+
+    env = multirank.rank_env()
+    assert env.world == world
+    return env
 
 
 def max_over_ranks(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from warpmpc_b200 import multirank
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return multirank.max_over_ranks(value, _env(world), "cuda") if world > 1 else value
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from warpmpc_b200 import multirank
 
-        dist.barrier()
+    if world > 1:
+        multirank.barrier(_env(world))
 
 
 def cpu_baseline(plan, batch_np, args, cores=None):
@@ -267,6 +268,65 @@ def run_reference(args):
     return 0
 
 
+def gradient_timing(args, dev, world):
+    """(forward + adjoint) / forward on nx=4, nu=1, N=50, 16384 instances.
+
+    Forward: persistent solve that keeps its factor; backward: the adjoint on
+    that factor (25 ADMM iterations, cotangent of ||u0 - u_target||^2).
+    """
+    import torch
+
+    from warpmpc_b200 import problems
+    from warpmpc_b200.jax_osqp import compile_osqp
+
+    cls = problems.CARTPOLE
+    b = problems.make_batch(cls, args.grad_batch, seed=3000)
+    plan = problems.make_plan(problems.make_batch(cls, 1, seed=3000))
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev,
+                        derivatives=True)
+    eng = comp.engine
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    P, A, Q, L, U = (t(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u))
+    ui = (cls.horizon + 1) * cls.nx
+    u_target = torch.from_numpy(np.random.default_rng(7).standard_normal((b.batch, cls.nu)).astype(np.float32)).to(dev)
+
+    def fwd():
+        return eng.solve(P, A, Q, L, U, keep_factor=True)
+
+    def bwd(out):
+        x, z, y = out[0], out[1], out[2]
+        dx = torch.zeros_like(x)
+        dx[:, ui : ui + cls.nu] = 2.0 * (x[:, ui : ui + cls.nu] - u_target)
+        return eng.adjoint(eng.last_workspace, P, A, L, U, x, z, y, dx, None)
+
+    for _ in range(3):
+        o = fwd()
+        bwd(o)
+    torch.cuda.synchronize()
+    reps = 5
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd_ms = bwd_ms = 0.0
+    for _ in range(reps):
+        e[0].record()
+        o = fwd()
+        e[1].record()
+        bwd(o)
+        e[2].record()
+        torch.cuda.synchronize()
+        fwd_ms += e[0].elapsed_time(e[1]) / reps
+        bwd_ms += e[1].elapsed_time(e[2]) / reps
+    fwd_ms = max_over_ranks(fwd_ms, world)
+    bwd_ms = max_over_ranks(bwd_ms, world)
+    return {
+        "workload": f"linear {cls.name} MPC nx={cls.nx} nu={cls.nu} N={cls.horizon}, {b.batch} instances/GPU, "
+                    f"loss ||u0 - u_target||^2, forward {plan.settings.max_iter} + adjoint {plan.settings.max_iter} ADMM iterations",
+        "fwd_ms": fwd_ms,
+        "adjoint_ms": bwd_ms,
+        "ratio": (fwd_ms + bwd_ms) / fwd_ms,
+        "refactorizations_in_backward": 0,
+    }
+
+
 def config_dict(args, cls, plan, batch):
     return {
         "workload": f"linear {cls.name} MPC nx={cls.nx} nu={cls.nu} N={cls.horizon}, warm-started closed loop",
@@ -287,15 +347,17 @@ def main():
 
     import torch
 
-    from warpmpc_b200 import native, problems
+    from warpmpc_b200 import multirank, native, problems
     from warpmpc_b200.jax_osqp import compile_osqp
 
     world, rank, local = dist_setup(args)
     dev = torch.device("cuda", local)
     cls = get_class(args.config)
-    b = problems.make_batch(cls, args.batch, seed=1000 + rank)
+    b = problems.make_batch(cls, args.batch, seed=multirank.instance_seed(1000, rank))
     b0 = problems.make_batch(cls, 1, seed=1000)  # plan from the same instance 0 on every rank
     plan = problems.make_plan(b0)
+    if world > 1:
+        multirank.check_plans_agree(plan, multirank.rank_env(), dev)
     comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
     plain = None if args.no_plain else compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True,
                                                     mode="plain", device=dev)
@@ -358,11 +420,7 @@ def main():
     ok_frac = float(np.mean((prim <= RES_TOL) & (dual <= RES_TOL)))
     total_ok = ok_frac * B
     if world > 1:
-        t = torch.tensor([total_ok], dtype=torch.float64, device=dev)
-        import torch.distributed as dist
-
-        dist.all_reduce(t)
-        total_ok = float(t.item())
+        total_ok = multirank.sum_over_ranks(total_ok, multirank.rank_env(), dev)
     value = total_ok / (step_ms * 1e-3)
 
     # launches per step (graph replays bypass the host launch counter: count one eager step)
@@ -411,7 +469,7 @@ def main():
         torch.cuda.synchronize()
         pms = max_over_ranks(e0.elapsed_time(e1) / psteps, world)
         pfrac = float(np.mean((pout[3].cpu().numpy() <= RES_TOL) & (pout[4].cpu().numpy() <= RES_TOL)))
-        plain_res = {"value": pfrac * B * world / (pms * 1e-3), "ms_per_step": pms, "converged_fraction": pfrac,
+        plain_res = {"value": multirank.sum_over_ranks(pfrac * B, multirank.rank_env(), dev) / (pms * 1e-3), "ms_per_step": pms, "converged_fraction": pfrac,
                      "steps": psteps}
 
     # ---- end to end through the public API with pinned host buffers --------------------
@@ -443,8 +501,13 @@ def main():
         torch.cuda.synchronize()
         ems = max_over_ranks(e0.elapsed_time(e1) / esteps, world)
         efrac = float(np.mean((hres[0].numpy() <= RES_TOL) & (hres[1].numpy() <= RES_TOL)))
-        e2e = {"value": efrac * B * world / (ems * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+        e2e = {"value": multirank.sum_over_ranks(efrac * B, multirank.rank_env(), dev) / (ems * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
+
+    # ---- forward + adjoint vs forward (cartpole-like class, loss on u0) ------------------
+    grad = None
+    if not args.no_grad:
+        grad = gradient_timing(args, dev, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -471,7 +534,8 @@ def main():
             "graphed": graphed,
             "plain": plain_res,
             "persistent_over_plain": (value / plain_res["value"]) if plain_res and plain_res["value"] else None,
-            "fwd_bwd_over_fwd": None,
+            "fwd_bwd_over_fwd": grad["ratio"] if grad else None,
+            "gradient": grad,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -480,10 +544,7 @@ def main():
             "algorithmic_bytes": {"per_instance": per_inst, "factor": fac_b, "iteration": it_b},
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    multirank.finalize(multirank.rank_env())
     return 0
 
 
