@@ -237,20 +237,23 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
 /* Host-only export of the streaming schedule the persistent kernel uses for
  * a pattern (no counterpart in the reference; used to verify the schedule
  * on the CPU).  rho/rhoinv: per-constraint values (n_primal = number of
- * primal variables; KKT rows >= n_primal are constraints).  ent/cols/rel:
- * chunk size targets (entries, columns, releases).  With out == NULL,
- * *out_words receives the buffer size; otherwise out (capacity
- * out_capacity int32 words) receives, in order:
- *   [n_chunks, stream_len, max_ent, max_cols, max_rel, max_meta_words, max_row_nnz, n_meta]
- *   chunk_pos[n_chunks+1] chunk_ent[n_chunks] chunk_cols[n_chunks]
- *   meta_off[n_chunks] meta_words[n_chunks] meta[n_meta]
- *   col_spos[n] dinv_spos[n] proc_spos[nnz_l] u_perm[n] u_orig[n]
+ * primal variables; KKT rows >= n_primal are constraints).  units/cols/rel:
+ * backward chunk size targets (4-entry units, columns, releases); funits:
+ * forward chunk target (units).  With out == NULL, *out_words receives the
+ * buffer size; otherwise out (capacity out_capacity int32 words) receives,
+ * in order:
+ *   [n_chunks, blen, max_units, max_cols, max_rel, max_meta_words, max_row_nnz, n_meta]
+ *   chunk_off[n_chunks+1] chunk_units[n_chunks] chunk_cols[n_chunks]
+ *   chunk_u0[n_chunks] chunk_nrel[n_chunks] meta_off[n_chunks] meta_words[n_chunks] meta[n_meta]
+ *   col_uoff[n] dinv_off[n] proc_boff[nnz_l] u_perm[n] u_orig[n]
  *   init_slot[init_ptr[n]] upd_ptr[nnz_l+1] upd_slot[upd_ptr[nnz_l]]
- *   [n_fchunks, max_fent, max_frows, max_fmeta_words, n_fmeta]
- *   fchunk_pos[n_fchunks+1] fmeta_off[n_fchunks] fmeta_words[n_fchunks] fmeta[n_fmeta] proc_fpos[nnz_l] */
+ *   [n_fchunks, flen, max_funits, max_fmeta_words, n_fmeta]
+ *   fchunk_off[n_fchunks+1] fchunk_units[n_fchunks] fmeta_off[n_fchunks]
+ *   fmeta_words[n_fchunks] fmeta[n_fmeta] proc_foff[nnz_l]
+ *   [n_pad_b, n_pad_f, dummy_units] pad_boff[n_pad_b] pad_foff[n_pad_f] */
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv,
-                              int32_t n_primal, int32_t ent, int32_t cols, int32_t rel, int32_t* out,
-                              int64_t out_capacity, int64_t* out_words);
+                              int32_t n_primal, int32_t units, int32_t cols, int32_t rel, int32_t funits,
+                              int32_t* out, int64_t out_capacity, int64_t* out_words);
 
 /* Profiling (no counterpart in the reference, which times with wall
  * clocks around jax.block_until_ready).  Between begin and end the library

@@ -12,7 +12,9 @@ from __future__ import annotations
 
 import numpy as np
 
-KMETA = 5
+KHDR = 8  # chunk meta header words
+KUW = 8  # words per unit
+FIRST, LAST, FWD = 1, 2, 4
 
 
 def _f32(x):
@@ -24,7 +26,6 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     qp = plan.qdldl_plan
     rg = sched["ragged"]
     n, nnz_l = qp.n, qp.nnz_l
-    S = sched["stream_len"]
     B = q.shape[0]
     assert B <= 32
     lanes = 32
@@ -35,9 +36,22 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     kkt = np.broadcast_to(plan.kkt_upper.data.astype(np.float32), (lanes, plan.nnz_kkt)).copy()
     kkt[:, plan.p_to_kkt] = P * plan.p_scale.astype(np.float32) + plan.p_diag_sigma.astype(np.float32)
     kkt[:, plan.a_to_kkt] = A * plan.a_scale.astype(np.float32)
-    # ---- factor_stream_kernel
-    L = np.full((S, lanes), np.nan, dtype=np.float32)
-    F = np.full((nnz_l, lanes), np.nan, dtype=np.float32)
+    # ---- factor_stream_kernel (streams as flat float arrays; unit entries lane stride 4, D^-1 stride 1)
+    lane = np.arange(lanes)
+    BL, FL = sched["blen"], sched["flen"]
+    Lb = np.full(BL, np.nan, dtype=np.float32)
+    Fs = np.full(FL, np.nan, dtype=np.float32)
+
+    def uidx(off, total):
+        idx = off + 4 * lane
+        assert off >= 0 and idx[-1] < total
+        return idx
+
+    def didx(off):
+        idx = off + lane
+        assert off >= 0 and idx[-1] < BL
+        return idx
+
     max_row = sched["max_row_nnz"]
     for k in range(n):
         p0, p1 = rg["proc_ptr"][k], rg["proc_ptr"][k + 1]
@@ -51,26 +65,27 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         for e in range(p0, p1):
             c = rg["proc_cols"][e]
             off = rg["proc_offsets"][e]
-            base = sched["col_spos"][c]
+            base = sched["col_uoff"][c]
             u0 = sched["upd_ptr"][e]
             val = ys[e - p0].copy()
             for qq in range(off):
                 s = sched["upd_slot"][u0 + qq]
-                assert 0 <= s < p1 - p0 and 0 <= base + qq < S and not np.isnan(L[base + qq]).any()
-                ys[s] = ys[s] - L[base + qq] * val
-            dpos = sched["dinv_spos"][c]
-            assert not np.isnan(L[dpos]).any()
-            lval = val * L[dpos]
-            wpos = sched["proc_spos"][e]
-            assert 0 <= wpos < S
-            L[wpos] = lval
-            fpos = sched["proc_fpos"][e]
-            assert 0 <= fpos < nnz_l
-            F[fpos] = lval
+                lv = Lb[uidx(base + (qq >> 2) * 128 + (qq & 3), BL)]
+                assert 0 <= s < p1 - p0 and not np.isnan(lv).any()
+                ys[s] = ys[s] - lv * val
+            dv = Lb[didx(sched["dinv_off"][c])]
+            assert not np.isnan(dv).any()
+            lval = val * dv
+            Lb[uidx(sched["proc_boff"][e], BL)] = lval
+            Fs[uidx(sched["proc_foff"][e], FL)] = lval
             dk = dk - val * lval
-        L[sched["dinv_spos"][k]] = _f32(1.0) / dk
-    assert not np.isnan(L).any(), "stream positions not all written"
-    assert not np.isnan(F).any(), "forward stream positions not all written"
+        Lb[didx(sched["dinv_off"][k])] = _f32(1.0) / dk
+    for off in sched["pad_boff"]:
+        Lb[uidx(off, BL)] = 0.0
+    for off in sched["pad_foff"]:
+        Fs[uidx(off, FL)] = 0.0
+    assert not np.isnan(Lb).any(), "backward stream positions not all written"
+    assert not np.isnan(Fs).any(), "forward stream positions not all written"
     # ---- state_to_stream_kernel (scaled)
     e_s = plan.scaling_e.astype(np.float32)
     qs = pick(q) * plan.q_scale.astype(np.float32)
@@ -96,75 +111,99 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     oma = _f32(1.0) - alpha
     iters = plan.settings.max_iter if max_iter is None else max_iter
     nch = sched["n_chunks"]
-    X = np.full((n, lanes), np.nan, dtype=np.float32)
+    X = np.full((n + 1, lanes), np.nan, dtype=np.float32)  # row n: the zero row
+    X[n] = 0.0
     meta_all = sched["meta"]
-
-    def meta_of(ch):
-        off, words = sched["meta_off"][ch], sched["meta_words"][ch]
-        assert words <= sched["max_meta_words"] and off + words <= meta_all.size and words % 4 == 0
-        return meta_all[off : off + words]
-
-    nfc = sched["n_fchunks"]
     fmeta_all = sched["fmeta"]
+    nfc = sched["n_fchunks"]
+
+    def block(all_, offs, words, ch, maxw):
+        off, w = offs[ch], words[ch]
+        assert w <= maxw and w % 4 == 0 and off % 4 == 0 and off + w <= all_.size
+        return all_[off : off + w]
+
+    def xrow(byte_off):
+        assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= n
+        return byte_off // 128
+
+    def run_units(m, nu, stage, backward):
+        """The consumer's unit loop, with unit u+1's loads taken before unit u's store."""
+        assert 1 <= nu and KHDR + nu * KUW <= m.size
+        units = m[KHDR : KHDR + nu * KUW].reshape(nu, KUW)
+        nfl = stage.size
+
+        def load(u):
+            src, ctl = units[u, :4], units[u, 4:]
+            lo = u * 128
+            assert lo + 128 <= nfl
+            lv = stage[lo : lo + 128].reshape(lanes, 4).T.copy()  # [slot][lane]
+            xs = [X[xrow(o)].copy() for o in src]
+            t = X[xrow(ctl[0])].copy()
+            return ctl, lv, xs, t
+
+        cur = load(0)
+        acc = np.zeros(lanes, np.float32)
+        prev = np.zeros(lanes, np.float32)
+        for u in range(nu):
+            nxt = load(u + 1 if u + 1 < nu else u)
+            ctl, lv, xs, t = cur
+            fl = int(ctl[1])
+            if backward:
+                doff = int(ctl[2])
+                assert doff % 4 == 0 and doff // 4 + 32 <= nfl
+                dinv = stage[doff // 4 : doff // 4 + 32]
+                x0 = prev if fl & FWD else xs[0]
+                acc = np.zeros(lanes, np.float32) if fl & FIRST else acc
+                acc = acc + lv[0] * x0
+                acc = acc + lv[1] * xs[1]
+                acc = acc + lv[2] * xs[2]
+                acc = acc + lv[3] * xs[3]
+                res = t * dinv - acc
+            else:
+                x3 = prev if fl & FWD else xs[3]
+                acc = t if fl & FIRST else acc
+                acc = acc - lv[0] * xs[0]
+                acc = acc - lv[1] * xs[1]
+                acc = acc - lv[2] * xs[2]
+                acc = acc - lv[3] * x3
+                res = acc
+            if fl & LAST:
+                tr = xrow(ctl[0])
+                assert tr < n
+                X[tr] = res
+            prev = res
+            cur = nxt
+
     items = [(0, nch - 1 - t) for t in range(nch)]
     for _ in range(iters):
         items += [(1, c) for c in range(nfc)] + [(2, c) for c in range(nch - 1, -1, -1)]
     for kind, ch in items:
         if kind == 1:
-            off, words = sched["fmeta_off"][ch], sched["fmeta_words"][ch]
-            assert words <= sched["max_fmeta_words"] and words % 4 == 0 and off + words <= fmeta_all.size
-            fm = fmeta_all[off : off + words]
-            nrows, nent, r0 = int(fm[0]), int(fm[1]), int(fm[2])
-            assert nent <= sched["max_fent"] and nrows <= sched["max_frows"]
-            row_start = fm[4 : 4 + nrows + 1]
-            coloff = fm[4 + nrows + 1 : 4 + nrows + 1 + nent]
-            assert 4 + nrows + 1 + nent <= fm.size and np.all(coloff % 32 == 0)
-            pos0 = sched["fchunk_pos"][ch]
-            assert pos0 + nent <= nnz_l and sched["fchunk_pos"][ch + 1] - pos0 == nent
-            Fs = F[pos0 : pos0 + nent]
-            for i in range(nrows):
-                acc = X[r0 + i].copy()
-                for e in range(row_start[i], row_start[i + 1]):
-                    c = coloff[e] // 32
-                    assert 0 <= c < r0 + i
-                    acc = acc - Fs[e] * X[c]
-                X[r0 + i] = acc
+            fm = block(fmeta_all, sched["fmeta_off"], sched["fmeta_words"], ch, sched["max_fmeta_words"])
+            nu = int(fm[0])
+            assert nu == sched["fchunk_units"][ch] and nu <= sched["max_funits"]
+            o0, o1 = sched["fchunk_off"][ch], sched["fchunk_off"][ch + 1]
+            assert o1 - o0 == nu * 128 and o1 <= FL
+            run_units(fm, nu, Fs[o0:o1], backward=False)
             continue
-        m = meta_of(ch)
-        ncols, nent, nrel, c0, u0 = (int(v) for v in m[:KMETA])
-        assert ncols == sched["chunk_cols"][ch] and nent == sched["chunk_ent"][ch]
-        assert nent <= sched["max_ent"] and ncols <= sched["max_cols"] and nrel <= sched["max_rel"]
-        col_start = m[KMETA : KMETA + ncols + 1]
-        rows = m[KMETA + ncols + 1 : KMETA + ncols + 1 + nent]
-        assert np.all(rows % 32 == 0)
-        rows = rows // 32
-        rel_i = m[KMETA + ncols + 1 + nent : KMETA + ncols + 1 + nent + nrel]
-        rel_kind = m[KMETA + ncols + 1 + nent + nrel : KMETA + ncols + 1 + nent + 2 * nrel]
-        rel_rho = m[KMETA + ncols + 1 + nent + 2 * nrel : KMETA + ncols + 1 + nent + 3 * nrel].view(np.float32)
-        rel_rinv = m[KMETA + ncols + 1 + nent + 3 * nrel : KMETA + ncols + 1 + nent + 4 * nrel].view(np.float32)
-        assert KMETA + ncols + 1 + nent + 4 * nrel <= m.size
-        pos0 = sched["chunk_pos"][ch]
-        count = nent if kind == 1 else nent + ncols if kind == 2 else 0
-        assert pos0 + count <= S
-        Ls = L[pos0 : pos0 + count]
-        if kind == 1:
-            for j in range(ncols):
-                e0, e1 = col_start[j], col_start[j + 1]
-                val = X[c0 + j].copy()
-                for e in range(e0, e1):
-                    r = rows[e]
-                    assert 0 <= r < n
-                    X[r] = X[r] - Ls[e] * val
-        elif kind == 2:
-            assert 0 <= u0 and u0 + nrel <= n
-            for j in range(ncols - 1, -1, -1):
-                e0, e1 = col_start[j], col_start[j + 1]
-                corr = np.zeros(lanes, np.float32)
-                for e in range(e0, e1):
-                    corr = corr + Ls[e] * X[rows[e]]
-                X[c0 + j] = X[c0 + j] * Ls[nent + j] - corr
+        m = block(meta_all, sched["meta_off"], sched["meta_words"], ch, sched["max_meta_words"])
+        nu, ncols, nrel, c0, u0 = (int(v) for v in m[:5])
+        assert nu == sched["chunk_units"][ch] and ncols == sched["chunk_cols"][ch] and nrel == sched["chunk_nrel"][ch]
+        assert u0 == sched["chunk_u0"][ch] and nu <= sched["max_units"] and ncols <= sched["max_cols"]
+        assert nrel <= sched["max_rel"] and 0 <= u0 and u0 + nrel <= n
+        r = KHDR + nu * KUW
+        assert r + 4 * nrel <= m.size
+        rel_i = m[r : r + nrel]
+        rel_kind = m[r + nrel : r + 2 * nrel]
+        rel_rho = m[r + 2 * nrel : r + 3 * nrel].view(np.float32)
+        rel_rinv = m[r + 3 * nrel : r + 4 * nrel].view(np.float32)
+        if kind == 2:
+            o0, o1 = sched["chunk_off"][ch], sched["chunk_off"][ch + 1]
+            assert o1 - o0 == nu * 128 + ncols * 32 and o1 <= BL
+            run_units(m, nu, Lb[o0:o1], backward=True)
             for k in range(nrel):
-                i = rel_i[k]
+                i = xrow(rel_i[k])
+                assert i < n
                 uu = u0 + k
                 sol = X[i].copy()
                 if rel_kind[k] == 0:
@@ -185,9 +224,11 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                     X[i] = zn - rinv * yn
         else:
             for k in range(nrel):
-                i = rel_i[k]
+                i = xrow(rel_i[k])
+                assert i < n
                 uu = u0 + k
                 X[i] = sigma * s0[uu] - pp0[uu] if rel_kind[k] == 0 else s0[uu] - rel_rinv[k] * s1[uu]
+        assert X[n].max() == 0.0 and X[n].min() == 0.0
     # ---- stream_to_state_kernel + unscale
     x = np.zeros((lanes, plan.n), np.float32)
     z = np.zeros((lanes, plan.m), np.float32)

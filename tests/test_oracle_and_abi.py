@@ -88,6 +88,11 @@ def test_stream_schedule_replay_bitexact(cls):
     for g, r in zip(got, ref[:3]):
         np.testing.assert_array_equal(g, r)
     # chunk invariants the kernel relies on
-    assert sched["chunk_pos"][-1] == sched["stream_len"] == plan.qdldl_plan.nnz_l + plan.qdldl_plan.n
-    assert sched["fchunk_pos"][-1] == plan.qdldl_plan.nnz_l
+    q = plan.qdldl_plan
+    assert sched["chunk_off"][-1] == sched["blen"] == 128 * sched["chunk_units"].sum() + 32 * q.n
+    assert sched["fchunk_off"][-1] == sched["flen"] == 128 * sched["fchunk_units"].sum()
+    # every L entry once in each stream, every other slot padding
+    assert 4 * sched["chunk_units"].sum() == q.nnz_l + sched["pad_boff"].size
+    assert 4 * sched["fchunk_units"].sum() == q.nnz_l + sched["pad_foff"].size
+    assert np.unique(sched["proc_boff"]).size == q.nnz_l and np.unique(sched["proc_foff"]).size == q.nnz_l
     assert sorted(sched["u_perm"].tolist()) == list(range(plan.qdldl_plan.n))

@@ -190,11 +190,11 @@ int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* to
 int64_t wmpc_launch_count(void) { return g_launches.load(); }
 
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv, int32_t n_primal,
-                              int32_t ent, int32_t cols, int32_t rel, int32_t* out, int64_t out_capacity,
-                              int64_t* out_words) {
+                              int32_t units, int32_t cols, int32_t rel, int32_t funits, int32_t* out,
+                              int64_t out_capacity, int64_t* out_words) {
   if (!desc || !out_words) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
   const int n = desc->n, nnz_l = desc->nnz_l;
-  if (n <= 0 || nnz_l < 0 || n_primal < 0 || n_primal > n || ent <= 0 || cols <= 0 || rel <= 0)
+  if (n <= 0 || nnz_l < 0 || n_primal < 0 || n_primal > n || units <= 0 || cols <= 0 || rel <= 0 || funits <= 0)
     return fail(WMPC_ERR_INVALID_ARGUMENT, "bad sizes");
   HostPattern hp;
   hp.n = n;
@@ -216,22 +216,27 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   int max_row = 0;
   HostStream hs;
   StreamTargets t;
-  t.ent = ent;
+  t.units = units;
   t.cols = cols;
   t.rel = rel;
+  t.funits = funits;
   if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
       !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
     return fail(WMPC_ERR_UNSUPPORTED, "%s", why.c_str());
-  std::vector<int> w{hs.n_chunks, hs.stream_len, hs.max_ent, hs.max_cols, hs.max_rel, hs.max_meta_words, max_row,
+  std::vector<int> w{hs.n_chunks, hs.blen, hs.max_units, hs.max_cols, hs.max_rel, hs.max_meta_words, max_row,
                      static_cast<int>(hs.meta.size())};
   auto app = [&](const std::vector<int>& v) { w.insert(w.end(), v.begin(), v.end()); };
-  app(hs.chunk_pos); app(hs.chunk_ent); app(hs.chunk_cols); app(hs.meta_off); app(hs.meta_words); app(hs.meta);
-  app(hs.col_spos); app(hs.dinv_spos); app(hs.proc_spos); app(hs.u_perm); app(hs.u_orig);
+  app(hs.chunk_off); app(hs.chunk_units); app(hs.chunk_cols); app(hs.chunk_u0); app(hs.chunk_nrel);
+  app(hs.meta_off); app(hs.meta_words); app(hs.meta);
+  app(hs.col_uoff); app(hs.dinv_off); app(hs.proc_boff); app(hs.u_perm); app(hs.u_orig);
   app(init_slot); app(upd_ptr);
   for (unsigned short v : upd_slot) w.push_back(v);
-  w.push_back(hs.n_fchunks); w.push_back(hs.max_fent); w.push_back(hs.max_frows); w.push_back(hs.max_fmeta_words);
+  w.push_back(hs.n_fchunks); w.push_back(hs.flen); w.push_back(hs.max_funits); w.push_back(hs.max_fmeta_words);
   w.push_back(static_cast<int>(hs.fmeta.size()));
-  app(hs.fchunk_pos); app(hs.fmeta_off); app(hs.fmeta_words); app(hs.fmeta); app(hs.proc_fpos);
+  app(hs.fchunk_off); app(hs.fchunk_units); app(hs.fmeta_off); app(hs.fmeta_words); app(hs.fmeta); app(hs.proc_foff);
+  w.push_back(static_cast<int>(hs.pad_boff.size())); w.push_back(static_cast<int>(hs.pad_foff.size()));
+  w.push_back(hs.dummy_units);
+  app(hs.pad_boff); app(hs.pad_foff);
   *out_words = static_cast<int64_t>(w.size());
   if (!out) return WMPC_OK;
   if (out_capacity < static_cast<int64_t>(w.size())) return fail(WMPC_ERR_INVALID_ARGUMENT, "output buffer too small");
@@ -514,13 +519,11 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     std::vector<unsigned short> upd_slot16;
     int max_row = 0;
     StreamTargets targets;
-    if (const char* v = getenv("WMPC_STREAM_ENT")) targets.ent = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_UNITS")) targets.units = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_COLS")) targets.cols = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_REL")) targets.rel = atoi(v);
-    if (const char* v = getenv("WMPC_STREAM_FENT")) targets.fent = atoi(v);
-    if (const char* v = getenv("WMPC_STREAM_FROWS")) targets.frows = atoi(v);
-    if (targets.ent <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.fent <= 0 || targets.frows <= 0)
-      targets = StreamTargets();
+    if (const char* v = getenv("WMPC_STREAM_FUNITS")) targets.funits = atoi(v);
+    if (targets.units <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.funits <= 0) targets = StreamTargets();
     bool ok = build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, &q->stream_why) &&
               build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why);
     StreamPlan& sp = q->sp;
@@ -528,16 +531,18 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sp.n = hp.n;
       sp.nnz_l = hp.nnz_l;
       sp.n_chunks = hs.n_chunks;
-      sp.stream_len = hs.stream_len;
-      sp.max_ent = hs.max_ent;
+      sp.blen = hs.blen;
+      sp.max_units = hs.max_units;
       sp.max_cols = hs.max_cols;
       sp.max_rel = hs.max_rel;
       sp.max_meta_words = hs.max_meta_words;
       sp.max_row_nnz = max_row;
       sp.n_fchunks = hs.n_fchunks;
-      sp.max_fent = hs.max_fent;
-      sp.max_frows = hs.max_frows;
+      sp.flen = hs.flen;
+      sp.max_funits = hs.max_funits;
       sp.max_fmeta_words = hs.max_fmeta_words;
+      sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
+      sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
       StreamLaunch cfg;
       if (!stream_launch_config(sp, &cfg)) {
         ok = false;
@@ -547,25 +552,30 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (ok) {
       std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
       Packer sk;
-      sk.add(hs.chunk_pos.data(), hs.chunk_pos.size(), &sp.chunk_pos);
-      sk.add(hs.chunk_ent.data(), hs.chunk_ent.size(), &sp.chunk_ent);
+      sk.add(hs.chunk_off.data(), hs.chunk_off.size(), &sp.chunk_off);
+      sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
       sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
+      sk.add(hs.chunk_u0.data(), hs.chunk_u0.size(), &sp.chunk_u0);
+      sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
       sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
       sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
       sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);
       sk.add(init_slot.data(), init_slot.size(), &sp.init_slot);
       sk.add(upd_ptr.data(), upd_ptr.size(), &sp.upd_ptr);
       sk.add(upd_slot.data(), upd_slot.size(), &sp.upd_slot);
-      sk.add(hs.col_spos.data(), hs.col_spos.size(), &sp.col_spos);
-      sk.add(hs.dinv_spos.data(), hs.dinv_spos.size(), &sp.dinv_spos);
-      sk.add(hs.proc_spos.data(), hs.proc_spos.size(), &sp.proc_spos);
+      sk.add(hs.col_uoff.data(), hs.col_uoff.size(), &sp.col_uoff);
+      sk.add(hs.dinv_off.data(), hs.dinv_off.size(), &sp.dinv_off);
+      sk.add(hs.proc_boff.data(), hs.proc_boff.size(), &sp.proc_boff);
+      sk.add(hs.proc_foff.data(), hs.proc_foff.size(), &sp.proc_foff);
+      sk.add(hs.pad_boff.data(), hs.pad_boff.size(), &sp.pad_boff);
+      sk.add(hs.pad_foff.data(), hs.pad_foff.size(), &sp.pad_foff);
       sk.add(hs.u_perm.data(), hs.u_perm.size(), &sp.u_perm);
       sk.add(hs.u_orig.data(), hs.u_orig.size(), &sp.u_orig);
-      sk.add(hs.fchunk_pos.data(), hs.fchunk_pos.size(), &sp.fchunk_pos);
+      sk.add(hs.fchunk_off.data(), hs.fchunk_off.size(), &sp.fchunk_off);
+      sk.add(hs.fchunk_units.data(), hs.fchunk_units.size(), &sp.fchunk_units);
       sk.add(hs.fmeta_off.data(), hs.fmeta_off.size(), &sp.fmeta_off);
       sk.add(hs.fmeta_words.data(), hs.fmeta_words.size(), &sp.fmeta_words);
       sk.add(hs.fmeta.data(), hs.fmeta.size(), &sp.fmeta);
-      sk.add(hs.proc_fpos.data(), hs.proc_fpos.size(), &sp.proc_fpos);
       int* sblock = nullptr;
       if (sk.upload(&sblock) == WMPC_OK) {
         q->stream_block = sblock;

@@ -2,16 +2,19 @@
 //
 // factor_stream_kernel: KKT assembly + LDL^T factorization, one lane per
 //   instance, compact accumulator (one shared-memory slot per etree-reach
-//   position instead of a dense work vector), L and D^-1 written in the
-//   stream-major tile layout (see stream.cuh).
+//   position instead of a dense work vector), L and D^-1 written into both
+//   sweep streams (unit layout, see stream.cuh); flags zero pivots.
 // admm_stream_kernel: one CTA per SM walks instance tiles; a producer warp
 //   streams every chunk of the factor into a shared-memory ring with
 //   cp.async.bulk (mbarrier completion), a consumer warp runs, per ADMM
-//   iteration, the forward sweep (L, column order), the backward sweep
-//   (D^-1 and L^T, reverse column order) and, as soon as the backward sweep
-//   is done with a KKT index, its ADMM update, writing the next iteration's
-//   right-hand side in place.  The work vector (KKT dimension x 32 lanes)
-//   stays in shared memory for all iterations of a tile.
+//   iteration, the forward sweep (row-gather), the backward sweep (D^-1 and
+//   L^T, column form, reverse order) and, as soon as the backward sweep is
+//   done with a KKT index, its ADMM update, writing the next iteration's
+//   right-hand side in place.  The sweeps walk 4-entry units with the next
+//   unit's loads issued before the current unit's arithmetic (registers
+//   forward the one value that may still be in flight).  The work vector
+//   (KKT dimension + 1 zero row, x 32 lanes) stays in shared memory for all
+//   iterations of a tile.
 //
 // Arithmetic is the reference's operation order (warp_backend.py:41-101,
 // 176-218; solver.py:806-820) with separately rounded products and sums.
@@ -40,8 +43,8 @@ __device__ __forceinline__ float kkt_value_at(const Osqp& o, const OsqpInputs& i
 // ---------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(128) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
-                                                            float* __restrict__ lstream, float* __restrict__ fstream,
-                                                            int n_tiles, int batch) {
+                                                            float* __restrict__ bstream, float* __restrict__ fstream,
+                                                            int* __restrict__ status, int n_tiles, int batch) {
   extern __shared__ float ys_all[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -50,9 +53,12 @@ __global__ void __launch_bounds__(128) factor_stream_kernel(Pattern pat, StreamP
   const int b = tile * 32 + lane;
   const int bb = b < batch ? b : batch - 1;  // padding lanes factor a copy of the last instance
   float* ys = ys_all + (size_t)warp * sp.max_row_nnz * 32 + lane;
-  float* L = lstream + (size_t)tile * sp.stream_len * 32 + lane;
-  float* F = fstream + (size_t)tile * sp.nnz_l * 32 + lane;
+  float* Lb = bstream + (size_t)tile * sp.blen;
+  float* F = fstream + (size_t)tile * sp.flen + lane * 4;
+  float* Lu = Lb + lane * 4;  // unit entries: lane stride 4
+  float* Ld = Lb + lane;      // D^-1 rows: lane stride 1
   const int n = pat.n;
+  bool bad = false;
   for (int k = 0; k < n; ++k) {
     const int p0 = __ldg(pat.proc_ptr + k), p1 = __ldg(pat.proc_ptr + k + 1);
     for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
@@ -65,20 +71,25 @@ __global__ void __launch_bounds__(128) factor_stream_kernel(Pattern pat, StreamP
     for (int e = p0; e < p1; ++e) {
       const int c = __ldg(pat.proc_cols + e);
       const int off = __ldg(pat.proc_offsets + e);
-      const int base = __ldg(sp.col_spos + c);
+      const float* col = Lu + __ldg(sp.col_uoff + c);
       const int u0 = __ldg(sp.upd_ptr + e);
       const float val = ys[(e - p0) * 32];
       for (int q = 0; q < off; ++q) {
         const int s = __ldg(sp.upd_slot + u0 + q);
-        ys[s * 32] = ys[s * 32] - L[(size_t)(base + q) * 32] * val;
+        ys[s * 32] = ys[s * 32] - col[(q >> 2) * 128 + (q & 3)] * val;
       }
-      const float lval = val * L[(size_t)__ldg(sp.dinv_spos + c) * 32];
-      L[(size_t)__ldg(sp.proc_spos + e) * 32] = lval;
-      F[(size_t)__ldg(sp.proc_fpos + e) * 32] = lval;
+      const float lval = val * Ld[__ldg(sp.dinv_off + c)];
+      Lu[__ldg(sp.proc_boff + e)] = lval;
+      F[__ldg(sp.proc_foff + e)] = lval;
       dk = dk - val * lval;
     }
-    L[(size_t)__ldg(sp.dinv_spos + k) * 32] = 1.0f / dk;
+    const float di = 1.0f / dk;
+    bad |= !(di != 0.0f) || !isfinite(di);
+    Ld[__ldg(sp.dinv_off + k)] = di;
   }
+  for (int i = 0; i < sp.n_pad_b; ++i) Lu[__ldg(sp.pad_boff + i)] = 0.0f;
+  for (int i = 0; i < sp.n_pad_f; ++i) F[__ldg(sp.pad_foff + i)] = 0.0f;
+  if (status) status[b] = bad ? WMPC_STATUS_ZERO_PIVOT : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -137,13 +148,12 @@ __global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float*
 
 struct StreamArgs {
   StreamPlan sp;
-  const float* lstream;
+  const float* bstream;
   const float* fstream;
   float* s0;
   float* s1;
   const float* p0;
   const float* p1;
-  int* status;  // [n_tiles * 32] (ZERO_PIVOT bit), may be null
   int* error;   // one word: 0 ok, 1 pipeline timeout
   int n_tiles, max_iter;
   float sigma, alpha, one_minus_alpha;
@@ -184,29 +194,30 @@ __device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_it
   return true;
 }
 
-// per-chunk producer table kept in shared memory (8 ints per chunk)
-struct ChunkInfo {
-  int pos, ent, cols, meta_off, meta_words, u0, nrel, pad;
-};
-
-// Shared-memory layout: X [n][32] | chunk table | L ring | S ring | barriers
-struct StreamSmem {
-  float* X;
-  const ChunkInfo* info;
-  unsigned char* lring;
-  unsigned char* sring;
-  uint64_t* lfull;
-  uint64_t* lempty;
-  uint64_t* sfull;
-  uint64_t* sempty;
-  volatile int* abort_flag;
-  volatile int* consumed_ctr;
-};
-
-__host__ __device__ inline size_t stream_smem_bytes(int n, int n_info, int lstages, int sstages, int lstage_bytes,
+// Shared-memory layout: X [n + 1][32] | L ring | S ring | barriers | flags
+__host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
-  return (size_t)n * 128 + (size_t)n_info * sizeof(int) * 8 + (size_t)lstages * lstage_bytes +
-         (size_t)sstages * sstage_bytes + 16 * (size_t)(lstages + sstages) + 16;
+  return (size_t)(n + 1) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
+         16 * (size_t)(lstages + sstages) + 16;
+}
+
+// One unit's operands, loaded ahead of its arithmetic.
+struct UnitOps {
+  int4 src, ctl;  // ctl: target byte offset, flags, D^-1 byte offset, 0
+  float4 l;
+  float x0, x1, x2, x3, t;
+};
+
+__device__ __forceinline__ void load_unit(const int4* __restrict__ mu, const unsigned char* lst, const unsigned char* xb,
+                                          int u, int lane, UnitOps& r) {
+  r.src = mu[2 * u];
+  r.ctl = mu[2 * u + 1];
+  r.l = *reinterpret_cast<const float4*>(lst + u * 512 + lane * 16);
+  r.x0 = *reinterpret_cast<const float*>(xb + r.src.x);
+  r.x1 = *reinterpret_cast<const float*>(xb + r.src.y);
+  r.x2 = *reinterpret_cast<const float*>(xb + r.src.z);
+  r.x3 = *reinterpret_cast<const float*>(xb + r.src.w);
+  r.t = *reinterpret_cast<const float*>(xb + r.ctl.x);
 }
 
 __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
@@ -214,58 +225,30 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
   const StreamPlan& sp = a.sp;
   const int n = sp.n;
   const int lstage_bytes = a.meta_bytes + a.lbytes;
-  StreamSmem sm;
-  sm.X = reinterpret_cast<float*>(smem);
-  ChunkInfo* info = reinterpret_cast<ChunkInfo*>(smem + (size_t)n * 128);
-  ChunkInfo* finfo = info + sp.n_chunks;
-  sm.info = info;
-  sm.lring = reinterpret_cast<unsigned char*>(finfo + sp.n_fchunks);
-  sm.sring = sm.lring + (size_t)a.lstages * lstage_bytes;
-  sm.lfull = reinterpret_cast<uint64_t*>(sm.sring + (size_t)a.sstages * a.sbytes);
-  sm.lempty = sm.lfull + a.lstages;
-  sm.sfull = sm.lempty + a.lstages;
-  sm.sempty = sm.sfull + a.sstages;
-  sm.abort_flag = reinterpret_cast<volatile int*>(sm.sempty + a.sstages);
-  sm.consumed_ctr = sm.abort_flag + 1;
+  float* X = reinterpret_cast<float*>(smem);
+  unsigned char* lring = smem + (size_t)(n + 1) * 128;
+  unsigned char* sring = lring + (size_t)a.lstages * lstage_bytes;
+  uint64_t* lfull = reinterpret_cast<uint64_t*>(sring + (size_t)a.sstages * a.sbytes);
+  uint64_t* lempty = lfull + a.lstages;
+  uint64_t* sfull = lempty + a.lstages;
+  uint64_t* sempty = sfull + a.sstages;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sempty + a.sstages);
+  volatile int* consumed_ctr = abort_flag + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = threadIdx.x; c < sp.n_chunks; c += blockDim.x) {
-    const int mw = __ldg(sp.meta_words + c), mo = __ldg(sp.meta_off + c);
-    ChunkInfo ci;
-    ci.pos = __ldg(sp.chunk_pos + c);
-    ci.ent = __ldg(sp.chunk_ent + c);
-    ci.cols = __ldg(sp.chunk_cols + c);
-    ci.meta_off = mo;
-    ci.meta_words = mw;
-    ci.u0 = __ldg(sp.meta + mo + 4);
-    ci.nrel = __ldg(sp.meta + mo + 2);
-    ci.pad = 0;
-    info[c] = ci;
-  }
-  for (int c = threadIdx.x; c < sp.n_fchunks; c += blockDim.x) {
-    ChunkInfo ci;
-    ci.pos = __ldg(sp.fchunk_pos + c);
-    ci.ent = __ldg(sp.fchunk_pos + c + 1) - ci.pos;
-    ci.cols = 0;
-    ci.meta_off = __ldg(sp.fmeta_off + c);
-    ci.meta_words = __ldg(sp.fmeta_words + c);
-    ci.u0 = 0;
-    ci.nrel = 0;
-    ci.pad = 0;
-    finfo[c] = ci;
-  }
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
-      mbar_init(sm.lfull + s, 1);
-      mbar_init(sm.lempty + s, 1);
+      mbar_init(lfull + s, 1);
+      mbar_init(lempty + s, 1);
     }
     for (int s = 0; s < a.sstages; ++s) {
-      mbar_init(sm.sfull + s, 1);
-      mbar_init(sm.sempty + s, 1);
+      mbar_init(sfull + s, 1);
+      mbar_init(sempty + s, 1);
     }
-    *sm.abort_flag = 0;
-    *sm.consumed_ctr = 0;
+    *abort_flag = 0;
+    *consumed_ctr = 0;
     fence_mbarrier_init();
   }
+  if (warp == 0) X[n * 32 + lane] = 0.0f;  // zero row read by padding slots
   __syncthreads();
 
   uint32_t issued_l = 0, issued_s = 0;
@@ -275,39 +258,40 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
     if (lane == 0) {
       Ring lr{0, 0}, sr{0, 0};
       uint32_t nl = 0, ns = 0;  // fills issued so far (ring reuse starts after one full lap)
-      for (int tile = blockIdx.x; tile < a.n_tiles && !*sm.abort_flag; tile += gridDim.x) {
-        const float* lt = a.lstream + (size_t)tile * sp.stream_len * 32;
-        const float* ft = a.fstream + (size_t)tile * sp.nnz_l * 32;
+      for (int tile = blockIdx.x; tile < a.n_tiles && !*abort_flag; tile += gridDim.x) {
+        const float* bt = a.bstream + (size_t)tile * sp.blen;
+        const float* ft = a.fstream + (size_t)tile * sp.flen;
         const size_t soff = (size_t)tile * n * 32;
         auto produce = [&](int kind, int ch) -> bool {
-          const ChunkInfo ci = kind == kItemFwd ? finfo[ch] : info[ch];
-          const int* meta_src = kind == kItemFwd ? sp.fmeta : sp.meta;
-          const float* lsrc = kind == kItemFwd ? ft : lt;
-          if (nl >= (uint32_t)a.lstages && !mbar_wait_bounded(sm.lempty + lr.stage, lr.phase ^ 1u, sm.abort_flag, kWaitLimitNs))
+          const bool fwd = kind == kItemFwd;
+          const int moff = __ldg((fwd ? sp.fmeta_off : sp.meta_off) + ch);
+          const int mwords = __ldg((fwd ? sp.fmeta_words : sp.meta_words) + ch);
+          const int loff = __ldg((fwd ? sp.fchunk_off : sp.chunk_off) + ch);
+          uint32_t lbytes = 0;
+          if (fwd) lbytes = (uint32_t)__ldg(sp.fchunk_units + ch) * 512u;
+          if (kind == kItemBwd) lbytes = (uint32_t)__ldg(sp.chunk_units + ch) * 512u + (uint32_t)__ldg(sp.chunk_cols + ch) * 128u;
+          if (nl >= (uint32_t)a.lstages && !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
             return false;
-          uint32_t lcount = 0;
-          if (kind == kItemFwd) lcount = ci.ent;
-          if (kind == kItemBwd) lcount = ci.ent + ci.cols;
-          unsigned char* st = sm.lring + (size_t)lr.stage * lstage_bytes;
-          mbar_arrive_expect_tx(sm.lfull + lr.stage, (uint32_t)ci.meta_words * 4u + lcount * 128u);
-          bulk_g2s(st, meta_src + ci.meta_off, (uint32_t)ci.meta_words * 4u, sm.lfull + lr.stage);
-          if (lcount) bulk_g2s(st + a.meta_bytes, lsrc + (size_t)ci.pos * 32, lcount * 128u, sm.lfull + lr.stage);
+          unsigned char* st = lring + (size_t)lr.stage * lstage_bytes;
+          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes);
+          bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + moff, (uint32_t)mwords * 4u, lfull + lr.stage);
+          if (lbytes) bulk_g2s(st + a.meta_bytes, (fwd ? ft : bt) + loff, lbytes, lfull + lr.stage);
           lr.advance(a.lstages);
           ++nl;
           ++issued_l;
-          if (kind != kItemFwd) {
-            if (ns >= (uint32_t)a.sstages && !mbar_wait_bounded(sm.sempty + sr.stage, sr.phase ^ 1u, sm.abort_flag, kWaitLimitNs))
+          if (!fwd) {
+            if (ns >= (uint32_t)a.sstages && !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
-            unsigned char* ss = sm.sring + (size_t)sr.stage * a.sbytes;
-            const uint32_t bytes = (uint32_t)ci.nrel * 128u;
+            unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
+            const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 128u;
             const int quarter = a.sbytes / 4;
-            mbar_arrive_expect_tx(sm.sfull + sr.stage, 4u * bytes);
+            mbar_arrive_expect_tx(sfull + sr.stage, 4u * bytes);
             if (bytes) {
-              const size_t off = soff + (size_t)ci.u0 * 32;
-              bulk_g2s(ss, a.s0 + off, bytes, sm.sfull + sr.stage);
-              bulk_g2s(ss + quarter, a.s1 + off, bytes, sm.sfull + sr.stage);
-              bulk_g2s(ss + 2 * quarter, a.p0 + off, bytes, sm.sfull + sr.stage);
-              bulk_g2s(ss + 3 * quarter, a.p1 + off, bytes, sm.sfull + sr.stage);
+              const size_t off = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
+              bulk_g2s(ss, a.s0 + off, bytes, sfull + sr.stage);
+              bulk_g2s(ss + quarter, a.s1 + off, bytes, sfull + sr.stage);
+              bulk_g2s(ss + 2 * quarter, a.p0 + off, bytes, sfull + sr.stage);
+              bulk_g2s(ss + 3 * quarter, a.p1 + off, bytes, sfull + sr.stage);
             }
             sr.advance(a.sstages);
             ++ns;
@@ -316,7 +300,7 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
           return true;
         };
         if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, produce)) {
-          *sm.abort_flag = 1;
+          *abort_flag = 1;
           break;
         }
       }
@@ -326,128 +310,83 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
     Ring lr{0, 0}, sr{0, 0};
     uint32_t consumed = 0;
     const float sigma = a.sigma, alpha = a.alpha, oma = a.one_minus_alpha;
-    float* xl = sm.X + lane;
+    const unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
     bool ok = true;
     const int quarter_f = a.sbytes / 16;  // floats per S array
     for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
       float* s0t = a.s0 + (size_t)tile * n * 32 + lane;
       float* s1t = a.s1 + (size_t)tile * n * 32 + lane;
-      int status = 0;
       auto consume = [&](int kind, int ch) -> bool {
         (void)ch;
-        if (!mbar_wait_bounded(sm.lfull + lr.stage, lr.phase, sm.abort_flag, kWaitLimitNs)) return false;
-        const int* meta = reinterpret_cast<const int*>(sm.lring + (size_t)lr.stage * lstage_bytes);
-        const float* Ls = reinterpret_cast<const float*>(sm.lring + (size_t)lr.stage * lstage_bytes + a.meta_bytes) + lane;
-        const int ncols = meta[0], nent = meta[1], nrel = meta[2], c0 = meta[3], u0 = meta[4];
-        const int* col_start = meta + kMetaHeader;
-        const int* rows = col_start + ncols + 1;
-        const int* rel_i = rows + nent;
-        const int* rel_kind = rel_i + nrel;
-        const float* rel_rho = reinterpret_cast<const float*>(rel_kind + nrel);
-        const float* rel_rinv = rel_rho + nrel;
+        if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) return false;
+        const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
+        const int* meta = reinterpret_cast<const int*>(stage);
+        const unsigned char* lst = stage + a.meta_bytes;
+        const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
+        const int nu = meta[0];
         if (kind == kItemFwd) {
-          // forward substitution in row-gather form: row i accumulates its
-          // columns in ascending order (the reference's order for that row);
-          // only a row's last entry can be the previous row, whose value is
-          // forwarded in a register.
-          const int nrows = meta[0], r0 = meta[2];
-          const int* row_start = meta + kFMetaHeader;
-          const int* coloff = row_start + nrows + 1;
-          int prev_off = -1;
-          float prevv = 0.0f;
-          for (int i = 0; i < nrows; ++i) {
-            const int e0 = row_start[i], e1 = row_start[i + 1];
-            const int roff = (r0 + i) * 32;
-            float acc = xl[roff];
-            if (e0 < e1) {
-              const int el = e1 - 1;
-              int e = e0;
-              for (; e + 4 <= el; e += 4) {
-                const int o0 = coloff[e], o1 = coloff[e + 1], o2 = coloff[e + 2], o3 = coloff[e + 3];
-                const float l0 = Ls[e * 32], l1 = Ls[(e + 1) * 32], l2 = Ls[(e + 2) * 32], l3 = Ls[(e + 3) * 32];
-                const float x0 = xl[o0], x1 = xl[o1], x2 = xl[o2], x3 = xl[o3];
-                acc = acc - l0 * x0;
-                acc = acc - l1 * x1;
-                acc = acc - l2 * x2;
-                acc = acc - l3 * x3;
-              }
-              if (e + 2 <= el) {
-                const int o0 = coloff[e], o1 = coloff[e + 1];
-                const float l0 = Ls[e * 32], l1 = Ls[(e + 1) * 32];
-                const float x0 = xl[o0], x1 = xl[o1];
-                acc = acc - l0 * x0;
-                acc = acc - l1 * x1;
-                e += 2;
-              }
-              if (e < el) {
-                acc = acc - Ls[e * 32] * xl[coloff[e]];
-                ++e;
-              }
-              const int cl = coloff[el];
-              acc = acc - Ls[el * 32] * (cl == prev_off ? prevv : xl[cl]);
-              xl[roff] = acc;
-            }
-            prev_off = roff;
-            prevv = acc;
+          // forward substitution, row-gather form: a row's sum starts from
+          // its right-hand side and subtracts L_ij x_j by ascending j
+          UnitOps cur, nxt;
+          load_unit(mu, lst, xb, 0, lane, cur);
+          float acc = 0.0f, prev = 0.0f;
+          for (int u = 0; u < nu; ++u) {
+            load_unit(mu, lst, xb, u + 1 < nu ? u + 1 : u, lane, nxt);
+            const int fl = cur.ctl.y;
+            const float x3 = (fl & kUnitFwd) ? prev : cur.x3;
+            acc = (fl & kUnitFirst) ? cur.t : acc;
+            acc = acc - cur.l.x * cur.x0;
+            acc = acc - cur.l.y * cur.x1;
+            acc = acc - cur.l.z * cur.x2;
+            acc = acc - cur.l.w * x3;
+            if (fl & kUnitLast) *reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + cur.ctl.x) = acc;
+            prev = acc;
+            cur = nxt;
           }
         } else {
+          const int nrel = meta[2], u0 = meta[4];
           if (kind == kItemBwd) {
-            // backward substitution, reverse column order; a column's first
-            // entry may read the column just finished (forwarded)
-            int prev_off = -1;
-            float prevv = 0.0f;
-            for (int j = ncols - 1; j >= 0; --j) {
-              const int e0 = col_start[j], e1 = col_start[j + 1];
-              const int coff = (c0 + j) * 32;
-              const float xself = xl[coff];
-              const float dinv = Ls[(nent + j) * 32];
-              float corr = 0.0f;
-              if (e0 < e1) {
-                const int r0 = rows[e0];
-                corr = corr + Ls[e0 * 32] * (r0 == prev_off ? prevv : xl[r0]);
-                int e = e0 + 1;
-                for (; e + 4 <= e1; e += 4) {
-                  const int o0 = rows[e], o1 = rows[e + 1], o2 = rows[e + 2], o3 = rows[e + 3];
-                  const float l0 = Ls[e * 32], l1 = Ls[(e + 1) * 32], l2 = Ls[(e + 2) * 32], l3 = Ls[(e + 3) * 32];
-                  const float x0 = xl[o0], x1 = xl[o1], x2 = xl[o2], x3 = xl[o3];
-                  corr = corr + l0 * x0;
-                  corr = corr + l1 * x1;
-                  corr = corr + l2 * x2;
-                  corr = corr + l3 * x3;
-                }
-                if (e + 2 <= e1) {
-                  const int o0 = rows[e], o1 = rows[e + 1];
-                  const float l0 = Ls[e * 32], l1 = Ls[(e + 1) * 32];
-                  const float x0 = xl[o0], x1 = xl[o1];
-                  corr = corr + l0 * x0;
-                  corr = corr + l1 * x1;
-                  e += 2;
-                }
-                if (e < e1) corr = corr + Ls[e * 32] * xl[rows[e]];
-              }
-              if (!(dinv != 0.0f) || !isfinite(dinv)) status |= WMPC_STATUS_ZERO_PIVOT;
-              const float res = xself * dinv - corr;
-              xl[coff] = res;
-              prev_off = coff;
-              prevv = res;
+            // backward substitution, column form: x_j = x_j D^-1_j - sum_i L_ij x_i
+            // (the sum by ascending i), columns in reverse order
+            UnitOps cur, nxt;
+            load_unit(mu, lst, xb, 0, lane, cur);
+            float corr = 0.0f, prev = 0.0f;
+            for (int u = 0; u < nu; ++u) {
+              load_unit(mu, lst, xb, u + 1 < nu ? u + 1 : u, lane, nxt);
+              const float dinv = *reinterpret_cast<const float*>(lst + cur.ctl.z + lane * 4);
+              const int fl = cur.ctl.y;
+              const float x0 = (fl & kUnitFwd) ? prev : cur.x0;
+              corr = (fl & kUnitFirst) ? 0.0f : corr;
+              corr = corr + cur.l.x * x0;
+              corr = corr + cur.l.y * cur.x1;
+              corr = corr + cur.l.z * cur.x2;
+              corr = corr + cur.l.w * cur.x3;
+              const float res = cur.t * dinv - corr;
+              if (fl & kUnitLast) *reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + cur.ctl.x) = res;
+              prev = res;
+              cur = nxt;
             }
           }
           // releases: ADMM update (backward items) or first right-hand side
-          if (!mbar_wait_bounded(sm.sfull + sr.stage, sr.phase, sm.abort_flag, kWaitLimitNs)) return false;
-          const float* S = reinterpret_cast<const float*>(sm.sring + (size_t)sr.stage * a.sbytes) + lane;
+          const int* rel_off = meta + kChunkHeader + nu * kUnitWords;
+          const int* rel_kind = rel_off + nrel;
+          const float* rel_rho = reinterpret_cast<const float*>(rel_kind + nrel);
+          const float* rel_rinv = rel_rho + nrel;
+          if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
+          const float* S = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           for (int k = 0; k < nrel; ++k) {
-            const int ioff = rel_i[k] * 32;
+            float* xi = reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + rel_off[k]);
             const float sv0 = S[k * 32], pv0 = S[2 * quarter_f + k * 32];
             const size_t u = (size_t)(u0 + k) * 32;
             if (kind == kItemRel) {
-              xl[ioff] = rel_kind[k] == 0 ? sigma * sv0 - pv0 : sv0 - rel_rinv[k] * S[quarter_f + k * 32];
+              *xi = rel_kind[k] == 0 ? sigma * sv0 - pv0 : sv0 - rel_rinv[k] * S[quarter_f + k * 32];
               continue;
             }
-            const float sol = xl[ioff];
+            const float sol = *xi;
             if (rel_kind[k] == 0) {
               const float xn = alpha * sol + oma * sv0;
               s0t[u] = xn;
-              xl[ioff] = sigma * xn - pv0;
+              *xi = sigma * xn - pv0;
             } else {
               const float yk = S[quarter_f + k * 32], pv1 = S[3 * quarter_f + k * 32];
               const float rinv = rel_rinv[k];
@@ -460,40 +399,39 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
               const float yn = yk + rel_rho[k] * (zr - zn);
               s0t[u] = zn;
               s1t[u] = yn;
-              xl[ioff] = zn - rinv * yn;
+              *xi = zn - rinv * yn;
             }
           }
           // order these generic-proxy state writes before the bulk copies
           // that read them back in the next iteration
           if (kind == kItemBwd) fence_proxy_async_global();
           __syncwarp();
-          if (lane == 0) mbar_arrive(sm.sempty + sr.stage);
+          if (lane == 0) mbar_arrive(sempty + sr.stage);
           sr.advance(a.sstages);
         }
         __syncwarp();
         if (lane == 0) {
-          mbar_arrive(sm.lempty + lr.stage);
-          *sm.consumed_ctr = (int)(consumed + 1);
+          mbar_arrive(lempty + lr.stage);
+          *consumed_ctr = (int)(consumed + 1);
         }
         lr.advance(a.lstages);
         ++consumed;
         return true;
       };
       if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, consume)) ok = false;
-      if (ok && a.status) a.status[tile * 32 + lane] = status;
     }
-    if (!ok && lane == 0) *sm.abort_flag = 1;
+    if (!ok && lane == 0) *abort_flag = 1;
   }
   __syncthreads();
-  if (*sm.abort_flag) {
+  if (*abort_flag) {
     if (threadIdx.x == 32) {
       // drain: wait (bounded) for every bulk copy issued but not consumed
-      const uint32_t consumed = (uint32_t)*sm.consumed_ctr;
+      const uint32_t consumed = (uint32_t)*consumed_ctr;
       for (uint32_t t = consumed; t < issued_l; ++t)
-        mbar_wait_bounded(sm.lfull + t % a.lstages, (t / a.lstages) & 1u, nullptr, kWaitLimitNs);
+        mbar_wait_bounded(lfull + t % a.lstages, (t / a.lstages) & 1u, nullptr, kWaitLimitNs);
       const uint32_t s_lo = issued_s > (uint32_t)a.sstages ? issued_s - a.sstages : 0;
       for (uint32_t t = s_lo; t < issued_s; ++t)
-        mbar_wait_bounded(sm.sfull + t % a.sstages, (t / a.sstages) & 1u, nullptr, kWaitLimitNs);
+        mbar_wait_bounded(sfull + t % a.sstages, (t / a.sstages) & 1u, nullptr, kWaitLimitNs);
     }
     if (threadIdx.x == 0) atomicExch(a.error, 1);
     __syncthreads();
@@ -507,13 +445,14 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
   const int mw = sp.max_meta_words > sp.max_fmeta_words ? sp.max_meta_words : sp.max_fmeta_words;
   const int meta_bytes = ((mw * 4 + 127) / 128) * 128;
-  const int lent = (sp.max_ent + sp.max_cols) > sp.max_fent ? (sp.max_ent + sp.max_cols) : sp.max_fent;
-  const int lbytes = lent * 128;
+  const int bl = sp.max_units * 512 + sp.max_cols * 128;
+  const int fl = sp.max_funits * 512;
+  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
   const int sbytes = 4 * (sp.max_rel > 0 ? sp.max_rel : 1) * 128;
   // prefer deep rings: as many L stages as fit with at least 3 S stages
   for (int ls = 12; ls >= 2; --ls)
     for (int ss = 6; ss >= 2; --ss) {
-      const size_t bytes = stream_smem_bytes(sp.n, sp.n_chunks + sp.n_fchunks, ls, ss, meta_bytes + lbytes, sbytes);
+      const size_t bytes = stream_smem_bytes(sp.n, ls, ss, meta_bytes + lbytes, sbytes);
       if (bytes <= (size_t)kMaxSmemBytes && (ss >= 3 || ls <= 3)) {
         cfg->stages = ls;
         cfg->sstages = ss;
@@ -529,7 +468,7 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
 
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
-  return tiles * 32 * ((size_t)sp.stream_len + (size_t)sp.nnz_l + 4 * (size_t)sp.n) + 64;
+  return tiles * ((size_t)sp.blen + (size_t)sp.flen + 4 * 32 * (size_t)sp.n) + 64;
 }
 
 int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
@@ -540,9 +479,9 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
   const size_t tl = (size_t)n_tiles * 32;
-  float* lstream = work;
-  float* fstream = lstream + tl * sp.stream_len;
-  float* s0 = fstream + tl * sp.nnz_l;
+  float* bstream = work;
+  float* fstream = bstream + (size_t)n_tiles * sp.blen;
+  float* s0 = fstream + (size_t)n_tiles * sp.flen;
   float* s1 = s0 + tl * sp.n;
   float* p0 = s1 + tl * sp.n;
   float* p1 = p0 + tl * sp.n;
@@ -551,8 +490,8 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
     const int warps = 4;
     const size_t smem = (size_t)warps * (sp.max_row_nnz > 0 ? sp.max_row_nnz : 1) * 32 * sizeof(float);
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    factor_stream_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, s>>>(pat, sp, o, in, lstream, fstream, n_tiles,
-                                                                            batch);
+    factor_stream_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, s>>>(pat, sp, o, in, bstream, fstream, status,
+                                                                            n_tiles, batch);
     WMPC_LAUNCH_CHECK();
   }
   {
@@ -560,7 +499,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
     state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, s0, s1, p0, p1, batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
-  StreamArgs a{sp, lstream, fstream, s0, s1, p0, p1, status, error, n_tiles, max_iter, o.sigma, o.alpha,
+  StreamArgs a{sp, bstream, fstream, s0, s1, p0, p1, error, n_tiles, max_iter, o.sigma, o.alpha,
                o.one_minus_alpha, cfg.stages, cfg.sstages, cfg.meta_bytes, cfg.lbytes, cfg.sbytes};
   const int grid = n_tiles < num_sms ? n_tiles : num_sms;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));

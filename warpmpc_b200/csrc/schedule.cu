@@ -57,11 +57,106 @@ bool build_factor_tables(const HostPattern& hp, std::vector<int>* init_slot, std
   return true;
 }
 
+// Units: the sweeps are cut into units of 4 L entries of one row (forward) or
+// one column (backward), stored [unit][lane][4 entries] so a lane loads its 4
+// values with one 16-byte access.  Forward rows are right-aligned (padding
+// first, so a row's last entry -- the one that may read the row just before
+// it -- is always slot 3); backward columns are left-aligned (padding last, so
+// a column's first entry -- the one that may read the column just after it --
+// is always slot 0).  Padding slots hold L = 0 and read the zero row n of the
+// work vector, which leaves the running sum bit-for-bit unchanged.
+//
+// The consumer loads unit u+1 before it stores unit u's result, so a slot of
+// unit u+1 that reads unit u's target sees a stale value: the builder marks
+// such a read in the designated slot (kUnitFwd: the consumer substitutes the
+// register result) and separates the units by a no-op unit otherwise.
+namespace {
+
+struct UnitBuild {
+  int src[4];
+  int target;
+  int flags;
+  int doff;
+};
+
+// Cut one row (forward, right-aligned) or column (backward, left-aligned)
+// with `cnt` entries into units; entry q (in accumulation order) reads
+// work-vector row entry_src(q).  Returns the units; slot_of[q] receives
+// (unit index within the returned vector) * 4 + slot.
+template <typename Src>
+std::vector<UnitBuild> cut_units(int cnt, bool right_aligned, int target, int zero_row, Src entry_src,
+                                 std::vector<int>* slot_of) {
+  const int nu = cnt == 0 ? 1 : (cnt + 3) / 4;
+  const int pad = nu * 4 - cnt;
+  std::vector<UnitBuild> units(nu);
+  slot_of->assign(cnt, -1);
+  for (int k = 0; k < nu; ++k) {
+    UnitBuild& ub = units[k];
+    ub.target = target;
+    ub.flags = (k == 0 ? kUnitFirst : 0) | (k == nu - 1 ? kUnitLast : 0);
+    ub.doff = 0;
+    for (int s = 0; s < 4; ++s) {
+      const int q = right_aligned ? k * 4 + s - pad : k * 4 + s;
+      if (q < 0 || q >= cnt) {
+        ub.src[s] = zero_row;
+      } else {
+        ub.src[s] = entry_src(q);
+        (*slot_of)[q] = k * 4 + s;
+      }
+    }
+  }
+  return units;
+}
+
+// Append one row's / column's units to a chunk.  The consumer loads a unit
+// before the previous unit's result is stored, so if the first new unit reads
+// the previous unit's target it must do so in the forwarding slot (flag
+// kUnitFwd); any other slot gets a no-op unit (flags 0, zero slots) in
+// between.  Returns the index of the first appended unit.
+int append_units(std::vector<UnitBuild>* chunk, std::vector<UnitBuild> add, int fwd_slot, int zero_row,
+                 int* dummies) {
+  if (!chunk->empty() && (chunk->back().flags & kUnitLast)) {
+    const int prev_target = chunk->back().target;
+    bool other = false, fwd = false;
+    for (int s = 0; s < 4; ++s)
+      if (add[0].src[s] == prev_target) (s == fwd_slot ? fwd : other) = true;
+    if (other) {
+      UnitBuild d;
+      for (int s = 0; s < 4; ++s) d.src[s] = zero_row;
+      d.target = zero_row;
+      d.flags = 0;
+      d.doff = 0;
+      chunk->push_back(d);
+      ++*dummies;
+    } else if (fwd) {
+      add[0].flags |= kUnitFwd;
+    }
+  }
+  const int first = static_cast<int>(chunk->size());
+  chunk->insert(chunk->end(), add.begin(), add.end());
+  return first;
+}
+
+void push_unit_meta(const UnitBuild& ub, std::vector<int>* m) {
+  for (int s = 0; s < 4; ++s) m->push_back(ub.src[s] * 128);
+  m->push_back(ub.target * 128);
+  m->push_back(ub.flags);
+  m->push_back(ub.doff);
+  m->push_back(0);
+}
+
+}  // namespace
+
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
                            const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why) {
   const int n = hp.n;
+  const int zero_row = n;
   HostStream& S = *out;
   S = HostStream();
+  if (t.units <= 0 || t.cols <= 0 || t.rel <= 0 || t.funits <= 0) {
+    *why = "bad stream targets";
+    return false;
+  }
   // release column of every index: smallest column whose L entry lies in row i
   std::vector<int> rel_col(n);
   for (int i = 0; i < n; ++i) rel_col[i] = i;
@@ -83,7 +178,6 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   }
   std::vector<int> rel_count(n, 0);
   for (int i = 0; i < n; ++i) rel_count[rel_col[i]]++;
-  // U start of the releases of column c (U is ordered by column descending)
   std::vector<int> rel_first(n + 1, 0);
   {
     int u = 0;
@@ -92,66 +186,83 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       u += rel_count[c];
     }
   }
-  // chunk columns: whole columns, entries <= t.ent, columns <= t.cols, releases <= t.rel
+  auto col_units = [&](int c) { const int ce = hp.lp[c + 1] - hp.lp[c]; return ce == 0 ? 1 : (ce + 3) / 4; };
+  // ---- backward chunks: whole columns, units <= t.units, columns <= t.cols, releases <= t.rel
   std::vector<int> bounds{0};
   {
-    int ent = 0, cols = 0, rel = 0;
+    int units = 0, cols = 0, rel = 0;
     for (int c = 0; c < n; ++c) {
-      const int ce = hp.lp[c + 1] - hp.lp[c];
-      const int cr = rel_count[c];
-      if (cols > 0 && (ent + ce > t.ent || cols + 1 > t.cols || rel + cr > t.rel)) {
+      const int cu = col_units(c), cr = rel_count[c];
+      if (cols > 0 && (units + cu > t.units || cols + 1 > t.cols || rel + cr > t.rel)) {
         bounds.push_back(c);
-        ent = cols = rel = 0;
+        units = cols = rel = 0;
       }
-      ent += ce;
+      units += cu;
       cols += 1;
       rel += cr;
     }
     bounds.push_back(n);
   }
   S.n_chunks = static_cast<int>(bounds.size()) - 1;
-  S.stream_len = hp.nnz_l + n;
-  S.col_spos.resize(n);
-  S.dinv_spos.resize(n);
-  S.chunk_pos.resize(S.n_chunks + 1);
-  S.chunk_ent.resize(S.n_chunks);
+  S.chunk_off.resize(S.n_chunks + 1);
+  S.chunk_units.resize(S.n_chunks);
   S.chunk_cols.resize(S.n_chunks);
+  S.chunk_u0.resize(S.n_chunks);
+  S.chunk_nrel.resize(S.n_chunks);
   S.meta_off.resize(S.n_chunks);
   S.meta_words.resize(S.n_chunks);
-  std::vector<int> chunk_of_col(n);
+  S.col_uoff.assign(n, 0);
+  S.dinv_off.assign(n, 0);
+  std::vector<int> entry_boff(hp.nnz_l, -1);  // CSC entry -> backward stream float offset (lane 0)
+  int boff = 0;                                // running float offset in the backward stream
   for (int ch = 0; ch < S.n_chunks; ++ch) {
     const int c0 = bounds[ch], c1 = bounds[ch + 1];
-    const int e0 = hp.lp[c0], e1 = hp.lp[c1];
-    S.chunk_pos[ch] = e0 + c0;
-    S.chunk_ent[ch] = e1 - e0;
-    S.chunk_cols[ch] = c1 - c0;
-    S.max_ent = std::max(S.max_ent, e1 - e0);
-    S.max_cols = std::max(S.max_cols, c1 - c0);
-    int nrel = 0;
-    for (int c = c0; c < c1; ++c) {
-      chunk_of_col[c] = ch;
-      S.col_spos[c] = hp.lp[c] + c0;
-      S.dinv_spos[c] = e1 + c;
-      nrel += rel_count[c];
+    std::vector<UnitBuild> units;
+    std::vector<int> col_first_unit(c1 - c0), col_last_unit(c1 - c0);
+    std::vector<std::pair<int, int>> placed;  // (CSC entry, unit * 4 + slot within the chunk)
+    for (int c = c1 - 1; c >= c0; --c) {  // the order the backward sweep visits the columns
+      const int e0 = hp.lp[c], cnt = hp.lp[c + 1] - e0;
+      std::vector<int> slot_of;
+      std::vector<UnitBuild> add = cut_units(cnt, false, c, zero_row, [&](int q) { return hp.li[e0 + q]; }, &slot_of);
+      const int nadd = static_cast<int>(add.size());
+      const int first = append_units(&units, std::move(add), 0, zero_row, &S.dummy_units);
+      col_first_unit[c - c0] = first;
+      col_last_unit[c - c0] = first + nadd - 1;
+      for (int q = 0; q < cnt; ++q) placed.emplace_back(e0 + q, first * 4 + slot_of[q]);
     }
+    const int nu = static_cast<int>(units.size());
+    const int units_floats = nu * 128;
+    for (const auto& pe : placed) entry_boff[pe.first] = boff + (pe.second >> 2) * 128 + (pe.second & 3);
+    for (int c = c0; c < c1; ++c) {
+      S.col_uoff[c] = boff + col_first_unit[c - c0] * 128;
+      S.dinv_off[c] = boff + units_floats + (c - c0) * 32;
+      // D^-1 offset (bytes, relative to the stage's L area) on the column's last unit
+      units[col_last_unit[c - c0]].doff = (units_floats + (c - c0) * 32) * 4;
+    }
+    int nrel = 0;
+    for (int c = c0; c < c1; ++c) nrel += rel_count[c];
+    const int u0 = rel_first[c1 - 1];
+    S.chunk_off[ch] = boff;
+    S.chunk_units[ch] = nu;
+    S.chunk_cols[ch] = c1 - c0;
+    S.chunk_u0[ch] = u0;
+    S.chunk_nrel[ch] = nrel;
+    S.max_units = std::max(S.max_units, nu);
+    S.max_cols = std::max(S.max_cols, c1 - c0);
     S.max_rel = std::max(S.max_rel, nrel);
-    // meta block
-    const int ncols = c1 - c0, nent = e1 - e0;
-    const int u0 = rel_first[c1 - 1];  // releases of the chunk start at its highest column
-    S.meta_off[ch] = static_cast<int>(S.meta.size());
-    std::vector<int> m;
-    m.push_back(ncols);
-    m.push_back(nent);
-    m.push_back(nrel);
-    m.push_back(c0);
-    m.push_back(u0);
-    for (int c = c0; c <= c1; ++c) m.push_back((c < c1 ? hp.lp[c] : e1) - e0);  // col_start
-    for (int e = e0; e < e1; ++e) m.push_back(hp.li[e] * 32);  // word offset of row li[e] in the work vector
+    boff += units_floats + (c1 - c0) * 32;
+    // meta block: header, units, releases
+    std::vector<int> m{nu, c1 - c0, nrel, c0, u0, 0, 0, 0};
+    for (const UnitBuild& ub : units) push_unit_meta(ub, &m);
     std::vector<int> rel_i, rel_kind, rel_rho, rel_rinv;
     for (int u = u0; u < u0 + nrel; ++u) {
       const int i = order[u];
+      if (rel_col[i] < c0 || rel_col[i] >= c1) {
+        *why = "release order does not match the chunking";
+        return false;
+      }
       const int o = hp.p[i];
-      rel_i.push_back(i);
+      rel_i.push_back(i * 128);
       const bool cons = o >= n_primal;
       rel_kind.push_back(cons ? 1 : 0);
       float rho = 0.f, rinv = 0.f;
@@ -170,85 +281,93 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     for (int v : rel_rho) m.push_back(v);
     for (int v : rel_rinv) m.push_back(v);
     while (m.size() % 4) m.push_back(0);
+    S.meta_off[ch] = static_cast<int>(S.meta.size());
     S.meta_words[ch] = static_cast<int>(m.size());
     S.max_meta_words = std::max(S.max_meta_words, static_cast<int>(m.size()));
     S.meta.insert(S.meta.end(), m.begin(), m.end());
+    for (int u = 0; u < nu; ++u)
+      for (int s = 0; s < 4; ++s)
+        if (units[u].src[s] == zero_row) S.pad_boff.push_back(S.chunk_off[ch] + u * 128 + s);
   }
-  S.chunk_pos[S.n_chunks] = S.stream_len;
-  // sanity: every chunk's releases are exactly its columns' releases
-  for (int ch = 0; ch < S.n_chunks; ++ch) {
-    const int c0 = bounds[ch], c1 = bounds[ch + 1];
-    int nrel = 0;
-    for (int c = c0; c < c1; ++c) nrel += rel_count[c];
-    const int u0 = rel_first[c1 - 1];
-    for (int u = u0; u < u0 + nrel; ++u) {
-      const int rc = rel_col[order[u]];
-      if (rc < c0 || rc >= c1) {
-        *why = "release order does not match the chunking";
-        return false;
-      }
+  S.chunk_off[S.n_chunks] = boff;
+  S.blen = boff;
+  for (int e = 0; e < hp.nnz_l; ++e)
+    if (entry_boff[e] < 0) {
+      *why = "backward stream misses an entry";
+      return false;
     }
-  }
-  // ---- forward sweep: L in CSR order (row-gather form), chunks of whole rows
+  // ---- forward sweep: rows in order (row-gather form), columns ascending in a row
+  std::vector<int> entry_foff(hp.nnz_l, -1);
   {
-    std::vector<int> rcount(n, 0);
-    for (int e = 0; e < hp.nnz_l; ++e) rcount[hp.li[e]]++;
-    std::vector<int> rowptr(n + 1, 0);
-    for (int i = 0; i < n; ++i) rowptr[i + 1] = rowptr[i] + rcount[i];
-    // CSR position of each CSC entry: within a row, columns ascending (the
-    // reference's accumulation order for that row)
-    std::vector<int> csr_of_csc(hp.nnz_l);
-    std::vector<int> csr_col(hp.nnz_l);
-    {
-      std::vector<int> fillp(rowptr.begin(), rowptr.end() - 1);
-      for (int c = 0; c < n; ++c)
-        for (int e = hp.lp[c]; e < hp.lp[c + 1]; ++e) {
-          const int pos = fillp[hp.li[e]]++;
-          csr_of_csc[e] = pos;
-          csr_col[pos] = c;
-        }
-    }
-    std::vector<int> fb{0};
-    int ent = 0, rows = 0;
-    for (int i = 0; i < n; ++i) {
-      const int re = rcount[i];
-      if (rows > 0 && (ent + re > t.fent || rows + 1 > t.frows)) {
-        fb.push_back(i);
-        ent = rows = 0;
+    std::vector<std::vector<int>> row_entries(n);  // CSC entry indices of each row, columns ascending
+    std::vector<int> col_of(hp.nnz_l);
+    for (int c = 0; c < n; ++c)
+      for (int e = hp.lp[c]; e < hp.lp[c + 1]; ++e) {
+        row_entries[hp.li[e]].push_back(e);
+        col_of[e] = c;
       }
-      ent += re;
-      rows += 1;
+    auto row_units = [&](int i) { return (static_cast<int>(row_entries[i].size()) + 3) / 4; };
+    std::vector<int> fb{0};
+    {
+      int units = 0;
+      for (int i = 0; i < n; ++i) {
+        const int ru = row_units(i);
+        if (units > 0 && units + ru > t.funits) {
+          fb.push_back(i);
+          units = 0;
+        }
+        units += ru;
+      }
+      fb.push_back(n);
     }
-    fb.push_back(n);
-    S.n_fchunks = static_cast<int>(fb.size()) - 1;
-    S.fchunk_pos.resize(S.n_fchunks + 1);
-    S.fmeta_off.resize(S.n_fchunks);
-    S.fmeta_words.resize(S.n_fchunks);
-    for (int ch = 0; ch < S.n_fchunks; ++ch) {
-      const int r0 = fb[ch], r1 = fb[ch + 1];
-      const int e0 = rowptr[r0], e1 = rowptr[r1];
-      S.fchunk_pos[ch] = e0;
-      S.max_fent = std::max(S.max_fent, e1 - e0);
-      S.max_frows = std::max(S.max_frows, r1 - r0);
-      std::vector<int> m{r1 - r0, e1 - e0, r0, 0};
-      for (int i = r0; i <= r1; ++i) m.push_back(rowptr[i] - e0);
-      for (int e = e0; e < e1; ++e) m.push_back(csr_col[e] * 32);
-      while (m.size() % 4) m.push_back(0);
-      S.fmeta_off[ch] = static_cast<int>(S.fmeta.size());
-      S.fmeta_words[ch] = static_cast<int>(m.size());
+    // drop empty chunks (rows without entries only)
+    int foff = 0;
+    for (size_t k = 0; k + 1 < fb.size(); ++k) {
+      const int r0 = fb[k], r1 = fb[k + 1];
+      std::vector<UnitBuild> units;
+      std::vector<std::pair<int, int>> placed;
+      for (int i = r0; i < r1; ++i) {
+        const std::vector<int>& re = row_entries[i];
+        const int cnt = static_cast<int>(re.size());
+        if (cnt == 0) continue;
+        std::vector<int> slot_of;
+        std::vector<UnitBuild> add = cut_units(cnt, true, i, zero_row, [&](int q) { return col_of[re[q]]; }, &slot_of);
+        const int first = append_units(&units, std::move(add), 3, zero_row, &S.dummy_units);
+        for (int q = 0; q < cnt; ++q) placed.emplace_back(re[q], first * 4 + slot_of[q]);
+      }
+      const int nu = static_cast<int>(units.size());
+      if (nu == 0) continue;
+      for (const auto& pe : placed) entry_foff[pe.first] = foff + (pe.second >> 2) * 128 + (pe.second & 3);
+      std::vector<int> m{nu, 0, 0, 0, 0, 0, 0, 0};
+      for (const UnitBuild& ub : units) push_unit_meta(ub, &m);
+      S.fchunk_off.push_back(foff);
+      S.fchunk_units.push_back(nu);
+      S.fmeta_off.push_back(static_cast<int>(S.fmeta.size()));
+      S.fmeta_words.push_back(static_cast<int>(m.size()));
       S.max_fmeta_words = std::max(S.max_fmeta_words, static_cast<int>(m.size()));
+      S.max_funits = std::max(S.max_funits, nu);
       S.fmeta.insert(S.fmeta.end(), m.begin(), m.end());
+      for (int u = 0; u < nu; ++u)
+        for (int s = 0; s < 4; ++s)
+          if (units[u].src[s] == zero_row) S.pad_foff.push_back(foff + u * 128 + s);
+      foff += nu * 128;
     }
-    S.fchunk_pos[S.n_fchunks] = rowptr[n];
-    S.proc_fpos.resize(hp.nnz_l);
-    for (int k = 0; k < n; ++k)
-      for (int e = hp.proc_ptr[k]; e < hp.proc_ptr[k + 1]; ++e) S.proc_fpos[e] = csr_of_csc[hp.proc_lidx[e]];
+    S.n_fchunks = static_cast<int>(S.fchunk_units.size());
+    S.fchunk_off.push_back(foff);
+    S.flen = foff;
   }
-  S.proc_spos.resize(hp.nnz_l);
+  for (int e = 0; e < hp.nnz_l; ++e)
+    if (entry_foff[e] < 0) {
+      *why = "forward stream misses an entry";
+      return false;
+    }
+  // factor program step -> stream offsets of the L entry it writes
+  S.proc_boff.resize(hp.nnz_l);
+  S.proc_foff.resize(hp.nnz_l);
   for (int k = 0; k < n; ++k)
     for (int e = hp.proc_ptr[k]; e < hp.proc_ptr[k + 1]; ++e) {
-      const int c = hp.proc_cols[e];
-      S.proc_spos[e] = hp.proc_lidx[e] + bounds[chunk_of_col[c]];
+      S.proc_boff[e] = entry_boff[hp.proc_lidx[e]];
+      S.proc_foff[e] = entry_foff[hp.proc_lidx[e]];
     }
   return true;
 }

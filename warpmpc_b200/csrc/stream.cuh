@@ -2,12 +2,11 @@
 // the device helpers shared by its kernels.
 //
 // Per instance tile (32 instances, one per lane) the LDL^T factor is stored
-// "stream-major": [tile][stream position][lane], where the stream visits the
-// columns of L in chunks of whole columns and stores, per chunk, the L entries
-// of its columns (CSC order) followed by D^-1 of those columns.  The forward
-// sweep reads the chunks' L parts in ascending order, the backward sweep reads
-// L + D^-1 of every chunk in descending order: each read is one contiguous
-// bulk copy (cp.async.bulk, 128 bytes per stream position).
+// twice, each copy in the order one sweep reads it: a forward stream (rows in
+// order, a row's entries by ascending column) and a backward stream (columns
+// in reverse order of use, a column's entries by ascending row, then D^-1 of
+// the chunk's columns).  Both are cut into chunks; every chunk is one
+// contiguous bulk copy (cp.async.bulk) into a shared-memory ring stage.
 //
 // ADMM state (x or z, y) and parameters (q or l, u) are stored per tile in
 // "release order" U: the order in which the backward sweep finishes with a KKT
@@ -24,46 +23,55 @@
 
 namespace wmpc {
 
-// Meta block of one chunk (int32 words, 16-byte padded), copied into the
-// shared-memory stage together with the chunk's L data:
-//   [0] ncols  [1] nent  [2] nrel  [3] c0 (first column)  [4] u0 (first U index)
-//   [5 .. 5+ncols]           col_start (entry offset of each column, ncols+1)
-//   [.. + nent]              row offset (32 * L row index of each entry)
-//   [.. + nrel]              rel_i (permuted KKT index released)
-//   [.. + nrel]              rel_kind (0 primal, 1 constraint)
-//   [.. + nrel]              rel_rho (float bits)
-//   [.. + nrel]              rel_rhoinv (float bits)
-constexpr int kMetaHeader = 5;
+// Sweeps run over "units" of 4 L entries of one row (forward) or one column
+// (backward), stored per tile as [unit][lane][4] floats (512 bytes).  Unit
+// meta (8 int32 words): byte offsets (row * 128) of the 4 work-vector rows the
+// slots read, the target row's byte offset, flags, the D^-1 byte offset
+// (backward, last unit of a column; relative to the stage's L area), 0.
+constexpr int kUnitFirst = 1;  // first unit of its row/column: start the sum
+constexpr int kUnitLast = 2;   // last unit: store the result
+constexpr int kUnitFwd = 4;    // the forwarding slot (3 forward, 0 backward) reads the previous unit's result
+constexpr int kUnitWords = 8;
+constexpr int kChunkHeader = 8;
+// Backward chunk meta block (int32 words, 16-byte padded):
+//   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5..7] 0
+//   units (8 words each)
+//   rel_off[nrel] (byte offset of the released row), rel_kind[nrel] (0 primal, 1 constraint),
+//   rel_rho[nrel], rel_rhoinv[nrel] (float bits)
+// Forward chunk meta block: [0] nunits [1..7] 0, units.
+// Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
 
 struct StreamPlan {
   int n;              // KKT dimension
   int nnz_l;
-  // forward sweep (row-gather form): L in CSR order, chunks of whole rows
-  int n_fchunks;
-  int max_fent, max_frows, max_fmeta_words;
-  const int* fchunk_pos;    // [n_fchunks + 1] position in the forward stream (= CSR entry index)
+  // forward sweep (row-gather form)
+  int n_fchunks, flen, max_funits, max_fmeta_words;
+  const int* fchunk_off;    // [n_fchunks + 1] float offset (lane 0) in the forward stream
+  const int* fchunk_units;  // [n_fchunks]
   const int* fmeta_off;     // [n_fchunks]
   const int* fmeta_words;   // [n_fchunks]
-  const int* fmeta;         // forward meta blocks:
-                            //   [0] nrows [1] nent [2] r0 [3] 0 | row_start[nrows+1] | col offset (32*c)[nent]
-  const int* proc_fpos;     // [nnz_l] forward-stream position of the L entry each program step writes
-  // backward sweep (column form): L in CSC order + D^-1, chunks of whole columns
-  int n_chunks;
-  int stream_len;     // nnz_l + n
-  int max_ent, max_cols, max_rel, max_meta_words;
-  const int* chunk_pos;     // [n_chunks + 1] stream position of chunk start
-  const int* chunk_ent;     // [n_chunks] entries in the chunk
-  const int* chunk_cols;    // [n_chunks] columns in the chunk
-  const int* meta_off;      // [n_chunks] word offset of the chunk's meta block
-  const int* meta_words;    // [n_chunks] words (multiple of 4)
-  const int* meta;          // all meta blocks
-  // factor (compact accumulator) tables
+  const int* fmeta;
+  // backward sweep (column form) + releases
+  int n_chunks, blen, max_units, max_cols, max_rel, max_meta_words;
+  const int* chunk_off;     // [n_chunks + 1] float offset (lane 0) in the backward stream
+  const int* chunk_units;   // [n_chunks]
+  const int* chunk_cols;    // [n_chunks]
+  const int* chunk_u0;      // [n_chunks] first U index released
+  const int* chunk_nrel;    // [n_chunks]
+  const int* meta_off;      // [n_chunks]
+  const int* meta_words;    // [n_chunks]
+  const int* meta;
+  // factorization (compact accumulator) tables and stream offsets
   const int* init_slot;     // [init_ptr[n]] slot of each init row in reach(k)
   const int* upd_ptr;       // [nnz_l + 1]
   const int* upd_slot;      // [upd_ptr[nnz_l]]
-  const int* col_spos;      // [n] stream position of column c's first L entry
-  const int* dinv_spos;     // [n] stream position of D^-1_c
-  const int* proc_spos;     // [nnz_l] stream position of the L entry each program step writes
+  const int* col_uoff;      // [n] backward-stream float offset of column c's first unit
+  const int* dinv_off;      // [n] backward-stream float offset of D^-1_c (lane stride 1)
+  const int* proc_boff;     // [nnz_l] backward-stream float offset of the entry each program step writes
+  const int* proc_foff;     // [nnz_l] forward-stream float offset of that entry
+  const int* pad_boff;      // [n_pad_b] padding slots (L = 0) of the backward stream
+  const int* pad_foff;      // [n_pad_f] padding slots of the forward stream
+  int n_pad_b, n_pad_f;
   // release order
   const int* u_perm;        // [n] U index -> permuted KKT index
   const int* u_orig;        // [n] U index -> original KKT index
@@ -145,18 +153,19 @@ struct HostPattern {
 };
 
 struct StreamTargets {
-  int ent = 32, cols = 12, rel = 8;  // backward chunks
-  int fent = 32, frows = 12;         // forward chunks
+  int units = 12, cols = 12, rel = 8;  // backward chunks
+  int funits = 12;                     // forward chunks
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.
 struct HostStream {
-  int n_chunks = 0, stream_len = 0, max_ent = 0, max_cols = 0, max_rel = 0, max_meta_words = 0, max_row_nnz = 0;
-  std::vector<int> chunk_pos, chunk_ent, chunk_cols, meta_off, meta_words, meta;
-  int n_fchunks = 0, max_fent = 0, max_frows = 0, max_fmeta_words = 0;
-  std::vector<int> fchunk_pos, fmeta_off, fmeta_words, fmeta, proc_fpos;
-  std::vector<int> init_slot, upd_ptr, col_spos, dinv_spos, proc_spos, u_perm, u_orig;
-  std::vector<unsigned short> upd_slot;
+  int n_chunks = 0, blen = 0, max_units = 0, max_cols = 0, max_rel = 0, max_meta_words = 0;
+  std::vector<int> chunk_off, chunk_units, chunk_cols, chunk_u0, chunk_nrel, meta_off, meta_words, meta;
+  int n_fchunks = 0, flen = 0, max_funits = 0, max_fmeta_words = 0;
+  std::vector<int> fchunk_off, fchunk_units, fmeta_off, fmeta_words, fmeta;
+  std::vector<int> col_uoff, dinv_off, proc_boff, proc_foff, pad_boff, pad_foff;
+  std::vector<int> u_perm, u_orig;
+  int dummy_units = 0;
   // host copies used by the OSQP side to lay out the state
   std::vector<int> u_of_perm;  // permuted index -> U index
 };
@@ -170,7 +179,6 @@ struct StreamLaunch {
   int stages, sstages, meta_bytes, lbytes, sbytes;
   size_t smem;
 };
-constexpr int kFMetaHeader = 4;
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
 size_t stream_workspace_floats(const StreamPlan& sp, int batch);
 

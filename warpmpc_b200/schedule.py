@@ -15,7 +15,7 @@ import numpy as np
 from . import native
 from .jax_qdldl.planning import plan_ragged_program
 
-DEFAULT_TARGETS = (32, 12, 8)  # entries, columns, releases per backward chunk
+DEFAULT_TARGETS = (12, 12, 8, 12)  # backward units, columns, releases; forward units
 
 
 def _pattern_desc(qp):
@@ -41,7 +41,10 @@ def _pattern_desc(qp):
 
 
 def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
-    """Schedule of an OSQP plan (rho per constraint) as NumPy arrays."""
+    """Schedule of an OSQP plan (rho per constraint) as NumPy arrays.
+
+    targets: (backward units, backward columns, backward releases, forward
+    units) per chunk."""
     qp = plan.qdldl_plan
     desc, keep, rg = _pattern_desc(qp)
     rho = native.f32(plan.rho_vec)
@@ -54,9 +57,9 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
     native.check(lib.wmpc_stream_schedule_host(*args, native.ptr_i32(buf), buf.size, ctypes.byref(words)))
     n, nnz_l = qp.n, qp.nnz_l
     hdr = buf[:8]
-    n_chunks, stream_len, max_ent, max_cols, max_rel, max_meta, max_row, n_meta = (int(v) for v in hdr)
+    n_chunks, blen, max_units, max_cols, max_rel, max_meta, max_row, n_meta = (int(v) for v in hdr)
     pos = 8
-    out = {"n_chunks": n_chunks, "stream_len": stream_len, "max_ent": max_ent, "max_cols": max_cols,
+    out = {"n_chunks": n_chunks, "blen": blen, "max_units": max_units, "max_cols": max_cols,
            "max_rel": max_rel, "max_meta_words": max_meta, "max_row_nnz": max_row}
 
     def take(name, count):
@@ -64,28 +67,36 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
         out[name] = buf[pos : pos + count].copy()
         pos += count
 
-    take("chunk_pos", n_chunks + 1)
-    take("chunk_ent", n_chunks)
+    take("chunk_off", n_chunks + 1)
+    take("chunk_units", n_chunks)
     take("chunk_cols", n_chunks)
+    take("chunk_u0", n_chunks)
+    take("chunk_nrel", n_chunks)
     take("meta_off", n_chunks)
     take("meta_words", n_chunks)
     take("meta", n_meta)
-    take("col_spos", n)
-    take("dinv_spos", n)
-    take("proc_spos", nnz_l)
+    take("col_uoff", n)
+    take("dinv_off", n)
+    take("proc_boff", nnz_l)
     take("u_perm", n)
     take("u_orig", n)
     take("init_slot", int(rg["init_ptr"][-1]))
     take("upd_ptr", nnz_l + 1)
     take("upd_slot", int(out["upd_ptr"][-1]))
-    nf, mfe, mfr, mfm, nfm = (int(v) for v in buf[pos : pos + 5])
+    nf, flen, mfu, mfm, nfm = (int(v) for v in buf[pos : pos + 5])
     pos += 5
-    out.update({"n_fchunks": nf, "max_fent": mfe, "max_frows": mfr, "max_fmeta_words": mfm})
-    take("fchunk_pos", nf + 1)
+    out.update({"n_fchunks": nf, "flen": flen, "max_funits": mfu, "max_fmeta_words": mfm})
+    take("fchunk_off", nf + 1)
+    take("fchunk_units", nf)
     take("fmeta_off", nf)
     take("fmeta_words", nf)
     take("fmeta", nfm)
-    take("proc_fpos", nnz_l)
+    take("proc_foff", nnz_l)
+    npb, npf, ndum = (int(v) for v in buf[pos : pos + 3])
+    pos += 3
+    out["dummy_units"] = ndum
+    take("pad_boff", npb)
+    take("pad_foff", npf)
     assert pos == buf.size
     out["ragged"] = rg
     return out
