@@ -111,7 +111,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     oma = _f32(1.0) - alpha
     iters = plan.settings.max_iter if max_iter is None else max_iter
     nch = sched["n_chunks"]
-    X = np.full((n + 1, lanes), np.nan, dtype=np.float32)  # row n: the zero row
+    X = np.full((n + 2, lanes), np.nan, dtype=np.float32)  # row n: the zero row, n + 1: trash
     X[n] = 0.0
     meta_all = sched["meta"]
     fmeta_all = sched["fmeta"]
@@ -123,42 +123,49 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         return all_[off : off + w]
 
     def xrow(byte_off):
-        assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= n
+        assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= n + 1
         return byte_off // 128
 
     def run_units(m, nu, stage, backward):
-        """The consumer's unit loop, with unit u+1's loads taken before unit u's store."""
-        assert 1 <= nu and KHDR + nu * KUW <= m.size
-        units = m[KHDR : KHDR + nu * KUW].reshape(nu, KUW)
+        """The consumer's unit loop: unit u+1 (u+1 == nu: the sentinel) is loaded
+        before unit u's arithmetic and store."""
+        assert 1 <= nu and KHDR + (nu + 1) * KUW <= m.size
+        units = m[KHDR : KHDR + (nu + 1) * KUW].reshape(nu + 1, KUW)
+        sent = units[nu]
+        assert np.all(sent[:5] == n * 128) and sent[5] == 0 and sent[7] == (n + 1) * 128
         nfl = stage.size
 
         def load(u):
             src, ctl = units[u, :4], units[u, 4:]
             lo = u * 128
-            assert lo + 128 <= nfl
-            lv = stage[lo : lo + 128].reshape(lanes, 4).T.copy()  # [slot][lane]
+            lv = stage[lo : lo + 128].reshape(lanes, 4).T.copy() if u < nu else None  # [slot][lane]
             xs = [X[xrow(o)].copy() for o in src]
             t = X[xrow(ctl[0])].copy()
-            return ctl, lv, xs, t
+            d = None
+            if backward and u < nu:
+                doff = int(ctl[2])
+                assert doff % 4 == 0 and doff // 4 + 32 <= nfl
+                d = stage[doff // 4 : doff // 4 + 32].copy()
+            if u < nu:
+                assert lo + 128 <= nfl
+                assert xrow(ctl[3]) == (xrow(ctl[0]) if int(ctl[1]) & LAST else n + 1)
+            return ctl, lv, xs, t, d
 
         cur = load(0)
         acc = np.zeros(lanes, np.float32)
         prev = np.zeros(lanes, np.float32)
         for u in range(nu):
-            nxt = load(u + 1 if u + 1 < nu else u)
-            ctl, lv, xs, t = cur
+            nxt = load(u + 1)
+            ctl, lv, xs, t, d = cur
             fl = int(ctl[1])
             if backward:
-                doff = int(ctl[2])
-                assert doff % 4 == 0 and doff // 4 + 32 <= nfl
-                dinv = stage[doff // 4 : doff // 4 + 32]
                 x0 = prev if fl & FWD else xs[0]
                 acc = np.zeros(lanes, np.float32) if fl & FIRST else acc
                 acc = acc + lv[0] * x0
                 acc = acc + lv[1] * xs[1]
                 acc = acc + lv[2] * xs[2]
                 acc = acc + lv[3] * xs[3]
-                res = t * dinv - acc
+                res = t * d - acc
             else:
                 x3 = prev if fl & FWD else xs[3]
                 acc = t if fl & FIRST else acc
@@ -167,10 +174,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 acc = acc - lv[2] * xs[2]
                 acc = acc - lv[3] * x3
                 res = acc
-            if fl & LAST:
-                tr = xrow(ctl[0])
-                assert tr < n
-                X[tr] = res
+            X[xrow(ctl[3])] = res
             prev = res
             cur = nxt
 
@@ -187,16 +191,17 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             run_units(fm, nu, Fs[o0:o1], backward=False)
             continue
         m = block(meta_all, sched["meta_off"], sched["meta_words"], ch, sched["max_meta_words"])
-        nu, ncols, nrel, c0, u0 = (int(v) for v in m[:5])
+        nu, ncols, nrel, c0, u0, nprim = (int(v) for v in m[:6])
         assert nu == sched["chunk_units"][ch] and ncols == sched["chunk_cols"][ch] and nrel == sched["chunk_nrel"][ch]
         assert u0 == sched["chunk_u0"][ch] and nu <= sched["max_units"] and ncols <= sched["max_cols"]
-        assert nrel <= sched["max_rel"] and 0 <= u0 and u0 + nrel <= n
-        r = KHDR + nu * KUW
-        assert r + 4 * nrel <= m.size
+        assert nrel <= sched["max_rel"] and 0 <= u0 and u0 + nrel <= n and 0 <= nprim <= nrel
+        r = KHDR + (nu + 1) * KUW
+        assert r + 3 * nrel <= m.size
         rel_i = m[r : r + nrel]
-        rel_kind = m[r + nrel : r + 2 * nrel]
-        rel_rho = m[r + 2 * nrel : r + 3 * nrel].view(np.float32)
-        rel_rinv = m[r + 3 * nrel : r + 4 * nrel].view(np.float32)
+        rel_rho = m[r + nrel : r + 2 * nrel].view(np.float32)
+        rel_rinv = m[r + 2 * nrel : r + 3 * nrel].view(np.float32)
+        for k in range(nrel):
+            assert (sched["u_orig"][u0 + k] < plan.n) == (k < nprim)
         if kind == 2:
             o0, o1 = sched["chunk_off"][ch], sched["chunk_off"][ch + 1]
             assert o1 - o0 == nu * 128 + ncols * 32 and o1 <= BL
@@ -206,7 +211,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 assert i < n
                 uu = u0 + k
                 sol = X[i].copy()
-                if rel_kind[k] == 0:
+                if k < nprim:
                     xn = alpha * sol + oma * s0[uu]
                     s0[uu] = xn
                     X[i] = sigma * xn - pp0[uu]
@@ -227,7 +232,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 i = xrow(rel_i[k])
                 assert i < n
                 uu = u0 + k
-                X[i] = sigma * s0[uu] - pp0[uu] if rel_kind[k] == 0 else s0[uu] - rel_rinv[k] * s1[uu]
+                X[i] = sigma * s0[uu] - pp0[uu] if k < nprim else s0[uu] - rel_rinv[k] * s1[uu]
         assert X[n].max() == 0.0 and X[n].min() == 0.0
     # ---- stream_to_state_kernel + unscale
     x = np.zeros((lanes, plan.n), np.float32)

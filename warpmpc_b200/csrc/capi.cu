@@ -543,6 +543,10 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sp.max_fmeta_words = hs.max_fmeta_words;
       sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
       sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
+      sp.max_lstages = 12;
+      sp.max_sstages = 6;
+      if (const char* v = getenv("WMPC_STREAM_LSTAGES")) sp.max_lstages = atoi(v);
+      if (const char* v = getenv("WMPC_STREAM_SSTAGES")) sp.max_sstages = atoi(v);
       StreamLaunch cfg;
       if (!stream_launch_config(sp, &cfg)) {
         ok = false;

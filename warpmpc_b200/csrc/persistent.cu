@@ -194,30 +194,79 @@ __device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_it
   return true;
 }
 
-// Shared-memory layout: X [n + 1][32] | L ring | S ring | barriers | flags
+// Shared-memory layout: X [n + 2][32] | L ring | S ring | barriers | flags
 __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
-  return (size_t)(n + 1) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
+  return (size_t)(n + 2) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
          16 * (size_t)(lstages + sstages) + 16;
 }
 
 // One unit's operands, loaded ahead of its arithmetic.
 struct UnitOps {
-  int4 src, ctl;  // ctl: target byte offset, flags, D^-1 byte offset, 0
+  int4 src, ctl;  // ctl: target byte offset, flags, D^-1 byte offset, store byte offset
   float4 l;
-  float x0, x1, x2, x3, t;
+  float x0, x1, x2, x3, t, d;
 };
 
-__device__ __forceinline__ void load_unit(const int4* __restrict__ mu, const unsigned char* lst, const unsigned char* xb,
-                                          int u, int lane, UnitOps& r) {
-  r.src = mu[2 * u];
-  r.ctl = mu[2 * u + 1];
-  r.l = *reinterpret_cast<const float4*>(lst + u * 512 + lane * 16);
+// mu: this unit's meta (2 x int4); lq: this lane's 4 L values of the unit
+template <bool kBackward>
+__device__ __forceinline__ void load_unit(const int4* __restrict__ mu, const float4* lq, const unsigned char* lst,
+                                          const unsigned char* xb, int lane, UnitOps& r) {
+  r.src = mu[0];
+  r.ctl = mu[1];
+  r.l = *lq;
   r.x0 = *reinterpret_cast<const float*>(xb + r.src.x);
   r.x1 = *reinterpret_cast<const float*>(xb + r.src.y);
   r.x2 = *reinterpret_cast<const float*>(xb + r.src.z);
   r.x3 = *reinterpret_cast<const float*>(xb + r.src.w);
   r.t = *reinterpret_cast<const float*>(xb + r.ctl.x);
+  if (kBackward) r.d = *reinterpret_cast<const float*>(lst + r.ctl.z + lane * 4);
+}
+
+// Forward unit: acc = (first ? rhs_i : acc) - L_i,c0 x_c0 - ... (ascending c)
+__device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, float& acc, float& prev) {
+  const int fl = r.ctl.y;
+  const float x3 = (fl & kUnitFwd) ? prev : r.x3;
+  acc = (fl & kUnitFirst) ? r.t : acc;
+  acc = acc - r.l.x * r.x0;
+  acc = acc - r.l.y * r.x1;
+  acc = acc - r.l.z * r.x2;
+  acc = acc - r.l.w * x3;
+  *reinterpret_cast<float*>(xb + r.ctl.w) = acc;
+  prev = acc;
+}
+
+// Backward unit: corr = (first ? 0 : corr) + L_r0,j x_r0 + ... (ascending r);
+// x_j = x_j D^-1_j - corr
+__device__ __forceinline__ void backward_unit(const UnitOps& r, unsigned char* xb, float& corr, float& prev) {
+  const int fl = r.ctl.y;
+  const float x0 = (fl & kUnitFwd) ? prev : r.x0;
+  corr = (fl & kUnitFirst) ? 0.0f : corr;
+  corr = corr + r.l.x * x0;
+  corr = corr + r.l.y * r.x1;
+  corr = corr + r.l.z * r.x2;
+  corr = corr + r.l.w * r.x3;
+  const float res = r.t * r.d - corr;
+  *reinterpret_cast<float*>(xb + r.ctl.w) = res;
+  prev = res;
+}
+
+// Run a chunk's units, unit u+1's loads issued before unit u's arithmetic and
+// store (two register sets, alternating; unit nu is the sentinel).
+template <bool kBackward>
+__device__ __forceinline__ void run_units(const int4* __restrict__ mu, const unsigned char* lst, unsigned char* xb,
+                                          int lane, int nu) {
+  const float4* lq = reinterpret_cast<const float4*>(lst + lane * 16);
+  UnitOps A, B;
+  float acc = 0.0f, prev = 0.0f;
+  load_unit<kBackward>(mu, lq, lst, xb, lane, A);
+  for (int u = 0; u < nu; u += 2) {
+    load_unit<kBackward>(mu + 2 * (u + 1), lq + 32 * (u + 1), lst, xb, lane, B);
+    if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit(A, xb, acc, prev);
+    if (u + 1 >= nu) break;
+    load_unit<kBackward>(mu + 2 * (u + 2), lq + 32 * (u + 2), lst, xb, lane, A);
+    if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit(B, xb, acc, prev);
+  }
 }
 
 __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
@@ -226,7 +275,7 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
   const int n = sp.n;
   const int lstage_bytes = a.meta_bytes + a.lbytes;
   float* X = reinterpret_cast<float*>(smem);
-  unsigned char* lring = smem + (size_t)(n + 1) * 128;
+  unsigned char* lring = smem + (size_t)(n + 2) * 128;
   unsigned char* sring = lring + (size_t)a.lstages * lstage_bytes;
   uint64_t* lfull = reinterpret_cast<uint64_t*>(sring + (size_t)a.sstages * a.sbytes);
   uint64_t* lempty = lfull + a.lstages;
@@ -324,81 +373,51 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
         const unsigned char* lst = stage + a.meta_bytes;
         const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
         const int nu = meta[0];
+        unsigned char* xw = const_cast<unsigned char*>(xb);
         if (kind == kItemFwd) {
-          // forward substitution, row-gather form: a row's sum starts from
-          // its right-hand side and subtracts L_ij x_j by ascending j
-          UnitOps cur, nxt;
-          load_unit(mu, lst, xb, 0, lane, cur);
-          float acc = 0.0f, prev = 0.0f;
-          for (int u = 0; u < nu; ++u) {
-            load_unit(mu, lst, xb, u + 1 < nu ? u + 1 : u, lane, nxt);
-            const int fl = cur.ctl.y;
-            const float x3 = (fl & kUnitFwd) ? prev : cur.x3;
-            acc = (fl & kUnitFirst) ? cur.t : acc;
-            acc = acc - cur.l.x * cur.x0;
-            acc = acc - cur.l.y * cur.x1;
-            acc = acc - cur.l.z * cur.x2;
-            acc = acc - cur.l.w * x3;
-            if (fl & kUnitLast) *reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + cur.ctl.x) = acc;
-            prev = acc;
-            cur = nxt;
-          }
+          // forward substitution, row-gather form
+          run_units<false>(mu, lst, xw, lane, nu);
         } else {
-          const int nrel = meta[2], u0 = meta[4];
-          if (kind == kItemBwd) {
-            // backward substitution, column form: x_j = x_j D^-1_j - sum_i L_ij x_i
-            // (the sum by ascending i), columns in reverse order
-            UnitOps cur, nxt;
-            load_unit(mu, lst, xb, 0, lane, cur);
-            float corr = 0.0f, prev = 0.0f;
-            for (int u = 0; u < nu; ++u) {
-              load_unit(mu, lst, xb, u + 1 < nu ? u + 1 : u, lane, nxt);
-              const float dinv = *reinterpret_cast<const float*>(lst + cur.ctl.z + lane * 4);
-              const int fl = cur.ctl.y;
-              const float x0 = (fl & kUnitFwd) ? prev : cur.x0;
-              corr = (fl & kUnitFirst) ? 0.0f : corr;
-              corr = corr + cur.l.x * x0;
-              corr = corr + cur.l.y * cur.x1;
-              corr = corr + cur.l.z * cur.x2;
-              corr = corr + cur.l.w * cur.x3;
-              const float res = cur.t * dinv - corr;
-              if (fl & kUnitLast) *reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + cur.ctl.x) = res;
-              prev = res;
-              cur = nxt;
-            }
-          }
+          const int nrel = meta[2], u0 = meta[4], nprim = meta[5];
+          // backward substitution, column form, columns in reverse order
+          if (kind == kItemBwd) run_units<true>(mu, lst, xw, lane, nu);
           // releases: ADMM update (backward items) or first right-hand side
-          const int* rel_off = meta + kChunkHeader + nu * kUnitWords;
-          const int* rel_kind = rel_off + nrel;
-          const float* rel_rho = reinterpret_cast<const float*>(rel_kind + nrel);
+          const int* rel_off = meta + kChunkHeader + (nu + 1) * kUnitWords;
+          const float* rel_rho = reinterpret_cast<const float*>(rel_off + nrel);
           const float* rel_rinv = rel_rho + nrel;
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
-          const float* S = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes) + lane;
-          for (int k = 0; k < nrel; ++k) {
-            float* xi = reinterpret_cast<float*>(const_cast<unsigned char*>(xb) + rel_off[k]);
-            const float sv0 = S[k * 32], pv0 = S[2 * quarter_f + k * 32];
-            const size_t u = (size_t)(u0 + k) * 32;
-            if (kind == kItemRel) {
-              *xi = rel_kind[k] == 0 ? sigma * sv0 - pv0 : sv0 - rel_rinv[k] * S[quarter_f + k * 32];
-              continue;
+          const float* S0 = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes) + lane;
+          const float* S1 = S0 + quarter_f;
+          const float* P0 = S1 + quarter_f;
+          const float* P1 = P0 + quarter_f;
+          float* s0u = s0t + (size_t)u0 * 32;
+          float* s1u = s1t + (size_t)u0 * 32;
+          if (kind == kItemRel) {
+            for (int k = 0; k < nprim; ++k)
+              *reinterpret_cast<float*>(xw + rel_off[k]) = sigma * S0[k * 32] - P0[k * 32];
+            for (int k = nprim; k < nrel; ++k)
+              *reinterpret_cast<float*>(xw + rel_off[k]) = S0[k * 32] - rel_rinv[k] * S1[k * 32];
+          } else {
+            for (int k = 0; k < nprim; ++k) {
+              float* xi = reinterpret_cast<float*>(xw + rel_off[k]);
+              const float xn = alpha * *xi + oma * S0[k * 32];
+              s0u[k * 32] = xn;
+              *xi = sigma * xn - P0[k * 32];
             }
-            const float sol = *xi;
-            if (rel_kind[k] == 0) {
-              const float xn = alpha * sol + oma * sv0;
-              s0t[u] = xn;
-              *xi = sigma * xn - pv0;
-            } else {
-              const float yk = S[quarter_f + k * 32], pv1 = S[3 * quarter_f + k * 32];
+            for (int k = nprim; k < nrel; ++k) {
+              float* xi = reinterpret_cast<float*>(xw + rel_off[k]);
+              const float sol = *xi;
+              const float sv0 = S0[k * 32], yk = S1[k * 32], lo = P0[k * 32], hi = P1[k * 32];
               const float rinv = rel_rinv[k];
               const float rz = sv0 - rinv * yk;
               const float zt = rz + rinv * sol;
               const float zr = alpha * zt + oma * sv0;
               float zn = zr + rinv * yk;
-              zn = (zn < pv0) ? pv0 : zn;
-              zn = (zn > pv1) ? pv1 : zn;
+              zn = (zn < lo) ? lo : zn;
+              zn = (zn > hi) ? hi : zn;
               const float yn = yk + rel_rho[k] * (zr - zn);
-              s0t[u] = zn;
-              s1t[u] = yn;
+              s0u[k * 32] = zn;
+              s1u[k * 32] = yn;
               *xi = zn - rinv * yn;
             }
           }
@@ -447,11 +466,13 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
   const int meta_bytes = ((mw * 4 + 127) / 128) * 128;
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
-  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
+  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128 + 512;  // + the sentinel unit's reads
   const int sbytes = 4 * (sp.max_rel > 0 ? sp.max_rel : 1) * 128;
   // prefer deep rings: as many L stages as fit with at least 3 S stages
-  for (int ls = 12; ls >= 2; --ls)
-    for (int ss = 6; ss >= 2; --ss) {
+  const int lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
+  const int smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
+  for (int ls = lmax; ls >= 2; --ls)
+    for (int ss = smax; ss >= 2; --ss) {
       const size_t bytes = stream_smem_bytes(sp.n, ls, ss, meta_bytes + lbytes, sbytes);
       if (bytes <= (size_t)kMaxSmemBytes && (ss >= 3 || ls <= 3)) {
         cfg->stages = ls;

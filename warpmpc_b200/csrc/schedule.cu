@@ -137,12 +137,22 @@ int append_units(std::vector<UnitBuild>* chunk, std::vector<UnitBuild> add, int 
   return first;
 }
 
-void push_unit_meta(const UnitBuild& ub, std::vector<int>* m) {
+void push_unit_meta(const UnitBuild& ub, int trash_row, std::vector<int>* m) {
   for (int s = 0; s < 4; ++s) m->push_back(ub.src[s] * 128);
   m->push_back(ub.target * 128);
   m->push_back(ub.flags);
   m->push_back(ub.doff);
+  m->push_back(((ub.flags & kUnitLast) ? ub.target : trash_row) * 128);
+}
+
+// Meta of the sentinel unit after a chunk's last unit: the consumer loads one
+// unit ahead, so unit `nunits` is read (never computed).
+void push_sentinel_meta(int zero_row, int trash_row, std::vector<int>* m) {
+  for (int s = 0; s < 4; ++s) m->push_back(zero_row * 128);
+  m->push_back(zero_row * 128);
   m->push_back(0);
+  m->push_back(0);
+  m->push_back(trash_row * 128);
 }
 
 }  // namespace
@@ -150,7 +160,7 @@ void push_unit_meta(const UnitBuild& ub, std::vector<int>* m) {
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
                            const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why) {
   const int n = hp.n;
-  const int zero_row = n;
+  const int zero_row = n, trash_row = n + 1;
   HostStream& S = *out;
   S = HostStream();
   if (t.units <= 0 || t.cols <= 0 || t.rel <= 0 || t.funits <= 0) {
@@ -169,13 +179,6 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     if (rel_col[a] != rel_col[b]) return rel_col[a] > rel_col[b];
     return a > b;
   });
-  S.u_perm = order;
-  S.u_orig.resize(n);
-  S.u_of_perm.resize(n);
-  for (int u = 0; u < n; ++u) {
-    S.u_orig[u] = hp.p[order[u]];
-    S.u_of_perm[order[u]] = u;
-  }
   std::vector<int> rel_count(n, 0);
   for (int i = 0; i < n; ++i) rel_count[rel_col[i]]++;
   std::vector<int> rel_first(n + 1, 0);
@@ -252,19 +255,25 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     S.max_rel = std::max(S.max_rel, nrel);
     boff += units_floats + (c1 - c0) * 32;
     // meta block: header, units, releases
-    std::vector<int> m{nu, c1 - c0, nrel, c0, u0, 0, 0, 0};
-    for (const UnitBuild& ub : units) push_unit_meta(ub, &m);
-    std::vector<int> rel_i, rel_kind, rel_rho, rel_rinv;
-    for (int u = u0; u < u0 + nrel; ++u) {
-      const int i = order[u];
-      if (rel_col[i] < c0 || rel_col[i] >= c1) {
+    // the chunk's releases: primal indices first, then constraints (two branch-free loops)
+    for (int u = u0; u < u0 + nrel; ++u)
+      if (rel_col[order[u]] < c0 || rel_col[order[u]] >= c1) {
         *why = "release order does not match the chunking";
         return false;
       }
+    std::stable_partition(order.begin() + u0, order.begin() + u0 + nrel,
+                          [&](int i) { return hp.p[i] < n_primal; });
+    int nprim = 0;
+    for (int u = u0; u < u0 + nrel; ++u) nprim += hp.p[order[u]] < n_primal ? 1 : 0;
+    std::vector<int> m{nu, c1 - c0, nrel, c0, u0, nprim, 0, 0};
+    for (const UnitBuild& ub : units) push_unit_meta(ub, trash_row, &m);
+    push_sentinel_meta(zero_row, trash_row, &m);
+    std::vector<int> rel_i, rel_rho, rel_rinv;
+    for (int u = u0; u < u0 + nrel; ++u) {
+      const int i = order[u];
       const int o = hp.p[i];
       rel_i.push_back(i * 128);
       const bool cons = o >= n_primal;
-      rel_kind.push_back(cons ? 1 : 0);
       float rho = 0.f, rinv = 0.f;
       if (cons && rho_by_constraint) {
         rho = rho_by_constraint[o - n_primal];
@@ -277,7 +286,6 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       rel_rinv.push_back(ib);
     }
     for (int v : rel_i) m.push_back(v);
-    for (int v : rel_kind) m.push_back(v);
     for (int v : rel_rho) m.push_back(v);
     for (int v : rel_rinv) m.push_back(v);
     while (m.size() % 4) m.push_back(0);
@@ -291,6 +299,13 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   }
   S.chunk_off[S.n_chunks] = boff;
   S.blen = boff;
+  S.u_perm = order;
+  S.u_orig.resize(n);
+  S.u_of_perm.resize(n);
+  for (int u = 0; u < n; ++u) {
+    S.u_orig[u] = hp.p[order[u]];
+    S.u_of_perm[order[u]] = u;
+  }
   for (int e = 0; e < hp.nnz_l; ++e)
     if (entry_boff[e] < 0) {
       *why = "backward stream misses an entry";
@@ -339,7 +354,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       if (nu == 0) continue;
       for (const auto& pe : placed) entry_foff[pe.first] = foff + (pe.second >> 2) * 128 + (pe.second & 3);
       std::vector<int> m{nu, 0, 0, 0, 0, 0, 0, 0};
-      for (const UnitBuild& ub : units) push_unit_meta(ub, &m);
+      for (const UnitBuild& ub : units) push_unit_meta(ub, trash_row, &m);
+      push_sentinel_meta(zero_row, trash_row, &m);
       S.fchunk_off.push_back(foff);
       S.fchunk_units.push_back(nu);
       S.fmeta_off.push_back(static_cast<int>(S.fmeta.size()));

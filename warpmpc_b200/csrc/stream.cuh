@@ -26,20 +26,23 @@ namespace wmpc {
 // Sweeps run over "units" of 4 L entries of one row (forward) or one column
 // (backward), stored per tile as [unit][lane][4] floats (512 bytes).  Unit
 // meta (8 int32 words): byte offsets (row * 128) of the 4 work-vector rows the
-// slots read, the target row's byte offset, flags, the D^-1 byte offset
-// (backward, last unit of a column; relative to the stage's L area), 0.
+// slots read; the target row's byte offset (read: right-hand side / x_j);
+// flags; the D^-1 byte offset (backward; relative to the stage's L area);
+// the byte offset the result is stored to (the target on a row's / column's
+// last unit, the trash row n + 1 otherwise).
 constexpr int kUnitFirst = 1;  // first unit of its row/column: start the sum
-constexpr int kUnitLast = 2;   // last unit: store the result
+constexpr int kUnitLast = 2;   // last unit: the stored result is final
 constexpr int kUnitFwd = 4;    // the forwarding slot (3 forward, 0 backward) reads the previous unit's result
 constexpr int kUnitWords = 8;
 constexpr int kChunkHeader = 8;
 // Backward chunk meta block (int32 words, 16-byte padded):
-//   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5..7] 0
-//   units (8 words each)
-//   rel_off[nrel] (byte offset of the released row), rel_kind[nrel] (0 primal, 1 constraint),
-//   rel_rho[nrel], rel_rhoinv[nrel] (float bits)
-// Forward chunk meta block: [0] nunits [1..7] 0, units.
+//   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5] nprim [6..7] 0
+//   units (8 words each), then one sentinel unit (loaded ahead, never used)
+//   rel_off[nrel] (byte offset of the released row; the nprim primal indices
+//   first), rel_rho[nrel], rel_rhoinv[nrel] (float bits)
+// Forward chunk meta block: [0] nunits [1..7] 0, units, sentinel.
 // Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
+// Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
 
 struct StreamPlan {
   int n;              // KKT dimension
@@ -76,6 +79,7 @@ struct StreamPlan {
   const int* u_perm;        // [n] U index -> permuted KKT index
   const int* u_orig;        // [n] U index -> original KKT index
   int max_row_nnz;
+  int max_lstages, max_sstages;  // ring depth limits (tuning; defaults 12 and 6)
 };
 
 // ---- PTX helpers -----------------------------------------------------------
