@@ -15,6 +15,8 @@ import numpy as np
 KHDR = 8  # chunk meta header words
 KUW = 8  # words per unit
 FIRST, LAST, FWD = 1, 2, 4
+DSHIFT = 8  # flags word: flags | D^-1 byte offset << 8
+NSENT = 4  # sentinel units per chunk
 
 
 def _f32(x):
@@ -127,56 +129,61 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         return byte_off // 128
 
     def run_units(m, nu, stage, backward):
-        """The consumer's unit loop: unit u+1 (u+1 == nu: the sentinel) is loaded
-        before unit u's arithmetic and store."""
-        assert 1 <= nu and KHDR + (nu + 1) * KUW <= m.size
-        units = m[KHDR : KHDR + (nu + 1) * KUW].reshape(nu + 1, KUW)
-        sent = units[nu]
-        assert np.all(sent[:5] == n * 128) and sent[5] == 0 and sent[7] == (n + 1) * 128
+        """The consumer's unit loop: units are computed in groups of 3, unit
+        u+1's operands loaded before unit u's arithmetic and store; units past
+        nu are sentinels (zero-row reads, unit 0's L values, trash-row
+        stores)."""
+        ncomp = -(-nu // 3) * 3
+        assert 1 <= nu and KHDR + (nu + NSENT) * KUW <= m.size and ncomp + 1 < nu + NSENT
+        units = m[KHDR : KHDR + (nu + NSENT) * KUW].reshape(nu + NSENT, KUW)
+        for sent in units[nu:]:
+            assert np.all(sent[:5] == n * 128) and sent[5] == 0 and sent[6] == 0 and sent[7] == (n + 1) * 128
         nfl = stage.size
 
         def load(u):
             src, ctl = units[u, :4], units[u, 4:]
-            lo = u * 128
-            lv = stage[lo : lo + 128].reshape(lanes, 4).T.copy() if u < nu else None  # [slot][lane]
+            lo = int(ctl[2])
+            assert lo % 512 == 0 and lo // 4 + 128 <= nfl
+            assert lo == (u * 512 if u < nu else 0)
+            lv = stage[lo // 4 : lo // 4 + 128].reshape(lanes, 4).T.copy()  # [slot][lane]
             xs = [X[xrow(o)].copy() for o in src]
             t = X[xrow(ctl[0])].copy()
             d = None
-            if backward and u < nu:
-                doff = int(ctl[2])
+            if backward:
+                doff = int(ctl[1]) >> DSHIFT
                 assert doff % 4 == 0 and doff // 4 + 32 <= nfl
                 d = stage[doff // 4 : doff // 4 + 32].copy()
             if u < nu:
-                assert lo + 128 <= nfl
                 assert xrow(ctl[3]) == (xrow(ctl[0]) if int(ctl[1]) & LAST else n + 1)
             return ctl, lv, xs, t, d
 
         cur = load(0)
         acc = np.zeros(lanes, np.float32)
         prev = np.zeros(lanes, np.float32)
-        for u in range(nu):
-            nxt = load(u + 1)
-            ctl, lv, xs, t, d = cur
-            fl = int(ctl[1])
-            if backward:
-                x0 = prev if fl & FWD else xs[0]
-                acc = np.zeros(lanes, np.float32) if fl & FIRST else acc
-                acc = acc + lv[0] * x0
-                acc = acc + lv[1] * xs[1]
-                acc = acc + lv[2] * xs[2]
-                acc = acc + lv[3] * xs[3]
-                res = t * d - acc
-            else:
-                x3 = prev if fl & FWD else xs[3]
-                acc = t if fl & FIRST else acc
-                acc = acc - lv[0] * xs[0]
-                acc = acc - lv[1] * xs[1]
-                acc = acc - lv[2] * xs[2]
-                acc = acc - lv[3] * x3
-                res = acc
-            X[xrow(ctl[3])] = res
-            prev = res
-            cur = nxt
+        with np.errstate(all="ignore"):
+            for u in range(ncomp):
+                nxt = load(u + 1)
+                ctl, lv, xs, t, d = cur
+                fl = int(ctl[1])
+                if backward:
+                    x0 = prev if fl & FWD else xs[0]
+                    acc = np.zeros(lanes, np.float32) if fl & FIRST else acc
+                    acc = acc + lv[0] * x0
+                    acc = acc + lv[1] * xs[1]
+                    acc = acc + lv[2] * xs[2]
+                    acc = acc + lv[3] * xs[3]
+                    res = t * d - acc
+                else:
+                    x3 = prev if fl & FWD else xs[3]
+                    acc = t if fl & FIRST else acc
+                    acc = acc - lv[0] * xs[0]
+                    acc = acc - lv[1] * xs[1]
+                    acc = acc - lv[2] * xs[2]
+                    acc = acc - lv[3] * x3
+                    res = acc
+                X[xrow(ctl[3])] = res
+                prev = res
+                cur = nxt
 
     items = [(0, nch - 1 - t) for t in range(nch)]
     for _ in range(iters):
@@ -195,7 +202,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         assert nu == sched["chunk_units"][ch] and ncols == sched["chunk_cols"][ch] and nrel == sched["chunk_nrel"][ch]
         assert u0 == sched["chunk_u0"][ch] and nu <= sched["max_units"] and ncols <= sched["max_cols"]
         assert nrel <= sched["max_rel"] and 0 <= u0 and u0 + nrel <= n and 0 <= nprim <= nrel
-        r = KHDR + (nu + 1) * KUW
+        r = KHDR + (nu + NSENT) * KUW
         assert r + 3 * nrel <= m.size
         rel_i = m[r : r + nrel]
         rel_rho = m[r + nrel : r + 2 * nrel].view(np.float32)

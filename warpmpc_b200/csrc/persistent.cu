@@ -203,31 +203,43 @@ __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int ssta
 
 // One unit's operands, loaded ahead of its arithmetic.
 struct UnitOps {
-  int4 src, ctl;  // ctl: target byte offset, flags, D^-1 byte offset, store byte offset
+  int4 src, ctl;  // meta; ctl: target byte offset, flags | D^-1 offset, L offset, store byte offset
   float4 l;
   float x0, x1, x2, x3, t, d;
 };
 
-// mu: this unit's meta (2 x int4); lq: this lane's 4 L values of the unit
+__device__ __forceinline__ void load_meta(const int4* __restrict__ mu, int u, UnitOps& r) {
+  r.src = mu[2 * u];
+  r.ctl = mu[2 * u + 1];
+}
+
+// lane_l: this lane's 16 bytes of unit 0 of the stage (lst + lane * 16)
 template <bool kBackward>
-__device__ __forceinline__ void load_unit(const int4* __restrict__ mu, const float4* lq, const unsigned char* lst,
+__device__ __forceinline__ void load_data(const unsigned char* lane_l, const unsigned char* lst,
                                           const unsigned char* xb, int lane, UnitOps& r) {
-  r.src = mu[0];
-  r.ctl = mu[1];
-  r.l = *lq;
+  r.l = *reinterpret_cast<const float4*>(lane_l + r.ctl.z);
   r.x0 = *reinterpret_cast<const float*>(xb + r.src.x);
   r.x1 = *reinterpret_cast<const float*>(xb + r.src.y);
   r.x2 = *reinterpret_cast<const float*>(xb + r.src.z);
   r.x3 = *reinterpret_cast<const float*>(xb + r.src.w);
   r.t = *reinterpret_cast<const float*>(xb + r.ctl.x);
-  if (kBackward) r.d = *reinterpret_cast<const float*>(lst + r.ctl.z + lane * 4);
+  if (kBackward) r.d = *reinterpret_cast<const float*>(lst + (r.ctl.y >> kUnitDoffShift) + lane * 4);
+}
+
+// flags & mask ? a : b, as a predicated select (no branch)
+__device__ __forceinline__ float select_flag(int flags, int mask, float a, float b) {
+  float r;
+  asm("{\n\t.reg .pred p;\n\t.reg .b32 t;\n\tand.b32 t, %1, %2;\n\tsetp.ne.b32 p, t, 0;\n\tselp.f32 %0, %3, %4, p;\n\t}"
+      : "=f"(r)
+      : "r"(flags), "r"(mask), "f"(a), "f"(b));
+  return r;
 }
 
 // Forward unit: acc = (first ? rhs_i : acc) - L_i,c0 x_c0 - ... (ascending c)
 __device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, float& acc, float& prev) {
   const int fl = r.ctl.y;
-  const float x3 = (fl & kUnitFwd) ? prev : r.x3;
-  acc = (fl & kUnitFirst) ? r.t : acc;
+  const float x3 = select_flag(fl, kUnitFwd, prev, r.x3);
+  acc = select_flag(fl, kUnitFirst, r.t, acc);
   acc = acc - r.l.x * r.x0;
   acc = acc - r.l.y * r.x1;
   acc = acc - r.l.z * r.x2;
@@ -240,8 +252,8 @@ __device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb
 // x_j = x_j D^-1_j - corr
 __device__ __forceinline__ void backward_unit(const UnitOps& r, unsigned char* xb, float& corr, float& prev) {
   const int fl = r.ctl.y;
-  const float x0 = (fl & kUnitFwd) ? prev : r.x0;
-  corr = (fl & kUnitFirst) ? 0.0f : corr;
+  const float x0 = select_flag(fl, kUnitFwd, prev, r.x0);
+  corr = select_flag(fl, kUnitFirst, 0.0f, corr);
   corr = corr + r.l.x * x0;
   corr = corr + r.l.y * r.x1;
   corr = corr + r.l.z * r.x2;
@@ -251,21 +263,116 @@ __device__ __forceinline__ void backward_unit(const UnitOps& r, unsigned char* x
   prev = res;
 }
 
-// Run a chunk's units, unit u+1's loads issued before unit u's arithmetic and
-// store (two register sets, alternating; unit nu is the sentinel).
+// Run a chunk's units as a software pipeline: while unit u is computed and
+// stored, unit u+1's operands and unit u+2's meta are already loaded (three
+// register sets in rotation, one exit test per three units).  The units past
+// nu are sentinels: computed when nu is not a multiple of 3, harmlessly (they
+// store to the trash row, and acc/prev are dead after the chunk).
 template <bool kBackward>
 __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const unsigned char* lst, unsigned char* xb,
                                           int lane, int nu) {
-  const float4* lq = reinterpret_cast<const float4*>(lst + lane * 16);
-  UnitOps A, B;
+  static_assert(kUnitGroup == 3 && kUnitSentinels >= 4, "loop shape and sentinel count disagree");
+  const unsigned char* lane_l = lst + lane * 16;
+  UnitOps A, B, C;
   float acc = 0.0f, prev = 0.0f;
-  load_unit<kBackward>(mu, lq, lst, xb, lane, A);
-  for (int u = 0; u < nu; u += 2) {
-    load_unit<kBackward>(mu + 2 * (u + 1), lq + 32 * (u + 1), lst, xb, lane, B);
+  load_meta(mu, 0, A);
+  load_data<kBackward>(lane_l, lst, xb, lane, A);
+  load_meta(mu, 1, B);
+  for (int u = 0; u < nu; u += 3) {
+    load_meta(mu, u + 2, C);
+    load_data<kBackward>(lane_l, lst, xb, lane, B);
     if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit(A, xb, acc, prev);
-    if (u + 1 >= nu) break;
-    load_unit<kBackward>(mu + 2 * (u + 2), lq + 32 * (u + 2), lst, xb, lane, A);
+    load_meta(mu, u + 3, A);
+    load_data<kBackward>(lane_l, lst, xb, lane, C);
     if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit(B, xb, acc, prev);
+    load_meta(mu, u + 4, B);
+    load_data<kBackward>(lane_l, lst, xb, lane, A);
+    if (kBackward) backward_unit(C, xb, acc, prev); else forward_unit(C, xb, acc, prev);
+  }
+}
+
+// Releases of a backward chunk in groups of 4, the next group's operands
+// loaded before the current group is computed and stored (every index is
+// released once per pass, so groups never share a row).  A group slot past
+// `end` repeats the group's first index: it loads the same operands, computes
+// the same values and stores them to the same places again.
+struct RelGroup {
+  int o[4], kk[4];
+  float x[4], s0[4], s1[4], p0[4], p1[4], rho[4], rinv[4];
+};
+
+template <bool kCons>
+__device__ __forceinline__ void load_rel_group(const int* rel_off, const float* rel_rho, const float* rel_rinv,
+                                               int k, int end, const float* S0, const float* S1, const float* P0,
+                                               const float* P1, const unsigned char* xb, RelGroup& g) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int kk = (k + j < end) ? k + j : k;
+    g.kk[j] = kk;
+    g.o[j] = rel_off[kk];
+    g.x[j] = *reinterpret_cast<const float*>(xb + g.o[j]);
+    g.s0[j] = S0[kk * 32];
+    g.p0[j] = P0[kk * 32];
+    if (kCons) {
+      g.s1[j] = S1[kk * 32];
+      g.p1[j] = P1[kk * 32];
+      g.rho[j] = rel_rho[kk];
+      g.rinv[j] = rel_rinv[kk];
+    }
+  }
+}
+
+struct RelParams {
+  float sigma, alpha, oma;
+};
+
+// primal index: x <- alpha x~ + (1 - alpha) x; next rhs sigma x - q
+// constraint: z, y update and next rhs z - rho^-1 y (solver.py:806-820)
+template <bool kCons>
+__device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
+                                                 float* s0u, float* s1u) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    float* xi = reinterpret_cast<float*>(xb + g.o[j]);
+    if (!kCons) {
+      const float xn = rp.alpha * g.x[j] + rp.oma * g.s0[j];
+      s0u[g.kk[j] * 32] = xn;
+      *xi = rp.sigma * xn - g.p0[j];
+    } else {
+      const float rinv = g.rinv[j];
+      const float sv0 = g.s0[j], yk = g.s1[j];
+      const float rz = sv0 - rinv * yk;
+      const float zt = rz + rinv * g.x[j];
+      const float zr = rp.alpha * zt + rp.oma * sv0;
+      float zn = zr + rinv * yk;
+      zn = (zn < g.p0[j]) ? g.p0[j] : zn;
+      zn = (zn > g.p1[j]) ? g.p1[j] : zn;
+      const float yn = yk + g.rho[j] * (zr - zn);
+      s0u[g.kk[j] * 32] = zn;
+      s1u[g.kk[j] * 32] = yn;
+      *xi = zn - rinv * yn;
+    }
+  }
+}
+
+template <bool kCons>
+__device__ __forceinline__ void run_releases(const int* rel_off, const float* rel_rho, const float* rel_rinv,
+                                             int begin, int end, const float* S0, const float* S1, const float* P0,
+                                             const float* P1, const RelParams& rp, unsigned char* xb, float* s0u,
+                                             float* s1u) {
+  if (begin >= end) return;
+  RelGroup a, b;
+  load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, begin, end, S0, S1, P0, P1, xb, a);
+  for (int k = begin;; k += 8) {
+    // a group starting at or past `end` clamps to end - 1 (loads only)
+    const int kb = k + 4 < end ? k + 4 : end - 1;
+    load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, kb, end, S0, S1, P0, P1, xb, b);
+    update_rel_group<kCons>(a, rp, xb, s0u, s1u);
+    if (k + 4 >= end) break;
+    const int ka = k + 8 < end ? k + 8 : end - 1;
+    load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, ka, end, S0, S1, P0, P1, xb, a);
+    update_rel_group<kCons>(b, rp, xb, s0u, s1u);
+    if (k + 8 >= end) break;
   }
 }
 
@@ -382,7 +489,7 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
           // backward substitution, column form, columns in reverse order
           if (kind == kItemBwd) run_units<true>(mu, lst, xw, lane, nu);
           // releases: ADMM update (backward items) or first right-hand side
-          const int* rel_off = meta + kChunkHeader + (nu + 1) * kUnitWords;
+          const int* rel_off = meta + kChunkHeader + (nu + kUnitSentinels) * kUnitWords;
           const float* rel_rho = reinterpret_cast<const float*>(rel_off + nrel);
           const float* rel_rinv = rel_rho + nrel;
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
@@ -398,28 +505,9 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
             for (int k = nprim; k < nrel; ++k)
               *reinterpret_cast<float*>(xw + rel_off[k]) = S0[k * 32] - rel_rinv[k] * S1[k * 32];
           } else {
-            for (int k = 0; k < nprim; ++k) {
-              float* xi = reinterpret_cast<float*>(xw + rel_off[k]);
-              const float xn = alpha * *xi + oma * S0[k * 32];
-              s0u[k * 32] = xn;
-              *xi = sigma * xn - P0[k * 32];
-            }
-            for (int k = nprim; k < nrel; ++k) {
-              float* xi = reinterpret_cast<float*>(xw + rel_off[k]);
-              const float sol = *xi;
-              const float sv0 = S0[k * 32], yk = S1[k * 32], lo = P0[k * 32], hi = P1[k * 32];
-              const float rinv = rel_rinv[k];
-              const float rz = sv0 - rinv * yk;
-              const float zt = rz + rinv * sol;
-              const float zr = alpha * zt + oma * sv0;
-              float zn = zr + rinv * yk;
-              zn = (zn < lo) ? lo : zn;
-              zn = (zn > hi) ? hi : zn;
-              const float yn = yk + rel_rho[k] * (zr - zn);
-              s0u[k * 32] = zn;
-              s1u[k * 32] = yn;
-              *xi = zn - rinv * yn;
-            }
+            const RelParams rp{sigma, alpha, oma};
+            run_releases<false>(rel_off, rel_rho, rel_rinv, 0, nprim, S0, S1, P0, P1, rp, xw, s0u, s1u);
+            run_releases<true>(rel_off, rel_rho, rel_rinv, nprim, nrel, S0, S1, P0, P1, rp, xw, s0u, s1u);
           }
           // order these generic-proxy state writes before the bulk copies
           // that read them back in the next iteration
@@ -466,7 +554,7 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
   const int meta_bytes = ((mw * 4 + 127) / 128) * 128;
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
-  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128 + 512;  // + the sentinel unit's reads
+  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
   const int sbytes = 4 * (sp.max_rel > 0 ? sp.max_rel : 1) * 128;
   // prefer deep rings: as many L stages as fit with at least 3 S stages
   const int lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;

@@ -137,22 +137,28 @@ int append_units(std::vector<UnitBuild>* chunk, std::vector<UnitBuild> add, int 
   return first;
 }
 
-void push_unit_meta(const UnitBuild& ub, int trash_row, std::vector<int>* m) {
+// Meta of unit `u` of its chunk (see stream.cuh for the word layout).
+void push_unit_meta(const UnitBuild& ub, int u, int trash_row, std::vector<int>* m) {
   for (int s = 0; s < 4; ++s) m->push_back(ub.src[s] * 128);
   m->push_back(ub.target * 128);
-  m->push_back(ub.flags);
-  m->push_back(ub.doff);
+  m->push_back(ub.flags | (ub.doff << kUnitDoffShift));
+  m->push_back(u * 512);
   m->push_back(((ub.flags & kUnitLast) ? ub.target : trash_row) * 128);
 }
 
-// Meta of the sentinel unit after a chunk's last unit: the consumer loads one
-// unit ahead, so unit `nunits` is read (never computed).
-void push_sentinel_meta(int zero_row, int trash_row, std::vector<int>* m) {
-  for (int s = 0; s < 4; ++s) m->push_back(zero_row * 128);
-  m->push_back(zero_row * 128);
-  m->push_back(0);
-  m->push_back(0);
-  m->push_back(trash_row * 128);
+// Meta of the sentinel units after a chunk's last unit.  The consumer
+// computes units in groups of kUnitGroup and loads operands one unit and meta
+// two units ahead, so up to kUnitSentinels units past the last one are read
+// and some computed: they read the zero row and unit 0's L values, and store
+// to the trash row.
+void push_sentinels(int zero_row, int trash_row, std::vector<int>* m) {
+  for (int k = 0; k < kUnitSentinels; ++k) {
+    for (int s = 0; s < 4; ++s) m->push_back(zero_row * 128);
+    m->push_back(zero_row * 128);
+    m->push_back(0);
+    m->push_back(0);
+    m->push_back(trash_row * 128);
+  }
 }
 
 }  // namespace
@@ -266,8 +272,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     int nprim = 0;
     for (int u = u0; u < u0 + nrel; ++u) nprim += hp.p[order[u]] < n_primal ? 1 : 0;
     std::vector<int> m{nu, c1 - c0, nrel, c0, u0, nprim, 0, 0};
-    for (const UnitBuild& ub : units) push_unit_meta(ub, trash_row, &m);
-    push_sentinel_meta(zero_row, trash_row, &m);
+    for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
+    push_sentinels(zero_row, trash_row, &m);
     std::vector<int> rel_i, rel_rho, rel_rinv;
     for (int u = u0; u < u0 + nrel; ++u) {
       const int i = order[u];
@@ -354,8 +360,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       if (nu == 0) continue;
       for (const auto& pe : placed) entry_foff[pe.first] = foff + (pe.second >> 2) * 128 + (pe.second & 3);
       std::vector<int> m{nu, 0, 0, 0, 0, 0, 0, 0};
-      for (const UnitBuild& ub : units) push_unit_meta(ub, trash_row, &m);
-      push_sentinel_meta(zero_row, trash_row, &m);
+      for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
+      push_sentinels(zero_row, trash_row, &m);
       S.fchunk_off.push_back(foff);
       S.fchunk_units.push_back(nu);
       S.fmeta_off.push_back(static_cast<int>(S.fmeta.size()));

@@ -27,20 +27,24 @@ namespace wmpc {
 // (backward), stored per tile as [unit][lane][4] floats (512 bytes).  Unit
 // meta (8 int32 words): byte offsets (row * 128) of the 4 work-vector rows the
 // slots read; the target row's byte offset (read: right-hand side / x_j);
-// flags; the D^-1 byte offset (backward; relative to the stage's L area);
-// the byte offset the result is stored to (the target on a row's / column's
-// last unit, the trash row n + 1 otherwise).
+// flags | D^-1 byte offset << kUnitDoffShift (backward; relative to the
+// stage's L area); the unit's L byte offset in the stage; the byte offset the
+// result is stored to (the target on a row's / column's last unit, the trash
+// row n + 1 otherwise).
 constexpr int kUnitFirst = 1;  // first unit of its row/column: start the sum
 constexpr int kUnitLast = 2;   // last unit: the stored result is final
 constexpr int kUnitFwd = 4;    // the forwarding slot (3 forward, 0 backward) reads the previous unit's result
+constexpr int kUnitDoffShift = 8;
 constexpr int kUnitWords = 8;
+constexpr int kUnitGroup = 3;      // units computed per loop trip
+constexpr int kUnitSentinels = 4;  // sentinel units after a chunk's last unit
 constexpr int kChunkHeader = 8;
 // Backward chunk meta block (int32 words, 16-byte padded):
 //   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5] nprim [6..7] 0
-//   units (8 words each), then one sentinel unit (loaded ahead, never used)
+//   units (8 words each), then kUnitSentinels sentinel units
 //   rel_off[nrel] (byte offset of the released row; the nprim primal indices
 //   first), rel_rho[nrel], rel_rhoinv[nrel] (float bits)
-// Forward chunk meta block: [0] nunits [1..7] 0, units, sentinel.
+// Forward chunk meta block: [0] nunits [1..7] 0, units, sentinels.
 // Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
 // Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
 
@@ -157,8 +161,8 @@ struct HostPattern {
 };
 
 struct StreamTargets {
-  int units = 12, cols = 12, rel = 8;  // backward chunks
-  int funits = 12;                     // forward chunks
+  int units = 16, cols = 16, rel = 12;  // backward chunks
+  int funits = 16;                      // forward chunks
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.

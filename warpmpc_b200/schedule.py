@@ -15,7 +15,7 @@ import numpy as np
 from . import native
 from .jax_qdldl.planning import plan_ragged_program
 
-DEFAULT_TARGETS = (12, 12, 8, 12)  # backward units, columns, releases; forward units
+DEFAULT_TARGETS = (16, 16, 12, 16)  # backward units, columns, releases; forward units
 
 
 def _pattern_desc(qp):
