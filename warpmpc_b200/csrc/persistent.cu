@@ -198,7 +198,7 @@ __device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_it
 __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
   return (size_t)(n + 2) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
-         16 * (size_t)(lstages + sstages) + 16;
+         16 * (size_t)(lstages + sstages) + 16;  // barriers, abort flag and the two counters
 }
 
 // One unit's operands, loaded ahead of its arithmetic.
@@ -376,7 +376,15 @@ __device__ __forceinline__ void run_releases(const int* rel_off, const float* re
   }
 }
 
-__global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
+// Shared-memory layout: X [n + 2][32] | L ring | S ring | barriers | flags.
+// Warps: 0 sweeps (forward and backward units), 1 produces (bulk copies),
+// 2 releases (first right-hand side, ADMM updates).  Every warp walks the same
+// item sequence; item t's L stage is freed by the warp that finishes with it
+// last (forward: sweeper; backward and first-rhs: releaser).  Two monotone
+// counters order the consumers: sweep_done (items the sweeper finished: a
+// backward item's releases need its columns solved) and rel_done (items the
+// releaser finished: a forward sweep needs every right-hand side).
+__global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const StreamPlan& sp = a.sp;
   const int n = sp.n;
@@ -389,7 +397,8 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
   uint64_t* sfull = lempty + a.lstages;
   uint64_t* sempty = sfull + a.sstages;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sempty + a.sstages);
-  volatile int* consumed_ctr = abort_flag + 1;
+  unsigned* sweep_done = reinterpret_cast<unsigned*>(sempty + a.sstages) + 1;
+  unsigned* rel_done = sweep_done + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
@@ -401,19 +410,19 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
       mbar_init(sempty + s, 1);
     }
     *abort_flag = 0;
-    *consumed_ctr = 0;
+    *sweep_done = 0;
+    *rel_done = 0;
     fence_mbarrier_init();
   }
   if (warp == 0) X[n * 32 + lane] = 0.0f;  // zero row read by padding slots
   __syncthreads();
 
-  uint32_t issued_l = 0, issued_s = 0;
+  uint32_t issued_l = 0, issued_s = 0;  // producer: copies issued per ring
 
   if (warp == 1) {
     // ------------------------------ producer ------------------------------
     if (lane == 0) {
       Ring lr{0, 0}, sr{0, 0};
-      uint32_t nl = 0, ns = 0;  // fills issued so far (ring reuse starts after one full lap)
       for (int tile = blockIdx.x; tile < a.n_tiles && !*abort_flag; tile += gridDim.x) {
         const float* bt = a.bstream + (size_t)tile * sp.blen;
         const float* ft = a.fstream + (size_t)tile * sp.flen;
@@ -426,17 +435,18 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
           uint32_t lbytes = 0;
           if (fwd) lbytes = (uint32_t)__ldg(sp.fchunk_units + ch) * 512u;
           if (kind == kItemBwd) lbytes = (uint32_t)__ldg(sp.chunk_units + ch) * 512u + (uint32_t)__ldg(sp.chunk_cols + ch) * 128u;
-          if (nl >= (uint32_t)a.lstages && !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
+          if (issued_l >= (uint32_t)a.lstages &&
+              !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
             return false;
           unsigned char* st = lring + (size_t)lr.stage * lstage_bytes;
           mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes);
           bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + moff, (uint32_t)mwords * 4u, lfull + lr.stage);
           if (lbytes) bulk_g2s(st + a.meta_bytes, (fwd ? ft : bt) + loff, lbytes, lfull + lr.stage);
           lr.advance(a.lstages);
-          ++nl;
           ++issued_l;
           if (!fwd) {
-            if (ns >= (uint32_t)a.sstages && !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
+            if (issued_s >= (uint32_t)a.sstages &&
+                !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
             const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 128u;
@@ -450,7 +460,6 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
               bulk_g2s(ss + 3 * quarter, a.p1 + off, bytes, sfull + sr.stage);
             }
             sr.advance(a.sstages);
-            ++ns;
             ++issued_s;
           }
           return true;
@@ -461,34 +470,65 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
         }
       }
     }
+  } else if (warp == 0) {
+    // ------------------------------ sweeper ------------------------------
+    Ring lr{0, 0};
+    unsigned t = 0;  // item index (all tiles)
+    unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
+      auto sweep = [&](int kind, int ch) -> bool {
+        if (kind != kItemRel) {
+          // a forward sweep needs every right-hand side of the previous pass
+          if (kind == kItemFwd && ch == 0 && !wait_counter_bounded(rel_done, t, abort_flag, kWaitLimitNs))
+            return false;
+          if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) return false;
+          const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
+          const int* meta = reinterpret_cast<const int*>(stage);
+          const unsigned char* lst = stage + a.meta_bytes;
+          const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
+          const int nu = meta[0];
+          if (kind == kItemFwd) {
+            run_units<false>(mu, lst, xb, lane, nu);  // forward substitution, row-gather form
+          } else {
+            run_units<true>(mu, lst, xb, lane, nu);   // backward substitution, column form
+          }
+          __syncwarp();
+          if (lane == 0) {
+            if (kind == kItemFwd) mbar_arrive(lempty + lr.stage);
+            st_release_cta(sweep_done, t + 1);
+          }
+          __syncwarp();
+        }
+        lr.advance(a.lstages);
+        ++t;
+        return true;
+      };
+      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, sweep)) ok = false;
+    }
+    if (!ok && lane == 0) *abort_flag = 1;
   } else {
-    // ------------------------------ consumer ------------------------------
+    // ------------------------------ releaser ------------------------------
     Ring lr{0, 0}, sr{0, 0};
-    uint32_t consumed = 0;
+    unsigned t = 0;
     const float sigma = a.sigma, alpha = a.alpha, oma = a.one_minus_alpha;
-    const unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
+    unsigned char* xb = smem + lane * 4;
     bool ok = true;
     const int quarter_f = a.sbytes / 16;  // floats per S array
     for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
       float* s0t = a.s0 + (size_t)tile * n * 32 + lane;
       float* s1t = a.s1 + (size_t)tile * n * 32 + lane;
-      auto consume = [&](int kind, int ch) -> bool {
+      auto release = [&](int kind, int ch) -> bool {
         (void)ch;
-        if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) return false;
-        const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
-        const int* meta = reinterpret_cast<const int*>(stage);
-        const unsigned char* lst = stage + a.meta_bytes;
-        const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
-        const int nu = meta[0];
-        unsigned char* xw = const_cast<unsigned char*>(xb);
-        if (kind == kItemFwd) {
-          // forward substitution, row-gather form
-          run_units<false>(mu, lst, xw, lane, nu);
-        } else {
-          const int nrel = meta[2], u0 = meta[4], nprim = meta[5];
-          // backward substitution, column form, columns in reverse order
-          if (kind == kItemBwd) run_units<true>(mu, lst, xw, lane, nu);
-          // releases: ADMM update (backward items) or first right-hand side
+        if (kind != kItemFwd) {
+          if (kind == kItemBwd) {
+            // the chunk's columns are solved (and its stage is full)
+            if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, kWaitLimitNs)) return false;
+          } else if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) {
+            return false;
+          }
+          const int* meta = reinterpret_cast<const int*>(lring + (size_t)lr.stage * lstage_bytes);
+          const int nu = meta[0], nrel = meta[2], u0 = meta[4], nprim = meta[5];
           const int* rel_off = meta + kChunkHeader + (nu + kUnitSentinels) * kUnitWords;
           const float* rel_rho = reinterpret_cast<const float*>(rel_off + nrel);
           const float* rel_rinv = rel_rho + nrel;
@@ -497,48 +537,53 @@ __global__ void __launch_bounds__(64, 1) admm_stream_kernel(StreamArgs a) {
           const float* S1 = S0 + quarter_f;
           const float* P0 = S1 + quarter_f;
           const float* P1 = P0 + quarter_f;
-          float* s0u = s0t + (size_t)u0 * 32;
-          float* s1u = s1t + (size_t)u0 * 32;
           if (kind == kItemRel) {
+            // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
             for (int k = 0; k < nprim; ++k)
-              *reinterpret_cast<float*>(xw + rel_off[k]) = sigma * S0[k * 32] - P0[k * 32];
+              *reinterpret_cast<float*>(xb + rel_off[k]) = sigma * S0[k * 32] - P0[k * 32];
             for (int k = nprim; k < nrel; ++k)
-              *reinterpret_cast<float*>(xw + rel_off[k]) = S0[k * 32] - rel_rinv[k] * S1[k * 32];
+              *reinterpret_cast<float*>(xb + rel_off[k]) = S0[k * 32] - rel_rinv[k] * S1[k * 32];
           } else {
+            float* s0u = s0t + (size_t)u0 * 32;
+            float* s1u = s1t + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false>(rel_off, rel_rho, rel_rinv, 0, nprim, S0, S1, P0, P1, rp, xw, s0u, s1u);
-            run_releases<true>(rel_off, rel_rho, rel_rinv, nprim, nrel, S0, S1, P0, P1, rp, xw, s0u, s1u);
+            run_releases<false>(rel_off, rel_rho, rel_rinv, 0, nprim, S0, S1, P0, P1, rp, xb, s0u, s1u);
+            run_releases<true>(rel_off, rel_rho, rel_rinv, nprim, nrel, S0, S1, P0, P1, rp, xb, s0u, s1u);
+            // order these generic-proxy state writes before the bulk copies
+            // that read them back in the next pass
+            fence_proxy_async_global();
           }
-          // order these generic-proxy state writes before the bulk copies
-          // that read them back in the next iteration
-          if (kind == kItemBwd) fence_proxy_async_global();
           __syncwarp();
-          if (lane == 0) mbar_arrive(sempty + sr.stage);
+          if (lane == 0) {
+            mbar_arrive(sempty + sr.stage);
+            mbar_arrive(lempty + lr.stage);
+          }
           sr.advance(a.sstages);
         }
         __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(lempty + lr.stage);
-          *consumed_ctr = (int)(consumed + 1);
-        }
+        if (lane == 0) st_release_cta(rel_done, t + 1);
+        __syncwarp();
         lr.advance(a.lstages);
-        ++consumed;
+        ++t;
         return true;
       };
-      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, consume)) ok = false;
+      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, release)) ok = false;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   }
   __syncthreads();
   if (*abort_flag) {
     if (threadIdx.x == 32) {
-      // drain: wait (bounded) for every bulk copy issued but not consumed
-      const uint32_t consumed = (uint32_t)*consumed_ctr;
-      for (uint32_t t = consumed; t < issued_l; ++t)
-        mbar_wait_bounded(lfull + t % a.lstages, (t / a.lstages) & 1u, nullptr, kWaitLimitNs);
-      const uint32_t s_lo = issued_s > (uint32_t)a.sstages ? issued_s - a.sstages : 0;
-      for (uint32_t t = s_lo; t < issued_s; ++t)
-        mbar_wait_bounded(sfull + t % a.sstages, (t / a.sstages) & 1u, nullptr, kWaitLimitNs);
+      // drain: wait (bounded) for the last bulk copy issued into every stage
+      // (earlier ones completed before their stage was reused)
+      for (uint32_t s = 0; s < (uint32_t)a.lstages && s < issued_l; ++s) {
+        const uint32_t last = s + (uint32_t)a.lstages * ((issued_l - 1 - s) / (uint32_t)a.lstages);
+        mbar_wait_bounded(lfull + s, (last / (uint32_t)a.lstages) & 1u, nullptr, kWaitLimitNs);
+      }
+      for (uint32_t s = 0; s < (uint32_t)a.sstages && s < issued_s; ++s) {
+        const uint32_t last = s + (uint32_t)a.sstages * ((issued_s - 1 - s) / (uint32_t)a.sstages);
+        mbar_wait_bounded(sfull + s, (last / (uint32_t)a.sstages) & 1u, nullptr, kWaitLimitNs);
+      }
     }
     if (threadIdx.x == 0) atomicExch(a.error, 1);
     __syncthreads();
@@ -613,7 +658,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   const int grid = n_tiles < num_sms ? n_tiles : num_sms;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
-  admm_stream_kernel<<<grid, 64, cfg.smem, s>>>(a);
+  admm_stream_kernel<<<grid, 96, cfg.smem, s>>>(a);
   profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
   {

@@ -144,6 +144,32 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// Shared-memory counters between warps of one CTA: release store / acquire load.
+__device__ __forceinline__ void st_release_cta(unsigned* p, unsigned v) {
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire_cta(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+
+// Bounded wait until *ctr >= target: gives up (false) after `limit_ns` or
+// when *abort is set.
+__device__ __forceinline__ bool wait_counter_bounded(const unsigned* ctr, unsigned target, const volatile int* abort,
+                                                     uint64_t limit_ns) {
+  if (ld_acquire_cta(ctr) >= target) return true;
+  const uint64_t start = global_timer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (ld_acquire_cta(ctr) >= target) return true;
+    if ((it & 255u) == 0) {
+      if (abort && *abort) return false;
+      if (global_timer_ns() - start > limit_ns) return false;
+    }
+  }
+}
+
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
