@@ -543,6 +543,7 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sp.max_fmeta_words = hs.max_fmeta_words;
       sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
       sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
+      sp.max_row_kv = hs.max_row_kv;
       sp.max_lstages = 12;
       sp.max_sstages = 6;
       if (const char* v = getenv("WMPC_STREAM_LSTAGES")) sp.max_lstages = atoi(v);
@@ -571,6 +572,8 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sk.add(hs.dinv_off.data(), hs.dinv_off.size(), &sp.dinv_off);
       sk.add(hs.proc_boff.data(), hs.proc_boff.size(), &sp.proc_boff);
       sk.add(hs.proc_foff.data(), hs.proc_foff.size(), &sp.proc_foff);
+      sk.add(hs.upd_pos.data(), hs.upd_pos.size(), &sp.upd_pos);
+      sk.add(hs.step_doff.data(), hs.step_doff.size(), &sp.step_doff);
       sk.add(hs.pad_boff.data(), hs.pad_boff.size(), &sp.pad_boff);
       sk.add(hs.pad_foff.data(), hs.pad_foff.size(), &sp.pad_foff);
       sk.add(hs.u_perm.data(), hs.u_perm.size(), &sp.u_perm);

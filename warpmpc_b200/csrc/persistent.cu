@@ -30,62 +30,132 @@ struct OsqpInputs {
   __device__ __forceinline__ float a(int j, int b) const { return aT[(long long)j * lda + (long long)b * sba]; }
 };
 
-__device__ __forceinline__ float kkt_value_at(const Osqp& o, const OsqpInputs& in, int s, int b) {
-  const int src = __ldg(o.kkt_src + s);
-  if (src < 0) return __ldg(o.kkt_base + s);
-  if (src < o.nnz_p) return in.p(src, b) * __ldg(o.p_scale + src) + __ldg(o.p_diag_sigma + src);
-  const int j = src - o.nnz_p;
-  return in.a(j, b) * __ldg(o.a_scale + j);
-}
 
 // ---------------------------------------------------------------------------
 // factorization into the stream layout
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(128) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
+// Per-warp shared memory of the factorization, in 4-byte words: per lane
+// (x 32) ys [max_row_nnz] (compact accumulator), staged D^-1 of the row's
+// steps [max_row_nnz], staged L re-reads [lbatch], staged raw KKT inputs
+// [max_row_kv]; shared by the warp: update slots [lbatch] and per-step
+// update counts, backward- and forward-stream offsets [3 x max_row_nnz].
+__host__ __device__ inline int factor_warp_words(const StreamPlan& sp, int lbatch) {
+  const int r = sp.max_row_nnz > 0 ? sp.max_row_nnz : 1;
+  return (2 * r + lbatch + sp.max_row_kv) * 32 + lbatch + 3 * r;
+}
+
+// KKT value of original slot idx from its staged raw input: the base value
+// (src < 0), P entry src scaled plus sigma on the diagonal, or A entry
+// src - nnz_p scaled (solver.py:764-776).
+__device__ __forceinline__ float staged_kkt_value(const Osqp& o, int idx, float raw) {
+  const int src = __ldg(o.kkt_src + idx);
+  if (src < 0) return __ldg(o.kkt_base + idx);
+  if (src < o.nnz_p) return raw * __ldg(o.p_scale + src) + __ldg(o.p_diag_sigma + src);
+  return raw * __ldg(o.a_scale + (src - o.nnz_p));
+}
+
+__device__ __forceinline__ int row_kkt_index(const Pattern& pat, int k, int i0, int j) {
+  return __ldg(pat.perm_to_orig + (j == 0 ? __ldg(pat.diag_pos + k) : __ldg(pat.init_pos + i0 + j - 1)));
+}
+
+// Up-looking LDL^T (QDLDL row program, warp_backend.py:41-101), one lane per
+// instance, one warp per tile.  Every value a row reads from memory -- its
+// KKT inputs, D^-1 of the columns it eliminates with, and the L entries of
+// those columns above the row (written by earlier rows) -- is independent of
+// the row's own arithmetic, so each row first stages them into shared memory
+// with asynchronous copies (one round trip per `lbatch` L entries), then
+// runs the program on shared memory.
+// Stage the L re-reads of updates [ub, ue): values per lane, slots warp-shared
+// (copied by all lanes in turn).
+__device__ __forceinline__ void stage_updates(const StreamPlan& sp, const float* Lu, float* lst, int* slot_w, int lane,
+                                              int ub, int ue) {
+  for (int u = ub; u < ue; ++u) cp_async4(lst + (u - ub) * 32, Lu + __ldg(sp.upd_pos + u));
+  for (int u = ub + lane; u < ue; u += 32) cp_async4(slot_w + (u - ub), sp.upd_slot + u);
+}
+
+__global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
                                                             float* __restrict__ bstream, float* __restrict__ fstream,
-                                                            int* __restrict__ status, int n_tiles, int batch) {
-  extern __shared__ float ys_all[];
+                                                            int* __restrict__ status, int n_tiles, int batch,
+                                                            int lbatch) {
+  extern __shared__ float fsm[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * (blockDim.x >> 5) + warp;
   if (tile >= n_tiles) return;
   const int b = tile * 32 + lane;
   const int bb = b < batch ? b : batch - 1;  // padding lanes factor a copy of the last instance
-  float* ys = ys_all + (size_t)warp * sp.max_row_nnz * 32 + lane;
+  const int rmax = sp.max_row_nnz > 0 ? sp.max_row_nnz : 1;
+  float* wbase = fsm + (size_t)warp * factor_warp_words(sp, lbatch);
+  float* ys = wbase + lane;
+  float* dst = ys + rmax * 32;
+  float* lst = dst + rmax * 32;
+  float* kst = lst + lbatch * 32;
+  int* slot_w = reinterpret_cast<int*>(wbase + (2 * rmax + lbatch + sp.max_row_kv) * 32);  // warp-shared
+  int* off_w = slot_w + lbatch;
+  int* boff_w = off_w + rmax;
+  int* foff_w = boff_w + rmax;
   float* Lb = bstream + (size_t)tile * sp.blen;
   float* F = fstream + (size_t)tile * sp.flen + lane * 4;
   float* Lu = Lb + lane * 4;  // unit entries: lane stride 4
   float* Ld = Lb + lane;      // D^-1 rows: lane stride 1
+  const float* pin = in.pT + (long long)bb * in.sbp;
+  const float* ain = in.aT + (long long)bb * in.sba;
   const int n = pat.n;
   bool bad = false;
   for (int k = 0; k < n; ++k) {
     const int p0 = __ldg(pat.proc_ptr + k), p1 = __ldg(pat.proc_ptr + k + 1);
-    for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
-    float dk = kkt_value_at(o, in, __ldg(pat.perm_to_orig + __ldg(pat.diag_pos + k)), bb);
     const int i0 = __ldg(pat.init_ptr + k), i1 = __ldg(pat.init_ptr + k + 1);
+    const int u_end = __ldg(sp.upd_ptr + p1);
+    int ub = __ldg(sp.upd_ptr + p0);
+    int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+    // stage this row's reads: KKT inputs, D^-1 of its steps, step tables, L re-reads
+    for (int j = 0; j < 1 + i1 - i0; ++j) {
+      const int src = __ldg(o.kkt_src + row_kkt_index(pat, k, i0, j));
+      if (src >= 0)
+        cp_async4(kst + j * 32, src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
+    }
+    for (int e = p0; e < p1; ++e) cp_async4(dst + (e - p0) * 32, Ld + __ldg(sp.step_doff + e));
+    for (int e = p0 + lane; e < p1; e += 32) {
+      cp_async4(off_w + (e - p0), pat.proc_offsets + e);
+      cp_async4(boff_w + (e - p0), sp.proc_boff + e);
+      cp_async4(foff_w + (e - p0), sp.proc_foff + e);
+    }
+    stage_updates(sp, Lu, lst, slot_w, lane, ub, ue);
+    cp_async_wait_all();
+    __syncwarp();
+    // the row program
+    for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
+    float dk = staged_kkt_value(o, row_kkt_index(pat, k, i0, 0), kst[0]);
     for (int e = i0; e < i1; ++e) {
       const int s = __ldg(sp.init_slot + e);
-      ys[s * 32] = ys[s * 32] + kkt_value_at(o, in, __ldg(pat.perm_to_orig + __ldg(pat.init_pos + e)), bb);
+      ys[s * 32] = ys[s * 32] + staged_kkt_value(o, row_kkt_index(pat, k, i0, 1 + e - i0), kst[(1 + e - i0) * 32]);
     }
-    for (int e = p0; e < p1; ++e) {
-      const int c = __ldg(pat.proc_cols + e);
-      const int off = __ldg(pat.proc_offsets + e);
-      const float* col = Lu + __ldg(sp.col_uoff + c);
-      const int u0 = __ldg(sp.upd_ptr + e);
-      const float val = ys[(e - p0) * 32];
-      for (int q = 0; q < off; ++q) {
-        const int s = __ldg(sp.upd_slot + u0 + q);
-        ys[s * 32] = ys[s * 32] - col[(q >> 2) * 128 + (q & 3)] * val;
+    int u = ub;
+    for (int e = 0; e < p1 - p0; ++e) {
+      const int off = off_w[e];
+      const float val = ys[e * 32];
+      for (int q = 0; q < off; ++q, ++u) {
+        if (u == ue) {  // next batch of this row's L re-reads
+          __syncwarp();
+          ub = ue;
+          ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+          stage_updates(sp, Lu, lst, slot_w, lane, ub, ue);
+          cp_async_wait_all();
+          __syncwarp();
+        }
+        const int su = slot_w[u - ub];
+        ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
       }
-      const float lval = val * Ld[__ldg(sp.dinv_off + c)];
-      Lu[__ldg(sp.proc_boff + e)] = lval;
-      F[__ldg(sp.proc_foff + e)] = lval;
+      const float lval = val * dst[e * 32];
+      Lu[boff_w[e]] = lval;
+      F[foff_w[e]] = lval;
       dk = dk - val * lval;
     }
     const float di = 1.0f / dk;
     bad |= !(di != 0.0f) || !isfinite(di);
     Ld[__ldg(sp.dinv_off + k)] = di;
+    __syncwarp();  // the warp-shared tables are restaged by the next row
   }
   for (int i = 0; i < sp.n_pad_b; ++i) Lu[__ldg(sp.pad_boff + i)] = 0.0f;
   for (int i = 0; i < sp.n_pad_f; ++i) F[__ldg(sp.pad_foff + i)] = 0.0f;
@@ -641,11 +711,18 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   float* p1 = p0 + tl * sp.n;
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
   if (!reuse_factor) {
-    const int warps = 4;
-    const size_t smem = (size_t)warps * (sp.max_row_nnz > 0 ? sp.max_row_nnz : 1) * 32 * sizeof(float);
+    // L-batch sized so that every tile's warp is resident at once (all of a
+    // launch's rows then wait out their round trips together)
+    const int warps = 2;
+    const int per_sm = ceil_div(n_tiles, num_sms > 0 ? num_sms : 1);
+    const int budget_floats = (200 * 1024 / 4) / (per_sm > 0 ? per_sm : 1);
+    int lbatch = (budget_floats - factor_warp_words(sp, 0)) / 33;
+    lbatch = lbatch < 8 ? 8 : (lbatch > 128 ? 128 : lbatch);
+    const size_t smem = (size_t)warps * factor_warp_words(sp, lbatch) * sizeof(float);
+    if (smem > (size_t)kMaxSmemBytes) return fail(WMPC_ERR_UNSUPPORTED, "factor rows too long for shared memory");
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     factor_stream_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, s>>>(pat, sp, o, in, bstream, fstream, status,
-                                                                            n_tiles, batch);
+                                                                            n_tiles, batch, lbatch);
     WMPC_LAUNCH_CHECK();
   }
   {

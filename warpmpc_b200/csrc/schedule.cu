@@ -383,6 +383,17 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       *why = "forward stream misses an entry";
       return false;
     }
+  // factorization re-reads: the L entry every update reads, D^-1 of every step's column
+  S.upd_pos.clear();
+  S.step_doff.resize(hp.nnz_l);
+  for (int k = 0; k < n; ++k) {
+    S.max_row_kv = std::max(S.max_row_kv, 1 + hp.init_ptr[k + 1] - hp.init_ptr[k]);
+    for (int e = hp.proc_ptr[k]; e < hp.proc_ptr[k + 1]; ++e) {
+      const int c = hp.proc_cols[e];
+      S.step_doff[e] = S.dinv_off[c];
+      for (int q = 0; q < hp.proc_offsets[e]; ++q) S.upd_pos.push_back(S.col_uoff[c] + (q >> 2) * 128 + (q & 3));
+    }
+  }
   // factor program step -> stream offsets of the L entry it writes
   S.proc_boff.resize(hp.nnz_l);
   S.proc_foff.resize(hp.nnz_l);

@@ -76,6 +76,9 @@ struct StreamPlan {
   const int* dinv_off;      // [n] backward-stream float offset of D^-1_c (lane stride 1)
   const int* proc_boff;     // [nnz_l] backward-stream float offset of the entry each program step writes
   const int* proc_foff;     // [nnz_l] forward-stream float offset of that entry
+  const int* upd_pos;       // [upd_ptr[nnz_l]] backward-stream float offset of the L entry each update reads
+  const int* step_doff;     // [nnz_l] backward-stream float offset of D^-1 of each program step's column
+  int max_row_kv;           // KKT values a factor row reads (diagonal + init entries), at most
   const int* pad_boff;      // [n_pad_b] padding slots (L = 0) of the backward stream
   const int* pad_foff;      // [n_pad_f] padding slots of the forward stream
   int n_pad_b, n_pad_f;
@@ -170,6 +173,14 @@ __device__ __forceinline__ bool wait_counter_bounded(const unsigned* ctr, unsign
   }
 }
 
+// 4-byte asynchronous global -> shared copy (this thread's), and the wait for
+// all of this thread's outstanding copies.
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
@@ -197,7 +208,8 @@ struct HostStream {
   std::vector<int> chunk_off, chunk_units, chunk_cols, chunk_u0, chunk_nrel, meta_off, meta_words, meta;
   int n_fchunks = 0, flen = 0, max_funits = 0, max_fmeta_words = 0;
   std::vector<int> fchunk_off, fchunk_units, fmeta_off, fmeta_words, fmeta;
-  std::vector<int> col_uoff, dinv_off, proc_boff, proc_foff, pad_boff, pad_foff;
+  std::vector<int> col_uoff, dinv_off, proc_boff, proc_foff, pad_boff, pad_foff, upd_pos, step_doff;
+  int max_row_kv = 0;
   std::vector<int> u_perm, u_orig;
   int dummy_units = 0;
   // host copies used by the OSQP side to lay out the state
