@@ -124,17 +124,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait that may suspend the thread until the phase completes (or the
+// hinted time passes), instead of returning at once.
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait: gives up (returns false) after `limit_ns` or when *abort is set.
+// Waiting threads are suspended in the barrier between checks.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, const volatile int* abort,
                                                   uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t start = global_timer_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0) {
-      if (abort && *abort) return false;
-      if (global_timer_ns() - start > limit_ns) return false;
-    }
+  for (;;) {
+    if (mbar_try_wait_suspend(bar, parity, 20000u)) return true;
+    if (abort && *abort) return false;
+    if (global_timer_ns() - start > limit_ns) return false;
   }
 }
 
@@ -159,14 +170,16 @@ __device__ __forceinline__ unsigned ld_acquire_cta(const unsigned* p) {
 }
 
 // Bounded wait until *ctr >= target: gives up (false) after `limit_ns` or
-// when *abort is set.
+// when *abort is set.  Polls with a short sleep so that a waiting warp does
+// not compete for the shared-memory pipe.
 __device__ __forceinline__ bool wait_counter_bounded(const unsigned* ctr, unsigned target, const volatile int* abort,
                                                      uint64_t limit_ns) {
   if (ld_acquire_cta(ctr) >= target) return true;
   const uint64_t start = global_timer_ns();
   for (uint32_t it = 1;; ++it) {
+    __nanosleep(64);
     if (ld_acquire_cta(ctr) >= target) return true;
-    if ((it & 255u) == 0) {
+    if ((it & 63u) == 0) {
       if (abort && *abort) return false;
       if (global_timer_ns() - start > limit_ns) return false;
     }
