@@ -136,6 +136,21 @@ def algorithmic_bytes_per_instance(plan, max_iter):
     return factor + max_iter * iteration, factor, iteration
 
 
+def measured_traffic(args, batch):
+    """DRAM bytes of one persistent-kernel launch at this batch, scaled from the
+    ncu capture summarised in profiles/ (traffic grows with the instance count:
+    every tile streams the same bytes); None when no capture covers the config."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", f"admm_stream_kernel_{args.config}.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"^traffic_bytes_per_instance:\s*(\d+)", f.read(), re.M)
+    except OSError:
+        return None
+    return float(m.group(1)) * batch if m else None
+
+
 def dist_setup(args):
     from warpmpc_b200 import multirank
 
@@ -446,7 +461,7 @@ def main():
     achieved = algo_bytes / (dom_ms_per_launch * 1e-3) / 1e9
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": None, "kernel": "persistent_kernel",
+        "traffic": measured_traffic(args, B), "kernel": "admm_stream_kernel",
         "kernel_ms": dom_ms_per_launch, "bytes_per_launch": algo_bytes,
         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
     }
