@@ -239,7 +239,8 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
  * on the CPU).  rho/rhoinv: per-constraint values (n_primal = number of
  * primal variables; KKT rows >= n_primal are constraints).  units/cols/rel:
  * backward chunk size targets (4-entry units, columns, releases); funits:
- * forward chunk target (units).  With out == NULL, *out_words receives the
+ * forward chunk target (units); offload: work also given to the releasing
+ * warp (bit 0: leaf columns, bit 1: rows whose entries all read leaf rows).  With out == NULL, *out_words receives the
  * buffer size; otherwise out (capacity out_capacity int32 words) receives,
  * in order:
  *   [n_chunks, blen, max_units, max_cols, max_rel, max_meta_words, max_row_nnz, n_meta]
@@ -250,10 +251,11 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
  *   [n_fchunks, flen, max_funits, max_fmeta_words, n_fmeta]
  *   fchunk_off[n_fchunks+1] fchunk_units[n_fchunks] fmeta_off[n_fchunks]
  *   fmeta_words[n_fchunks] fmeta[n_fmeta] proc_foff[nnz_l]
- *   [n_pad_b, n_pad_f, dummy_units] pad_boff[n_pad_b] pad_foff[n_pad_f] */
+ *   [n_pad_b, n_pad_f, dummy_units] pad_boff[n_pad_b] pad_foff[n_pad_f]
+ *   chunk_pre_u0[n_chunks] chunk_pre_units[n_chunks] */
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv,
                               int32_t n_primal, int32_t units, int32_t cols, int32_t rel, int32_t funits,
-                              int32_t* out, int64_t out_capacity, int64_t* out_words);
+                              int32_t offload, int32_t* out, int64_t out_capacity, int64_t* out_words);
 
 /* Profiling (no counterpart in the reference, which times with wall
  * clocks around jax.block_until_ready).  Between begin and end the library

@@ -79,7 +79,11 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             assert not np.isnan(dv).any()
             lval = val * dv
             Lb[uidx(sched["proc_boff"][e], BL)] = lval
-            Fs[uidx(sched["proc_foff"][e], FL)] = lval
+            fo = int(sched["proc_foff"][e])
+            if fo >= 0:
+                Fs[uidx(fo, FL)] = lval
+            else:  # a releaser forward unit in the backward stream
+                Lb[uidx(-1 - fo, BL)] = lval
             dk = dk - val * lval
         Lb[didx(sched["dinv_off"][k])] = _f32(1.0) / dk
     for off in sched["pad_boff"]:
@@ -128,14 +132,16 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= n + 1
         return byte_off // 128
 
-    def run_units(m, nu, stage, backward):
+    def run_units(m, nu, stage, backward, first_unit=0):
         """The consumer's unit loop: units are computed in groups of 3, unit
         u+1's operands loaded before unit u's arithmetic and store; units past
         nu are sentinels (zero-row reads, unit 0's L values, trash-row
         stores)."""
         ncomp = -(-nu // 3) * 3
-        assert 1 <= nu and KHDR + (nu + NSENT) * KUW <= m.size and ncomp + 1 < nu + NSENT
-        units = m[KHDR : KHDR + (nu + NSENT) * KUW].reshape(nu + NSENT, KUW)
+        off = KHDR + first_unit * KUW
+        assert 1 <= nu and off + (nu + NSENT) * KUW <= m.size and ncomp + 1 < nu + NSENT
+        units = m[off : off + (nu + NSENT) * KUW].reshape(nu + NSENT, KUW)
+        ubase = int(units[0][6]) // 512  # stage position of the list's first unit
         for sent in units[nu:]:
             assert np.all(sent[:5] == n * 128) and sent[5] == 0 and sent[6] == 0 and sent[7] == (n + 1) * 128
         nfl = stage.size
@@ -144,7 +150,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             src, ctl = units[u, :4], units[u, 4:]
             lo = int(ctl[2])
             assert lo % 512 == 0 and lo // 4 + 128 <= nfl
-            assert lo == (u * 512 if u < nu else 0)
+            assert lo == ((ubase + u) * 512 if u < nu else 0)
             lv = stage[lo // 4 : lo // 4 + 128].reshape(lanes, 4).T.copy()  # [slot][lane]
             xs = [X[xrow(o)].copy() for o in src]
             t = X[xrow(ctl[0])].copy()
@@ -198,21 +204,34 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             run_units(fm, nu, Fs[o0:o1], backward=False)
             continue
         m = block(meta_all, sched["meta_off"], sched["meta_words"], ch, sched["max_meta_words"])
-        nu, ncols, nrel, c0, u0, nprim = (int(v) for v in m[:6])
+        ns, ncols, nrel, c0, u0, nprim, nl, npre = (int(v) for v in m[:8])
+        nu = ns + nl + npre
         assert nu == sched["chunk_units"][ch] and ncols == sched["chunk_cols"][ch] and nrel == sched["chunk_nrel"][ch]
         assert u0 == sched["chunk_u0"][ch] and nu <= sched["max_units"] and ncols <= sched["max_cols"]
         assert nrel <= sched["max_rel"] and 0 <= u0 and u0 + nrel <= n and 0 <= nprim <= nrel
-        r = KHDR + (nu + NSENT) * KUW
-        assert r + 3 * nrel <= m.size
-        rel_i = m[r : r + nrel]
-        rel_rho = m[r + nrel : r + 2 * nrel].view(np.float32)
-        rel_rinv = m[r + 2 * nrel : r + 3 * nrel].view(np.float32)
+        r = KHDR + (nu + 3 * NSENT) * KUW
+        assert r + 4 * nrel <= m.size and r % 4 == 0
+        recs = m[r : r + 4 * nrel].reshape(nrel, 4)
+        rel_i = recs[:, 0].copy()
+        rel_rho = recs[:, 1].copy().view(np.float32)
+        rel_rinv = recs[:, 2].copy().view(np.float32)
         for k in range(nrel):
             assert (sched["u_orig"][u0 + k] < plan.n) == (k < nprim)
+        o0, o1 = sched["chunk_off"][ch], sched["chunk_off"][ch + 1]
+        assert o1 - o0 == nu * 128 + ncols * 32 and o1 <= BL
+        stage = Lb[o0:o1]
+        leaf_at, pre_at = ns + NSENT, ns + nl + 2 * NSENT
+        if kind == 0:
+            # the first-right-hand-side pass copies only the releaser's forward units
+            assert sched["chunk_pre_u0"][ch] == ns + nl and sched["chunk_pre_units"][ch] == npre
+            stage = np.full_like(stage, np.nan)
+            p0, p1 = (ns + nl) * 128, (ns + nl + npre) * 128
+            stage[p0:p1] = Lb[o0 + p0 : o0 + p1]
         if kind == 2:
-            o0, o1 = sched["chunk_off"][ch], sched["chunk_off"][ch + 1]
-            assert o1 - o0 == nu * 128 + ncols * 32 and o1 <= BL
-            run_units(m, nu, Lb[o0:o1], backward=True)
+            if ns:
+                run_units(m, ns, stage, backward=True)
+            if nl:
+                run_units(m, nl, stage, backward=True, first_unit=leaf_at)
             for k in range(nrel):
                 i = xrow(rel_i[k])
                 assert i < n
@@ -240,6 +259,8 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 assert i < n
                 uu = u0 + k
                 X[i] = sigma * s0[uu] - pp0[uu] if k < nprim else s0[uu] - rel_rinv[k] * s1[uu]
+        if npre:
+            run_units(m, npre, stage, backward=False, first_unit=pre_at)
         assert X[n].max() == 0.0 and X[n].min() == 0.0
     # ---- stream_to_state_kernel + unscale
     x = np.zeros((lanes, plan.n), np.float32)

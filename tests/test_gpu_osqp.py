@@ -70,6 +70,26 @@ def test_osqp_shared_matrices_and_warm_start(cuda_device, mode):
     assert got2[3].max() <= got[3].max() + 1e-6
 
 
+@pytest.mark.parametrize("offload", [1, 2, 3])
+def test_persistent_releaser_offload_warm_start(cuda_device, monkeypatch, offload):
+    """The releasing warp also solving leaf columns (1) and/or rows that read
+    only leaf rows (2): same bits as the oracle, cold and warm started (the
+    first pass then needs those rows' coefficients)."""
+    monkeypatch.setenv("WMPC_STREAM_OFFLOAD", str(offload))
+    b = problems.make_batch(problems.CARTPOLE, 70, seed=6)
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    got = _run(comp, b)
+    ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u)
+    for g, r in zip(got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r)
+    warm = (got[0], got[1], got[2])
+    got2 = _run(comp, b, warm=warm)
+    ref2 = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, *warm)
+    for g, r in zip(got2[:3], ref2[:3]):
+        np.testing.assert_array_equal(g, r)
+
+
 def test_factor_reuse_matches_solve(cuda_device):
     import torch
 

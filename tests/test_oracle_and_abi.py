@@ -71,6 +71,28 @@ def test_invalid_arguments_fail_cleanly():
     assert lib.wmpc_osqp_solve(None, None, None, None, None, 0, 0, None, 0, None) == native.WMPC_ERR_INVALID_ARGUMENT
 
 
+@pytest.mark.parametrize("offload", [0, 1, 2, 3])
+@pytest.mark.parametrize("cls", [problems.SMALL, problems.CARTPOLE], ids=lambda c: c.name)
+def test_stream_schedule_replay_warm_start(cls, offload):
+    """Warm start: the first right-hand side is non-zero everywhere, so every
+    coefficient the first pass reads must have been copied into its stage."""
+    import sys
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    import stream_sim
+    from oracle import osqp_ref
+    from warpmpc_b200.schedule import stream_schedule
+
+    b = problems.make_batch(cls, 8, seed=7)
+    plan = problems.make_plan(b)
+    sched = stream_schedule(plan, targets=(16, 16, 12, 16, offload))
+    x, z, y = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3)[:3]
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, x0=x, z0=z, y0=y, max_iter=3)
+    ref = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, x, z, y, max_iter=3)
+    for g, r in zip(got, ref[:3]):
+        np.testing.assert_array_equal(g, r)
+
+
 @pytest.mark.parametrize("cls", [problems.SMALL, problems.CARTPOLE], ids=lambda c: c.name)
 def test_stream_schedule_replay_bitexact(cls):
     import sys
@@ -91,8 +113,10 @@ def test_stream_schedule_replay_bitexact(cls):
     q = plan.qdldl_plan
     assert sched["chunk_off"][-1] == sched["blen"] == 128 * sched["chunk_units"].sum() + 32 * q.n
     assert sched["fchunk_off"][-1] == sched["flen"] == 128 * sched["fchunk_units"].sum()
-    # every L entry once in each stream, every other slot padding
-    assert 4 * sched["chunk_units"].sum() == q.nnz_l + sched["pad_boff"].size
-    assert 4 * sched["fchunk_units"].sum() == q.nnz_l + sched["pad_foff"].size
+    # every L entry once in each stream (entries of rows the releaser solves forward sit in the
+    # backward stream a second time), every other slot padding
+    n_pre = int((sched["proc_foff"] < 0).sum())
+    assert 4 * sched["chunk_units"].sum() == q.nnz_l + n_pre + sched["pad_boff"].size
+    assert 4 * sched["fchunk_units"].sum() == q.nnz_l - n_pre + sched["pad_foff"].size
     assert np.unique(sched["proc_boff"]).size == q.nnz_l and np.unique(sched["proc_foff"]).size == q.nnz_l
     assert sorted(sched["u_perm"].tolist()) == list(range(plan.qdldl_plan.n))

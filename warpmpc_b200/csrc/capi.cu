@@ -190,8 +190,8 @@ int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* to
 int64_t wmpc_launch_count(void) { return g_launches.load(); }
 
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv, int32_t n_primal,
-                              int32_t units, int32_t cols, int32_t rel, int32_t funits, int32_t* out,
-                              int64_t out_capacity, int64_t* out_words) {
+                              int32_t units, int32_t cols, int32_t rel, int32_t funits, int32_t offload,
+                              int32_t* out, int64_t out_capacity, int64_t* out_words) {
   if (!desc || !out_words) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
   const int n = desc->n, nnz_l = desc->nnz_l;
   if (n <= 0 || nnz_l < 0 || n_primal < 0 || n_primal > n || units <= 0 || cols <= 0 || rel <= 0 || funits <= 0)
@@ -220,6 +220,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   t.cols = cols;
   t.rel = rel;
   t.funits = funits;
+  t.offload = offload & 3;
   if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
       !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
     return fail(WMPC_ERR_UNSUPPORTED, "%s", why.c_str());
@@ -237,6 +238,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   w.push_back(static_cast<int>(hs.pad_boff.size())); w.push_back(static_cast<int>(hs.pad_foff.size()));
   w.push_back(hs.dummy_units);
   app(hs.pad_boff); app(hs.pad_foff);
+  app(hs.chunk_pre_u0); app(hs.chunk_pre_units);
   *out_words = static_cast<int64_t>(w.size());
   if (!out) return WMPC_OK;
   if (out_capacity < static_cast<int64_t>(w.size())) return fail(WMPC_ERR_INVALID_ARGUMENT, "output buffer too small");
@@ -523,6 +525,7 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (const char* v = getenv("WMPC_STREAM_COLS")) targets.cols = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_REL")) targets.rel = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_FUNITS")) targets.funits = atoi(v);
+    if (const char* v = getenv("WMPC_STREAM_OFFLOAD")) targets.offload = atoi(v) & 3;
     if (targets.units <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.funits <= 0) targets = StreamTargets();
     bool ok = build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, &q->stream_why) &&
               build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why);
@@ -562,6 +565,8 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
       sk.add(hs.chunk_u0.data(), hs.chunk_u0.size(), &sp.chunk_u0);
       sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
+      sk.add(hs.chunk_pre_u0.data(), hs.chunk_pre_u0.size(), &sp.chunk_pre_u0);
+      sk.add(hs.chunk_pre_units.data(), hs.chunk_pre_units.size(), &sp.chunk_pre_units);
       sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
       sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
       sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);

@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
       }
       const float lval = val * dst[e * 32];
       Lu[boff_w[e]] = lval;
-      F[foff_w[e]] = lval;
+      const int fo = foff_w[e];  // forward stream, or (-1 - offset) a releaser forward unit in the backward stream
+      if (fo >= 0) F[fo] = lval; else Lu[-1 - fo] = lval;
       dk = dk - val * lval;
     }
     const float di = 1.0f / dk;
@@ -166,11 +167,13 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
 // state layout conversions: symbolic-major (KKT row, instance) <-> tile-major U order
 // ---------------------------------------------------------------------------
 
+// ADMM state per tile in release order U, one 16-byte record per (index, lane):
+// (x, 0, sigma-scaled q, 0) for a primal index, (z, y, l, u) for a constraint.
 __global__ void state_to_stream_kernel(StreamPlan sp, int n_primal, const float* __restrict__ x,
                                        const float* __restrict__ z, const float* __restrict__ y,
                                        const float* __restrict__ qs, const float* __restrict__ ls,
-                                       const float* __restrict__ us, float* __restrict__ s0, float* __restrict__ s1,
-                                       float* __restrict__ p0, float* __restrict__ p1, int batch, int n_tiles) {
+                                       const float* __restrict__ us, float4* __restrict__ state, int batch,
+                                       int n_tiles) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n_tiles * 32) return;
   const int bb = b < batch ? b : batch - 1;
@@ -179,35 +182,30 @@ __global__ void state_to_stream_kernel(StreamPlan sp, int n_primal, const float*
     const int o = __ldg(sp.u_orig + u);
     const size_t dst = ((size_t)tile * sp.n + u) * 32 + lane;
     if (o < n_primal) {
-      s0[dst] = x[(size_t)o * batch + bb];
-      s1[dst] = 0.0f;
-      p0[dst] = qs[(size_t)o * batch + bb];
-      p1[dst] = 0.0f;
+      state[dst] = make_float4(x[(size_t)o * batch + bb], 0.0f, qs[(size_t)o * batch + bb], 0.0f);
     } else {
       const int r = o - n_primal;
-      s0[dst] = z[(size_t)r * batch + bb];
-      s1[dst] = y[(size_t)r * batch + bb];
-      p0[dst] = ls[(size_t)r * batch + bb];
-      p1[dst] = us[(size_t)r * batch + bb];
+      state[dst] = make_float4(z[(size_t)r * batch + bb], y[(size_t)r * batch + bb], ls[(size_t)r * batch + bb],
+                               us[(size_t)r * batch + bb]);
     }
   }
 }
 
-__global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float* __restrict__ s0,
-                                       const float* __restrict__ s1, float* __restrict__ x, float* __restrict__ z,
-                                       float* __restrict__ y, int batch) {
+__global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float4* __restrict__ state,
+                                       float* __restrict__ x, float* __restrict__ z, float* __restrict__ y,
+                                       int batch) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
   const int tile = b >> 5, lane = b & 31;
   for (int u = blockIdx.y; u < sp.n; u += gridDim.y) {
     const int o = __ldg(sp.u_orig + u);
-    const size_t src = ((size_t)tile * sp.n + u) * 32 + lane;
+    const float4 v = state[((size_t)tile * sp.n + u) * 32 + lane];
     if (o < n_primal) {
-      x[(size_t)o * batch + b] = s0[src];
+      x[(size_t)o * batch + b] = v.x;
     } else {
       const int r = o - n_primal;
-      z[(size_t)r * batch + b] = s0[src];
-      y[(size_t)r * batch + b] = s1[src];
+      z[(size_t)r * batch + b] = v.x;
+      y[(size_t)r * batch + b] = v.y;
     }
   }
 }
@@ -220,17 +218,14 @@ struct StreamArgs {
   StreamPlan sp;
   const float* bstream;
   const float* fstream;
-  float* s0;
-  float* s1;
-  const float* p0;
-  const float* p1;
+  float4* state;  // [tile][U][lane] ADMM state records
   int* error;   // one word: 0 ok, 1 pipeline timeout
   int n_tiles, max_iter;
   float sigma, alpha, one_minus_alpha;
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
   int lbytes;       // per L stage L area
-  int sbytes;       // per S stage: 4 arrays x max_rel x 128 bytes
+  int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes
 };
 
 enum : int { kItemRel = 0, kItemFwd = 1, kItemBwd = 2 };
@@ -366,29 +361,26 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 // released once per pass, so groups never share a row).  A group slot past
 // `end` repeats the group's first index: it loads the same operands, computes
 // the same values and stores them to the same places again.
+//   rel: per release (row byte offset, rho bits, rho^-1 bits, 0)
+//   S:   this lane's state record of release 0 in the stage (k-th at S[32 k])
 struct RelGroup {
   int o[4], kk[4];
-  float x[4], s0[4], s1[4], p0[4], p1[4], rho[4], rinv[4];
+  float x[4], rho[4], rinv[4];
+  float4 st[4];
 };
 
-template <bool kCons>
-__device__ __forceinline__ void load_rel_group(const int* rel_off, const float* rel_rho, const float* rel_rinv,
-                                               int k, int end, const float* S0, const float* S1, const float* P0,
-                                               const float* P1, const unsigned char* xb, RelGroup& g) {
+__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S,
+                                               const unsigned char* xb, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int kk = (k + j < end) ? k + j : k;
+    const int4 r = rel[kk];
     g.kk[j] = kk;
-    g.o[j] = rel_off[kk];
-    g.x[j] = *reinterpret_cast<const float*>(xb + g.o[j]);
-    g.s0[j] = S0[kk * 32];
-    g.p0[j] = P0[kk * 32];
-    if (kCons) {
-      g.s1[j] = S1[kk * 32];
-      g.p1[j] = P1[kk * 32];
-      g.rho[j] = rel_rho[kk];
-      g.rinv[j] = rel_rinv[kk];
-    }
+    g.o[j] = r.x;
+    g.rho[j] = __int_as_float(r.y);
+    g.rinv[j] = __int_as_float(r.z);
+    g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
+    g.st[j] = S[kk * 32];
   }
 }
 
@@ -400,48 +392,46 @@ struct RelParams {
 // constraint: z, y update and next rhs z - rho^-1 y (solver.py:806-820)
 template <bool kCons>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float* s0u, float* s1u) {
+                                                 float4* stu) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
+    float2* out = reinterpret_cast<float2*>(stu + g.kk[j] * 32);
     if (!kCons) {
-      const float xn = rp.alpha * g.x[j] + rp.oma * g.s0[j];
-      s0u[g.kk[j] * 32] = xn;
-      *xi = rp.sigma * xn - g.p0[j];
+      const float xn = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
+      *out = make_float2(xn, g.st[j].y);
+      *xi = rp.sigma * xn - g.st[j].z;
     } else {
       const float rinv = g.rinv[j];
-      const float sv0 = g.s0[j], yk = g.s1[j];
+      const float sv0 = g.st[j].x, yk = g.st[j].y;
       const float rz = sv0 - rinv * yk;
       const float zt = rz + rinv * g.x[j];
       const float zr = rp.alpha * zt + rp.oma * sv0;
       float zn = zr + rinv * yk;
-      zn = (zn < g.p0[j]) ? g.p0[j] : zn;
-      zn = (zn > g.p1[j]) ? g.p1[j] : zn;
+      zn = (zn < g.st[j].z) ? g.st[j].z : zn;
+      zn = (zn > g.st[j].w) ? g.st[j].w : zn;
       const float yn = yk + g.rho[j] * (zr - zn);
-      s0u[g.kk[j] * 32] = zn;
-      s1u[g.kk[j] * 32] = yn;
+      *out = make_float2(zn, yn);
       *xi = zn - rinv * yn;
     }
   }
 }
 
 template <bool kCons>
-__device__ __forceinline__ void run_releases(const int* rel_off, const float* rel_rho, const float* rel_rinv,
-                                             int begin, int end, const float* S0, const float* S1, const float* P0,
-                                             const float* P1, const RelParams& rp, unsigned char* xb, float* s0u,
-                                             float* s1u) {
+__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const RelParams& rp,
+                                             unsigned char* xb, float4* stu) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, begin, end, S0, S1, P0, P1, xb, a);
+  load_rel_group(rel, begin, end, S, xb, a);
   for (int k = begin;; k += 8) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + 4 < end ? k + 4 : end - 1;
-    load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, kb, end, S0, S1, P0, P1, xb, b);
-    update_rel_group<kCons>(a, rp, xb, s0u, s1u);
+    load_rel_group(rel, kb, end, S, xb, b);
+    update_rel_group<kCons>(a, rp, xb, stu);
     if (k + 4 >= end) break;
     const int ka = k + 8 < end ? k + 8 : end - 1;
-    load_rel_group<kCons>(rel_off, rel_rho, rel_rinv, ka, end, S0, S1, P0, P1, xb, a);
-    update_rel_group<kCons>(b, rp, xb, s0u, s1u);
+    load_rel_group(rel, ka, end, S, xb, a);
+    update_rel_group<kCons>(b, rp, xb, stu);
     if (k + 8 >= end) break;
   }
 }
@@ -509,9 +499,16 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
               !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
             return false;
           unsigned char* st = lring + (size_t)lr.stage * lstage_bytes;
+          // first-right-hand-side pass: only the releaser's forward units need coefficients
+          uint32_t pre_at = 0;
+          if (kind == kItemRel) {
+            pre_at = (uint32_t)__ldg(sp.chunk_pre_u0 + ch);
+            lbytes = (uint32_t)__ldg(sp.chunk_pre_units + ch) * 512u;
+          }
           mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes);
           bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + moff, (uint32_t)mwords * 4u, lfull + lr.stage);
-          if (lbytes) bulk_g2s(st + a.meta_bytes, (fwd ? ft : bt) + loff, lbytes, lfull + lr.stage);
+          if (lbytes)
+            bulk_g2s(st + a.meta_bytes + pre_at * 512u, (fwd ? ft : bt) + loff + pre_at * 128u, lbytes, lfull + lr.stage);
           lr.advance(a.lstages);
           ++issued_l;
           if (!fwd) {
@@ -519,16 +516,9 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 128u;
-            const int quarter = a.sbytes / 4;
-            mbar_arrive_expect_tx(sfull + sr.stage, 4u * bytes);
-            if (bytes) {
-              const size_t off = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
-              bulk_g2s(ss, a.s0 + off, bytes, sfull + sr.stage);
-              bulk_g2s(ss + quarter, a.s1 + off, bytes, sfull + sr.stage);
-              bulk_g2s(ss + 2 * quarter, a.p0 + off, bytes, sfull + sr.stage);
-              bulk_g2s(ss + 3 * quarter, a.p1 + off, bytes, sfull + sr.stage);
-            }
+            const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 512u;
+            mbar_arrive_expect_tx(sfull + sr.stage, bytes);
+            if (bytes) bulk_g2s(ss, a.state + soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32, bytes, sfull + sr.stage);
             sr.advance(a.sstages);
             ++issued_s;
           }
@@ -558,10 +548,12 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
           const unsigned char* lst = stage + a.meta_bytes;
           const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
           const int nu = meta[0];
-          if (kind == kItemFwd) {
-            run_units<false>(mu, lst, xb, lane, nu);  // forward substitution, row-gather form
-          } else {
-            run_units<true>(mu, lst, xb, lane, nu);   // backward substitution, column form
+          if (nu > 0) {
+            if (kind == kItemFwd) {
+              run_units<false>(mu, lst, xb, lane, nu);  // forward substitution, row-gather form
+            } else {
+              run_units<true>(mu, lst, xb, lane, nu);   // backward substitution, column form
+            }
           }
           __syncwarp();
           if (lane == 0) {
@@ -584,10 +576,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     const float sigma = a.sigma, alpha = a.alpha, oma = a.one_minus_alpha;
     unsigned char* xb = smem + lane * 4;
     bool ok = true;
-    const int quarter_f = a.sbytes / 16;  // floats per S array
     for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
-      float* s0t = a.s0 + (size_t)tile * n * 32 + lane;
-      float* s1t = a.s1 + (size_t)tile * n * 32 + lane;
+      float4* stt = a.state + (size_t)tile * n * 32 + lane;
       auto release = [&](int kind, int ch) -> bool {
         (void)ch;
         if (kind != kItemFwd) {
@@ -597,31 +587,41 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
           } else if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) {
             return false;
           }
-          const int* meta = reinterpret_cast<const int*>(lring + (size_t)lr.stage * lstage_bytes);
-          const int nu = meta[0], nrel = meta[2], u0 = meta[4], nprim = meta[5];
-          const int* rel_off = meta + kChunkHeader + (nu + kUnitSentinels) * kUnitWords;
-          const float* rel_rho = reinterpret_cast<const float*>(rel_off + nrel);
-          const float* rel_rinv = rel_rho + nrel;
+          const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
+          const int* meta = reinterpret_cast<const int*>(stage);
+          const unsigned char* lst = stage + a.meta_bytes;
+          const int ns = meta[0], nrel = meta[2], u0 = meta[4], nprim = meta[5], nl = meta[6], np = meta[7];
+          const int4* mu_leaf = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + kUnitSentinels) * kUnitWords);
+          const int4* mu_pre = mu_leaf + (nl + kUnitSentinels) * (kUnitWords / 4);
+          const int4* rel = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + nl + np + 3 * kUnitSentinels) * kUnitWords);
+          // leaf columns (read by no other column): solved here, just before their release
+          if (kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
-          const float* S0 = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes) + lane;
-          const float* S1 = S0 + quarter_f;
-          const float* P0 = S1 + quarter_f;
-          const float* P1 = P0 + quarter_f;
+          const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
-            for (int k = 0; k < nprim; ++k)
-              *reinterpret_cast<float*>(xb + rel_off[k]) = sigma * S0[k * 32] - P0[k * 32];
-            for (int k = nprim; k < nrel; ++k)
-              *reinterpret_cast<float*>(xb + rel_off[k]) = S0[k * 32] - rel_rinv[k] * S1[k * 32];
+            for (int k = 0; k < nprim; ++k) {
+              const float4 st = S[k * 32];
+              *reinterpret_cast<float*>(xb + rel[k].x) = sigma * st.x - st.z;
+            }
+            for (int k = nprim; k < nrel; ++k) {
+              const int4 r = rel[k];
+              const float4 st = S[k * 32];
+              *reinterpret_cast<float*>(xb + r.x) = st.x - __int_as_float(r.z) * st.y;
+            }
           } else {
-            float* s0u = s0t + (size_t)u0 * 32;
-            float* s1u = s1t + (size_t)u0 * 32;
+            float4* stu = stt + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false>(rel_off, rel_rho, rel_rinv, 0, nprim, S0, S1, P0, P1, rp, xb, s0u, s1u);
-            run_releases<true>(rel_off, rel_rho, rel_rinv, nprim, nrel, S0, S1, P0, P1, rp, xb, s0u, s1u);
+            run_releases<false>(rel, 0, nprim, S, rp, xb, stu);
+            run_releases<true>(rel, nprim, nrel, S, rp, xb, stu);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
+          }
+          // forward rows whose entries all read leaf rows: their right-hand sides are now final
+          if (np > 0) {
+            __syncwarp();
+            run_units<false>(mu_pre, lst, xb, lane, np);
           }
           __syncwarp();
           if (lane == 0) {
@@ -670,7 +670,7 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
   const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
-  const int sbytes = 4 * (sp.max_rel > 0 ? sp.max_rel : 1) * 128;
+  const int sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
   // prefer deep rings: as many L stages as fit with at least 3 S stages
   const int lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
   const int smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
@@ -705,10 +705,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   const size_t tl = (size_t)n_tiles * 32;
   float* bstream = work;
   float* fstream = bstream + (size_t)n_tiles * sp.blen;
-  float* s0 = fstream + (size_t)n_tiles * sp.flen;
-  float* s1 = s0 + tl * sp.n;
-  float* p0 = s1 + tl * sp.n;
-  float* p1 = p0 + tl * sp.n;
+  float4* state = reinterpret_cast<float4*>(fstream + (size_t)n_tiles * sp.flen);
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
   if (!reuse_factor) {
     // L-batch sized so that every tile's warp is resident at once (all of a
@@ -727,10 +724,10 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   }
   {
     dim3 grid(ceil_div(tl, 128), sp.n < 1024 ? sp.n : 1024);
-    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, s0, s1, p0, p1, batch, n_tiles);
+    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, state, batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
-  StreamArgs a{sp, bstream, fstream, s0, s1, p0, p1, error, n_tiles, max_iter, o.sigma, o.alpha,
+  StreamArgs a{sp, bstream, fstream, state, error, n_tiles, max_iter, o.sigma, o.alpha,
                o.one_minus_alpha, cfg.stages, cfg.sstages, cfg.meta_bytes, cfg.lbytes, cfg.sbytes};
   const int grid = n_tiles < num_sms ? n_tiles : num_sms;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
@@ -740,7 +737,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
   WMPC_LAUNCH_CHECK();
   {
     dim3 grid2(ceil_div(batch, 128), sp.n < 1024 ? sp.n : 1024);
-    stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, s0, s1, x, z, y, batch);
+    stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, state, x, z, y, batch);
     WMPC_LAUNCH_CHECK();
   }
   return WMPC_OK;

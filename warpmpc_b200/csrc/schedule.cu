@@ -195,13 +195,39 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       u += rel_count[c];
     }
   }
+  // Rows of L.  A leaf row (no entries) is read by no column of the backward
+  // sweep, so its column can be solved by the releaser right before its own
+  // release, and its forward value is its right-hand side.  A row whose entries
+  // all read leaf rows ("pre row") can be solved forward by the releaser as
+  // soon as it and its leaves are released (all in the chunk of its release
+  // column).  The sweeper walks everything else.
+  std::vector<int> rcount(n, 0);
+  std::vector<std::vector<int>> row_entries(n);  // CSC entry indices of each row, columns ascending
+  std::vector<int> col_of(hp.nnz_l);
+  for (int c = 0; c < n; ++c)
+    for (int e = hp.lp[c]; e < hp.lp[c + 1]; ++e) {
+      rcount[hp.li[e]]++;
+      row_entries[hp.li[e]].push_back(e);
+      col_of[e] = c;
+    }
+  std::vector<char> pre_row(n, 0), leaf_col(n, 0);
+  for (int i = 0; i < n; ++i) leaf_col[i] = (t.offload & 1) && rcount[i] == 0;
+  for (int i = 0; i < n && (t.offload & 2); ++i) {
+    if (rcount[i] == 0) continue;
+    bool all_leaf = true;
+    for (int e : row_entries[i]) all_leaf = all_leaf && rcount[col_of[e]] == 0;
+    pre_row[i] = all_leaf ? 1 : 0;
+  }
   auto col_units = [&](int c) { const int ce = hp.lp[c + 1] - hp.lp[c]; return ce == 0 ? 1 : (ce + 3) / 4; };
+  std::vector<int> pre_units_at(n, 0);  // pre-row units run in the chunk of the row's release column
+  for (int i = 0; i < n; ++i)
+    if (pre_row[i]) pre_units_at[rel_col[i]] += (rcount[i] + 3) / 4;
   // ---- backward chunks: whole columns, units <= t.units, columns <= t.cols, releases <= t.rel
   std::vector<int> bounds{0};
   {
     int units = 0, cols = 0, rel = 0;
     for (int c = 0; c < n; ++c) {
-      const int cu = col_units(c), cr = rel_count[c];
+      const int cu = col_units(c) + pre_units_at[c], cr = rel_count[c];
       if (cols > 0 && (units + cu > t.units || cols + 1 > t.cols || rel + cr > t.rel)) {
         bounds.push_back(c);
         units = cols = rel = 0;
@@ -223,35 +249,60 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   S.col_uoff.assign(n, 0);
   S.dinv_off.assign(n, 0);
   std::vector<int> entry_boff(hp.nnz_l, -1);  // CSC entry -> backward stream float offset (lane 0)
+  std::vector<int> entry_foff(hp.nnz_l, -1);  // CSC entry -> forward position; -1 - offset: a pre unit slot
   int boff = 0;                                // running float offset in the backward stream
   for (int ch = 0; ch < S.n_chunks; ++ch) {
     const int c0 = bounds[ch], c1 = bounds[ch + 1];
-    std::vector<UnitBuild> units;
-    std::vector<int> col_first_unit(c1 - c0), col_last_unit(c1 - c0);
-    std::vector<std::pair<int, int>> placed;  // (CSC entry, unit * 4 + slot within the chunk)
+    // three unit lists: sweeper columns, leaf columns, pre rows; placement is (list, index, slot)
+    std::vector<UnitBuild> lists[3];
+    std::vector<int> col_list(c1 - c0), col_first(c1 - c0), col_last(c1 - c0);
+    struct Placed { int entry, list, pos; };  // pos = unit * 4 + slot within its list
+    std::vector<Placed> placed, placed_pre;
     for (int c = c1 - 1; c >= c0; --c) {  // the order the backward sweep visits the columns
       const int e0 = hp.lp[c], cnt = hp.lp[c + 1] - e0;
+      const int li = leaf_col[c] ? 1 : 0;
       std::vector<int> slot_of;
       std::vector<UnitBuild> add = cut_units(cnt, false, c, zero_row, [&](int q) { return hp.li[e0 + q]; }, &slot_of);
       const int nadd = static_cast<int>(add.size());
-      const int first = append_units(&units, std::move(add), 0, zero_row, &S.dummy_units);
-      col_first_unit[c - c0] = first;
-      col_last_unit[c - c0] = first + nadd - 1;
-      for (int q = 0; q < cnt; ++q) placed.emplace_back(e0 + q, first * 4 + slot_of[q]);
+      const int first = append_units(&lists[li], std::move(add), 0, zero_row, &S.dummy_units);
+      col_list[c - c0] = li;
+      col_first[c - c0] = first;
+      col_last[c - c0] = first + nadd - 1;
+      for (int q = 0; q < cnt; ++q) placed.push_back({e0 + q, li, first * 4 + slot_of[q]});
     }
-    const int nu = static_cast<int>(units.size());
+    for (int v = 0; v < n; ++v) {
+      if (!pre_row[v] || rel_col[v] < c0 || rel_col[v] >= c1) continue;
+      const std::vector<int>& re = row_entries[v];
+      const int cnt = static_cast<int>(re.size());
+      std::vector<int> slot_of;
+      std::vector<UnitBuild> add = cut_units(cnt, true, v, zero_row, [&](int q) { return col_of[re[q]]; }, &slot_of);
+      const int first = append_units(&lists[2], std::move(add), 3, zero_row, &S.dummy_units);
+      for (int q = 0; q < cnt; ++q) placed_pre.push_back({re[q], 2, first * 4 + slot_of[q]});
+    }
+    const int ns = static_cast<int>(lists[0].size()), nl = static_cast<int>(lists[1].size());
+    const int np = static_cast<int>(lists[2].size());
+    const int base[3] = {0, ns, ns + nl};  // unit index of each list in the stage
+    const int nu = ns + nl + np;
     const int units_floats = nu * 128;
-    for (const auto& pe : placed) entry_boff[pe.first] = boff + (pe.second >> 2) * 128 + (pe.second & 3);
+    auto stream_pos = [&](const Placed& pl) {
+      const int u = base[pl.list] + (pl.pos >> 2);
+      return boff + u * 128 + (pl.pos & 3);
+    };
+    for (const Placed& pl : placed) entry_boff[pl.entry] = stream_pos(pl);
+    for (const Placed& pl : placed_pre) entry_foff[pl.entry] = -1 - stream_pos(pl);
     for (int c = c0; c < c1; ++c) {
-      S.col_uoff[c] = boff + col_first_unit[c - c0] * 128;
+      const int li = col_list[c - c0];
+      S.col_uoff[c] = boff + (base[li] + col_first[c - c0]) * 128;
       S.dinv_off[c] = boff + units_floats + (c - c0) * 32;
       // D^-1 offset (bytes, relative to the stage's L area) on the column's last unit
-      units[col_last_unit[c - c0]].doff = (units_floats + (c - c0) * 32) * 4;
+      lists[li][col_last[c - c0]].doff = (units_floats + (c - c0) * 32) * 4;
     }
     int nrel = 0;
     for (int c = c0; c < c1; ++c) nrel += rel_count[c];
     const int u0 = rel_first[c1 - 1];
     S.chunk_off[ch] = boff;
+    S.chunk_pre_u0.push_back(ns + nl);
+    S.chunk_pre_units.push_back(np);
     S.chunk_units[ch] = nu;
     S.chunk_cols[ch] = c1 - c0;
     S.chunk_u0[ch] = u0;
@@ -260,7 +311,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     S.max_cols = std::max(S.max_cols, c1 - c0);
     S.max_rel = std::max(S.max_rel, nrel);
     boff += units_floats + (c1 - c0) * 32;
-    // meta block: header, units, releases
+    // meta block: header, the three unit lists (each followed by its sentinels), releases
     // the chunk's releases: primal indices first, then constraints (two branch-free loops)
     for (int u = u0; u < u0 + nrel; ++u)
       if (rel_col[order[u]] < c0 || rel_col[order[u]] >= c1) {
@@ -271,9 +322,11 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
                           [&](int i) { return hp.p[i] < n_primal; });
     int nprim = 0;
     for (int u = u0; u < u0 + nrel; ++u) nprim += hp.p[order[u]] < n_primal ? 1 : 0;
-    std::vector<int> m{nu, c1 - c0, nrel, c0, u0, nprim, 0, 0};
-    for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
-    push_sentinels(zero_row, trash_row, &m);
+    std::vector<int> m{ns, c1 - c0, nrel, c0, u0, nprim, nl, np};
+    for (int li = 0; li < 3; ++li) {
+      for (int u = 0; u < static_cast<int>(lists[li].size()); ++u) push_unit_meta(lists[li][u], base[li] + u, trash_row, &m);
+      push_sentinels(zero_row, trash_row, &m);
+    }
     std::vector<int> rel_i, rel_rho, rel_rinv;
     for (int u = u0; u < u0 + nrel; ++u) {
       const int i = order[u];
@@ -291,17 +344,21 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       rel_rho.push_back(rb);
       rel_rinv.push_back(ib);
     }
-    for (int v : rel_i) m.push_back(v);
-    for (int v : rel_rho) m.push_back(v);
-    for (int v : rel_rinv) m.push_back(v);
+    for (int k = 0; k < nrel; ++k) {  // one 16-byte record per release
+      m.push_back(rel_i[k]);
+      m.push_back(rel_rho[k]);
+      m.push_back(rel_rinv[k]);
+      m.push_back(0);
+    }
     while (m.size() % 4) m.push_back(0);
     S.meta_off[ch] = static_cast<int>(S.meta.size());
     S.meta_words[ch] = static_cast<int>(m.size());
     S.max_meta_words = std::max(S.max_meta_words, static_cast<int>(m.size()));
     S.meta.insert(S.meta.end(), m.begin(), m.end());
-    for (int u = 0; u < nu; ++u)
-      for (int s = 0; s < 4; ++s)
-        if (units[u].src[s] == zero_row) S.pad_boff.push_back(S.chunk_off[ch] + u * 128 + s);
+    for (int li = 0; li < 3; ++li)
+      for (int u = 0; u < static_cast<int>(lists[li].size()); ++u)
+        for (int s2 = 0; s2 < 4; ++s2)
+          if (lists[li][u].src[s2] == zero_row) S.pad_boff.push_back(S.chunk_off[ch] + (base[li] + u) * 128 + s2);
   }
   S.chunk_off[S.n_chunks] = boff;
   S.blen = boff;
@@ -317,17 +374,9 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       *why = "backward stream misses an entry";
       return false;
     }
-  // ---- forward sweep: rows in order (row-gather form), columns ascending in a row
-  std::vector<int> entry_foff(hp.nnz_l, -1);
+  // ---- forward sweep (sweeper): rows in order (row-gather form), columns ascending in a row; pre rows excluded
   {
-    std::vector<std::vector<int>> row_entries(n);  // CSC entry indices of each row, columns ascending
-    std::vector<int> col_of(hp.nnz_l);
-    for (int c = 0; c < n; ++c)
-      for (int e = hp.lp[c]; e < hp.lp[c + 1]; ++e) {
-        row_entries[hp.li[e]].push_back(e);
-        col_of[e] = c;
-      }
-    auto row_units = [&](int i) { return (static_cast<int>(row_entries[i].size()) + 3) / 4; };
+    auto row_units = [&](int i) { return pre_row[i] ? 0 : (rcount[i] + 3) / 4; };
     std::vector<int> fb{0};
     {
       int units = 0;
@@ -341,7 +390,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       }
       fb.push_back(n);
     }
-    // drop empty chunks (rows without entries only)
+    // drop empty chunks (rows without sweeper work only)
     int foff = 0;
     for (size_t k = 0; k + 1 < fb.size(); ++k) {
       const int r0 = fb[k], r1 = fb[k + 1];
@@ -350,7 +399,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       for (int i = r0; i < r1; ++i) {
         const std::vector<int>& re = row_entries[i];
         const int cnt = static_cast<int>(re.size());
-        if (cnt == 0) continue;
+        if (cnt == 0 || pre_row[i]) continue;
         std::vector<int> slot_of;
         std::vector<UnitBuild> add = cut_units(cnt, true, i, zero_row, [&](int q) { return col_of[re[q]]; }, &slot_of);
         const int first = append_units(&units, std::move(add), 3, zero_row, &S.dummy_units);
@@ -370,8 +419,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       S.max_funits = std::max(S.max_funits, nu);
       S.fmeta.insert(S.fmeta.end(), m.begin(), m.end());
       for (int u = 0; u < nu; ++u)
-        for (int s = 0; s < 4; ++s)
-          if (units[u].src[s] == zero_row) S.pad_foff.push_back(foff + u * 128 + s);
+        for (int s2 = 0; s2 < 4; ++s2)
+          if (units[u].src[s2] == zero_row) S.pad_foff.push_back(foff + u * 128 + s2);
       foff += nu * 128;
     }
     S.n_fchunks = static_cast<int>(S.fchunk_units.size());
@@ -379,7 +428,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     S.flen = foff;
   }
   for (int e = 0; e < hp.nnz_l; ++e)
-    if (entry_foff[e] < 0) {
+    if (entry_foff[e] == -1 && !pre_row[hp.li[e]]) {
       *why = "forward stream misses an entry";
       return false;
     }

@@ -8,10 +8,11 @@
 // the chunk's columns).  Both are cut into chunks; every chunk is one
 // contiguous bulk copy (cp.async.bulk) into a shared-memory ring stage.
 //
-// ADMM state (x or z, y) and parameters (q or l, u) are stored per tile in
-// "release order" U: the order in which the backward sweep finishes with a KKT
-// index (after the smallest column whose correction reads it), so each chunk
-// of the backward sweep updates one contiguous U range.
+// ADMM state (x or z, y) and parameters (q or l, u) are stored per tile as one
+// 16-byte record per (index, lane), in "release order" U: the order in which
+// the backward sweep finishes with a KKT index (after the smallest column
+// whose correction reads it), so each chunk of the backward sweep updates one
+// contiguous U range.
 #pragma once
 
 #include <stdint.h>
@@ -42,8 +43,8 @@ constexpr int kChunkHeader = 8;
 // Backward chunk meta block (int32 words, 16-byte padded):
 //   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5] nprim [6..7] 0
 //   units (8 words each), then kUnitSentinels sentinel units
-//   rel_off[nrel] (byte offset of the released row; the nprim primal indices
-//   first), rel_rho[nrel], rel_rhoinv[nrel] (float bits)
+//   one record per release (4 words: byte offset of the released row, rho and
+//   rho^-1 float bits, 0); the nprim primal indices first
 // Forward chunk meta block: [0] nunits [1..7] 0, units, sentinels.
 // Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
 // Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
@@ -65,6 +66,8 @@ struct StreamPlan {
   const int* chunk_cols;    // [n_chunks]
   const int* chunk_u0;      // [n_chunks] first U index released
   const int* chunk_nrel;    // [n_chunks]
+  const int* chunk_pre_u0;     // [n_chunks] stage position of the releaser's forward units
+  const int* chunk_pre_units;  // [n_chunks] their count (copied in the first-right-hand-side pass too)
   const int* meta_off;      // [n_chunks]
   const int* meta_words;    // [n_chunks]
   const int* meta;
@@ -213,12 +216,14 @@ struct HostPattern {
 struct StreamTargets {
   int units = 16, cols = 16, rel = 12;  // backward chunks
   int funits = 16;                      // forward chunks
+  int offload = 0;                      // also give the releaser warp: 1 leaf columns, 2 pre rows (bits)
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.
 struct HostStream {
   int n_chunks = 0, blen = 0, max_units = 0, max_cols = 0, max_rel = 0, max_meta_words = 0;
   std::vector<int> chunk_off, chunk_units, chunk_cols, chunk_u0, chunk_nrel, meta_off, meta_words, meta;
+  std::vector<int> chunk_pre_u0, chunk_pre_units;
   int n_fchunks = 0, flen = 0, max_funits = 0, max_fmeta_words = 0;
   std::vector<int> fchunk_off, fchunk_units, fmeta_off, fmeta_words, fmeta;
   std::vector<int> col_uoff, dinv_off, proc_boff, proc_foff, pad_boff, pad_foff, upd_pos, step_doff;

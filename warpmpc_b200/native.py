@@ -199,7 +199,7 @@ SIGNATURES = {
     "wmpc_stream_schedule_host": (
         ctypes.c_int,
         [ctypes.POINTER(PatternDesc), _f32p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-         ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+         ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
     ),
     "wmpc_profile_begin": (ctypes.c_int, []),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),

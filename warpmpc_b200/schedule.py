@@ -15,7 +15,7 @@ import numpy as np
 from . import native
 from .jax_qdldl.planning import plan_ragged_program
 
-DEFAULT_TARGETS = (16, 16, 12, 16)  # backward units, columns, releases; forward units
+DEFAULT_TARGETS = (16, 16, 12, 16, 0)  # backward units, columns, releases; forward units; offload bits
 
 
 def _pattern_desc(qp):
@@ -44,7 +44,8 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
     """Schedule of an OSQP plan (rho per constraint) as NumPy arrays.
 
     targets: (backward units, backward columns, backward releases, forward
-    units) per chunk."""
+    units) per chunk, and the offload bits (1: leaf columns, 2: rows reading
+    only leaf rows, solved by the releasing warp)."""
     qp = plan.qdldl_plan
     desc, keep, rg = _pattern_desc(qp)
     rho = native.f32(plan.rho_vec)
@@ -97,6 +98,8 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
     out["dummy_units"] = ndum
     take("pad_boff", npb)
     take("pad_foff", npf)
+    take("chunk_pre_u0", n_chunks)
+    take("chunk_pre_units", n_chunks)
     assert pos == buf.size
     out["ragged"] = rg
     return out
