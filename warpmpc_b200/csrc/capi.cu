@@ -527,8 +527,13 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (const char* v = getenv("WMPC_STREAM_FUNITS")) targets.funits = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_OFFLOAD")) targets.offload = atoi(v) & 3;
     if (targets.units <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.funits <= 0) targets = StreamTargets();
+    // iterate-change unscale factors (original KKT order) for early termination
+    std::vector<float> unscale(hp.n, 1.0f);
+    for (int j = 0; j < n; ++j) unscale[j] = desc->scaling_d[j];
+    for (int r = 0; r < m; ++r) unscale[n + r] = std::max(desc->scaling_einv[r], desc->y_unscale[r]);
     bool ok = build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, &q->stream_why) &&
-              build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why);
+              build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why,
+                                    unscale.data());
     StreamPlan& sp = q->sp;
     if (ok) {
       sp.n = hp.n;

@@ -237,10 +237,13 @@ __device__ __forceinline__ bool finite_res(const Residuals& r) {
   return isfinite(r.prim) && isfinite(r.dual) && isfinite(r.obj);
 }
 
+// Exact residuals of the final iterate, status, unscaling.  eps_abs >= 0: also
+// set SOLVED when OSQP's termination test holds (solves run with termination).
 __global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
                                 const float* __restrict__ aT, long long lda, int sba, State st,
                                 const float* __restrict__ qT, float* prim, float* dual, float* obj,
-                                int* status, int batch, const int* status_in, const int* abort_word) {
+                                int* status, int batch, const int* status_in, const int* abort_word,
+                                float eps_abs = -1.0f, float eps_rel = 0.0f) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
   InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
@@ -250,6 +253,11 @@ __global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long 
   obj[b] = r.obj;
   if (status) {
     int v = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
+    if (eps_abs >= 0.0f && finite_res(r)) {
+      const float eps_p = eps_abs + eps_rel * fmaxf(r.ax_norm, r.z_norm);
+      const float eps_d = eps_abs + eps_rel * fmaxf(fmaxf(r.px_norm, r.aty_norm), r.q_norm);
+      if (r.prim <= eps_p && r.dual <= eps_d) v |= WMPC_STATUS_SOLVED;
+    }
     if (status_in) v |= status_in[b];
     if (abort_word && *abort_word) v |= WMPC_STATUS_KERNEL_ABORT;
     status[b] = v;
@@ -432,10 +440,12 @@ int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int 
 int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
                         int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
                         const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int batch, int max_iter, int num_sms, bool reuse_factor, cudaStream_t s);
+                        int* iters, int batch, int max_iter, int check_every, float chg_eps, int num_sms,
+                        bool reuse_factor, cudaStream_t s);
 
 static bool stream_eligible(const wmpc_osqp& q, const wmpc_osqp_options* opt) {
-  return q.has_stream && (opt == nullptr || opt->check_termination == 0) && !env_disabled("WMPC_DISABLE_STREAM");
+  (void)opt;
+  return q.has_stream && !env_disabled("WMPC_DISABLE_STREAM");
 }
 
 size_t osqp_workspace_bytes(const wmpc_osqp& q, int batch, int pb, int ab, int mode, bool external) {
@@ -513,14 +523,19 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
 
   if (L.streaming) {
     WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
+    // termination: a tile stops once every instance's largest unscaled iterate
+    // change over an iteration is below eps_abs; SOLVED comes from the exact
+    // residuals of the final iterate
+    const int check = opt.check_termination > 0 ? opt.check_termination : 0;
     if ((rc = launch_stream_solve(pat, q.sp, o, L.pT, ldp, sbp, L.aT, lda, sba, L.x, L.z, L.y, L.qs, L.ls, L.us,
-                                  L.stream_ws, L.stream_status, L.error_word, B, opt.max_iter, q.num_sms,
-                                  opt.reuse_factor != 0, s)))
+                                  L.stream_ws, L.stream_status, L.error_word, check ? d.iters : nullptr, B,
+                                  opt.max_iter, check, opt.eps_abs, q.num_sms, opt.reuse_factor != 0, s)))
       return rc;
     residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
-                                                     d.dual_res, d.obj, d.status, B, L.stream_status, L.error_word);
+                                                     d.dual_res, d.obj, d.status, B, L.stream_status, L.error_word,
+                                                     check ? opt.eps_abs : -1.0f, opt.eps_rel);
     WMPC_LAUNCH_CHECK();
-    if (d.iters) {
+    if (d.iters && !check) {
       fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
       WMPC_LAUNCH_CHECK();
     }

@@ -220,7 +220,10 @@ struct StreamArgs {
   const float* fstream;
   float4* state;  // [tile][U][lane] ADMM state records
   int* error;   // one word: 0 ok, 1 pipeline timeout
-  int n_tiles, max_iter;
+  int* iters;   // [batch] iterations run (may be null)
+  int n_tiles, max_iter, batch;
+  int check_every;  // > 0: stop a tile once every lane's largest unscaled iterate change <= chg_eps
+  float chg_eps;
   float sigma, alpha, one_minus_alpha;
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
@@ -245,12 +248,19 @@ struct Ring {
 
 // Visit one tile's items: backward chunks descending with releases only
 // (first right-hand side), then per iteration the forward chunks ascending
-// and the backward chunks descending.  Stops (false) when f does.
-template <typename F>
-__device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_iter, F& f) {
+// and the backward chunks descending.  Before every iteration after the first
+// cont(it) decides: 1 go on, 0 the tile converged (stop here), -1 abort.
+// Returns false when f or cont aborts.
+template <typename F, typename C>
+__device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_iter, F& f, C& cont) {
   for (int ch = n_chunks - 1; ch >= 0; --ch)
     if (!f(kItemRel, ch)) return false;
   for (int it = 0; it < max_iter; ++it) {
+    if (it > 0) {
+      const int c = cont(it);
+      if (c < 0) return false;
+      if (c == 0) return true;
+    }
     for (int ch = 0; ch < n_fchunks; ++ch)
       if (!f(kItemFwd, ch)) return false;
     for (int ch = n_chunks - 1; ch >= 0; --ch)
@@ -259,11 +269,15 @@ __device__ __forceinline__ bool traverse(int n_chunks, int n_fchunks, int max_it
   return true;
 }
 
+// Early termination is decided before iteration `it` when checking is on and
+// `it` is a multiple of the check period.
+__device__ __forceinline__ bool check_point(int check_every, int it) { return check_every > 0 && it % check_every == 0; }
+
 // Shared-memory layout: X [n + 2][32] | L ring | S ring | barriers | flags
 __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
   return (size_t)(n + 2) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
-         16 * (size_t)(lstages + sstages) + 16;  // barriers, abort flag and the two counters
+         16 * (size_t)(lstages + sstages) + 16;  // barriers, abort flag, the two counters, the stop item
 }
 
 // One unit's operands, loaded ahead of its arithmetic.
@@ -365,7 +379,7 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 //   S:   this lane's state record of release 0 in the stage (k-th at S[32 k])
 struct RelGroup {
   int o[4], kk[4];
-  float x[4], rho[4], rinv[4];
+  float x[4], rho[4], rinv[4], f[4];
   float4 st[4];
 };
 
@@ -379,6 +393,7 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
     g.o[j] = r.x;
     g.rho[j] = __int_as_float(r.y);
     g.rinv[j] = __int_as_float(r.z);
+    g.f[j] = __int_as_float(r.w);
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
     g.st[j] = S[kk * 32];
   }
@@ -390,36 +405,42 @@ struct RelParams {
 
 // primal index: x <- alpha x~ + (1 - alpha) x; next rhs sigma x - q
 // constraint: z, y update and next rhs z - rho^-1 y (solver.py:806-820)
+// frozen: this lane's instance has converged; its state and next right-hand
+// side stay as they are (recomputed from the unchanged state).
 template <bool kCons>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float4* stu) {
+                                                 float4* stu, float& chg, bool frozen) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
     float2* out = reinterpret_cast<float2*>(stu + g.kk[j] * 32);
     if (!kCons) {
-      const float xn = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
+      const float xa = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
+      const float xn = frozen ? g.st[j].x : xa;
       *out = make_float2(xn, g.st[j].y);
       *xi = rp.sigma * xn - g.st[j].z;
+      chg = fmaxf(chg, fabsf(xn - g.st[j].x) * g.f[j]);
     } else {
       const float rinv = g.rinv[j];
       const float sv0 = g.st[j].x, yk = g.st[j].y;
       const float rz = sv0 - rinv * yk;
       const float zt = rz + rinv * g.x[j];
       const float zr = rp.alpha * zt + rp.oma * sv0;
-      float zn = zr + rinv * yk;
-      zn = (zn < g.st[j].z) ? g.st[j].z : zn;
-      zn = (zn > g.st[j].w) ? g.st[j].w : zn;
-      const float yn = yk + g.rho[j] * (zr - zn);
+      float za = zr + rinv * yk;
+      za = (za < g.st[j].z) ? g.st[j].z : za;
+      za = (za > g.st[j].w) ? g.st[j].w : za;
+      const float ya = yk + g.rho[j] * (zr - za);
+      const float zn = frozen ? sv0 : za, yn = frozen ? yk : ya;
       *out = make_float2(zn, yn);
       *xi = zn - rinv * yn;
+      chg = fmaxf(chg, fmaxf(fabsf(zn - sv0), fabsf(yn - yk)) * g.f[j]);
     }
   }
 }
 
 template <bool kCons>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const RelParams& rp,
-                                             unsigned char* xb, float4* stu) {
+                                             unsigned char* xb, float4* stu, float& chg, bool frozen) {
   if (begin >= end) return;
   RelGroup a, b;
   load_rel_group(rel, begin, end, S, xb, a);
@@ -427,11 +448,11 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + 4 < end ? k + 4 : end - 1;
     load_rel_group(rel, kb, end, S, xb, b);
-    update_rel_group<kCons>(a, rp, xb, stu);
+    update_rel_group<kCons>(a, rp, xb, stu, chg, frozen);
     if (k + 4 >= end) break;
     const int ka = k + 8 < end ? k + 8 : end - 1;
     load_rel_group(rel, ka, end, S, xb, a);
-    update_rel_group<kCons>(b, rp, xb, stu);
+    update_rel_group<kCons>(b, rp, xb, stu, chg, frozen);
     if (k + 8 >= end) break;
   }
 }
@@ -459,6 +480,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sempty + a.sstages);
   unsigned* sweep_done = reinterpret_cast<unsigned*>(sempty + a.sstages) + 1;
   unsigned* rel_done = sweep_done + 1;
+  volatile unsigned* stop_at = rel_done + 1;  // item index where a converged tile's items end
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
@@ -472,6 +494,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     *abort_flag = 0;
     *sweep_done = 0;
     *rel_done = 0;
+    *stop_at = 0xffffffffu;
     fence_mbarrier_init();
   }
   if (warp == 0) X[n * 32 + lane] = 0.0f;  // zero row read by padding slots
@@ -524,7 +547,13 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
           }
           return true;
         };
-        if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, produce)) {
+        // before a checked iteration: wait until the releaser has decided
+        auto cont = [&](int it) -> int {
+          if (!check_point(a.check_every, it)) return 1;
+          if (!wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return -1;
+          return *stop_at == issued_l ? 0 : 1;
+        };
+        if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, produce, cont)) {
           *abort_flag = 1;
           break;
         }
@@ -566,7 +595,12 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         ++t;
         return true;
       };
-      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, sweep)) ok = false;
+      auto cont = [&](int it) -> int {
+        if (!check_point(a.check_every, it)) return 1;
+        if (!wait_counter_bounded(rel_done, t, abort_flag, kWaitLimitNs)) return -1;
+        return *stop_at == t ? 0 : 1;
+      };
+      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, sweep, cont)) ok = false;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   } else {
@@ -578,8 +612,10 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     bool ok = true;
     for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
       float4* stt = a.state + (size_t)tile * n * 32 + lane;
+      float chg = 0.0f;  // this lane's largest unscaled iterate change in the current iteration
+      int iters_run = 0, frozen_at = 0;
+      bool stop = false, frozen = false;
       auto release = [&](int kind, int ch) -> bool {
-        (void)ch;
         if (kind != kItemFwd) {
           if (kind == kItemBwd) {
             // the chunk's columns are solved (and its stage is full)
@@ -612,8 +648,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
           } else {
             float4* stu = stt + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false>(rel, 0, nprim, S, rp, xb, stu);
-            run_releases<true>(rel, nprim, nrel, S, rp, xb, stu);
+            run_releases<false>(rel, 0, nprim, S, rp, xb, stu, chg, frozen);
+            run_releases<true>(rel, nprim, nrel, S, rp, xb, stu, chg, frozen);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -630,6 +666,19 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
           }
           sr.advance(a.sstages);
         }
+        if (kind == kItemBwd && ch == 0) {
+          // an iteration is complete: decide (before publishing it) whether the tile stops here
+          ++iters_run;
+          if (check_point(a.check_every, iters_run) && iters_run < a.max_iter) {
+            if (!frozen && chg <= a.chg_eps) {
+              frozen = true;
+              frozen_at = iters_run;
+            }
+            stop = __all_sync(0xffffffffu, frozen);
+            if (stop && lane == 0) *stop_at = t + 1;
+          }
+          chg = 0.0f;
+        }
         __syncwarp();
         if (lane == 0) st_release_cta(rel_done, t + 1);
         __syncwarp();
@@ -637,7 +686,9 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         ++t;
         return true;
       };
-      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, release)) ok = false;
+      auto cont = [&](int it) -> int { (void)it; return stop ? 0 : 1; };
+      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, release, cont)) ok = false;
+      if (ok && a.iters && tile * 32 + lane < a.batch) a.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   }
@@ -698,7 +749,8 @@ size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
 int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
                         int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
                         const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int batch, int max_iter, int num_sms, bool reuse_factor, cudaStream_t s) {
+                        int* iters, int batch, int max_iter, int check_every, float chg_eps, int num_sms,
+                        bool reuse_factor, cudaStream_t s) {
   StreamLaunch cfg;
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
@@ -727,7 +779,7 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
     state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, state, batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
-  StreamArgs a{sp, bstream, fstream, state, error, n_tiles, max_iter, o.sigma, o.alpha,
+  StreamArgs a{sp, bstream, fstream, state, error, iters, n_tiles, max_iter, batch, check_every, chg_eps, o.sigma, o.alpha,
                o.one_minus_alpha, cfg.stages, cfg.sstages, cfg.meta_bytes, cfg.lbytes, cfg.sbytes};
   const int grid = n_tiles < num_sms ? n_tiles : num_sms;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));

@@ -164,7 +164,8 @@ void push_sentinels(int zero_row, int trash_row, std::vector<int>* m) {
 }  // namespace
 
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
-                           const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why) {
+                           const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why,
+                           const float* unscale_by_index) {
   const int n = hp.n;
   const int zero_row = n, trash_row = n + 1;
   HostStream& S = *out;
@@ -327,11 +328,17 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       for (int u = 0; u < static_cast<int>(lists[li].size()); ++u) push_unit_meta(lists[li][u], base[li] + u, trash_row, &m);
       push_sentinels(zero_row, trash_row, &m);
     }
-    std::vector<int> rel_i, rel_rho, rel_rinv;
+    std::vector<int> rel_i, rel_rho, rel_rinv, rel_unscale;
     for (int u = u0; u < u0 + nrel; ++u) {
       const int i = order[u];
       const int o = hp.p[i];
       rel_i.push_back(i * 128);
+      {
+        const float f = unscale_by_index ? unscale_by_index[o] : 1.0f;
+        int fb;
+        memcpy(&fb, &f, 4);
+        rel_unscale.push_back(fb);
+      }
       const bool cons = o >= n_primal;
       float rho = 0.f, rinv = 0.f;
       if (cons && rho_by_constraint) {
@@ -348,7 +355,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       m.push_back(rel_i[k]);
       m.push_back(rel_rho[k]);
       m.push_back(rel_rinv[k]);
-      m.push_back(0);
+      m.push_back(rel_unscale[k]);
     }
     while (m.size() % 4) m.push_back(0);
     S.meta_off[ch] = static_cast<int>(S.meta.size());

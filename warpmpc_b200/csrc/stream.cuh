@@ -44,7 +44,7 @@ constexpr int kChunkHeader = 8;
 //   [0] nunits [1] ncols [2] nrel [3] c0 [4] u0 [5] nprim [6..7] 0
 //   units (8 words each), then kUnitSentinels sentinel units
 //   one record per release (4 words: byte offset of the released row, rho and
-//   rho^-1 float bits, 0); the nprim primal indices first
+//   rho^-1 float bits, the index's unscale factor); the nprim primal indices first
 // Forward chunk meta block: [0] nunits [1..7] 0, units, sentinels.
 // Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
 // Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
@@ -234,8 +234,12 @@ struct HostStream {
   std::vector<int> u_of_perm;  // permuted index -> U index
 };
 
+// unscale_by_index (optional, original KKT order): the factor turning a scaled
+// iterate change into an unscaled one (D_j for a primal index, max(E^-1, E/c)
+// for a constraint), kept in the release records for early termination.
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
-                           const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why);
+                           const float* rhoinv_by_constraint, int n_primal, HostStream* out, std::string* why,
+                           const float* unscale_by_index = nullptr);
 bool build_factor_tables(const HostPattern& hp, std::vector<int>* init_slot, std::vector<int>* upd_ptr,
                          std::vector<unsigned short>* upd_slot, int* max_row_nnz, std::string* why);
 
