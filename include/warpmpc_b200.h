@@ -234,6 +234,23 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
                     int32_t factor_batch, int32_t mode, void* workspace, size_t workspace_bytes,
                     wmpc_stream_t stream);
 
+/* Several problem classes (sparsity patterns) in one persistent launch: the
+ * work-queue form of wmpc_osqp_solve(mode = WMPC_OSQP_PERSISTENT) for a
+ * mixed-size batch (the reference solves each pattern with its own compiled
+ * solver, solver.py:685-982; this walks every class's instance tiles in one
+ * kernel, costliest class first, so classes of different sizes share the
+ * GPU).  Per class i: osqps[i], options[i] (reuse_factor must be 0), data[i]
+ * and its own workspace (workspaces[i], at least
+ * wmpc_osqp_workspace_bytes(osqps[i], data[i].batch, WMPC_OSQP_PERSISTENT, 0)
+ * bytes).  1 <= n_classes <= 6, all on one device.  Results as wmpc_osqp_solve,
+ * per class; with options[i].check_termination > 0 an instance stops once its
+ * largest unscaled iterate change over an iteration is at most eps_abs
+ * (data[i].iters receives its iteration count; SOLVED in data[i].status comes
+ * from the exact residuals of the returned iterate). */
+int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_options* options,
+                               const wmpc_osqp_batch* data, int32_t n_classes, void* const* workspaces,
+                               const size_t* workspace_bytes, wmpc_stream_t stream);
+
 /* Host-only export of the streaming schedule the persistent kernel uses for
  * a pattern (no counterpart in the reference; used to verify the schedule
  * on the CPU).  rho/rhoinv: per-constraint values (n_primal = number of

@@ -120,3 +120,20 @@ def test_stream_schedule_replay_bitexact(cls):
     assert 4 * sched["fchunk_units"].sum() == q.nnz_l - n_pre + sched["pad_foff"].size
     assert np.unique(sched["proc_boff"]).size == q.nnz_l and np.unique(sched["proc_foff"]).size == q.nnz_l
     assert sorted(sched["u_perm"].tolist()) == list(range(plan.qdldl_plan.n))
+
+
+def test_multiclass_entry_rejects_bad_arguments():
+    """wmpc_osqp_solve_persistent validates before touching a device."""
+    import ctypes
+
+    lib = native.lib()
+    null = ctypes.POINTER(ctypes.c_void_p)()
+    rc = lib.wmpc_osqp_solve_persistent(null, None, None, 1, null, None, None)
+    assert rc != 0 and b"null" in lib.wmpc_last_error_string()
+    handles = (ctypes.c_void_p * 1)(None)
+    opts = (native.OsqpOptions * 1)()
+    data = (native.OsqpBatch * 1)()
+    ws = (ctypes.c_void_p * 1)(None)
+    wsb = (ctypes.c_size_t * 1)(0)
+    rc = lib.wmpc_osqp_solve_persistent(handles, opts, data, 7, ws, wsb, None)
+    assert rc != 0 and b"n_classes" in lib.wmpc_last_error_string()

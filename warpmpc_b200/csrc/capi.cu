@@ -78,6 +78,8 @@ int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb
 int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
                const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
                cudaStream_t s);
+int osqp_solve_multi(const wmpc_osqp* const* qs, const wmpc_osqp_options* opts, const wmpc_osqp_batch* ds, int n,
+                     void* const* ws, const size_t* ws_bytes, cudaStream_t s);
 
 namespace {
 
@@ -682,6 +684,31 @@ int wmpc_osqp_solve(const wmpc_osqp* osqp, const wmpc_osqp_options* options, con
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
   return osqp_solve(*osqp, *options, d, lx, dinv, factor_batch, mode, workspace, workspace_bytes,
                     static_cast<cudaStream_t>(stream));
+}
+
+int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_options* options,
+                               const wmpc_osqp_batch* data, int32_t n_classes, void* const* workspaces,
+                               const size_t* workspace_bytes, wmpc_stream_t stream) {
+  if (!osqps || !options || !data || !workspaces || !workspace_bytes) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  if (n_classes < 1 || n_classes > 6) return fail(WMPC_ERR_INVALID_ARGUMENT, "n_classes must be 1..6, got %d", n_classes);
+  for (int i = 0; i < n_classes; ++i) {
+    const wmpc_osqp_batch& d = data[i];
+    if (!osqps[i]) return fail(WMPC_ERR_INVALID_ARGUMENT, "null handle for class %d", i);
+    if (d.batch < 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "negative batch (class %d)", i);
+    if (d.batch == 0) continue;
+    if ((d.p_batch != 1 && d.p_batch != d.batch) || (d.a_batch != 1 && d.a_batch != d.batch))
+      return fail(WMPC_ERR_INVALID_ARGUMENT, "p_batch/a_batch must be 1 or batch (class %d)", i);
+    if (!d.p_values || !d.a_values || !d.q || !d.l || !d.u || !d.x || !d.z || !d.y || !d.prim_res || !d.dual_res ||
+        !d.obj)
+      return fail(WMPC_ERR_INVALID_ARGUMENT, "null buffer (class %d)", i);
+    if (options[i].max_iter < 0 || options[i].check_termination < 0)
+      return fail(WMPC_ERR_INVALID_ARGUMENT, "max_iter and check_termination must be nonnegative (class %d)", i);
+    if (options[i].reuse_factor) return fail(WMPC_ERR_UNSUPPORTED, "multi-class solves factor every class");
+  }
+  DeviceGuard guard(osqps[0]->device);
+  if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqps[0]->device);
+  return osqp_solve_multi(osqps, options, data, n_classes, workspaces, workspace_bytes,
+                          static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

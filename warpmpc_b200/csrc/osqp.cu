@@ -7,6 +7,8 @@
 // residuals 866-871); -fmad=false keeps every product and sum separately
 // rounded.
 #include "common.cuh"
+#include <vector>
+
 #include "osqp.cuh"
 #include "qdldl.cuh"
 
@@ -437,11 +439,13 @@ int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int 
 
 }  // namespace
 
-int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
-                        int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
-                        const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int* iters, int batch, int max_iter, int check_every, float chg_eps, int num_sms,
-                        bool reuse_factor, cudaStream_t s);
+int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
+                 const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
+                 const float* qs, const float* ls, const float* us, float* work, int* status, int batch,
+                 int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s);
+int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s);
+int stream_end(const StreamPlan& sp, const Osqp& o, const StreamJobDesc& job, float* x, float* z, float* y,
+               cudaStream_t s);
 
 static bool stream_eligible(const wmpc_osqp& q, const wmpc_osqp_options* opt) {
   (void)opt;
@@ -485,21 +489,14 @@ int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb
   return assemble_and_factor(o, pat, pT, pb, aT, ab, kkt, lx, d, dinv, scratch, f, s);
 }
 
-int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
-               const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
-               cudaStream_t s) {
-  const Osqp& o = q.dev;
-  const Pattern& pat = q.kkt_plan->pat;
-  const int B = d.batch;
-  if (B <= 0) return WMPC_OK;
-  const int pb = d.p_batch, ab = d.a_batch;
-  const bool external = lx_ext != nullptr;
-  size_t need = 0;
-  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need, &q, stream_eligible(q, &opt));
-  if (ws == nullptr || ws_bytes < need)
-    return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
+namespace {
+
+// Batch-major inputs -> symbolic-major, scaled where the reference scales;
+// the starting iterate (warm start, or zero).
+int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
+                 cudaStream_t s) {
+  const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
   int rc;
-  // batch-major inputs -> symbolic-major, scaled where the reference scales
   if ((rc = transpose_in(d.p_values, o.nnz_p, pb, o.nnz_p, nullptr, L.pT, pb, s))) return rc;
   if ((rc = transpose_in(d.a_values, o.nnz_a, ab, o.nnz_a, nullptr, L.aT, ab, s))) return rc;
   if ((rc = transpose_in(d.q, o.n, B, o.n, nullptr, L.qT, B, s))) return rc;
@@ -516,34 +513,82 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
     WMPC_CUDA_TRY(cudaMemsetAsync(L.z, 0, sizeof(float) * (size_t)o.m * B, s));
     WMPC_CUDA_TRY(cudaMemsetAsync(L.y, 0, sizeof(float) * (size_t)o.m * B, s));
   }
+  return WMPC_OK;
+}
+
+// Streaming solve, first half: inputs staged, factor, state records; fills `job`.
+int stream_solve_begin(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
+                       StreamJobDesc* job, cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
+  int rc;
+  if ((rc = stage_inputs(o, opt, d, L, s))) return rc;
+  WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
+  if ((rc = stream_begin(q.kkt_plan->pat, q.sp, o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, L.x, L.z, L.y,
+                         L.qs, L.ls, L.us, L.stream_ws, L.stream_status, B, q.num_sms, opt.reuse_factor != 0, job, s)))
+    return rc;
+  // termination: an instance stops (freezes) once its largest unscaled iterate
+  // change over an iteration is at most eps_abs -- a heuristic stand-in for
+  // OSQP's residual test, which needs P and A products the streaming kernel
+  // does not form; SOLVED comes from the exact residuals of the final iterate
+  const int check = opt.check_termination > 0 ? opt.check_termination : 0;
+  job->max_iter = opt.max_iter;
+  job->check_every = check;
+  job->chg_eps = opt.eps_abs;
+  job->iters = check ? d.iters : nullptr;
+  return WMPC_OK;
+}
+
+// Streaming solve, second half: state back, exact residuals and status, outputs.
+int stream_solve_end(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
+                     const StreamJobDesc& job, const int* error_word, cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
+  const int check = opt.check_termination > 0 ? opt.check_termination : 0;
+  int rc;
+  if ((rc = stream_end(q.sp, o, job, L.x, L.z, L.y, s))) return rc;
+  State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
+  residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT,
+                                                   d.prim_res, d.dual_res, d.obj, d.status, B, L.stream_status,
+                                                   error_word, check ? opt.eps_abs : -1.0f, opt.eps_rel);
+  WMPC_LAUNCH_CHECK();
+  if (d.iters && !check) {
+    fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
+    WMPC_LAUNCH_CHECK();
+  }
+  if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
+  if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
+  if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
+  return WMPC_OK;
+}
+
+}  // namespace
+
+int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+               const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
+               cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const Pattern& pat = q.kkt_plan->pat;
+  const int B = d.batch;
+  if (B <= 0) return WMPC_OK;
+  const int pb = d.p_batch, ab = d.a_batch;
+  const bool external = lx_ext != nullptr;
+  size_t need = 0;
+  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need, &q, stream_eligible(q, &opt));
+  if (ws == nullptr || ws_bytes < need)
+    return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
+  int rc;
+  if (L.streaming) {
+    StreamJobDesc job;
+    if ((rc = stream_solve_begin(q, opt, d, L, &job, s))) return rc;
+    if ((rc = stream_run(&job, 1, L.error_word, q.num_sms, s))) return rc;
+    return stream_solve_end(q, opt, d, L, job, L.error_word, s);
+  }
+  if ((rc = stage_inputs(o, opt, d, L, s))) return rc;
   State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
   const int sbp = pb > 1 ? 1 : 0, sba = ab > 1 ? 1 : 0;
   const long long ldp = pb, lda = ab;
   const int kb = pb > ab ? pb : ab;
-
-  if (L.streaming) {
-    WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
-    // termination: a tile stops once every instance's largest unscaled iterate
-    // change over an iteration is below eps_abs; SOLVED comes from the exact
-    // residuals of the final iterate
-    const int check = opt.check_termination > 0 ? opt.check_termination : 0;
-    if ((rc = launch_stream_solve(pat, q.sp, o, L.pT, ldp, sbp, L.aT, lda, sba, L.x, L.z, L.y, L.qs, L.ls, L.us,
-                                  L.stream_ws, L.stream_status, L.error_word, check ? d.iters : nullptr, B,
-                                  opt.max_iter, check, opt.eps_abs, q.num_sms, opt.reuse_factor != 0, s)))
-      return rc;
-    residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
-                                                     d.dual_res, d.obj, d.status, B, L.stream_status, L.error_word,
-                                                     check ? opt.eps_abs : -1.0f, opt.eps_rel);
-    WMPC_LAUNCH_CHECK();
-    if (d.iters && !check) {
-      fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
-      WMPC_LAUNCH_CHECK();
-    }
-    if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
-    if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
-    if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
-    return WMPC_OK;
-  }
 
   // the factorization the iterations use
   const float* lx = lx_ext;
@@ -618,6 +663,42 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if ((rc = transpose_out(L.x, B, B, o.n, d.x, o.n, s))) return rc;
   if ((rc = transpose_out(L.z, B, B, o.m, d.z, o.m, s))) return rc;
   if ((rc = transpose_out(L.y, B, B, o.m, d.y, o.m, s))) return rc;
+  return WMPC_OK;
+}
+
+// Several OSQP classes (patterns) in one streaming launch: each class is
+// staged, factored and converted on its own, then one persistent kernel walks
+// every class's tiles (costliest class first), then each class's epilogue.
+int osqp_solve_multi(const wmpc_osqp* const* qs, const wmpc_osqp_options* opts, const wmpc_osqp_batch* ds, int n,
+                     void* const* ws, const size_t* ws_bytes, cudaStream_t s) {
+  if (n < 1 || n > 6) return fail(WMPC_ERR_INVALID_ARGUMENT, "1 to 6 classes per launch, got %d", n);
+  std::vector<Layout> L(n);
+  std::vector<StreamJobDesc> jobs(n);
+  std::vector<int> active;
+  int rc;
+  for (int i = 0; i < n; ++i) {
+    const wmpc_osqp& q = *qs[i];
+    const wmpc_osqp_batch& d = ds[i];
+    if (q.device != qs[0]->device) return fail(WMPC_ERR_INVALID_ARGUMENT, "all classes must be on one device");
+    if (!stream_eligible(q, &opts[i]))
+      return fail(WMPC_ERR_UNSUPPORTED, "class %d cannot use the streaming kernel: %s", i,
+                  q.has_stream ? "disabled by the environment" : q.stream_why.c_str());
+    if (d.batch <= 0) continue;
+    size_t need = 0;
+    L[i] = carve(q.dev, q.kkt_plan->pat, d.batch, d.p_batch, d.a_batch, WMPC_OSQP_PERSISTENT, false,
+                 static_cast<char*>(ws[i]), &need, &q, true);
+    if (ws[i] == nullptr || ws_bytes[i] < need)
+      return fail(WMPC_ERR_WORKSPACE, "class %d needs %zu workspace bytes, got %zu", i, need, ws_bytes[i]);
+    if ((rc = stream_solve_begin(q, opts[i], d, L[i], &jobs[i], s))) return rc;
+    active.push_back(i);
+  }
+  if (active.empty()) return WMPC_OK;
+  std::vector<StreamJobDesc> run;
+  for (int i : active) run.push_back(jobs[i]);
+  int* error_word = L[active[0]].error_word;
+  if ((rc = stream_run(run.data(), static_cast<int>(run.size()), error_word, qs[active[0]]->num_sms, s))) return rc;
+  for (int i : active)
+    if ((rc = stream_solve_end(*qs[i], opts[i], ds[i], L[i], jobs[i], error_word, s))) return rc;
   return WMPC_OK;
 }
 

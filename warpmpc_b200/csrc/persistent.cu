@@ -18,6 +18,8 @@
 //
 // Arithmetic is the reference's operation order (warp_backend.py:41-101,
 // 176-218; solver.py:806-820) with separately rounded products and sums.
+#include <algorithm>
+
 #include "osqp.cuh"
 #include "stream.cuh"
 
@@ -214,22 +216,42 @@ __global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float4
 // streaming ADMM kernel
 // ---------------------------------------------------------------------------
 
-struct StreamArgs {
+// One class of instances (one sparsity pattern) in a launch.
+struct StreamJob {
   StreamPlan sp;
   const float* bstream;
   const float* fstream;
   float4* state;  // [tile][U][lane] ADMM state records
-  int* error;   // one word: 0 ok, 1 pipeline timeout
-  int* iters;   // [batch] iterations run (may be null)
+  int* iters;     // [batch] iterations run (may be null)
   int n_tiles, max_iter, batch;
   int check_every;  // > 0: stop a tile once every lane's largest unscaled iterate change <= chg_eps
   float chg_eps;
   float sigma, alpha, one_minus_alpha;
+};
+
+constexpr int kMaxStreamJobs = 6;
+
+// A launch: up to kMaxStreamJobs classes; CTAs walk the combined tile list
+// (job 0's tiles first; jobs are ordered by cost).  The shared-memory layout
+// is sized for the largest class.
+struct StreamArgs {
+  StreamJob job[kMaxStreamJobs];
+  int tile_end[kMaxStreamJobs];  // cumulative tile counts
+  int n_jobs;
+  int x_rows;       // work vector rows reserved (largest KKT dimension + 2)
+  int* error;       // one word: 0 ok, 1 pipeline timeout
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
   int lbytes;       // per L stage L area
   int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes
 };
+static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
+
+__device__ __forceinline__ int job_of(const StreamArgs& a, int g) {
+  int c = 0;
+  while (c + 1 < a.n_jobs && g >= a.tile_end[c]) ++c;
+  return c;
+}
 
 enum : int { kItemRel = 0, kItemFwd = 1, kItemBwd = 2 };
 
@@ -465,13 +487,12 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // counters order the consumers: sweep_done (items the sweeper finished: a
 // backward item's releases need its columns solved) and rel_done (items the
 // releaser finished: a forward sweep needs every right-hand side).
-__global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
+__global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const StreamPlan& sp = a.sp;
-  const int n = sp.n;
   const int lstage_bytes = a.meta_bytes + a.lbytes;
+  const int total_tiles = a.tile_end[a.n_jobs - 1];
   float* X = reinterpret_cast<float*>(smem);
-  unsigned char* lring = smem + (size_t)(n + 2) * 128;
+  unsigned char* lring = smem + (size_t)a.x_rows * 128;
   unsigned char* sring = lring + (size_t)a.lstages * lstage_bytes;
   uint64_t* lfull = reinterpret_cast<uint64_t*>(sring + (size_t)a.sstages * a.sbytes);
   uint64_t* lempty = lfull + a.lstages;
@@ -497,7 +518,6 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     *stop_at = 0xffffffffu;
     fence_mbarrier_init();
   }
-  if (warp == 0) X[n * 32 + lane] = 0.0f;  // zero row read by padding slots
   __syncthreads();
 
   uint32_t issued_l = 0, issued_s = 0;  // producer: copies issued per ring
@@ -506,9 +526,14 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     // ------------------------------ producer ------------------------------
     if (lane == 0) {
       Ring lr{0, 0}, sr{0, 0};
-      for (int tile = blockIdx.x; tile < a.n_tiles && !*abort_flag; tile += gridDim.x) {
-        const float* bt = a.bstream + (size_t)tile * sp.blen;
-        const float* ft = a.fstream + (size_t)tile * sp.flen;
+      for (int g = blockIdx.x; g < total_tiles && !*abort_flag; g += gridDim.x) {
+        const int c = job_of(a, g);
+        const StreamJob& J = a.job[c];
+        const StreamPlan& sp = J.sp;
+        const int n = sp.n;
+        const int tile = g - (c ? a.tile_end[c - 1] : 0);
+        const float* bt = J.bstream + (size_t)tile * sp.blen;
+        const float* ft = J.fstream + (size_t)tile * sp.flen;
         const size_t soff = (size_t)tile * n * 32;
         auto produce = [&](int kind, int ch) -> bool {
           const bool fwd = kind == kItemFwd;
@@ -541,7 +566,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
             const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 512u;
             mbar_arrive_expect_tx(sfull + sr.stage, bytes);
-            if (bytes) bulk_g2s(ss, a.state + soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32, bytes, sfull + sr.stage);
+            if (bytes) bulk_g2s(ss, J.state + soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32, bytes, sfull + sr.stage);
             sr.advance(a.sstages);
             ++issued_s;
           }
@@ -549,11 +574,11 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         };
         // before a checked iteration: wait until the releaser has decided
         auto cont = [&](int it) -> int {
-          if (!check_point(a.check_every, it)) return 1;
+          if (!check_point(J.check_every, it)) return 1;
           if (!wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return -1;
           return *stop_at == issued_l ? 0 : 1;
         };
-        if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, produce, cont)) {
+        if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, produce, cont)) {
           *abort_flag = 1;
           break;
         }
@@ -565,7 +590,9 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
     unsigned t = 0;  // item index (all tiles)
     unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
     bool ok = true;
-    for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
+    for (int g = blockIdx.x; g < total_tiles && ok; g += gridDim.x) {
+      const StreamJob& J = a.job[job_of(a, g)];
+      const StreamPlan& sp = J.sp;
       auto sweep = [&](int kind, int ch) -> bool {
         if (kind != kItemRel) {
           // a forward sweep needs every right-hand side of the previous pass
@@ -596,22 +623,29 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         return true;
       };
       auto cont = [&](int it) -> int {
-        if (!check_point(a.check_every, it)) return 1;
+        if (!check_point(J.check_every, it)) return 1;
         if (!wait_counter_bounded(rel_done, t, abort_flag, kWaitLimitNs)) return -1;
         return *stop_at == t ? 0 : 1;
       };
-      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, sweep, cont)) ok = false;
+      if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, sweep, cont)) ok = false;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   } else {
     // ------------------------------ releaser ------------------------------
     Ring lr{0, 0}, sr{0, 0};
     unsigned t = 0;
-    const float sigma = a.sigma, alpha = a.alpha, oma = a.one_minus_alpha;
     unsigned char* xb = smem + lane * 4;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
-      float4* stt = a.state + (size_t)tile * n * 32 + lane;
+    for (int g = blockIdx.x; g < total_tiles && ok; g += gridDim.x) {
+      const int c = job_of(a, g);
+      const StreamJob& J = a.job[c];
+      const StreamPlan& sp = J.sp;
+      const int n = sp.n;
+      const int tile = g - (c ? a.tile_end[c - 1] : 0);
+      const float sigma = J.sigma, alpha = J.alpha, oma = J.one_minus_alpha;
+      // this class's zero row (read by padding slots); every earlier tile is done with X
+      X[n * 32 + lane] = 0.0f;
+      float4* stt = J.state + (size_t)tile * n * 32 + lane;
       float chg = 0.0f;  // this lane's largest unscaled iterate change in the current iteration
       int iters_run = 0, frozen_at = 0;
       bool stop = false, frozen = false;
@@ -669,8 +703,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         if (kind == kItemBwd && ch == 0) {
           // an iteration is complete: decide (before publishing it) whether the tile stops here
           ++iters_run;
-          if (check_point(a.check_every, iters_run) && iters_run < a.max_iter) {
-            if (!frozen && chg <= a.chg_eps) {
+          if (check_point(J.check_every, iters_run) && iters_run < J.max_iter) {
+            if (!frozen && chg <= J.chg_eps) {
               frozen = true;
               frozen_at = iters_run;
             }
@@ -687,8 +721,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
         return true;
       };
       auto cont = [&](int it) -> int { (void)it; return stop ? 0 : 1; };
-      if (!traverse(sp.n_chunks, sp.n_fchunks, a.max_iter, release, cont)) ok = false;
-      if (ok && a.iters && tile * 32 + lane < a.batch) a.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
+      if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, release, cont)) ok = false;
+      if (ok && J.iters && tile * 32 + lane < J.batch) J.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   }
@@ -715,25 +749,37 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(StreamArgs a) {
 // host side
 // ---------------------------------------------------------------------------
 
-bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
+namespace {
+
+struct RingSizes {
+  int meta_bytes, lbytes, sbytes, x_rows, lmax, smax;
+};
+
+RingSizes ring_sizes(const StreamPlan& sp) {
+  RingSizes r;
   const int mw = sp.max_meta_words > sp.max_fmeta_words ? sp.max_meta_words : sp.max_fmeta_words;
-  const int meta_bytes = ((mw * 4 + 127) / 128) * 128;
+  r.meta_bytes = ((mw * 4 + 127) / 128) * 128;
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
-  const int lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
-  const int sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
+  r.lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
+  r.sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
+  r.x_rows = sp.n + 2;
+  r.lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
+  r.smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
+  return r;
+}
+
+bool ring_config(const RingSizes& r, StreamLaunch* cfg) {
   // prefer deep rings: as many L stages as fit with at least 3 S stages
-  const int lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
-  const int smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
-  for (int ls = lmax; ls >= 2; --ls)
-    for (int ss = smax; ss >= 2; --ss) {
-      const size_t bytes = stream_smem_bytes(sp.n, ls, ss, meta_bytes + lbytes, sbytes);
+  for (int ls = r.lmax; ls >= 2; --ls)
+    for (int ss = r.smax; ss >= 2; --ss) {
+      const size_t bytes = stream_smem_bytes(r.x_rows - 2, ls, ss, r.meta_bytes + r.lbytes, r.sbytes);
       if (bytes <= (size_t)kMaxSmemBytes && (ss >= 3 || ls <= 3)) {
         cfg->stages = ls;
         cfg->sstages = ss;
-        cfg->meta_bytes = meta_bytes;
-        cfg->lbytes = lbytes;
-        cfg->sbytes = sbytes;
+        cfg->meta_bytes = r.meta_bytes;
+        cfg->lbytes = r.lbytes;
+        cfg->sbytes = r.sbytes;
         cfg->smem = bytes;
         return true;
       }
@@ -741,16 +787,20 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) {
   return false;
 }
 
+}  // namespace
+
+bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring_config(ring_sizes(sp), cfg); }
+
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
   return tiles * ((size_t)sp.blen + (size_t)sp.flen + 4 * 32 * (size_t)sp.n) + 64;
 }
 
-int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp,
-                        int sbp, const float* aT, long long lda, int sba, float* x, float* z, float* y,
-                        const float* qs, const float* ls, const float* us, float* work, int* status, int* error,
-                        int* iters, int batch, int max_iter, int check_every, float chg_eps, int num_sms,
-                        bool reuse_factor, cudaStream_t s) {
+// Factorization into the streams and the state into its records (one class).
+int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
+                 const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
+                 const float* qs, const float* ls, const float* us, float* work, int* status, int batch,
+                 int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s) {
   StreamLaunch cfg;
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
@@ -779,19 +829,83 @@ int launch_stream_solve(const Pattern& pat, const StreamPlan& sp, const Osqp& o,
     state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, state, batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
-  StreamArgs a{sp, bstream, fstream, state, error, iters, n_tiles, max_iter, batch, check_every, chg_eps, o.sigma, o.alpha,
-               o.one_minus_alpha, cfg.stages, cfg.sstages, cfg.meta_bytes, cfg.lbytes, cfg.sbytes};
-  const int grid = n_tiles < num_sms ? n_tiles : num_sms;
+  job->sp = sp;
+  job->bstream = bstream;
+  job->fstream = fstream;
+  job->state = state;
+  job->n_tiles = n_tiles;
+  job->batch = batch;
+  job->sigma = o.sigma;
+  job->alpha = o.alpha;
+  job->one_minus_alpha = o.one_minus_alpha;
+  return WMPC_OK;
+}
+
+// One launch over every class's tiles, the costliest class first.
+int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s) {
+  if (n_jobs < 1 || n_jobs > kMaxStreamJobs) return fail(WMPC_ERR_INVALID_ARGUMENT, "1 to %d classes per launch", kMaxStreamJobs);
+  RingSizes r{0, 0, 0, 0, 12, 6};
+  int order[kMaxStreamJobs];
+  double cost[kMaxStreamJobs];
+  for (int i = 0; i < n_jobs; ++i) {
+    const RingSizes ri = ring_sizes(jobs[i].sp);
+    r.meta_bytes = std::max(r.meta_bytes, ri.meta_bytes);
+    r.lbytes = std::max(r.lbytes, ri.lbytes);
+    r.sbytes = std::max(r.sbytes, ri.sbytes);
+    r.x_rows = std::max(r.x_rows, ri.x_rows);
+    r.lmax = std::min(r.lmax, ri.lmax);
+    r.smax = std::min(r.smax, ri.smax);
+    order[i] = i;
+    cost[i] = (double)(jobs[i].max_iter + 1) * ((double)jobs[i].sp.blen + jobs[i].sp.flen);
+  }
+  std::sort(order, order + n_jobs, [&](int x, int y) { return cost[x] > cost[y]; });
+  StreamLaunch cfg;
+  if (!ring_config(r, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "these classes do not fit one launch's shared memory");
+  StreamArgs a{};
+  int total = 0;
+  for (int k = 0; k < n_jobs; ++k) {
+    const StreamJobDesc& d = jobs[order[k]];
+    StreamJob& J = a.job[k];
+    J.sp = d.sp;
+    J.bstream = d.bstream;
+    J.fstream = d.fstream;
+    J.state = d.state;
+    J.iters = d.iters;
+    J.n_tiles = d.n_tiles;
+    J.max_iter = d.max_iter;
+    J.batch = d.batch;
+    J.check_every = d.check_every;
+    J.chg_eps = d.chg_eps;
+    J.sigma = d.sigma;
+    J.alpha = d.alpha;
+    J.one_minus_alpha = d.one_minus_alpha;
+    total += d.n_tiles;
+    a.tile_end[k] = total;
+  }
+  if (total == 0) return WMPC_OK;
+  a.n_jobs = n_jobs;
+  a.x_rows = r.x_rows;
+  a.error = error;
+  a.lstages = cfg.stages;
+  a.sstages = cfg.sstages;
+  a.meta_bytes = cfg.meta_bytes;
+  a.lbytes = cfg.lbytes;
+  a.sbytes = cfg.sbytes;
+  const int grid = total < num_sms ? total : num_sms;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
   admm_stream_kernel<<<grid, 96, cfg.smem, s>>>(a);
   profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
-  {
-    dim3 grid2(ceil_div(batch, 128), sp.n < 1024 ? sp.n : 1024);
-    stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, state, x, z, y, batch);
-    WMPC_LAUNCH_CHECK();
-  }
+  return WMPC_OK;
+}
+
+// The state records back to x, z, y (one class).
+int stream_end(const StreamPlan& sp, const Osqp& o, const StreamJobDesc& job, float* x, float* z, float* y,
+               cudaStream_t s) {
+  dim3 grid2(ceil_div(job.batch, 128), sp.n < 1024 ? sp.n : 1024);
+  stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, job.state, x, z, y, job.batch);
+  WMPC_LAUNCH_CHECK();
   return WMPC_OK;
 }
 

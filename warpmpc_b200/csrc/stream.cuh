@@ -250,4 +250,17 @@ struct StreamLaunch {
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
 size_t stream_workspace_floats(const StreamPlan& sp, int batch);
 
+// One class of a streaming launch (host view): its plan, stream buffers and
+// iteration settings.  stream_begin fills the buffers and sizes; the caller
+// sets max_iter, check_every, chg_eps and iters.
+struct StreamJobDesc {
+  StreamPlan sp;
+  const float* bstream = nullptr;
+  const float* fstream = nullptr;
+  float4* state = nullptr;
+  int* iters = nullptr;
+  int n_tiles = 0, max_iter = 0, batch = 0, check_every = 0;
+  float chg_eps = 0.0f, sigma = 0.0f, alpha = 0.0f, one_minus_alpha = 0.0f;
+};
+
 }  // namespace wmpc

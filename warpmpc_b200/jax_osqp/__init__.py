@@ -8,7 +8,8 @@ from .types import CompiledOSQP, FixedOSQPPlan, OSQPDerivativePlan, OSQPSettings
 
 
 def __getattr__(name):
-    if name in ("compile_osqp", "values_for_compiled_qdldl", "rhs_for_compiled_qdldl", "batch_from_compiled_qdldl"):
+    if name in ("compile_osqp", "solve_classes", "values_for_compiled_qdldl", "rhs_for_compiled_qdldl",
+                "batch_from_compiled_qdldl"):
         from . import solver
 
         return getattr(solver, name)
@@ -25,5 +26,6 @@ __all__ = [
     "build_osqp_plan",
     "compile_osqp",
     "rhs_for_compiled_qdldl",
+    "solve_classes",
     "values_for_compiled_qdldl",
 ]

@@ -160,15 +160,8 @@ class OSQPEngine:
                                           native.current_stream_handle(self.device)))
         return lx, dinv
 
-    def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
-              mode=None, out=None, keep_factor=False):
-        """Batched solve; returns ``(x, z, y, prim_res, dual_res, obj_val)``.
-
-        ``out`` optionally supplies those six output tensors (plus ``iters``,
-        ``status`` int32) to write into; warm-start inputs may alias ``out``
-        (they are consumed before the outputs are written), which lets a CUDA
-        graph chain solves without copies.
-        """
+    def _batch_args(self, p_values, a_values, q, l, u, warm, max_iter, check_termination, out):
+        """The C batch descriptor, options, tensors to keep alive and outputs of one solve."""
         import torch
 
         pl = self.plan
@@ -199,7 +192,7 @@ class OSQPEngine:
             for t, shp in zip(out, shapes):
                 if tuple(t.shape) != shp or not t.is_contiguous() or t.device != dev:
                     raise ValueError("out tensors have the wrong shape, layout or device")
-        keep = []
+        keep = [p, a, qm, lm, um]
         if warm is not None:
             wx = self._vec(warm[0], pl.n, batch, "warm_start_x")
             wz = self._vec(warm[1], pl.m, batch, "warm_start_z")
@@ -219,6 +212,22 @@ class OSQPEngine:
             check_termination=int(s.check_termination if check_termination is None else check_termination),
             eps_abs=np.float32(s.eps_abs), eps_rel=np.float32(s.eps_rel), warm_start=1 if warm is not None else 0,
         )
+        return data, opts, keep, (x, z, y, prim, dual, obj, iters, status), batch
+
+    def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
+              mode=None, out=None, keep_factor=False):
+        """Batched solve; returns ``(x, z, y, prim_res, dual_res, obj_val)``.
+
+        ``out`` optionally supplies those six output tensors (plus ``iters``,
+        ``status`` int32) to write into; warm-start inputs may alias ``out``
+        (they are consumed before the outputs are written), which lets a CUDA
+        graph chain solves without copies.
+        """
+        pl = self.plan
+        dev = self.device
+        data, opts, keep, outs, batch = self._batch_args(p_values, a_values, q, l, u, warm, max_iter,
+                                                         check_termination, out)
+        x, z, y, prim, dual, obj, iters, status = outs
         mode_id = _MODES[self.mode if mode is None else mode]
         lib = native.lib()
         if factor is not None:
@@ -393,3 +402,40 @@ def compile_osqp(
         solve_xy=extra.get("solve_xy"),
         engine=engine,
     )
+
+
+def solve_classes(problems_, max_iter=None, check_termination=None):
+    """Several problem classes (one OSQP engine each, persistent mode, one
+    device) solved by one persistent launch: ``problems_`` is a sequence of
+    ``(engine, p_values, a_values, q, l, u, warm)`` (``warm`` None or
+    ``(x, z, y)``); returns one ``(x, z, y, prim_res, dual_res, obj_val, iters,
+    status)`` per class.  The work-queue form of ``engine.solve`` for a
+    mixed-size batch (``wmpc_osqp_solve_persistent``)."""
+    lib = native.lib()
+    n = len(problems_)
+    if not 1 <= n <= 6:
+        raise ValueError("1 to 6 classes per launch")
+    datas, optss, keeps, outs, wss = [], [], [], [], []
+    dev = None
+    for engine, p, a, q, l, u, warm in problems_:
+        if engine.mode != "persistent":
+            raise ValueError("every class needs a persistent-mode engine")
+        if dev is None:
+            dev = engine.device
+        elif engine.device != dev:
+            raise ValueError("every class must be on one device")
+        data, opts, keep, out, batch = engine._batch_args(p, a, q, l, u, warm, max_iter, check_termination, None)
+        ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(engine.dev.handle, batch, _MODES["persistent"], 0), dev)
+        datas.append(data)
+        optss.append(opts)
+        keeps.append(keep)
+        outs.append(out)
+        wss.append((ws, wsb))
+    handles = (ctypes.c_void_p * n)(*[e.dev.handle for e, *_ in problems_])
+    opts_arr = (native.OsqpOptions * n)(*optss)
+    data_arr = (native.OsqpBatch * n)(*datas)
+    ws_arr = (ctypes.c_void_p * n)(*[native.tensor_ptr(w) for w, _ in wss])
+    wsb_arr = (ctypes.c_size_t * n)(*[b for _, b in wss])
+    native.check(lib.wmpc_osqp_solve_persistent(handles, opts_arr, data_arr, n, ws_arr, wsb_arr,
+                                                native.current_stream_handle(dev)))
+    return outs

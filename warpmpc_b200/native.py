@@ -196,6 +196,11 @@ SIGNATURES = {
         [ctypes.c_void_p, ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpAdjointBatch), ctypes.c_int32,
          ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p],
     ),
+    "wmpc_osqp_solve_persistent": (
+        ctypes.c_int,
+        [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpBatch), ctypes.c_int32,
+         ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p],
+    ),
     "wmpc_stream_schedule_host": (
         ctypes.c_int,
         [ctypes.POINTER(PatternDesc), _f32p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
