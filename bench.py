@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU-baseline sample duration")
     ap.add_argument("--no-grad", action="store_true", help="skip the forward+adjoint timing")
     ap.add_argument("--grad-batch", type=int, default=16384)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-size multi-class measurement")
+    ap.add_argument("--mixed-batch", type=int, default=131072, help="instances over the four mixed classes")
     return ap.parse_args()
 
 
@@ -342,6 +344,68 @@ def gradient_timing(args, dev, world):
     }
 
 
+def mixed_timing(args, dev, world):
+    """Mixed-size batch: args.mixed_batch instances spread over four linear MPC
+    classes (nx, nu, N) = (4, 2, 10), (4, 2, 40), (12, 4, 20), (12, 4, 30),
+    one multi-class persistent launch per step (wmpc_osqp_solve_persistent),
+    at most 50 ADMM iterations with early exit (an instance stops once its
+    iterate stops changing by more than 1e-3; SOLVED from exact residuals),
+    warm-started closed loop.  Also times the same launch with a fixed 50
+    iterations.  Value: instances at primal/dual residual <= 1e-3 per second."""
+    import torch
+
+    from warpmpc_b200 import multirank, problems
+    from warpmpc_b200.jax_osqp import OSQPSettings, compile_osqp, solve_classes
+
+    classes = problems.MIXED_CLASSES
+    per = max(1, args.mixed_batch // len(classes))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    items = []
+    for k, cls in enumerate(classes):
+        settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 50})
+        plan = problems.make_plan(problems.make_batch(cls, 1, seed=4000 + k), settings)
+        b = problems.make_batch(cls, per, seed=multirank.instance_seed(4000 + 10 * k, multirank.rank_env().rank))
+        comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
+        items.append([comp.engine, t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), None])
+
+    def step(check):
+        outs = solve_classes([tuple(it) for it in items], check_termination=check)
+        for it, o in zip(items, outs):
+            it[6] = (o[0], o[1], o[2])
+        return outs
+
+    res = {}
+    for label, check in (("early_exit", 1), ("fixed50", 0)):
+        for it in items:
+            it[6] = None
+        for _ in range(max(3, args.warmup)):
+            step(check)
+        torch.cuda.synchronize()
+        barrier(world)
+        steps = max(1, min(args.steps, 5))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            outs = step(check)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
+        ok = sum(int(((o[3] <= RES_TOL) & (o[4] <= RES_TOL)).sum().item()) for o in outs)
+        total_ok = multirank.sum_over_ranks(ok, multirank.rank_env(), dev) if world > 1 else ok
+        res[label] = {
+            "value": total_ok / (ms * 1e-3),
+            "ms_per_step": ms,
+            "converged_fraction": ok / (per * len(classes)),
+            "mean_iters": {cls.name: float(o[6].float().mean().item()) for cls, o in zip(classes, outs)},
+        }
+    return {
+        "workload": f"{per * len(classes)} instances/GPU over 4 linear MPC classes "
+                    "(4,2,10) (4,2,40) (12,4,20) (12,4,30), warm-started closed loop, <= 50 ADMM iterations",
+        "unit": "solves/s",
+        **res,
+    }
+
+
 def config_dict(args, cls, plan, batch):
     return {
         "workload": f"linear {cls.name} MPC nx={cls.nx} nu={cls.nu} N={cls.horizon}, warm-started closed loop",
@@ -523,6 +587,9 @@ def main():
     grad = None
     if not args.no_grad:
         grad = gradient_timing(args, dev, world)
+    mixed = None
+    if not args.no_mixed:
+        mixed = mixed_timing(args, dev, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -551,6 +618,7 @@ def main():
             "persistent_over_plain": (value / plain_res["value"]) if plain_res and plain_res["value"] else None,
             "fwd_bwd_over_fwd": grad["ratio"] if grad else None,
             "gradient": grad,
+            "mixed": mixed,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
