@@ -72,3 +72,37 @@ def test_classes_with_termination(cuda_device):
         ref_ok = (ref[3] <= 1e-3) & (ref[4] <= 1e-3)
         assert solved.sum() >= 0.9 * ref_ok.sum(), (solved.sum(), ref_ok.sum())
     assert sum(stopped_early) > 0
+
+
+def test_classes_warm_started_termination_is_sound(cuda_device):
+    """Warm starts near a solution: an instance may stop at its first check,
+    but only once its exact primal residual is within eps_abs (the kernel
+    carries A x - z through the iterations), so the early stops keep their
+    solutions -- in a closed loop the starting iterate is often already
+    primal-infeasible by more than eps while barely moving."""
+    specs = [(problems.SMALL, 64), (problems.QUADROTOR, 50)]
+    items, plans, batches = [], [], []
+    for k, (cls, batch) in enumerate(specs):
+        b = problems.make_batch(cls, batch, seed=60 + k)
+        settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 300})
+        plan = problems.make_plan(b, settings)
+        # start from the solution of a neighbouring problem (q and the bounds moved)
+        rng = np.random.default_rng(70 + k)
+        q0 = (b.q + 0.05 * rng.standard_normal(b.q.shape)).astype(np.float32)
+        cold = osqp_ref.solve(plan, b.p_values, b.a_values, q0, b.l, b.u, max_iter=100)
+        warm = tuple(np.asarray(w, dtype=np.float32) for w in cold[:3])
+        comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+        items.append(_problem(comp, b, warm))
+        plans.append(plan)
+        batches.append((b, warm))
+    outs = solve_classes(items, check_termination=1)
+    for out, plan, (b, warm) in zip(outs, plans, batches):
+        x, z, y, prim, dual, obj, iters, status = (t.cpu().numpy() for t in out)
+        a64 = b.a_values.astype(np.float64)
+        prim64 = np.abs(osqp_ref.a_matvec(plan, a64, x.astype(np.float64)) - z).max(1)
+        early = iters < 300
+        assert np.all(prim64[early] <= 1e-3 * 1.01), prim64[early].max()
+        ref = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, *warm)
+        ref_ok = (ref[3] <= 1e-3) & (ref[4] <= 1e-3)
+        solved = (status & 1) != 0
+        assert solved.sum() >= 0.9 * ref_ok.sum(), (solved.sum(), ref_ok.sum())

@@ -441,8 +441,8 @@ int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int 
 
 int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
                  const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
-                 const float* qs, const float* ls, const float* us, float* work, int* status, int batch,
-                 int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s);
+                 const float* qs, const float* ls, const float* us, bool warm, bool track, float* work,
+                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s);
 int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s);
 int stream_end(const StreamPlan& sp, const Osqp& o, const StreamJobDesc& job, float* x, float* z, float* y,
                cudaStream_t s);
@@ -521,17 +521,20 @@ int stream_solve_begin(const wmpc_osqp& q, const wmpc_osqp_options& opt, const w
                        StreamJobDesc* job, cudaStream_t s) {
   const Osqp& o = q.dev;
   const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
+  const int check = opt.check_termination > 0 ? opt.check_termination : 0;
   int rc;
   if ((rc = stage_inputs(o, opt, d, L, s))) return rc;
   WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
   if ((rc = stream_begin(q.kkt_plan->pat, q.sp, o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, L.x, L.z, L.y,
-                         L.qs, L.ls, L.us, L.stream_ws, L.stream_status, B, q.num_sms, opt.reuse_factor != 0, job, s)))
+                         L.qs, L.ls, L.us, opt.warm_start != 0, check > 0, L.stream_ws, L.stream_status, B,
+                         q.num_sms, opt.reuse_factor != 0, job, s)))
     return rc;
-  // termination: an instance stops (freezes) once its largest unscaled iterate
-  // change over an iteration is at most eps_abs -- a heuristic stand-in for
-  // OSQP's residual test, which needs P and A products the streaming kernel
-  // does not form; SOLVED comes from the exact residuals of the final iterate
-  const int check = opt.check_termination > 0 ? opt.check_termination : 0;
+  // termination: an instance stops (freezes) once both its primal residual
+  // (A x - z, carried exactly through the iterations) and its largest iterate
+  // change over an iteration are at most eps_abs, unscaled; the change stands
+  // in for the dual residual, which needs P and A-transpose products the
+  // streaming kernel does not form.  SOLVED comes from the exact residuals of
+  // the final iterate.
   job->max_iter = opt.max_iter;
   job->check_every = check;
   job->chg_eps = opt.eps_abs;

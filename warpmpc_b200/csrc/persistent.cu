@@ -170,25 +170,42 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
 // ---------------------------------------------------------------------------
 
 // ADMM state per tile in release order U, one 16-byte record per (index, lane):
-// (x, 0, sigma-scaled q, 0) for a primal index, (z, y, l, u) for a constraint.
-__global__ void state_to_stream_kernel(StreamPlan sp, int n_primal, const float* __restrict__ x,
+// (x, 0, sigma-scaled q, 0) for a primal index, (z, y, l, u) for a constraint;
+// and, when termination is checked (pres != null), the scaled primal residual
+// (A x - z)_r of a constraint (0 for a primal index), formed here for a warm
+// start (a cold start's x = z = 0 gives 0).
+__global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, bool warm, const float* __restrict__ x,
                                        const float* __restrict__ z, const float* __restrict__ y,
                                        const float* __restrict__ qs, const float* __restrict__ ls,
-                                       const float* __restrict__ us, float4* __restrict__ state, int batch,
-                                       int n_tiles) {
+                                       const float* __restrict__ us, float4* __restrict__ state,
+                                       float* __restrict__ pres, int batch, int n_tiles) {
+  const int n_primal = o.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n_tiles * 32) return;
   const int bb = b < batch ? b : batch - 1;
   const int tile = b >> 5, lane = b & 31;
   for (int u = blockIdx.y; u < sp.n; u += gridDim.y) {
-    const int o = __ldg(sp.u_orig + u);
+    const int k = __ldg(sp.u_orig + u);
     const size_t dst = ((size_t)tile * sp.n + u) * 32 + lane;
-    if (o < n_primal) {
-      state[dst] = make_float4(x[(size_t)o * batch + bb], 0.0f, qs[(size_t)o * batch + bb], 0.0f);
+    if (k < n_primal) {
+      state[dst] = make_float4(x[(size_t)k * batch + bb], 0.0f, qs[(size_t)k * batch + bb], 0.0f);
+      if (pres) pres[dst] = 0.0f;
     } else {
-      const int r = o - n_primal;
-      state[dst] = make_float4(z[(size_t)r * batch + bb], y[(size_t)r * batch + bb], ls[(size_t)r * batch + bb],
-                               us[(size_t)r * batch + bb]);
+      const int r = k - n_primal;
+      const float zr = z[(size_t)r * batch + bb];
+      state[dst] = make_float4(zr, y[(size_t)r * batch + bb], ls[(size_t)r * batch + bb], us[(size_t)r * batch + bb]);
+      if (!pres) continue;
+      float e = 0.0f;
+      if (warm) {
+        float ax = 0.0f;
+        const int e0 = __ldg(o.a_row_ptr + r), e1 = __ldg(o.a_row_ptr + r + 1);
+        for (int t = e0; t < e1; ++t) {
+          const int j = __ldg(o.a_row_ent + t);
+          ax = ax + (in.a(j, bb) * __ldg(o.a_scale + j)) * x[(size_t)__ldg(o.a_cols + j) * batch + bb];
+        }
+        e = ax - zr;
+      }
+      pres[dst] = e;
     }
   }
 }
@@ -222,6 +239,7 @@ struct StreamJob {
   const float* bstream;
   const float* fstream;
   float4* state;  // [tile][U][lane] ADMM state records
+  float* pres;    // [tile][U][lane] scaled primal residual of each constraint
   int* iters;     // [batch] iterations run (may be null)
   int n_tiles, max_iter, batch;
   int check_every;  // > 0: stop a tile once every lane's largest unscaled iterate change <= chg_eps
@@ -243,7 +261,7 @@ struct StreamArgs {
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
   int lbytes;       // per L stage L area
-  int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes
+  int sbytes;       // per S stage: max_rel x 32 lanes x (16 + 4) bytes
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
 
@@ -401,11 +419,12 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 //   S:   this lane's state record of release 0 in the stage (k-th at S[32 k])
 struct RelGroup {
   int o[4], kk[4];
-  float x[4], rho[4], rinv[4], f[4];
+  float x[4], rho[4], rinv[4], f[4], e[4];
   float4 st[4];
 };
 
-__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S,
+template <bool kTrack>
+__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
                                                const unsigned char* xb, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -418,6 +437,7 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
     g.f[j] = __int_as_float(r.w);
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
     g.st[j] = S[kk * 32];
+    g.e[j] = kTrack ? SE[kk * 32] : 0.0f;
   }
 }
 
@@ -429,9 +449,13 @@ struct RelParams {
 // constraint: z, y update and next rhs z - rho^-1 y (solver.py:806-820)
 // frozen: this lane's instance has converged; its state and next right-hand
 // side stay as they are (recomputed from the unchanged state).
-template <bool kCons>
+// The scaled primal residual follows the iterates exactly (A x~ = z~ from the
+// KKT solve): e_{k+1} = (z_relaxed - z_{k+1}) + (1 - alpha) e_k.  chg / pres:
+// this lane's largest unscaled iterate change / primal residual so far
+// (the residual is carried only when termination is checked: kTrack).
+template <bool kCons, bool kTrack>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float4* stu, float& chg, bool frozen) {
+                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
@@ -454,27 +478,33 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
       const float ya = yk + g.rho[j] * (zr - za);
       const float zn = frozen ? sv0 : za, yn = frozen ? yk : ya;
       *out = make_float2(zn, yn);
+      if (kTrack) {
+        const float en = frozen ? g.e[j] : (zr - za) + rp.oma * g.e[j];
+        peu[g.kk[j] * 32] = en;
+        pres = fmaxf(pres, fabsf(en) * g.f[j]);
+      }
       *xi = zn - rinv * yn;
       chg = fmaxf(chg, fmaxf(fabsf(zn - sv0), fabsf(yn - yk)) * g.f[j]);
     }
   }
 }
 
-template <bool kCons>
-__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const RelParams& rp,
-                                             unsigned char* xb, float4* stu, float& chg, bool frozen) {
+template <bool kCons, bool kTrack>
+__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
+                                             const RelParams& rp, unsigned char* xb, float4* stu, float* peu,
+                                             float& chg, float& pres, bool frozen) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group(rel, begin, end, S, xb, a);
+  load_rel_group<kTrack>(rel, begin, end, S, SE, xb, a);
   for (int k = begin;; k += 8) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + 4 < end ? k + 4 : end - 1;
-    load_rel_group(rel, kb, end, S, xb, b);
-    update_rel_group<kCons>(a, rp, xb, stu, chg, frozen);
+    load_rel_group<kTrack>(rel, kb, end, S, SE, xb, b);
+    update_rel_group<kCons, kTrack>(a, rp, xb, stu, peu, chg, pres, frozen);
     if (k + 4 >= end) break;
     const int ka = k + 8 < end ? k + 8 : end - 1;
-    load_rel_group(rel, ka, end, S, xb, a);
-    update_rel_group<kCons>(b, rp, xb, stu, chg, frozen);
+    load_rel_group<kTrack>(rel, ka, end, S, SE, xb, a);
+    update_rel_group<kCons, kTrack>(b, rp, xb, stu, peu, chg, pres, frozen);
     if (k + 8 >= end) break;
   }
 }
@@ -564,9 +594,15 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            const uint32_t bytes = (uint32_t)__ldg(sp.chunk_nrel + ch) * 512u;
-            mbar_arrive_expect_tx(sfull + sr.stage, bytes);
-            if (bytes) bulk_g2s(ss, J.state + soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32, bytes, sfull + sr.stage);
+            // primal residuals travel with the records when termination is checked
+            const bool track = J.check_every > 0;
+            const uint32_t nrel = (uint32_t)__ldg(sp.chunk_nrel + ch);
+            mbar_arrive_expect_tx(sfull + sr.stage, nrel * (track ? 640u : 512u));
+            if (nrel) {
+              const size_t u = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
+              bulk_g2s(ss, J.state + u, nrel * 512u, sfull + sr.stage);
+              if (track) bulk_g2s(ss + (size_t)(a.sbytes / 640) * 512, J.pres + u, nrel * 128u, sfull + sr.stage);
+            }
             sr.advance(a.sstages);
             ++issued_s;
           }
@@ -646,6 +682,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
       // this class's zero row (read by padding slots); every earlier tile is done with X
       X[n * 32 + lane] = 0.0f;
       float4* stt = J.state + (size_t)tile * n * 32 + lane;
+      float* pet = J.pres + (size_t)tile * n * 32 + lane;
+      float pres = 0.0f;  // this lane's largest unscaled primal residual in the current iteration
       float chg = 0.0f;  // this lane's largest unscaled iterate change in the current iteration
       int iters_run = 0, frozen_at = 0;
       bool stop = false, frozen = false;
@@ -668,6 +706,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
           if (kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
+          const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + (size_t)(a.sbytes / 640) * 512) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
             for (int k = 0; k < nprim; ++k) {
@@ -681,9 +720,15 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
             }
           } else {
             float4* stu = stt + (size_t)u0 * 32;
+            float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false>(rel, 0, nprim, S, rp, xb, stu, chg, frozen);
-            run_releases<true>(rel, nprim, nrel, S, rp, xb, stu, chg, frozen);
+            if (J.check_every > 0) {
+              run_releases<false, true>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+              run_releases<true, true>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            } else {
+              run_releases<false, false>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+              run_releases<true, false>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            }
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -704,7 +749,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
           // an iteration is complete: decide (before publishing it) whether the tile stops here
           ++iters_run;
           if (check_point(J.check_every, iters_run) && iters_run < J.max_iter) {
-            if (!frozen && chg <= J.chg_eps) {
+            if (!frozen && chg <= J.chg_eps && pres <= J.chg_eps) {
               frozen = true;
               frozen_at = iters_run;
             }
@@ -712,6 +757,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
             if (stop && lane == 0) *stop_at = t + 1;
           }
           chg = 0.0f;
+          pres = 0.0f;
         }
         __syncwarp();
         if (lane == 0) st_release_cta(rel_done, t + 1);
@@ -762,7 +808,7 @@ RingSizes ring_sizes(const StreamPlan& sp) {
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
   r.lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
-  r.sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
+  r.sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 640;  // records + primal residuals
   r.x_rows = sp.n + 2;
   r.lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
   r.smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
@@ -793,14 +839,14 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring
 
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
-  return tiles * ((size_t)sp.blen + (size_t)sp.flen + 4 * 32 * (size_t)sp.n) + 64;
+  return tiles * ((size_t)sp.blen + (size_t)sp.flen + 5 * 32 * (size_t)sp.n) + 64;
 }
 
 // Factorization into the streams and the state into its records (one class).
 int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
                  const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
-                 const float* qs, const float* ls, const float* us, float* work, int* status, int batch,
-                 int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s) {
+                 const float* qs, const float* ls, const float* us, bool warm, bool track, float* work,
+                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s) {
   StreamLaunch cfg;
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
@@ -808,6 +854,7 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   float* bstream = work;
   float* fstream = bstream + (size_t)n_tiles * sp.blen;
   float4* state = reinterpret_cast<float4*>(fstream + (size_t)n_tiles * sp.flen);
+  float* pres = reinterpret_cast<float*>(state + tl * sp.n);
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
   if (!reuse_factor) {
     // L-batch sized so that every tile's warp is resident at once (all of a
@@ -826,13 +873,15 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   }
   {
     dim3 grid(ceil_div(tl, 128), sp.n < 1024 ? sp.n : 1024);
-    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o.n, x, z, y, qs, ls, us, state, batch, n_tiles);
+    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm, x, z, y, qs, ls, us, state, track ? pres : nullptr,
+                                                 batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
   job->sp = sp;
   job->bstream = bstream;
   job->fstream = fstream;
   job->state = state;
+  job->pres = pres;
   job->n_tiles = n_tiles;
   job->batch = batch;
   job->sigma = o.sigma;
@@ -870,6 +919,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     J.bstream = d.bstream;
     J.fstream = d.fstream;
     J.state = d.state;
+    J.pres = d.pres;
     J.iters = d.iters;
     J.n_tiles = d.n_tiles;
     J.max_iter = d.max_iter;

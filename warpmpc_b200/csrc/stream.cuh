@@ -258,6 +258,7 @@ struct StreamJobDesc {
   const float* bstream = nullptr;
   const float* fstream = nullptr;
   float4* state = nullptr;
+  float* pres = nullptr;
   int* iters = nullptr;
   int n_tiles = 0, max_iter = 0, batch = 0, check_every = 0;
   float chg_eps = 0.0f, sigma = 0.0f, alpha = 0.0f, one_minus_alpha = 0.0f;
