@@ -171,10 +171,10 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
 
 // ADMM state per tile in release order U, one 16-byte record per (index, lane):
 // (x, 0, sigma-scaled q, 0) for a primal index, (z, y, l, u) for a constraint;
-// and, when termination is checked (pres != null), the scaled primal residual
-// (A x - z)_r of a constraint (0 for a primal index), formed here for a warm
-// start (a cold start's x = z = 0 gives 0).
-__global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, bool warm, const float* __restrict__ x,
+// and the scaled primal residual (A x - z)_r of a constraint (0 for a primal
+// index), formed when `form` (a warm start whose termination is checked; a
+// cold start's x = z = 0 gives 0; without checks nothing reads it).
+__global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, bool form, const float* __restrict__ x,
                                        const float* __restrict__ z, const float* __restrict__ y,
                                        const float* __restrict__ qs, const float* __restrict__ ls,
                                        const float* __restrict__ us, float4* __restrict__ state,
@@ -189,14 +189,13 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
     const size_t dst = ((size_t)tile * sp.n + u) * 32 + lane;
     if (k < n_primal) {
       state[dst] = make_float4(x[(size_t)k * batch + bb], 0.0f, qs[(size_t)k * batch + bb], 0.0f);
-      if (pres) pres[dst] = 0.0f;
+      pres[dst] = 0.0f;
     } else {
       const int r = k - n_primal;
       const float zr = z[(size_t)r * batch + bb];
       state[dst] = make_float4(zr, y[(size_t)r * batch + bb], ls[(size_t)r * batch + bb], us[(size_t)r * batch + bb]);
-      if (!pres) continue;
       float e = 0.0f;
-      if (warm) {
+      if (form) {
         float ax = 0.0f;
         const int e0 = __ldg(o.a_row_ptr + r), e1 = __ldg(o.a_row_ptr + r + 1);
         for (int t = e0; t < e1; ++t) {
@@ -261,7 +260,8 @@ struct StreamArgs {
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
   int lbytes;       // per L stage L area
-  int sbytes;       // per S stage: max_rel x 32 lanes x (16 + 4) bytes
+  int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes of records (+ 4 of residuals)
+  int pres_off;     // byte offset of the residuals in an S stage (end of the records)
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
 
@@ -423,9 +423,8 @@ struct RelGroup {
   float4 st[4];
 };
 
-template <bool kTrack>
 __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
-                                               const unsigned char* xb, RelGroup& g) {
+                                               bool track, const unsigned char* xb, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int kk = (k + j < end) ? k + j : k;
@@ -437,7 +436,7 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
     g.f[j] = __int_as_float(r.w);
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
     g.st[j] = S[kk * 32];
-    g.e[j] = kTrack ? SE[kk * 32] : 0.0f;
+    g.e[j] = track ? SE[kk * 32] : 0.0f;
   }
 }
 
@@ -452,10 +451,11 @@ struct RelParams {
 // The scaled primal residual follows the iterates exactly (A x~ = z~ from the
 // KKT solve): e_{k+1} = (z_relaxed - z_{k+1}) + (1 - alpha) e_k.  chg / pres:
 // this lane's largest unscaled iterate change / primal residual so far
-// (the residual is carried only when termination is checked: kTrack).
-template <bool kCons, bool kTrack>
+// (the residual is carried only when termination is checked: track).
+template <bool kCons>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen) {
+                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen,
+                                                 bool track) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
@@ -478,7 +478,7 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
       const float ya = yk + g.rho[j] * (zr - za);
       const float zn = frozen ? sv0 : za, yn = frozen ? yk : ya;
       *out = make_float2(zn, yn);
-      if (kTrack) {
+      if (track) {
         const float en = frozen ? g.e[j] : (zr - za) + rp.oma * g.e[j];
         peu[g.kk[j] * 32] = en;
         pres = fmaxf(pres, fabsf(en) * g.f[j]);
@@ -489,22 +489,22 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
   }
 }
 
-template <bool kCons, bool kTrack>
+template <bool kCons>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
                                              const RelParams& rp, unsigned char* xb, float4* stu, float* peu,
-                                             float& chg, float& pres, bool frozen) {
+                                             float& chg, float& pres, bool frozen, bool track) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kTrack>(rel, begin, end, S, SE, xb, a);
+  load_rel_group(rel, begin, end, S, SE, track, xb, a);
   for (int k = begin;; k += 8) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + 4 < end ? k + 4 : end - 1;
-    load_rel_group<kTrack>(rel, kb, end, S, SE, xb, b);
-    update_rel_group<kCons, kTrack>(a, rp, xb, stu, peu, chg, pres, frozen);
+    load_rel_group(rel, kb, end, S, SE, track, xb, b);
+    update_rel_group<kCons>(a, rp, xb, stu, peu, chg, pres, frozen, track);
     if (k + 4 >= end) break;
     const int ka = k + 8 < end ? k + 8 : end - 1;
-    load_rel_group<kTrack>(rel, ka, end, S, SE, xb, a);
-    update_rel_group<kCons, kTrack>(b, rp, xb, stu, peu, chg, pres, frozen);
+    load_rel_group(rel, ka, end, S, SE, track, xb, a);
+    update_rel_group<kCons>(b, rp, xb, stu, peu, chg, pres, frozen, track);
     if (k + 8 >= end) break;
   }
 }
@@ -517,6 +517,8 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // counters order the consumers: sweep_done (items the sweeper finished: a
 // backward item's releases need its columns solved) and rel_done (items the
 // releaser finished: a forward sweep needs every right-hand side).
+// kTrack: the primal residuals travel with the state (some class checks termination).
+template <bool kTrack>
 __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int lstage_bytes = a.meta_bytes + a.lbytes;
@@ -594,14 +596,13 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            // primal residuals travel with the records when termination is checked
-            const bool track = J.check_every > 0;
+            constexpr bool track = kTrack;
             const uint32_t nrel = (uint32_t)__ldg(sp.chunk_nrel + ch);
             mbar_arrive_expect_tx(sfull + sr.stage, nrel * (track ? 640u : 512u));
             if (nrel) {
               const size_t u = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
               bulk_g2s(ss, J.state + u, nrel * 512u, sfull + sr.stage);
-              if (track) bulk_g2s(ss + (size_t)(a.sbytes / 640) * 512, J.pres + u, nrel * 128u, sfull + sr.stage);
+              if (track) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
             }
             sr.advance(a.sstages);
             ++issued_s;
@@ -706,7 +707,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
           if (kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
-          const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + (size_t)(a.sbytes / 640) * 512) + lane;
+          const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
             for (int k = 0; k < nprim; ++k) {
@@ -722,13 +723,9 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            if (J.check_every > 0) {
-              run_releases<false, true>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-              run_releases<true, true>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-            } else {
-              run_releases<false, false>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-              run_releases<true, false>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-            }
+            constexpr bool track = kTrack;
+            run_releases<false>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen, track);
+            run_releases<true>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen, track);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -798,17 +795,19 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
 namespace {
 
 struct RingSizes {
-  int meta_bytes, lbytes, sbytes, x_rows, lmax, smax;
+  int meta_bytes, lbytes, sbytes, pres_off, x_rows, lmax, smax;
 };
 
-RingSizes ring_sizes(const StreamPlan& sp) {
+// track: the S stages also carry the primal residuals (termination checked)
+RingSizes ring_sizes(const StreamPlan& sp, bool track) {
   RingSizes r;
   const int mw = sp.max_meta_words > sp.max_fmeta_words ? sp.max_meta_words : sp.max_fmeta_words;
   r.meta_bytes = ((mw * 4 + 127) / 128) * 128;
   const int bl = sp.max_units * 512 + sp.max_cols * 128;
   const int fl = sp.max_funits * 512;
   r.lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
-  r.sbytes = (sp.max_rel > 0 ? sp.max_rel : 1) * 640;  // records + primal residuals
+  r.pres_off = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
+  r.sbytes = r.pres_off + (track ? r.pres_off / 4 : 0);
   r.x_rows = sp.n + 2;
   r.lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
   r.smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
@@ -826,6 +825,7 @@ bool ring_config(const RingSizes& r, StreamLaunch* cfg) {
         cfg->meta_bytes = r.meta_bytes;
         cfg->lbytes = r.lbytes;
         cfg->sbytes = r.sbytes;
+        cfg->pres_off = r.pres_off;
         cfg->smem = bytes;
         return true;
       }
@@ -835,7 +835,8 @@ bool ring_config(const RingSizes& r, StreamLaunch* cfg) {
 
 }  // namespace
 
-bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring_config(ring_sizes(sp), cfg); }
+// (sized with the residuals: a pattern that fits this fits every launch)
+bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring_config(ring_sizes(sp, true), cfg); }
 
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
@@ -873,8 +874,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   }
   {
     dim3 grid(ceil_div(tl, 128), sp.n < 1024 ? sp.n : 1024);
-    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm, x, z, y, qs, ls, us, state, track ? pres : nullptr,
-                                                 batch, n_tiles);
+    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm && track, x, z, y, qs, ls, us, state, pres, batch,
+                                                 n_tiles);
     WMPC_LAUNCH_CHECK();
   }
   job->sp = sp;
@@ -893,14 +894,17 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
 // One launch over every class's tiles, the costliest class first.
 int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s) {
   if (n_jobs < 1 || n_jobs > kMaxStreamJobs) return fail(WMPC_ERR_INVALID_ARGUMENT, "1 to %d classes per launch", kMaxStreamJobs);
-  RingSizes r{0, 0, 0, 0, 12, 6};
+  RingSizes r{0, 0, 0, 0, 0, 12, 6};
   int order[kMaxStreamJobs];
   double cost[kMaxStreamJobs];
+  bool track = false;
+  for (int i = 0; i < n_jobs; ++i) track = track || jobs[i].check_every > 0;
   for (int i = 0; i < n_jobs; ++i) {
-    const RingSizes ri = ring_sizes(jobs[i].sp);
+    const RingSizes ri = ring_sizes(jobs[i].sp, track);
     r.meta_bytes = std::max(r.meta_bytes, ri.meta_bytes);
     r.lbytes = std::max(r.lbytes, ri.lbytes);
     r.sbytes = std::max(r.sbytes, ri.sbytes);
+    r.pres_off = std::max(r.pres_off, ri.pres_off);
     r.x_rows = std::max(r.x_rows, ri.x_rows);
     r.lmax = std::min(r.lmax, ri.lmax);
     r.smax = std::min(r.smax, ri.smax);
@@ -941,10 +945,12 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.meta_bytes = cfg.meta_bytes;
   a.lbytes = cfg.lbytes;
   a.sbytes = cfg.sbytes;
+  a.pres_off = cfg.pres_off;
   const int grid = total < num_sms ? total : num_sms;
-  WMPC_CUDA_TRY(cudaFuncSetAttribute(admm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  auto kernel = track ? admm_stream_kernel<true> : admm_stream_kernel<false>;
+  WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
-  admm_stream_kernel<<<grid, 96, cfg.smem, s>>>(a);
+  kernel<<<grid, 96, cfg.smem, s>>>(a);
   profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;

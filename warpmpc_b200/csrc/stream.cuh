@@ -244,7 +244,7 @@ bool build_factor_tables(const HostPattern& hp, std::vector<int>* init_slot, std
                          std::vector<unsigned short>* upd_slot, int* max_row_nnz, std::string* why);
 
 struct StreamLaunch {
-  int stages, sstages, meta_bytes, lbytes, sbytes;
+  int stages, sstages, meta_bytes, lbytes, sbytes, pres_off;
   size_t smem;
 };
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
