@@ -423,8 +423,9 @@ struct RelGroup {
   float4 st[4];
 };
 
+template <bool kTrack>
 __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
-                                               bool track, const unsigned char* xb, RelGroup& g) {
+                                               const unsigned char* xb, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int kk = (k + j < end) ? k + j : k;
@@ -436,7 +437,7 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
     g.f[j] = __int_as_float(r.w);
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
     g.st[j] = S[kk * 32];
-    g.e[j] = track ? SE[kk * 32] : 0.0f;
+    if constexpr (kTrack) g.e[j] = SE[kk * 32];
   }
 }
 
@@ -451,11 +452,10 @@ struct RelParams {
 // The scaled primal residual follows the iterates exactly (A x~ = z~ from the
 // KKT solve): e_{k+1} = (z_relaxed - z_{k+1}) + (1 - alpha) e_k.  chg / pres:
 // this lane's largest unscaled iterate change / primal residual so far
-// (the residual is carried only when termination is checked: track).
-template <bool kCons>
+// (the residual is carried only when termination is checked: kTrack).
+template <bool kCons, bool kTrack>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen,
-                                                 bool track) {
+                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
@@ -478,7 +478,7 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
       const float ya = yk + g.rho[j] * (zr - za);
       const float zn = frozen ? sv0 : za, yn = frozen ? yk : ya;
       *out = make_float2(zn, yn);
-      if (track) {
+      if constexpr (kTrack) {
         const float en = frozen ? g.e[j] : (zr - za) + rp.oma * g.e[j];
         peu[g.kk[j] * 32] = en;
         pres = fmaxf(pres, fabsf(en) * g.f[j]);
@@ -489,22 +489,22 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
   }
 }
 
-template <bool kCons>
+template <bool kCons, bool kTrack>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
                                              const RelParams& rp, unsigned char* xb, float4* stu, float* peu,
-                                             float& chg, float& pres, bool frozen, bool track) {
+                                             float& chg, float& pres, bool frozen) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group(rel, begin, end, S, SE, track, xb, a);
+  load_rel_group<kTrack>(rel, begin, end, S, SE, xb, a);
   for (int k = begin;; k += 8) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + 4 < end ? k + 4 : end - 1;
-    load_rel_group(rel, kb, end, S, SE, track, xb, b);
-    update_rel_group<kCons>(a, rp, xb, stu, peu, chg, pres, frozen, track);
+    load_rel_group<kTrack>(rel, kb, end, S, SE, xb, b);
+    update_rel_group<kCons, kTrack>(a, rp, xb, stu, peu, chg, pres, frozen);
     if (k + 4 >= end) break;
     const int ka = k + 8 < end ? k + 8 : end - 1;
-    load_rel_group(rel, ka, end, S, SE, track, xb, a);
-    update_rel_group<kCons>(b, rp, xb, stu, peu, chg, pres, frozen, track);
+    load_rel_group<kTrack>(rel, ka, end, S, SE, xb, a);
+    update_rel_group<kCons, kTrack>(b, rp, xb, stu, peu, chg, pres, frozen);
     if (k + 8 >= end) break;
   }
 }
@@ -596,13 +596,12 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            constexpr bool track = kTrack;
             const uint32_t nrel = (uint32_t)__ldg(sp.chunk_nrel + ch);
-            mbar_arrive_expect_tx(sfull + sr.stage, nrel * (track ? 640u : 512u));
+            mbar_arrive_expect_tx(sfull + sr.stage, nrel * (kTrack ? 640u : 512u));
             if (nrel) {
               const size_t u = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
               bulk_g2s(ss, J.state + u, nrel * 512u, sfull + sr.stage);
-              if (track) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
+              if constexpr (kTrack) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
             }
             sr.advance(a.sstages);
             ++issued_s;
@@ -723,9 +722,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            constexpr bool track = kTrack;
-            run_releases<false>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen, track);
-            run_releases<true>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen, track);
+            run_releases<false, kTrack>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            run_releases<true, kTrack>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -746,7 +744,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
           // an iteration is complete: decide (before publishing it) whether the tile stops here
           ++iters_run;
           if (check_point(J.check_every, iters_run) && iters_run < J.max_iter) {
-            if (!frozen && chg <= J.chg_eps && pres <= J.chg_eps) {
+            if (!frozen && chg <= J.chg_eps && (!kTrack || pres <= J.chg_eps)) {
               frozen = true;
               frozen_at = iters_run;
             }
