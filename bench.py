@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--grad-batch", type=int, default=16384)
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-size multi-class measurement")
     ap.add_argument("--mixed-batch", type=int, default=131072, help="instances over the four mixed classes")
+    ap.add_argument("--no-line-search", action="store_true", help="skip the SQP line-search step timing")
     return ap.parse_args()
 
 
@@ -344,6 +345,56 @@ def gradient_timing(args, dev, world):
     }
 
 
+def line_search_timing(args, dev, world, plan, hbm_peak):
+    """The SQP line-search step after the QP solve (wmpc_sqp_line_search_step):
+    bound violation, Armijo metric, filter selection over the default 4-step
+    ladder and z + step d, one launch over args.batch instances of the bench
+    class's QP sizes (z of size n, m constraint rows).  HBM-bound: reads z, d,
+    q, l, g, u and the candidate evaluations, writes z_next."""
+    import torch
+
+    from warpmpc_b200.jax_sqp import FilterLineSearchSettings, line_search_step, make_step_lengths
+
+    s = FilterLineSearchSettings()
+    steps = torch.from_numpy(make_step_lengths(s).astype(np.float32)).to(dev)
+    B, n, m, k = args.batch, plan.n, plan.m, int(steps.numel())
+    g = torch.Generator(device=dev).manual_seed(5)
+    r = lambda *shape: torch.randn(*shape, device=dev, generator=g)  # noqa: E731
+    z, d, q, gv = r(B, n), r(B, n), r(B, n), r(B, m)
+    lo, up = gv - r(B, m).abs(), gv + r(B, m).abs()
+    bc, cc, cv = r(B), r(k, B), r(k, B).abs()
+
+    def run():
+        return line_search_step(settings=s, step_lengths=steps, z=z, direction=d, q=q, constraint_l=lo, g=gv,
+                                constraint_u=up, baseline_cost=bc, candidate_costs=cc,
+                                candidate_constraint_violations=cv)
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    from warpmpc_b200 import native
+
+    reps = 20
+    native.profile_begin()
+    for _ in range(reps):
+        run()
+    torch.cuda.synchronize()
+    # the library's own event pair brackets each launch on its stream
+    ms_sum, launches, _ = native.profile_end()
+    ms = max_over_ranks(ms_sum / max(launches, 1), world)
+    per = 4 * (4 * n + 3 * m + 2 * k + 1) + 4 * 4 + 3
+    gbs = B * per / (ms * 1e-3) / 1e9
+    return {
+        "workload": f"SQP line-search step after the QP solve: {B} instances/GPU, z of {n}, {m} constraint rows, "
+                    f"{k}-step ladder, one launch (wmpc_sqp_line_search_step)",
+        "ms": ms,
+        "bytes_per_instance": per,
+        "achieved_gbs": gbs,
+        "frac_of_measured_hbm": gbs / hbm_peak,
+        "launches_timed": launches,
+    }
+
+
 def mixed_timing(args, dev, world):
     """Mixed-size batch: args.mixed_batch instances spread over four linear MPC
     classes (nx, nu, N) = (4, 2, 10), (4, 2, 40), (12, 4, 20), (12, 4, 30),
@@ -590,6 +641,9 @@ def main():
     mixed = None
     if not args.no_mixed:
         mixed = mixed_timing(args, dev, world)
+    line_search = None
+    if not args.no_line_search:
+        line_search = line_search_timing(args, dev, world, plan, roofline["peak"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -619,6 +673,7 @@ def main():
             "fwd_bwd_over_fwd": grad["ratio"] if grad else None,
             "gradient": grad,
             "mixed": mixed,
+            "line_search": line_search,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,

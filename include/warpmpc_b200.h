@@ -319,6 +319,71 @@ int wmpc_osqp_adjoint(const wmpc_osqp* osqp, const wmpc_osqp_options* options,
                       const wmpc_osqp_adjoint_batch* data, int32_t mode, void* workspace,
                       size_t workspace_bytes, wmpc_stream_t stream);
 
+/* ------------------------------------------------------------------ */
+/* Filter line search of the SQP outer loop.                           */
+/* ------------------------------------------------------------------ */
+/* Reasons (warpmpc/jax_sqp/line_search.py:12-15). */
+enum {
+  WMPC_LINE_SEARCH_MAX_ITER = 0,            /* nothing accepted: last step of the ladder */
+  WMPC_LINE_SEARCH_CONSTRAINT = 1,
+  WMPC_LINE_SEARCH_COST = 2,
+  WMPC_LINE_SEARCH_COST_OR_CONSTRAINT = 3
+};
+
+/* FilterLineSearchSettings (line_search.py:18-29), in float32; the step
+ * ladder itself (make_step_lengths, line_search.py:45-59) is host data. */
+typedef struct wmpc_line_search_settings {
+  float g_max;                  /* line_search_g_max          (1e-1) */
+  float g_min;                  /* line_search_g_min          (1e-3) */
+  float gamma_c;                /* line_search_gamma_c        (1e-3) */
+  float armijo_factor;          /* line_search_armijo_factor  (1e-4) */
+  float constraint_scale;       /* line_search_constraint_scale (0.1) */
+  int32_t cost_accept_uses_trial_cost; /* 1 (reference default) or 0 */
+} wmpc_line_search_settings;
+
+/* constraint_violation (line_search.py:62-69): out[b] = scale *
+ * sqrt(sum_r max(l - g, 0)^2 + sum_r min(u - g, 0)^2) over batch-major
+ * [batch x m] rows. */
+int wmpc_constraint_violation(const float* lower, const float* g, const float* upper, int32_t batch,
+                              int32_t m, float scale, float* out, wmpc_stream_t stream);
+
+/* filter_line_search_from_evaluations (line_search.py:72-169).  Candidate
+ * arrays are [n_candidates x batch] (row k = step k of the ladder); the
+ * selected index is the first accepted candidate, else n_steps - 1, and the
+ * candidate/step gathers clamp it into range.  cost, violation, reason,
+ * accepted and candidate_acceptance ([n_candidates x batch], 0/1) may be
+ * NULL.  Replaces the jnp computation; bit-exact with a float32 restatement. */
+int wmpc_filter_line_search(const wmpc_line_search_settings* settings, const float* step_lengths,
+                            int32_t n_steps, const float* baseline_cost, const float* baseline_violation,
+                            const float* armijo_metric, const float* candidate_costs,
+                            const float* candidate_violations, int32_t n_candidates, int32_t batch,
+                            float* step_length, float* cost, float* violation, int32_t* reason,
+                            uint8_t* accepted, uint8_t* candidate_acceptance, wmpc_stream_t stream);
+
+/* The line-search SQP step after its QP solve (sparse_mpc.py:1013-1052), one
+ * launch: the baseline violation of (constraint_l, g, constraint_u), the
+ * Armijo metric q . direction, the filter selection over the candidates'
+ * evaluations (costs and violations of z + step_k direction, computed by the
+ * caller's NLP), z_next = z + step direction and is_finite.  Batch-major
+ * [batch x n] / [batch x m]; outputs other than z_next and step_length may
+ * be NULL. */
+typedef struct wmpc_sqp_step_batch {
+  int32_t batch, n, m, n_steps, n_candidates;
+  const float* step_lengths;                    /* [n_steps] */
+  const float* z; const float* direction;       /* [batch x n] */
+  const float* q;                               /* linearization's q [batch x n] */
+  const float* constraint_l; const float* g; const float* constraint_u; /* [batch x m] */
+  const float* baseline_cost;                   /* [batch] */
+  const float* candidate_costs;                 /* [n_candidates x batch] */
+  const float* candidate_violations;            /* [n_candidates x batch] */
+  float* z_next;                                /* [batch x n] */
+  float* step_length; float* cost; float* violation; float* baseline_violation; /* [batch] */
+  int32_t* reason; uint8_t* accepted; uint8_t* is_finite; /* [batch] */
+  uint8_t* candidate_acceptance;                /* [n_candidates x batch] */
+} wmpc_sqp_step_batch;
+int wmpc_sqp_line_search_step(const wmpc_line_search_settings* settings, const wmpc_sqp_step_batch* data,
+                              wmpc_stream_t stream);
+
 const char* wmpc_last_error_string(void);
 /* Library version string, e.g. "0.1.0 sm_100a". */
 const char* wmpc_version(void);

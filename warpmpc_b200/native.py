@@ -148,6 +148,46 @@ class OsqpBatch(ctypes.Structure):
     ]
 
 
+class LineSearchSettings(ctypes.Structure):
+    _fields_ = [
+        ("g_max", ctypes.c_float),
+        ("g_min", ctypes.c_float),
+        ("gamma_c", ctypes.c_float),
+        ("armijo_factor", ctypes.c_float),
+        ("constraint_scale", ctypes.c_float),
+        ("cost_accept_uses_trial_cost", ctypes.c_int32),
+    ]
+
+
+class SqpStepBatch(ctypes.Structure):
+    _fields_ = [
+        ("batch", ctypes.c_int32),
+        ("n", ctypes.c_int32),
+        ("m", ctypes.c_int32),
+        ("n_steps", ctypes.c_int32),
+        ("n_candidates", ctypes.c_int32),
+        ("step_lengths", ctypes.c_void_p),
+        ("z", ctypes.c_void_p),
+        ("direction", ctypes.c_void_p),
+        ("q", ctypes.c_void_p),
+        ("constraint_l", ctypes.c_void_p),
+        ("g", ctypes.c_void_p),
+        ("constraint_u", ctypes.c_void_p),
+        ("baseline_cost", ctypes.c_void_p),
+        ("candidate_costs", ctypes.c_void_p),
+        ("candidate_violations", ctypes.c_void_p),
+        ("z_next", ctypes.c_void_p),
+        ("step_length", ctypes.c_void_p),
+        ("cost", ctypes.c_void_p),
+        ("violation", ctypes.c_void_p),
+        ("baseline_violation", ctypes.c_void_p),
+        ("reason", ctypes.c_void_p),
+        ("accepted", ctypes.c_void_p),
+        ("is_finite", ctypes.c_void_p),
+        ("candidate_acceptance", ctypes.c_void_p),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol; also used by the
 # symbol-export test.
 SIGNATURES = {
@@ -205,6 +245,20 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.POINTER(PatternDesc), _f32p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
          ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)],
+    ),
+    "wmpc_constraint_violation": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+         ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "wmpc_filter_line_search": (
+        ctypes.c_int,
+        [ctypes.POINTER(LineSearchSettings), ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "wmpc_sqp_line_search_step": (
+        ctypes.c_int, [ctypes.POINTER(LineSearchSettings), ctypes.POINTER(SqpStepBatch), ctypes.c_void_p]
     ),
     "wmpc_profile_begin": (ctypes.c_int, []),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
