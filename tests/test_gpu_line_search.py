@@ -88,8 +88,9 @@ def test_filter_selection_bitexact(cuda_device, trial_cost, n_cand):
     np.testing.assert_array_equal(_np(got.reason), want[3])
     np.testing.assert_array_equal(_np(got.accepted), want[4])
     np.testing.assert_array_equal(_np(got.candidate_acceptance), want[5])
-    # every branch was exercised
-    assert len(set(want[3].tolist())) == 4
+    # every branch was selected somewhere (with the baseline cost on the left of the
+    # Armijo test the cost branch can never accept: armijo < 0 on that branch)
+    assert set(want[3].tolist()) == ({0, 1, 2, 3} if trial_cost else {0, 1, 3})
 
 
 def test_constraint_violation_rows(cuda_device):
