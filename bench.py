@@ -345,7 +345,7 @@ def gradient_timing(args, dev, world):
     }
 
 
-def line_search_timing(args, dev, world, plan, hbm_peak):
+def line_search_timing(args, dev, world, plan, hbm_peak, peak_source):
     """The SQP line-search step after the QP solve (wmpc_sqp_line_search_step):
     bound violation, Armijo metric, filter selection over the default 4-step
     ladder and z + step d, one launch over args.batch instances of the bench
@@ -390,7 +390,9 @@ def line_search_timing(args, dev, world, plan, hbm_peak):
         "ms": ms,
         "bytes_per_instance": per,
         "achieved_gbs": gbs,
-        "frac_of_measured_hbm": gbs / hbm_peak,
+        "peak_gbs": hbm_peak,
+        "peak_source": peak_source,
+        "frac": gbs / hbm_peak,
         "launches_timed": launches,
     }
 
@@ -643,7 +645,7 @@ def main():
         mixed = mixed_timing(args, dev, world)
     line_search = None
     if not args.no_line_search:
-        line_search = line_search_timing(args, dev, world, plan, roofline["peak"])
+        line_search = line_search_timing(args, dev, world, plan, roofline["peak"], roofline["peak_source"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -104,11 +104,12 @@ def test_constraint_violation_rows(cuda_device):
         np.testing.assert_allclose(got, want, rtol=1e-5, atol=0)
 
 
-def test_line_search_step_against_oracle(cuda_device):
+@pytest.mark.parametrize("n,m", [(61, 47), (64, 48)])  # element-wise and 16-byte row paths
+def test_line_search_step_against_oracle(cuda_device, n, m):
     rng = np.random.default_rng(11)
     s = FilterLineSearchSettings()
     steps = make_step_lengths(s).astype(np.float32)
-    batch, n, m, n_cand = 5000, 61, 47, 4
+    batch, n_cand = 5000, 4
     f = np.float32
     z = rng.standard_normal((batch, n)).astype(f)
     d = rng.standard_normal((batch, n)).astype(f)

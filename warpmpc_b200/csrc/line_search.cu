@@ -121,6 +121,30 @@ __device__ __forceinline__ float row_violation_sq(const float* __restrict__ lo, 
   return warp_sum(sl) + warp_sum(su);
 }
 
+// The same with 16-byte loads (rows 16-byte aligned, m a multiple of 4):
+// four independent loads per lane in flight per trip.
+__device__ __forceinline__ float row_violation_sq4(const float4* __restrict__ lo, const float4* __restrict__ g,
+                                                   const float4* __restrict__ up, int m4, int lane) {
+  float sl = 0.0f, su = 0.0f;
+#pragma unroll 4
+  for (int r = lane; r < m4; r += 32) {
+    const float4 gr = g[r], l = lo[r], u = up[r];
+    const float a0 = fmaxf(l.x - gr.x, 0.0f), a1 = fmaxf(l.y - gr.y, 0.0f);
+    const float a2 = fmaxf(l.z - gr.z, 0.0f), a3 = fmaxf(l.w - gr.w, 0.0f);
+    const float c0 = fminf(u.x - gr.x, 0.0f), c1 = fminf(u.y - gr.y, 0.0f);
+    const float c2 = fminf(u.z - gr.z, 0.0f), c3 = fminf(u.w - gr.w, 0.0f);
+    sl = sl + a0 * a0;
+    sl = sl + a1 * a1;
+    sl = sl + a2 * a2;
+    sl = sl + a3 * a3;
+    su = su + c0 * c0;
+    su = su + c1 * c1;
+    su = su + c2 * c2;
+    su = su + c3 * c3;
+  }
+  return warp_sum(sl) + warp_sum(su);
+}
+
 __global__ void constraint_violation_kernel(const float* __restrict__ lo, const float* __restrict__ g,
                                             const float* __restrict__ up, int batch, int m, float scale,
                                             float* __restrict__ out) {
@@ -149,24 +173,56 @@ struct StepArgs {
 // sparse_mpc.py:1013-1052 from the QP solve onwards, one warp per instance:
 // the baseline violation of (constraint_l, g, constraint_u), the Armijo
 // metric q . d, the filter selection over the candidate evaluations, then
-// z_next = z + step d and whether z_next is finite.
+// z_next = z + step d and whether z_next is finite.  kVec: every row is
+// 16-byte aligned with n and m multiples of 4, so rows move as float4.
+template <bool kVec>
 __global__ void __launch_bounds__(256) sqp_line_search_step_kernel(const __grid_constant__ StepArgs a) {
   const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (b >= a.batch) return;
   const size_t om = (size_t)b * a.m, on = (size_t)b * a.n;
-  const float base_viol = a.p.scale * sqrtf(row_violation_sq(a.cl + om, a.g + om, a.cu + om, a.m, lane));
-  float qd = 0.0f;
-  for (int j = lane; j < a.n; j += 32) qd = qd + a.q[on + j] * a.d[on + j];
+  float vsq, qd = 0.0f;
+  if (kVec) {
+    vsq = row_violation_sq4(reinterpret_cast<const float4*>(a.cl + om), reinterpret_cast<const float4*>(a.g + om),
+                            reinterpret_cast<const float4*>(a.cu + om), a.m >> 2, lane);
+    const float4* q4 = reinterpret_cast<const float4*>(a.q + on);
+    const float4* d4 = reinterpret_cast<const float4*>(a.d + on);
+#pragma unroll 4
+    for (int j = lane; j < (a.n >> 2); j += 32) {
+      const float4 qv = q4[j], dv = d4[j];
+      qd = qd + qv.x * dv.x;
+      qd = qd + qv.y * dv.y;
+      qd = qd + qv.z * dv.z;
+      qd = qd + qv.w * dv.w;
+    }
+  } else {
+    vsq = row_violation_sq(a.cl + om, a.g + om, a.cu + om, a.m, lane);
+    for (int j = lane; j < a.n; j += 32) qd = qd + a.q[on + j] * a.d[on + j];
+  }
+  const float base_viol = a.p.scale * sqrtf(vsq);
   const float armijo = warp_sum(qd);
   // every lane selects (same inputs, same result): no broadcast needed
   const LsChoice r = select_step(a.p, a.steps, a.n_steps, a.base_cost[b], base_viol, armijo, a.cand_cost + b,
                                  a.cand_viol + b, a.n_cand, a.batch,
                                  (a.acceptance_out && lane == 0) ? a.acceptance_out + b : nullptr);
   bool finite = true;
-  for (int j = lane; j < a.n; j += 32) {
-    const float v = a.z[on + j] + r.step * a.d[on + j];
-    a.z_next[on + j] = v;
-    finite = finite && isfinite(v);
+  if (kVec) {
+    const float4* z4 = reinterpret_cast<const float4*>(a.z + on);
+    const float4* d4 = reinterpret_cast<const float4*>(a.d + on);
+    float4* o4 = reinterpret_cast<float4*>(a.z_next + on);
+#pragma unroll 4
+    for (int j = lane; j < (a.n >> 2); j += 32) {
+      const float4 zv = z4[j], dv = d4[j];
+      const float4 v = make_float4(zv.x + r.step * dv.x, zv.y + r.step * dv.y, zv.z + r.step * dv.z,
+                                   zv.w + r.step * dv.w);
+      o4[j] = v;
+      finite = finite && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
+    }
+  } else {
+    for (int j = lane; j < a.n; j += 32) {
+      const float v = a.z[on + j] + r.step * a.d[on + j];
+      a.z_next[on + j] = v;
+      finite = finite && isfinite(v);
+    }
   }
   finite = __all_sync(0xffffffffu, finite);
   if (lane == 0) {
@@ -186,6 +242,8 @@ bool settings_ok(const wmpc_line_search_settings* s) {
 }
 
 int warps_grid(int batch) { return (batch + 7) / 8; }  // 8 warps (256 threads) per block
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
 }  // namespace wmpc
@@ -264,7 +322,13 @@ extern "C" int wmpc_sqp_line_search_step(const wmpc_line_search_settings* settin
   a.acceptance_out = d->candidate_acceptance;
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   profile_mark_begin(s);
-  sqp_line_search_step_kernel<<<warps_grid(d->batch), 256, 0, s>>>(a);
+  const bool vec = d->n % 4 == 0 && d->m % 4 == 0 && aligned16(d->z) && aligned16(d->direction) &&
+                   aligned16(d->q) && aligned16(d->z_next) && aligned16(d->constraint_l) && aligned16(d->g) &&
+                   aligned16(d->constraint_u);
+  if (vec)
+    sqp_line_search_step_kernel<true><<<warps_grid(d->batch), 256, 0, s>>>(a);
+  else
+    sqp_line_search_step_kernel<false><<<warps_grid(d->batch), 256, 0, s>>>(a);
   profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
