@@ -255,6 +255,131 @@ class OSQPEngine:
         self.last_workspace = (ws, wsb, mode_id, int(opts.check_termination)) if keep_factor else None
         return x, z, y, prim, dual, obj
 
+    def solve_host(self, p_values, a_values, q, l, u, warm=None, out=None, chunks=2, max_iter=None,
+                   check_termination=None, granule=None):
+        """Batched solve of host (CPU) tensors into host tensors, transfers overlapped with the solves.
+
+        The batch is cut into ``chunks`` slices with boundaries on whole waves
+        of 32-instance tiles over the device's SMs (``granule`` overrides that
+        unit of 32 x the SM count); slice k's host-to-device copy runs on a
+        copy stream while slice k-1 is solved on the current stream, and slice
+        k-1's results go back on a second copy stream while slice k is
+        solved.  Two slices suit the persistent path: each slice pays the
+        factorization's latency floor once.  Each slice is an ordinary ``solve`` of its instances, so
+        the results equal a one-shot ``solve`` of the whole batch bit for bit.
+        Inputs should be in pinned memory (pageable tensors still work, without
+        the overlap).  ``out`` optionally gives the six host output tensors
+        ``(x, z, y, prim_res, dual_res, obj_val)``; otherwise they are
+        allocated pinned; the warm start may alias them (each slice's start is
+        copied in before its results are copied out).  Returns them once the
+        results are on the host (the
+        call synchronizes the current stream); ``last_iters`` and
+        ``last_status`` are host tensors afterwards.
+        """
+        import torch
+
+        pl = self.plan
+        dev = self.device
+
+        def host(t, width, name):
+            if not isinstance(t, torch.Tensor):
+                t = torch.as_tensor(np.asarray(t, dtype=np.float32))
+            if t.device.type != "cpu" or t.dtype != torch.float32:
+                raise ValueError(f"{name} must be a float32 host tensor")
+            t = t if t.dim() == 2 else t.reshape(1, -1)
+            if t.shape[1] != width:
+                raise ValueError(f"{name} must have shape (batch, {width}) or ({width},)")
+            return t.contiguous()
+
+        p = host(p_values, pl.nnz_p, "p_values")
+        a = host(a_values, pl.nnz_a, "a_values")
+        qh, lh, uh = host(q, pl.n, "q"), host(l, pl.m, "l"), host(u, pl.m, "u")
+        wh = None if warm is None else (host(warm[0], pl.n, "warm_start_x"), host(warm[1], pl.m, "warm_start_z"),
+                                        host(warm[2], pl.m, "warm_start_y"))
+        rows = [p, a, qh, lh, uh] + ([] if wh is None else list(wh))
+        batch = max(int(t.shape[0]) for t in rows)
+        for t, name in zip(rows, ("p_values", "a_values", "q", "l", "u", "warm_start_x", "warm_start_z",
+                                  "warm_start_y")):
+            if t.shape[0] not in (1, batch):
+                raise ValueError(f"{name} batch must be 1 or {batch}")
+        shapes = [(batch, pl.n), (batch, pl.m), (batch, pl.m), (batch,), (batch,), (batch,)]
+        if out is None:
+            out = tuple(torch.empty(s, dtype=torch.float32).pin_memory() for s in shapes)
+        else:
+            out = tuple(out)
+            if len(out) != 6 or any(tuple(t.shape) != s or t.device.type != "cpu" or not t.is_contiguous()
+                                    or t.dtype != torch.float32 for t, s in zip(out, shapes)):
+                raise ValueError("out must be six contiguous float32 host tensors (x, z, y, prim, dual, obj)")
+        iters_h = torch.empty(batch, dtype=torch.int32).pin_memory()
+        status_h = torch.empty(batch, dtype=torch.int32).pin_memory()
+        if batch == 0:
+            return out
+        # slice boundaries on whole waves of tiles (a partial wave costs a whole one)
+        wave = int(granule) if granule else 32 * torch.cuda.get_device_properties(dev).multi_processor_count
+        waves = -(-batch // wave)
+        k = max(1, min(int(chunks), waves))
+        bounds = [min(batch, wave * (waves * i // k)) for i in range(k + 1)]
+        bounds[-1] = batch
+        size = max(bounds[i + 1] - bounds[i] for i in range(k))
+
+        cur = torch.cuda.current_stream(dev)
+        if getattr(self, "_copy_streams", None) is None:
+            self._copy_streams = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+        up, down = self._copy_streams
+        start = torch.cuda.Event()
+        start.record(cur)
+        up.wait_event(start)
+        down.wait_event(start)
+
+        def dbuf(t, rows_):
+            return torch.empty((rows_ if t.shape[0] == batch else 1, t.shape[1]), dtype=torch.float32, device=dev)
+
+        sets = []
+        for _ in range(min(2, k)):
+            ins = [dbuf(t, size) for t in rows]
+            outs = [torch.empty((size,) + s[1:], dtype=torch.float32, device=dev) for s in shapes]
+            outs += [torch.empty(size, dtype=torch.int32, device=dev) for _ in range(2)]
+            sets.append((ins, outs))
+        in_ready, solved, copied = [], [], []
+        for i in range(k):
+            s0, s1 = bounds[i], bounds[i + 1]
+            n = s1 - s0
+            ins, outs = sets[i % 2]
+            if i >= 2:
+                up.wait_event(solved[i - 2])  # the set's inputs were read by slice i - 2
+            with torch.cuda.stream(up):
+                for h, d in zip(rows, ins):
+                    if h.shape[0] == batch:
+                        d[:n].copy_(h[s0:s1], non_blocking=True)
+                    elif i < 2:
+                        d.copy_(h, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(up)
+            in_ready.append(ev)
+            cur.wait_event(ev)
+            if i >= 2:
+                cur.wait_event(copied[i - 2])  # the set's outputs went back for slice i - 2
+            dv = [d if d.shape[0] == 1 else d[:n] for d in ins]
+            o = tuple(t[:n] for t in outs)
+            self.solve(dv[0], dv[1], dv[2], dv[3], dv[4], warm=None if wh is None else tuple(dv[5:8]),
+                       max_iter=max_iter, check_termination=check_termination, out=o)
+            ev = torch.cuda.Event()
+            ev.record(cur)
+            solved.append(ev)
+            down.wait_event(ev)
+            with torch.cuda.stream(down):
+                for h, d in zip(list(out) + [iters_h, status_h], o):
+                    h[s0:s1].copy_(d, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(down)
+            copied.append(ev)
+        cur.wait_event(copied[-1])
+        cur.wait_event(in_ready[-1])
+        cur.synchronize()
+        self.last_iters = iters_h
+        self.last_status = status_h
+        return out
+
     def adjoint(self, workspace, p_values, a_values, l, u, x, z, y, dx, dy=None, max_iter=None):
         """Reverse-mode derivatives on the factor kept by ``solve(keep_factor=True)``.
 
