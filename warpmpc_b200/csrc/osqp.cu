@@ -182,6 +182,11 @@ struct Residuals {
   float ax_norm, z_norm, px_norm, aty_norm, q_norm;
 };
 
+// The objective's sums run in kResParts interleaved partial sums (column j
+// into part j % kResParts), added in part order: the split residual_kernel
+// and this one-thread form give the same bits.
+constexpr int kResParts = 4;
+
 // q is the unscaled linear term: q[j * ldq]
 __device__ Residuals residuals(const Osqp& o, const InstanceData& in, const State& st, int b,
                                const float* __restrict__ q, long long ldq) {
@@ -199,8 +204,14 @@ __device__ Residuals residuals(const Osqp& o, const InstanceData& in, const Stat
     r.ax_norm = fmaxf(r.ax_norm, fabsf(ax));
     r.z_norm = fmaxf(r.z_norm, fabsf(zu));
   }
-  float quad = 0.0f, lin = 0.0f;
-  for (int j = 0; j < o.n; ++j) {
+  float quad_p[kResParts], lin_p[kResParts];
+#pragma unroll
+  for (int p = 0; p < kResParts; ++p) quad_p[p] = lin_p[p] = 0.0f;
+  for (int j0 = 0; j0 < o.n; j0 += kResParts)
+#pragma unroll
+   for (int p = 0; p < kResParts; ++p) {
+    const int j = j0 + p;
+    if (j >= o.n) break;
     float px = 0.0f;
     const int f0 = __ldg(o.pf_row_ptr + j), f1 = __ldg(o.pf_row_ptr + j + 1);
     for (int t = f0; t < f1; ++t) px = px + in.p(__ldg(o.pf_val + t)) * xu(__ldg(o.pf_col + t));
@@ -216,8 +227,14 @@ __device__ Residuals residuals(const Osqp& o, const InstanceData& in, const Stat
     r.px_norm = fmaxf(r.px_norm, fabsf(px));
     r.aty_norm = fmaxf(r.aty_norm, fabsf(aty));
     r.q_norm = fmaxf(r.q_norm, fabsf(qj));
-    quad = quad + xj * px;
-    lin = lin + qj * xj;
+    quad_p[p] = quad_p[p] + xj * px;
+    lin_p[p] = lin_p[p] + qj * xj;
+  }
+  float quad = 0.0f, lin = 0.0f;
+#pragma unroll
+  for (int p = 0; p < kResParts; ++p) {
+    quad = quad + quad_p[p];
+    lin = lin + lin_p[p];
   }
   r.obj = 0.5f * quad + lin;
   return r;
@@ -239,32 +256,104 @@ __device__ __forceinline__ bool finite_res(const Residuals& r) {
   return isfinite(r.prim) && isfinite(r.dual) && isfinite(r.obj);
 }
 
-// Exact residuals of the final iterate, status, unscaling.  eps_abs >= 0: also
-// set SOLVED when OSQP's termination test holds (solves run with termination).
-__global__ void residual_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
-                                const float* __restrict__ aT, long long lda, int sba, State st,
-                                const float* __restrict__ qT, float* prim, float* dual, float* obj,
-                                int* status, int batch, const int* status_in, const int* abort_word,
-                                float eps_abs = -1.0f, float eps_rel = 0.0f) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= batch) return;
-  InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
-  const Residuals r = residuals(o, in, st, b, qT + b, batch);
-  prim[b] = r.prim;
-  dual[b] = r.dual;
-  obj[b] = r.obj;
-  if (status) {
-    int v = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
-    if (eps_abs >= 0.0f && finite_res(r)) {
-      const float eps_p = eps_abs + eps_rel * fmaxf(r.ax_norm, r.z_norm);
-      const float eps_d = eps_abs + eps_rel * fmaxf(fmaxf(r.px_norm, r.aty_norm), r.q_norm);
-      if (r.prim <= eps_p && r.dual <= eps_d) v |= WMPC_STATUS_SOLVED;
+// Exact residuals of the final iterate (residuals() above), status,
+// unscaling.  eps_abs >= 0: also set SOLVED when OSQP's termination test
+// holds (solves run with termination).  Each instance is split over
+// kResParts threads (blockDim (32, kResParts): lane = instance, y = part):
+// part p takes A's rows and the columns j = p, p + kResParts, ...; every
+// row's and column's sum is still formed by one thread in the reference's
+// order, so prim, dual and the norms (maxima) equal residuals()' exactly; the
+// objective's two sums are added part by part.  Four times the warps in
+// flight for a latency-bound loop of dependent index and value loads.
+__global__ void __launch_bounds__(32 * kResParts) residual_kernel(
+    Osqp o, const float* __restrict__ pT, long long ldp, int sbp, const float* __restrict__ aT, long long lda,
+    int sba, State st, const float* __restrict__ qT, float* prim, float* dual, float* obj, int* status, int batch,
+    const int* status_in, const int* abort_word, float eps_abs, float eps_rel) {
+  __shared__ float part_val[kResParts][9][32];
+  const int lane = threadIdx.x, part = threadIdx.y;
+  const int b = blockIdx.x * 32 + lane;
+  const bool active = b < batch;
+  if (active) {
+    InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
+    auto xu = [&](int j) { return st.x[(long long)j * st.ld + b] * __ldg(o.scaling_d + j); };
+    float rp = 0.f, axn = 0.f, zn = 0.f;
+    for (int row = part; row < o.m; row += kResParts) {
+      float ax = 0.0f;
+      const int e0 = __ldg(o.a_row_ptr + row), e1 = __ldg(o.a_row_ptr + row + 1);
+      for (int t = e0; t < e1; ++t) {
+        const int e = __ldg(o.a_row_ent + t);
+        ax = ax + in.a(e) * xu(__ldg(o.a_cols + e));
+      }
+      const float zu = st.z[(long long)row * st.ld + b] * __ldg(o.scaling_einv + row);
+      rp = fmaxf(rp, fabsf(ax - zu));
+      axn = fmaxf(axn, fabsf(ax));
+      zn = fmaxf(zn, fabsf(zu));
     }
-    if (status_in) v |= status_in[b];
-    if (abort_word && *abort_word) v |= WMPC_STATUS_KERNEL_ABORT;
-    status[b] = v;
+    float rd = 0.f, pxn = 0.f, atyn = 0.f, qn = 0.f, quad = 0.f, lin = 0.f;
+    for (int j = part; j < o.n; j += kResParts) {
+      float px = 0.0f;
+      const int f0 = __ldg(o.pf_row_ptr + j), f1 = __ldg(o.pf_row_ptr + j + 1);
+      for (int t = f0; t < f1; ++t) px = px + in.p(__ldg(o.pf_val + t)) * xu(__ldg(o.pf_col + t));
+      float aty = 0.0f;
+      const int c0 = __ldg(o.a_col_ptr + j), c1 = __ldg(o.a_col_ptr + j + 1);
+      for (int e = c0; e < c1; ++e) {
+        const int row = __ldg(o.a_rows + e);
+        aty = aty + in.a(e) * (st.y[(long long)row * st.ld + b] * __ldg(o.y_unscale + row));
+      }
+      const float qj = qT[(long long)j * batch + b];
+      const float xj = xu(j);
+      rd = fmaxf(rd, fabsf(px + qj + aty));
+      pxn = fmaxf(pxn, fabsf(px));
+      atyn = fmaxf(atyn, fabsf(aty));
+      qn = fmaxf(qn, fabsf(qj));
+      quad = quad + xj * px;
+      lin = lin + qj * xj;
+    }
+    const float v[9] = {rp, axn, zn, rd, pxn, atyn, qn, quad, lin};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) part_val[part][k][lane] = v[k];
   }
-  unscale_in_place(o, st, b);
+  __syncthreads();  // every part has read the scaled iterate before any part unscales it
+  if (active && part == 0) {
+    Residuals r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float quad = 0.f, lin = 0.f;
+    for (int q = 0; q < kResParts; ++q) {
+      r.prim = fmaxf(r.prim, part_val[q][0][lane]);
+      r.ax_norm = fmaxf(r.ax_norm, part_val[q][1][lane]);
+      r.z_norm = fmaxf(r.z_norm, part_val[q][2][lane]);
+      r.dual = fmaxf(r.dual, part_val[q][3][lane]);
+      r.px_norm = fmaxf(r.px_norm, part_val[q][4][lane]);
+      r.aty_norm = fmaxf(r.aty_norm, part_val[q][5][lane]);
+      r.q_norm = fmaxf(r.q_norm, part_val[q][6][lane]);
+      quad = quad + part_val[q][7][lane];
+      lin = lin + part_val[q][8][lane];
+    }
+    r.obj = 0.5f * quad + lin;
+    prim[b] = r.prim;
+    dual[b] = r.dual;
+    obj[b] = r.obj;
+    if (status) {
+      int v = finite_res(r) ? WMPC_STATUS_MAX_ITER : WMPC_STATUS_NONFINITE;
+      if (eps_abs >= 0.0f && finite_res(r)) {
+        const float eps_p = eps_abs + eps_rel * fmaxf(r.ax_norm, r.z_norm);
+        const float eps_d = eps_abs + eps_rel * fmaxf(fmaxf(r.px_norm, r.aty_norm), r.q_norm);
+        if (r.prim <= eps_p && r.dual <= eps_d) v |= WMPC_STATUS_SOLVED;
+      }
+      if (status_in) v |= status_in[b];
+      if (abort_word && *abort_word) v |= WMPC_STATUS_KERNEL_ABORT;
+      status[b] = v;
+    }
+  }
+  if (!active) return;
+  for (int j = part; j < o.n; j += kResParts) {
+    const long long k = (long long)j * st.ld + b;
+    st.x[k] = st.x[k] * __ldg(o.scaling_d + j);
+  }
+  for (int r = part; r < o.m; r += kResParts) {
+    const long long k = (long long)r * st.ld + b;
+    st.z[k] = st.z[k] * __ldg(o.scaling_einv + r);
+    st.y[k] = st.y[k] * __ldg(o.y_unscale + r);
+  }
 }
 
 __global__ void fill_int_kernel(int* out, int value, int count) {
@@ -551,9 +640,9 @@ int stream_solve_end(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmp
   int rc;
   if ((rc = stream_end(q.sp, o, job, L.x, L.z, L.y, s))) return rc;
   State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
-  residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT,
-                                                   d.prim_res, d.dual_res, d.obj, d.status, B, L.stream_status,
-                                                   error_word, check ? opt.eps_abs : -1.0f, opt.eps_rel);
+  residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
+      o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B,
+      L.stream_status, error_word, check ? opt.eps_abs : -1.0f, opt.eps_rel);
   WMPC_LAUNCH_CHECK();
   if (d.iters && !check) {
     fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
@@ -620,8 +709,9 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
       admm_update_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
       WMPC_LAUNCH_CHECK();
     }
-    residual_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res,
-                                                     d.dual_res, d.obj, d.status, B, nullptr, nullptr);
+    residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
+        o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B, nullptr, nullptr,
+        -1.0f, 0.0f);
     WMPC_LAUNCH_CHECK();
     if (d.iters) {
       fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
