@@ -70,8 +70,18 @@ def _save_qdldl(name, ns, matrix, upper, perm):
 def _save_osqp(name, ns, p, a, l, u, settings_kw, q=None):
     ref_import.PERMUTATION_PROVIDER = amd_order
     settings = ns.osqp_types.OSQPSettings(**settings_kw)
-    plan = ns.solver.build_osqp_plan(p, a, l, u, settings, scaling_q=q)
+    plan = ns.solver.build_osqp_plan(p, a, l, u, settings, scaling_q=q, derivatives=True)
     out = {f"plan_{f}": getattr(plan, f) for f in OSQP_FIELDS}
+    dp = plan.derivative_plan  # the reference's adjoint KKT plan (solver.py:413-571)
+    for f in dp.__dataclass_fields__:
+        v = getattr(dp, f)
+        if isinstance(v, np.ndarray):
+            out[f"dplan_{f}"] = v
+        elif isinstance(v, (int, float)) and not isinstance(v, bool):
+            out[f"dplan_{f}"] = np.asarray(v)
+    out["dplan_adj_data"], out["dplan_adj_indices"], out["dplan_adj_indptr"] = (
+        dp.adjoint_upper.data, dp.adjoint_upper.indices, dp.adjoint_upper.indptr)
+    out["dplan_perm"], out["dplan_lp"], out["dplan_li"] = dp.qdldl_plan.p, dp.qdldl_plan.lp, dp.qdldl_plan.li
     out["scaling_c"] = plan.scaling_c
     out["scaling_cinv"] = plan.scaling_cinv
     out["kkt_data"], out["kkt_indices"], out["kkt_indptr"] = plan.kkt_upper.data, plan.kkt_upper.indices, plan.kkt_upper.indptr

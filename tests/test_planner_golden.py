@@ -64,10 +64,22 @@ def test_osqp_plan_matches_reference(path):
     settings = OSQPSettings(rho=rho, sigma=sigma, alpha=alpha, max_iter=int(max_iter), scaling=int(scaling),
                             rho_is_vec=bool(g["rho_is_vec"]))
     q = g["q"] if g["q"].size else None
-    plan = build_osqp_plan(p, a, g["l"], g["u"], settings, scaling_q=q, perm=g["perm"])
+    plan = build_osqp_plan(p, a, g["l"], g["u"], settings, scaling_q=q, perm=g["perm"], derivatives=True)
     for k in g.files:
         if k.startswith("plan_"):
             _eq(getattr(plan, k[5:]), g[k], k)
+    # the reference-style adjoint KKT plan (solver.py:413-571)
+    dp = plan.derivative_plan
+    special = {"dplan_adj_data", "dplan_adj_indices", "dplan_adj_indptr", "dplan_perm", "dplan_lp", "dplan_li"}
+    for k in g.files:
+        if k.startswith("dplan_") and k not in special:
+            _eq(np.asarray(getattr(dp, k[6:])), g[k], k)
+    _eq(dp.adjoint_upper.data, g["dplan_adj_data"], "adjoint data")
+    _eq(dp.adjoint_upper.indices, g["dplan_adj_indices"], "adjoint indices")
+    _eq(dp.adjoint_upper.indptr, g["dplan_adj_indptr"], "adjoint indptr")
+    _eq(dp.qdldl_plan.p, g["dplan_perm"], "adjoint perm")
+    _eq(dp.qdldl_plan.lp, g["dplan_lp"], "adjoint lp")
+    _eq(dp.qdldl_plan.li, g["dplan_li"], "adjoint li")
     assert plan.scaling_c == float(g["scaling_c"]) and plan.scaling_cinv == float(g["scaling_cinv"])
     _eq(plan.kkt_upper.data, g["kkt_data"], "kkt_data")
     _eq(plan.kkt_upper.indices, g["kkt_indices"], "kkt_indices")
