@@ -384,6 +384,22 @@ typedef struct wmpc_sqp_step_batch {
 int wmpc_sqp_line_search_step(const wmpc_line_search_settings* settings, const wmpc_sqp_step_batch* data,
                               wmpc_stream_t stream);
 
+/* ------------------------------------------------------------------ */
+/* Reference-style adjoint (parity mode) helper.                       */
+/* ------------------------------------------------------------------ */
+/* y = S x - r per instance (r may be NULL: y = S x), S symmetric with one
+ * pattern: `values` holds its upper triangle symbolic-major
+ * ([nnz x batch], leading dimension values_ld); the device table
+ * row_ptr[n+1] / ent_pos / ent_col lists, per row i, the (value position,
+ * column) terms of the full symmetric pattern.  x, r, y are [n x batch];
+ * y must not alias x.  Replaces _adjoint_matvec (warpmpc/jax_osqp/
+ * solver.py:1035-1044) in the refinement loop of the reference's adjoint
+ * solve (1133-1141), whose factor and solves run on wmpc_factor /
+ * wmpc_solve. */
+int wmpc_sym_matvec(const int32_t* row_ptr, const int32_t* ent_pos, const int32_t* ent_col, int32_t n,
+                    const float* values, int64_t values_ld, const float* x, const float* r, float* y,
+                    int32_t batch, wmpc_stream_t stream);
+
 const char* wmpc_last_error_string(void);
 /* Library version string, e.g. "0.1.0 sm_100a". */
 const char* wmpc_version(void);

@@ -22,6 +22,7 @@ Restates ``warpmpc/jax_osqp/solver.py``:
 from __future__ import annotations
 
 import numpy as np
+import scipy.linalg
 
 OSQP_INFTY = 1e30
 OSQP_MIN_SCALING = 1e-4
@@ -67,9 +68,10 @@ def adjoint(plan, p_values, a_values, l, u, x, y, dx, dy, eps=1e-6, refinement_i
     rhs[n + lower.size : n + ni] = -dy[upper]
     d_nu = np.where(y[eq] >= 0.0, dy[eq], -dy[eq])
     rhs[n + ni : half] = -d_nu
-    sol = np.linalg.solve(K, rhs)
+    lu = scipy.linalg.lu_factor(K)  # one factorization, reused by every refinement solve
+    sol = scipy.linalg.lu_solve(lu, rhs)
     for _ in range(refinement_iters):
-        sol = sol - np.linalg.solve(K, K0 @ sol - rhs)
+        sol = sol - scipy.linalg.lu_solve(lu, K0 @ sol - rhs)
     rx = sol[half : half + n]
     r_yl = np.zeros(m)
     r_yu = np.zeros(m)

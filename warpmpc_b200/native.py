@@ -260,6 +260,11 @@ SIGNATURES = {
     "wmpc_sqp_line_search_step": (
         ctypes.c_int, [ctypes.POINTER(LineSearchSettings), ctypes.POINTER(SqpStepBatch), ctypes.c_void_p]
     ),
+    "wmpc_sym_matvec": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p],
+    ),
     "wmpc_profile_begin": (ctypes.c_int, []),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
     "wmpc_launch_count": (ctypes.c_int64, []),
