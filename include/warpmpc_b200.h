@@ -400,6 +400,29 @@ int wmpc_sym_matvec(const int32_t* row_ptr, const int32_t* ent_pos, const int32_
                     const float* values, int64_t values_ld, const float* x, const float* r, float* y,
                     int32_t batch, wmpc_stream_t stream);
 
+/* ------------------------------------------------------------------ */
+/* Sparse MPC QP assembly (SQP linearization).                         */
+/* ------------------------------------------------------------------ */
+typedef struct wmpc_sqp_assemble_dims {
+  int32_t batch, n, nnz_p, nnz_a, m, n_stages, width;
+} wmpc_sqp_assemble_dims;
+
+/* The scatter half of _linearize_jit (warpmpc/jax_sqp/sparse_mpc.py:
+ * 855-901): values [batch x width] hold each instance's packed stage
+ * values (per stage: cost, g, lower, upper, grad, hess, jac).  Device
+ * tables: add_ptr[n + nnz_p + nnz_a + 1] / add_src list, for every entry of
+ * [q | P values | A values], the value columns added into it, in stage
+ * order (summed from zero in that order); row_src[2 m] the g column of
+ * each constraint row, then its stage's constraint_dim (lower and upper sit
+ * that far and twice that far after g); cost_src[n_stages] the cost
+ * columns.  Outputs batch-major: q [batch x n], p_values, a_values, l =
+ * lower - g, u = upper - g, g, constraint_l (lower), constraint_u (upper)
+ * [batch x m], cost [batch]. */
+int wmpc_sqp_assemble(const wmpc_sqp_assemble_dims* dims, const int32_t* add_ptr, const int32_t* add_src,
+                      const int32_t* row_src, const int32_t* cost_src, const float* values, float* q,
+                      float* p_values, float* a_values, float* l, float* u, float* cost, float* g,
+                      float* constraint_l, float* constraint_u, wmpc_stream_t stream);
+
 const char* wmpc_last_error_string(void);
 /* Library version string, e.g. "0.1.0 sm_100a". */
 const char* wmpc_version(void);

@@ -113,6 +113,12 @@ def _install_stubs() -> None:
     qdldl.Solver = Solver
     sys.modules.setdefault("qdldl", qdldl)
 
+    # casadi: only named in annotations and stage-compilation code paths the
+    # planners do not run (warpmpc/jax_sqp/casadi_stage.py)
+    casadi = types.ModuleType("casadi")
+    casadi.__getattr__ = lambda name: type(name, (), {})
+    sys.modules.setdefault("casadi", casadi)
+
 
 def load():
     """Return a namespace with the reference modules (core, warp_backend, solver)."""
@@ -134,3 +140,12 @@ def load():
         core=core, warp_backend=warp_backend, solver=solver, osqp_types=types_mod
     )
     return _loaded
+
+
+def load_sqp():
+    """The reference's sparse MPC module (warpmpc/jax_sqp/sparse_mpc.py), whose
+    plan builder (532-691) is NumPy/SciPy given stage objects."""
+    load()
+    import importlib
+
+    return importlib.import_module("warpmpc.jax_sqp.sparse_mpc")

@@ -97,6 +97,31 @@ def _save_osqp(name, ns, p, a, l, u, settings_kw, q=None):
     np.savez_compressed(os.path.join(HERE, f"osqp_{name}.npz"), **out)
 
 
+def _save_sqp(name, cls):
+    """The reference's sparse MPC plan (sparse_mpc.py:532-691) of a synthetic
+    stage-wise problem (warpmpc_b200/sqp_problems.py stage descriptions)."""
+    from warpmpc_b200 import sqp_problems
+
+    ref_import.PERMUTATION_PROVIDER = amd_order
+    sm = ref_import.load_sqp()
+    prob = sqp_problems.make_problem(cls)
+    plan = sm.build_sparse_mpc_plan(sm.SparseMPCProblem(stages=prob.stages))
+    out = {}
+    for k in ("stage_var_dims", "param_dims", "constraint_dims"):
+        out[k] = np.asarray(getattr(plan, k))
+    for k in ("z_offsets", "param_offsets", "constraint_offsets", "representative_l", "representative_u"):
+        out[k] = getattr(plan, k)
+    for k in ("p_pattern", "a_pattern"):
+        out[k + "_indices"], out[k + "_indptr"] = getattr(plan, k).indices, getattr(plan, k).indptr
+    for k in ("q_cols", "p_pos", "a_pos"):
+        out["asm_" + k] = np.concatenate([getattr(a, k) for a in plan.assemblies])
+        out["asm_" + k + "_counts"] = np.asarray([getattr(a, k).size for a in plan.assemblies])
+    for k in ("z_offset", "next_z_offset", "param_offset", "constraint_offset"):
+        out["asm_" + k] = np.asarray([getattr(a, k) for a in plan.assemblies])
+    out.update({f"osqp_{f}": getattr(plan.osqp_plan, f) for f in OSQP_FIELDS})
+    np.savez_compressed(os.path.join(HERE, f"sqp_plan_{name}.npz"), **out)
+
+
 def main():
     ns = ref_import.load()
     rng = np.random.default_rng(2024)
@@ -119,6 +144,8 @@ def main():
         b = problems.make_batch(cls, 1, seed=7)
         _save_osqp(f"mpc_{cls.name}", ns, b.p_matrix0, b.a_matrix0, b.l[0].astype(float), b.u[0].astype(float),
                    dict(problems.DEFAULT_SETTINGS), q=b.q[0].astype(float))
+    _save_sqp("small", problems.SMALL)
+    _save_sqp("quadrotor_n5", problems.MPCClass("quadrotor-n5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"))
     print("fixtures written to", HERE)
 
 

@@ -1,10 +1,19 @@
 """SQP outer-loop pieces with a CUDA backend.
 
-Mirror of ``warpmpc.jax_sqp`` for the filter line search
-(``warpmpc/jax_sqp/line_search.py``) and the line-search step that follows
-the QP solve (``warpmpc/jax_sqp/sparse_mpc.py`` 997-1053).
+Mirror of ``warpmpc.jax_sqp`` for the sparse MPC plan and batched QP
+assembly (``warpmpc/jax_sqp/sparse_mpc.py`` 532-691, 855-901), the filter
+line search (``warpmpc/jax_sqp/line_search.py``) and the line-search step
+that follows the QP solve (``sparse_mpc.py`` 997-1053).
 """
 
+from .assembly import (
+    QPAssembler,
+    SparseMPCPlan,
+    SparseMPCProblem,
+    SQPLinearization,
+    StageAssembly,
+    build_sparse_mpc_plan,
+)
 from .line_search import (
     LINE_SEARCH_CONSTRAINT,
     LINE_SEARCH_COST,
@@ -20,6 +29,12 @@ from .line_search import (
 )
 
 __all__ = [
+    "QPAssembler",
+    "SQPLinearization",
+    "SparseMPCPlan",
+    "SparseMPCProblem",
+    "StageAssembly",
+    "build_sparse_mpc_plan",
     "FilterLineSearchResult",
     "FilterLineSearchSettings",
     "LINE_SEARCH_CONSTRAINT",

@@ -188,6 +188,10 @@ class SqpStepBatch(ctypes.Structure):
     ]
 
 
+class SqpAssembleDims(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("batch", "n", "nnz_p", "nnz_a", "m", "n_stages", "width")]
+
+
 # (name, restype, argtypes) of every exported symbol; also used by the
 # symbol-export test.
 SIGNATURES = {
@@ -264,6 +268,10 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p],
+    ),
+    "wmpc_sqp_assemble": (
+        ctypes.c_int,
+        [ctypes.POINTER(SqpAssembleDims)] + [ctypes.c_void_p] * 14 + [ctypes.c_void_p],
     ),
     "wmpc_profile_begin": (ctypes.c_int, []),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
