@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-size multi-class measurement")
     ap.add_argument("--mixed-batch", type=int, default=131072, help="instances over the four mixed classes")
     ap.add_argument("--no-line-search", action="store_true", help="skip the SQP line-search step timing")
+    ap.add_argument("--no-assembly", action="store_true", help="skip the SQP QP assembly timing")
     return ap.parse_args()
 
 
@@ -397,6 +398,47 @@ def line_search_timing(args, dev, world, plan, hbm_peak, peak_source):
     }
 
 
+def assembly_timing(args, dev, world, hbm_peak, peak_source):
+    """Batched SQP QP assembly (wmpc_sqp_assemble) of the stage-wise quadrotor
+    MPC (nx=12, nu=4, N=30: 31 stages) for args.batch instances: stage values
+    evaluated and packed once outside the timed launches."""
+    import torch
+
+    from warpmpc_b200 import native, problems, sqp_problems
+    from warpmpc_b200.jax_sqp import QPAssembler, build_sparse_mpc_plan
+
+    cls = problems.QUADROTOR
+    prob = sqp_problems.make_problem(cls)
+    plan = build_sparse_mpc_plan(prob)
+    B = args.batch
+    data = sqp_problems.make_data(cls, B, seed=6)
+    g = torch.Generator(device=dev).manual_seed(6)
+    z = torch.randn(B, int(plan.z_offsets[-1]), device=dev, generator=g)
+    p = torch.randn(B, cls.nx, device=dev, generator=g)
+    asm = QPAssembler(plan, prob, device=dev)
+    packed = asm.pack(sqp_problems.evaluate_stages(prob, data, z, p))
+    del z, p
+    for _ in range(3):
+        asm.assemble(packed)
+    torch.cuda.synchronize()
+    reps = 10
+    native.profile_begin()
+    for _ in range(reps):
+        asm.assemble(packed)
+    torch.cuda.synchronize()
+    ms_sum, launches, _ = native.profile_end()
+    ms = max_over_ranks(ms_sum / max(launches, 1), world)
+    t = asm.tables
+    per = 4 * (asm.width + t["n"] + t["nnz_p"] + t["nnz_a"] + 5 * t["m"] + 1)
+    gbs = B * per / (ms * 1e-3) / 1e9
+    return {
+        "workload": f"SQP QP assembly, stage-wise quadrotor MPC nx={cls.nx} nu={cls.nu} N={cls.horizon} "
+                    f"({len(prob.stages)} stages), {B} instances/GPU, one launch (wmpc_sqp_assemble)",
+        "ms": ms, "bytes_per_instance": per, "achieved_gbs": gbs, "peak_gbs": hbm_peak, "peak_source": peak_source,
+        "frac": gbs / hbm_peak, "launches_timed": launches,
+    }
+
+
 def mixed_timing(args, dev, world):
     """Mixed-size batch: args.mixed_batch instances spread over four linear MPC
     classes (nx, nu, N) = (4, 2, 10), (4, 2, 40), (12, 4, 20), (12, 4, 30),
@@ -644,6 +686,9 @@ def main():
     line_search = None
     if not args.no_line_search:
         line_search = line_search_timing(args, dev, world, plan, roofline["peak"], roofline["peak_source"])
+    assembly = None
+    if not args.no_assembly:
+        assembly = assembly_timing(args, dev, world, roofline["peak"], roofline["peak_source"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -674,6 +719,7 @@ def main():
             "gradient": grad,
             "mixed": mixed,
             "line_search": line_search,
+            "assembly": assembly,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,

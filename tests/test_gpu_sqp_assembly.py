@@ -14,9 +14,10 @@ from warpmpc_b200.jax_sqp import QPAssembler, build_sparse_mpc_plan
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("cls,batch", [(problems.SMALL, 300), (problems.MPCClass("q5", 12, 4, 5, 10.0, 2.0, 1.0,
-                                                                                  "quadrotor"), 77)],
-                         ids=["small", "quadrotor_n5"])
+@pytest.mark.parametrize("cls,batch", [(problems.SMALL, 300),
+                                       (problems.MPCClass("q5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"), 77),
+                                       (problems.MPCClass("q120", 12, 4, 120, 10.0, 2.0, 1.0, "quadrotor"), 5)],
+                         ids=["small", "quadrotor_n5", "quadrotor_n120"])
 def test_assembly_bitexact(cuda_device, cls, batch):
     import torch
 

@@ -5,7 +5,10 @@
 // Gather form: every output entry sums its sources (stage values that the
 // reference scatter-adds into it) in stage order, starting from zero, so no
 // atomics and a fixed float32 operation order.  One block per instance;
-// threads stride over that instance's outputs (coalesced batch-major rows).
+// threads stride over that instance's outputs (coalesced batch-major rows;
+// the gathers hit the instance's packed row in L1).  Staging the row in
+// shared memory first was measured slower (2.65 ms against 1.95 ms for the
+// quadrotor N=30 stages at 65536 instances): fewer blocks fit per SM.
 #include "common.cuh"
 
 namespace wmpc {
@@ -71,9 +74,11 @@ extern "C" int wmpc_sqp_assemble(const wmpc_sqp_assemble_dims* dims, const int32
       (d.m > 0 && (!row_src || !l || !u || !g || !constraint_l || !constraint_u)))
     return fail(WMPC_ERR_INVALID_ARGUMENT, "sqp assemble: null pointer");
   const int grid = d.batch < 65536 ? d.batch : 65536;
-  sqp_assemble_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      d, add_ptr, add_src, row_src, cost_src, values, q, p_values, a_values, l, u, cost, g, constraint_l,
-      constraint_u);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  profile_mark_begin(s);
+  sqp_assemble_kernel<<<grid, 256, 0, s>>>(d, add_ptr, add_src, row_src, cost_src, values, q, p_values, a_values, l,
+                                           u, cost, g, constraint_l, constraint_u);
+  profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
 }
