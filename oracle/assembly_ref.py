@@ -16,9 +16,11 @@ from __future__ import annotations
 import numpy as np
 
 
-def assemble(plan, problem, stage_values):
+def assemble(plan, problem, stage_values, values_only=False):
     """stage_values: per stage (cost [B], g, lower, upper [B, nc], grad, hess,
-    jac [B, k]) float32 arrays.  Returns the nine SQPLinearization arrays."""
+    jac [B, k]) float32 arrays (values_only: the first four; the derivative
+    outputs stay zero, as _evaluate_values has none, sparse_mpc.py:840-853).
+    Returns the nine SQPLinearization arrays."""
     f = np.float32
     b = np.asarray(stage_values[0][0]).shape[0]
     n, m = int(plan.z_offsets[-1]), int(plan.constraint_offsets[-1])
@@ -28,16 +30,19 @@ def assemble(plan, problem, stage_values):
     g_all, lo_all, up_all = np.zeros((b, m), f), np.zeros((b, m), f), np.zeros((b, m), f)
     cost = np.zeros(b, f)
     for st, asm, vals in zip(problem.stages, plan.assemblies, stage_values):
-        c, g, lo, up, grad, hess, jac = (np.asarray(v, f) for v in vals)
+        c, g, lo, up = (np.asarray(v, f) for v in vals[:4])
+        r0, nc = asm.constraint_offset, st.constraint_dim
+        g_all[:, r0 : r0 + nc] = g
+        lo_all[:, r0 : r0 + nc] = lo
+        up_all[:, r0 : r0 + nc] = up
+        cost = cost + c
+        if values_only:
+            continue
+        grad, hess, jac = (np.asarray(v, f) for v in vals[4:7])
         for j, col in enumerate(asm.q_cols):
             q[:, col] = q[:, col] + grad[:, j]
         for j, pos in enumerate(asm.p_pos):
             pv[:, pos] = pv[:, pos] + hess[:, j]
         for j, pos in enumerate(asm.a_pos):
             av[:, pos] = av[:, pos] + jac[:, j]
-        r0, nc = asm.constraint_offset, st.constraint_dim
-        g_all[:, r0 : r0 + nc] = g
-        lo_all[:, r0 : r0 + nc] = lo
-        up_all[:, r0 : r0 + nc] = up
-        cost = cost + c
     return pv, av, q, lo_all - g_all, up_all - g_all, cost, g_all, lo_all, up_all

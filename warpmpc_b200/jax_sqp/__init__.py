@@ -14,6 +14,7 @@ from .assembly import (
     StageAssembly,
     build_sparse_mpc_plan,
 )
+from .sqp import SparseMPCSQP, SQPLineSearchStepResult, SQPSolveResult
 from .line_search import (
     LINE_SEARCH_CONSTRAINT,
     LINE_SEARCH_COST,
@@ -33,6 +34,9 @@ __all__ = [
     "SQPLinearization",
     "SparseMPCPlan",
     "SparseMPCProblem",
+    "SparseMPCSQP",
+    "SQPLineSearchStepResult",
+    "SQPSolveResult",
     "StageAssembly",
     "build_sparse_mpc_plan",
     "FilterLineSearchResult",

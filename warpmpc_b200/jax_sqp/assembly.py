@@ -243,14 +243,15 @@ def build_sparse_mpc_plan(problem: SparseMPCProblem, *, osqp_settings: OSQPSetti
 # batched assembly on the GPU
 # ---------------------------------------------------------------------------
 
-def stage_value_layout(plan: SparseMPCPlan, problem: SparseMPCProblem):
+def stage_value_layout(plan: SparseMPCPlan, problem: SparseMPCProblem, values_only: bool = False):
     """Column offsets of each stage's values in the packed per-instance row the
     kernel reads: per stage [cost (1) | g | lower | upper (constraint_dim each)
-    | grad | hess | jac], stages in order.  Returns (offsets [stages, 7], width)."""
+    | grad | hess | jac] (values_only: without the derivative parts), stages in
+    order.  Returns (offsets [stages, 7], width)."""
     offs, col = [], 0
     for st, asm in zip(problem.stages, plan.assemblies):
         nc = st.constraint_dim
-        parts = [1, nc, nc, nc, asm.q_cols.size, asm.p_pos.size, asm.a_pos.size]
+        parts = [1, nc, nc, nc] + ([0, 0, 0] if values_only else [asm.q_cols.size, asm.p_pos.size, asm.a_pos.size])
         o = []
         for w in parts:
             o.append(col)
@@ -259,17 +260,22 @@ def stage_value_layout(plan: SparseMPCPlan, problem: SparseMPCProblem):
     return np.asarray(offs, dtype=np.int64), col
 
 
-def assembly_tables(plan: SparseMPCPlan, problem: SparseMPCProblem):
+def assembly_tables(plan: SparseMPCPlan, problem: SparseMPCProblem, values_only: bool = False):
     """Gather tables of the assembly kernel.  Output row of one instance:
     [q (n) | P values (nnz_p) | A values (nnz_a)] summed from their sources in
     stage order (``add_ptr``/``add_src``), then the m constraint rows' g,
     lower and upper sources (``row_src``: the g column of each row, then each
     row's stage constraint_dim nc: lower and upper sit nc and 2 nc further),
-    and the stages' cost columns."""
-    offs, width = stage_value_layout(plan, problem)
+    and the stages' cost columns.  values_only: no q/P/A outputs (the
+    reference's _evaluate_values, sparse_mpc.py:840-853)."""
+    offs, width = stage_value_layout(plan, problem, values_only)
     n, nnz_p, nnz_a = int(plan.z_offsets[-1]), plan.p_pattern.nnz, plan.a_pattern.nnz
+    if values_only:
+        n = nnz_p = nnz_a = 0
     dest, src = [], []
     for s, (st, asm) in enumerate(zip(problem.stages, plan.assemblies)):
+        if values_only:
+            break
         dest += [asm.q_cols.astype(np.int64), n + asm.p_pos.astype(np.int64), n + nnz_p + asm.a_pos.astype(np.int64)]
         src += [offs[s, 4] + np.arange(asm.q_cols.size), offs[s, 5] + np.arange(asm.p_pos.size),
                 offs[s, 6] + np.arange(asm.a_pos.size)]
@@ -295,15 +301,17 @@ def assembly_tables(plan: SparseMPCPlan, problem: SparseMPCProblem):
 
 
 class QPAssembler:
-    """Device tables of one plan; ``assemble(values)`` -> SQPLinearization."""
+    """Device tables of one plan; ``assemble(values)`` -> SQPLinearization.
+    ``values_only``: stage values without derivatives in, only cost, g and the
+    bounds out (q, P and A empty)."""
 
-    def __init__(self, plan: SparseMPCPlan, problem: SparseMPCProblem, device=None):
+    def __init__(self, plan: SparseMPCPlan, problem: SparseMPCProblem, device=None, values_only: bool = False):
         import torch
 
         native.require_cuda()
-        self.plan, self.problem = plan, problem
+        self.plan, self.problem, self.values_only = plan, problem, values_only
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
-        t = assembly_tables(plan, problem)
+        t = assembly_tables(plan, problem, values_only)
         self.tables = t
         i32 = lambda a: torch.as_tensor(a, dtype=torch.int32, device=self.device)  # noqa: E731
         self.add_ptr, self.add_src = i32(t["add_ptr"]), i32(t["add_src"])
@@ -315,8 +323,9 @@ class QPAssembler:
         import torch
 
         cols = []
-        for (cost, g, lo, up, grad, hess, jac) in stage_values:
-            cols += [cost.reshape(-1, 1), g, lo, up, grad, hess, jac]
+        for vals in stage_values:
+            cost, g, lo, up = vals[:4]
+            cols += [cost.reshape(-1, 1), g, lo, up] + ([] if self.values_only else list(vals[4:7]))
         return torch.cat([c.to(self.device, torch.float32) for c in cols], dim=1).contiguous()
 
     def assemble(self, values) -> SQPLinearization:

@@ -138,9 +138,10 @@ def make_data(cls: problems.MPCClass, batch: int, seed: int = 0) -> StageData:
     return StageData(f(a), f(b), f(q), f(r))
 
 
-def evaluate_stages(problem: SparseMPCProblem, data, z, params):
+def evaluate_stages(problem: SparseMPCProblem, data, z, params, values_only: bool = False):
     """Every stage's (cost, g, lower, upper, grad, hess, jac) at z (batch-major
-    torch tensors, float32), entries in the stage's pattern order."""
+    torch tensors, float32), entries in the stage's pattern order; values_only:
+    (cost, g, lower, upper)."""
     import torch
 
     out = []
@@ -157,7 +158,7 @@ def evaluate_stages(problem: SparseMPCProblem, data, z, params):
         hess = w.clone()
         if st.terminal:
             e = z.new_zeros((z.shape[0], 0))
-            out.append((cost, e, e, e, grad, hess, e))
+            out.append((cost, e, e, e) if values_only else (cost, e, e, e, grad, hess, e))
             break
         zn = z[:, off + st.z_dim : off + st.z_dim + st.next_z_dim]
         x, u = zk[:, :nx], zk[:, nx:]
@@ -168,9 +169,26 @@ def evaluate_stages(problem: SparseMPCProblem, data, z, params):
                                                        z.new_full((z.shape[0], nu), -st.u_max)]
         up = ([params[:, :nx]] if st.first else []) + [z.new_zeros((z.shape[0], nx)),
                                                        z.new_full((z.shape[0], nu), st.u_max)]
-        jac = [z.new_ones((z.shape[0], nx))] if st.first else []
-        dyn_j = torch.cat([-A, -Bm, z.new_ones((z.shape[0], nx, 1))], dim=2).reshape(z.shape[0], -1)
-        jac += [dyn_j, z.new_ones((z.shape[0], nu))]
-        out.append((cost, torch.cat(g, 1), torch.cat(lo, 1), torch.cat(up, 1), grad, hess, torch.cat(jac, 1)))
+        vals = (cost, torch.cat(g, 1), torch.cat(lo, 1), torch.cat(up, 1))
+        if values_only:
+            out.append(vals)
+        else:
+            jac = [z.new_ones((z.shape[0], nx))] if st.first else []
+            dyn_j = torch.cat([-A, -Bm, z.new_ones((z.shape[0], nx, 1))], dim=2).reshape(z.shape[0], -1)
+            jac += [dyn_j, z.new_ones((z.shape[0], nu))]
+            out.append(vals + (grad, hess, torch.cat(jac, 1)))
         off += st.z_dim
     return out
+
+
+def make_evaluator(problem: SparseMPCProblem, data: StageData, device):
+    """The model callable of SparseMPCSQP: evaluate(z, params, values_only).
+    The model data are moved to the device once."""
+    import torch
+
+    dev_data = StageData(*(torch.as_tensor(v, device=device) for v in (data.a, data.b, data.q, data.r)))
+
+    def evaluate(z, params, values_only):
+        return evaluate_stages(problem, dev_data, z, params, values_only)
+
+    return evaluate
