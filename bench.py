@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--mixed-batch", type=int, default=131072, help="instances over the four mixed classes")
     ap.add_argument("--no-line-search", action="store_true", help="skip the SQP line-search step timing")
     ap.add_argument("--no-assembly", action="store_true", help="skip the SQP QP assembly timing")
+    ap.add_argument("--no-sqp", action="store_true", help="skip the SQP step timing")
     return ap.parse_args()
 
 
@@ -439,6 +440,55 @@ def assembly_timing(args, dev, world, hbm_peak, peak_source):
     }
 
 
+def sqp_timing(args, dev, world):
+    """One SQP step with the filter line search (SparseMPCSQP.line_search_step)
+    of the stage-wise quadrotor MPC (nx=12, nu=4, N=30) for args.batch
+    instances, replayed from a CUDA graph: model evaluation (torch, the
+    caller's part), QP assembly, persistent OSQP solve (25 iterations), four
+    candidate evaluations and the fused line-search step."""
+    import torch
+
+    from warpmpc_b200 import problems, sqp_problems
+    from warpmpc_b200.jax_sqp import SparseMPCSQP, build_sparse_mpc_plan
+
+    cls = problems.QUADROTOR
+    prob = sqp_problems.make_problem(cls)
+    plan = build_sparse_mpc_plan(prob)
+    B = args.batch
+    ev = sqp_problems.make_evaluator(prob, sqp_problems.make_data(cls, B, seed=8), dev)
+    sqp = SparseMPCSQP(prob, plan, ev, device=dev)
+    g = torch.Generator(device=dev).manual_seed(8)
+    params = torch.rand(B, cls.nx, device=dev, generator=g) * 2 - 1
+    z = torch.zeros(B, int(plan.z_offsets[-1]), device=dev)
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            sqp.line_search_step(z, params, None)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        out = sqp.line_search_step(z, params, None)
+    for _ in range(3):
+        graph.replay()
+    torch.cuda.synchronize()
+    reps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / reps, world)
+    accepted = float(out.line_search.accepted.float().mean())
+    del graph
+    return {
+        "workload": f"SQP step with filter line search, stage-wise quadrotor MPC nx={cls.nx} nu={cls.nu} "
+                    f"N={cls.horizon}, {B} instances/GPU, 25 ADMM iterations, 4-step ladder, CUDA graph",
+        "ms_per_step": ms, "instance_steps_per_s": B / (ms * 1e-3), "accepted_fraction": accepted,
+    }
+
+
 def mixed_timing(args, dev, world):
     """Mixed-size batch: args.mixed_batch instances spread over four linear MPC
     classes (nx, nu, N) = (4, 2, 10), (4, 2, 40), (12, 4, 20), (12, 4, 30),
@@ -689,6 +739,9 @@ def main():
     assembly = None
     if not args.no_assembly:
         assembly = assembly_timing(args, dev, world, roofline["peak"], roofline["peak_source"])
+    sqp = None
+    if not args.no_sqp:
+        sqp = sqp_timing(args, dev, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -720,6 +773,7 @@ def main():
             "mixed": mixed,
             "line_search": line_search,
             "assembly": assembly,
+            "sqp_step": sqp,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
