@@ -452,10 +452,12 @@ struct RelParams {
 // The scaled primal residual follows the iterates exactly (A x~ = z~ from the
 // KKT solve): e_{k+1} = (z_relaxed - z_{k+1}) + (1 - alpha) e_k.  chg / pres:
 // this lane's largest unscaled iterate change / primal residual so far
-// (the residual is carried only when termination is checked: kTrack).
+// (both are tracked, and lanes freeze, only when termination is checked:
+// kTrack; without it the update is the plain ADMM step).
 template <bool kCons, bool kTrack>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
-                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen) {
+                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen_in) {
+  const bool frozen = kTrack && frozen_in;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     float* xi = reinterpret_cast<float*>(xb + g.o[j]);
@@ -465,7 +467,7 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
       const float xn = frozen ? g.st[j].x : xa;
       *out = make_float2(xn, g.st[j].y);
       *xi = rp.sigma * xn - g.st[j].z;
-      chg = fmaxf(chg, fabsf(xn - g.st[j].x) * g.f[j]);
+      if constexpr (kTrack) chg = fmaxf(chg, fabsf(xn - g.st[j].x) * g.f[j]);
     } else {
       const float rinv = g.rinv[j];
       const float sv0 = g.st[j].x, yk = g.st[j].y;
@@ -484,7 +486,7 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
         pres = fmaxf(pres, fabsf(en) * g.f[j]);
       }
       *xi = zn - rinv * yn;
-      chg = fmaxf(chg, fmaxf(fabsf(zn - sv0), fabsf(yn - yk)) * g.f[j]);
+      if constexpr (kTrack) chg = fmaxf(chg, fmaxf(fabsf(zn - sv0), fabsf(yn - yk)) * g.f[j]);
     }
   }
 }
