@@ -317,7 +317,7 @@ __device__ __forceinline__ bool check_point(int check_every, int it) { return ch
 __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
   return (size_t)(n + 2) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
-         16 * (size_t)(lstages + sstages) + 16;  // barriers, abort flag, the two counters, the stop item
+         16 * (size_t)(lstages + sstages) + 32;  // barriers; abort flag, three counters, the stop item
 }
 
 // One unit's operands, loaded ahead of its arithmetic.
@@ -513,15 +513,21 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 
 // Shared-memory layout: X [n + 2][32] | L ring | S ring | barriers | flags.
 // Warps: 0 sweeps (forward and backward units), 1 produces (bulk copies),
-// 2 releases (first right-hand side, ADMM updates).  Every warp walks the same
+// 2 releases (first right-hand side, ADMM updates; with fixed iterations warp
+// 3 releases half of each chunk's indices alongside).  Every warp walks the same
 // item sequence; item t's L stage is freed by the warp that finishes with it
 // last (forward: sweeper; backward and first-rhs: releaser).  Two monotone
 // counters order the consumers: sweep_done (items the sweeper finished: a
 // backward item's releases need its columns solved) and rel_done (items the
 // releaser finished: a forward sweep needs every right-hand side).
-// kTrack: the primal residuals travel with the state (some class checks termination).
+// kTrack: the primal residuals travel with the state (some class checks
+// termination).  Without it (fixed iterations) a second releaser warp takes
+// half of every chunk's releases (the releaser is on the critical path with
+// the sweeper); the first releaser frees the stages and publishes rel_done
+// once both halves are done.
 template <bool kTrack>
-__global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
+__global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
+  constexpr bool kSplit = !kTrack;
   extern __shared__ __align__(128) unsigned char smem[];
   const int lstage_bytes = a.meta_bytes + a.lbytes;
   const int total_tiles = a.tile_end[a.n_jobs - 1];
@@ -536,6 +542,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
   unsigned* sweep_done = reinterpret_cast<unsigned*>(sempty + a.sstages) + 1;
   unsigned* rel_done = sweep_done + 1;
   volatile unsigned* stop_at = rel_done + 1;  // item index where a converged tile's items end
+  unsigned* rel_done1 = rel_done + 2;         // items the second releaser finished (kSplit)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
@@ -550,6 +557,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
     *sweep_done = 0;
     *rel_done = 0;
     *stop_at = 0xffffffffu;
+    *rel_done1 = 0;
     fence_mbarrier_init();
   }
   __syncthreads();
@@ -670,6 +678,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
     if (!ok && lane == 0) *abort_flag = 1;
   } else {
     // ------------------------------ releaser ------------------------------
+    const int rw = warp - 2;  // releaser 0, or (kSplit) releaser 1
     Ring lr{0, 0}, sr{0, 0};
     unsigned t = 0;
     unsigned char* xb = smem + lane * 4;
@@ -682,7 +691,7 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
       const int tile = g - (c ? a.tile_end[c - 1] : 0);
       const float sigma = J.sigma, alpha = J.alpha, oma = J.one_minus_alpha;
       // this class's zero row (read by padding slots); every earlier tile is done with X
-      X[n * 32 + lane] = 0.0f;
+      if (rw == 0) X[n * 32 + lane] = 0.0f;
       float4* stt = J.state + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
       float pres = 0.0f;  // this lane's largest unscaled primal residual in the current iteration
@@ -704,18 +713,30 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
           const int4* mu_leaf = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + kUnitSentinels) * kUnitWords);
           const int4* mu_pre = mu_leaf + (nl + kUnitSentinels) * (kUnitWords / 4);
           const int4* rel = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + nl + np + 3 * kUnitSentinels) * kUnitWords);
+          // this warp's share of the releases: halves of the primal and of the
+          // constraint range (all of them, on releaser 0, when the chunk has
+          // releaser units, which need every release of the chunk done first)
+          const bool split = kSplit && nl == 0 && np == 0;
+          auto share = [&](int b0, int e0, int& b1, int& e1) {
+            const int h = split ? b0 + (e0 - b0 + 1) / 2 : e0;
+            b1 = rw == 0 ? b0 : h;
+            e1 = rw == 0 ? h : e0;
+          };
+          int pb, pe, cb, ce;
+          share(0, nprim, pb, pe);
+          share(nprim, nrel, cb, ce);
           // leaf columns (read by no other column): solved here, just before their release
-          if (kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
+          if (rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
-            for (int k = 0; k < nprim; ++k) {
+            for (int k = pb; k < pe; ++k) {
               const float4 st = S[k * 32];
               *reinterpret_cast<float*>(xb + rel[k].x) = sigma * st.x - st.z;
             }
-            for (int k = nprim; k < nrel; ++k) {
+            for (int k = cb; k < ce; ++k) {
               const int4 r = rel[k];
               const float4 st = S[k * 32];
               *reinterpret_cast<float*>(xb + r.x) = st.x - __int_as_float(r.z) * st.y;
@@ -724,23 +745,34 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false, kTrack>(rel, 0, nprim, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-            run_releases<true, kTrack>(rel, nprim, nrel, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            run_releases<false, kTrack>(rel, pb, pe, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            run_releases<true, kTrack>(rel, cb, ce, S, SE, rp, xb, stu, peu, chg, pres, frozen);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
           }
           // forward rows whose entries all read leaf rows: their right-hand sides are now final
-          if (np > 0) {
+          if (rw == 0 && np > 0) {
             __syncwarp();
             run_units<false>(mu_pre, lst, xb, lane, np);
           }
           __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(sempty + sr.stage);
-            mbar_arrive(lempty + lr.stage);
+          if (rw == 1) {
+            if (lane == 0) st_release_cta(rel_done1, t + 1);
+          } else {
+            // both halves done before the stages are freed
+            if (kSplit && !wait_counter_bounded(rel_done1, t + 1, abort_flag, kWaitLimitNs)) return false;
+            if (lane == 0) {
+              mbar_arrive(sempty + sr.stage);
+              mbar_arrive(lempty + lr.stage);
+            }
           }
           sr.advance(a.sstages);
+        }
+        if (rw == 1) {  // the second releaser publishes nothing else and makes no decisions
+          lr.advance(a.lstages);
+          ++t;
+          return true;
         }
         if (kind == kItemBwd && ch == 0) {
           // an iteration is complete: decide (before publishing it) whether the tile stops here
@@ -765,7 +797,8 @@ __global__ void __launch_bounds__(96, 1) admm_stream_kernel(const __grid_constan
       };
       auto cont = [&](int it) -> int { (void)it; return stop ? 0 : 1; };
       if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, release, cont)) ok = false;
-      if (ok && J.iters && tile * 32 + lane < J.batch) J.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
+      if (ok && rw == 0 && J.iters && tile * 32 + lane < J.batch)
+        J.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
     }
     if (!ok && lane == 0) *abort_flag = 1;
   }
@@ -950,7 +983,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   auto kernel = track ? admm_stream_kernel<true> : admm_stream_kernel<false>;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
-  kernel<<<grid, 96, cfg.smem, s>>>(a);
+  kernel<<<grid, track ? 96 : 128, cfg.smem, s>>>(a);
   profile_mark_end(s);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
