@@ -110,3 +110,41 @@ def test_live_reference_planners_random():
             x = getattr(ref, f)
             if isinstance(x, np.ndarray):
                 _eq(getattr(mine, f), x, f)
+
+
+def test_live_reference_derivative_plans_random():
+    """The adjoint KKT plan against the reference's builder on random QPs with
+    equality rows, one-sided and free rows (where the reference tree exists)."""
+    from oracle import ref_import
+
+    if not ref_import.available():
+        pytest.skip("reference checkout not present (fixtures cover this case)")
+    ns = ref_import.load()
+    from warpmpc_b200.jax_osqp.derivative_plan import build_derivative_plan
+    from warpmpc_b200.jax_qdldl.amd import amd_order
+
+    ref_import.PERMUTATION_PROVIDER = amd_order
+    rng = np.random.default_rng(9)
+    for trial in range(8):
+        n, m = int(rng.integers(2, 12)), int(rng.integers(1, 14))
+        p = sp.random(n, n, density=0.3, random_state=int(rng.integers(1 << 30)))
+        p = sp.triu(sp.csc_matrix(p @ p.T + sp.eye(n)), format="csc")
+        a = sp.csc_matrix(sp.random(m, n, density=0.4, random_state=int(rng.integers(1 << 30))))
+        a.sum_duplicates()
+        a.sort_indices()
+        kind = rng.integers(0, 4, m)  # 0 box, 1 equality, 2 lower only, 3 free
+        l = np.where(kind == 3, -1e30, rng.standard_normal(m) - 1.0)
+        u = np.where(kind == 2, 1e30, np.where(kind == 1, l, l + rng.uniform(0.1, 2.0, m)))
+        u = np.where(kind == 3, 1e30, u)
+        ref = ns.solver._build_derivative_plan(p, a, l, u)
+        mine = build_derivative_plan(p, a, l, u)
+        for f in ref.__dataclass_fields__:
+            x = getattr(ref, f)
+            if isinstance(x, np.ndarray):
+                _eq(getattr(mine, f), x, f"trial {trial}: {f}")
+            elif isinstance(x, (int, float)):
+                assert getattr(mine, f) == x, (trial, f)
+        _eq(mine.adjoint_upper.indices, ref.adjoint_upper.indices, "adjoint indices")
+        _eq(mine.adjoint_upper.indptr, ref.adjoint_upper.indptr, "adjoint indptr")
+        _eq(mine.adjoint_upper.data, ref.adjoint_upper.data, "adjoint data")
+        _eq(mine.qdldl_plan.li, ref.qdldl_plan.li, "adjoint li")
