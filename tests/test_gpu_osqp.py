@@ -185,3 +185,22 @@ def test_solve_host_pipelined_matches_device_solve(cuda_device, warm, chunks):
         assert g.device.type == "cpu"
         np.testing.assert_array_equal(g.numpy(), r.cpu().numpy())
     assert eng.last_iters.shape == (200,)
+
+
+def test_two_ctas_per_sm_small_class_bitexact(cuda_device, monkeypatch):
+    """A small pattern with more tiles than SMs runs two streaming CTAs per SM
+    (two sweepers); the iterates stay bit-exact with the oracle, and equal the
+    one-CTA-per-SM launch."""
+    import torch
+
+    b = problems.make_batch(problems.SMALL, 9500, seed=13)  # 297 tiles > 148 SMs
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    got = _run(comp, b)
+    ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u)
+    for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r, err_msg=name)
+    monkeypatch.setenv("WMPC_STREAM_CTAS", "1")
+    one = _run(comp, b)
+    for g, o in zip(got[:3], one[:3]):
+        np.testing.assert_array_equal(g, o)

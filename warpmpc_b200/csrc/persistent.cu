@@ -849,12 +849,12 @@ RingSizes ring_sizes(const StreamPlan& sp, bool track) {
   return r;
 }
 
-bool ring_config(const RingSizes& r, StreamLaunch* cfg) {
+bool ring_config(const RingSizes& r, StreamLaunch* cfg, size_t limit = (size_t)kMaxSmemBytes) {
   // prefer deep rings: as many L stages as fit with at least 3 S stages
   for (int ls = r.lmax; ls >= 2; --ls)
     for (int ss = r.smax; ss >= 2; --ss) {
       const size_t bytes = stream_smem_bytes(r.x_rows - 2, ls, ss, r.meta_bytes + r.lbytes, r.sbytes);
-      if (bytes <= (size_t)kMaxSmemBytes && (ss >= 3 || ls <= 3)) {
+      if (bytes <= limit && (ss >= 3 || ls <= 3)) {
         cfg->stages = ls;
         cfg->sstages = ss;
         cfg->meta_bytes = r.meta_bytes;
@@ -926,6 +926,12 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   return WMPC_OK;
 }
 
+static int total_tiles_of(const StreamJobDesc* jobs, int n_jobs) {
+  int t = 0;
+  for (int i = 0; i < n_jobs; ++i) t += jobs[i].n_tiles;
+  return t;
+}
+
 // One launch over every class's tiles, the costliest class first.
 int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s) {
   if (n_jobs < 1 || n_jobs > kMaxStreamJobs) return fail(WMPC_ERR_INVALID_ARGUMENT, "1 to %d classes per launch", kMaxStreamJobs);
@@ -949,6 +955,30 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   std::sort(order, order + n_jobs, [&](int x, int y) { return cost[x] > cost[y]; });
   StreamLaunch cfg;
   if (!ring_config(r, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "these classes do not fit one launch's shared memory");
+  // Two CTAs (two sweepers) per SM when both fit with 4-stage L and 3-stage S
+  // rings (the ring depth does not limit the sweep; the sweeper's instruction
+  // stream does): small patterns, enough tiles for both.
+  int ctas_per_sm = 1;
+  {
+    int dev = 0, sm_bytes = 0, reserved = 0;
+    const char* env = getenv("WMPC_STREAM_CTAS");
+    const bool allow = !(env && atoi(env) == 1);
+    if (allow && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess) {
+      RingSizes r2 = r;
+      r2.lmax = std::min(r2.lmax, 4);
+      r2.smax = std::min(r2.smax, 3);
+      StreamLaunch cfg2;
+      const size_t half = (size_t)(sm_bytes / 2 - reserved);
+      if (ring_config(r2, &cfg2, half) && total_tiles_of(jobs, n_jobs) > num_sms) {
+        cfg = cfg2;
+        ctas_per_sm = 2;
+      }
+    } else {
+      (void)cudaGetLastError();
+    }
+  }
   StreamArgs a{};
   int total = 0;
   for (int k = 0; k < n_jobs; ++k) {
@@ -981,7 +1011,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.lbytes = cfg.lbytes;
   a.sbytes = cfg.sbytes;
   a.pres_off = cfg.pres_off;
-  const int grid = total < num_sms ? total : num_sms;
+  const int grid = total < ctas_per_sm * num_sms ? total : ctas_per_sm * num_sms;
   auto kernel = track ? admm_stream_kernel<true> : admm_stream_kernel<false>;
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
