@@ -204,3 +204,19 @@ def test_two_ctas_per_sm_small_class_bitexact(cuda_device, monkeypatch):
     one = _run(comp, b)
     for g, o in zip(got[:3], one[:3]):
         np.testing.assert_array_equal(g, o)
+
+
+def test_autotune_stream_candidates_agree(cuda_device, tmp_path):
+    """Every schedule candidate gives the same iterates; the fastest is picked
+    and cached per pattern and device."""
+    from warpmpc_b200.jax_osqp.autotune import autotune_stream
+
+    b = problems.make_batch(problems.SMALL, 600, seed=21)
+    plan = problems.make_plan(b)
+    cands = ({}, {"units": 8, "cols": 8, "rel": 6, "funits": 8}, {"units": 24, "cols": 24, "rel": 16, "funits": 24},
+             {"offload": 3})
+    cache = str(tmp_path / "tune.json")
+    r = autotune_stream(plan, b.p_values, b.a_values, b.q, b.l, b.u, candidates=cands, repeats=2, cache_path=cache)
+    assert r.best in [dict(c) for c in cands] and len(r.timings_ms) == len(cands) and not r.cached
+    again = autotune_stream(plan, b.p_values, b.a_values, b.q, b.l, b.u, candidates=cands, cache_path=cache)
+    assert again.cached and again.best == r.best
