@@ -257,7 +257,11 @@ int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_op
  * primal variables; KKT rows >= n_primal are constraints).  units/cols/rel:
  * backward chunk size targets (4-entry units, columns, releases); funits:
  * forward chunk target (units); offload: work also given to the releasing
- * warp (bit 0: leaf columns, bit 1: rows whose entries all read leaf rows).  With out == NULL, *out_words receives the
+ * warp (bit 0: leaf columns, bit 1: rows whose entries all read leaf rows);
+ * bit 2 asks for the frontier-slot form (offload bits 0): the work vector
+ * holds only the values a sweep still reads, in slots; right-hand sides and
+ * forward results travel through the stages (host schedule only: the
+ * streaming kernel does not run it yet).  With out == NULL, *out_words receives the
  * buffer size; otherwise out (capacity out_capacity int32 words) receives,
  * in order:
  *   [n_chunks, blen, max_units, max_cols, max_rel, max_meta_words, max_row_nnz, n_meta]
@@ -269,7 +273,8 @@ int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_op
  *   fchunk_off[n_fchunks+1] fchunk_units[n_fchunks] fmeta_off[n_fchunks]
  *   fmeta_words[n_fchunks] fmeta[n_fmeta] proc_foff[nnz_l]
  *   [n_pad_b, n_pad_f, dummy_units] pad_boff[n_pad_b] pad_foff[n_pad_f]
- *   chunk_pre_u0[n_chunks] chunk_pre_units[n_chunks] */
+ *   chunk_pre_u0[n_chunks] chunk_pre_units[n_chunks]
+ *   [frontier_slots, frontier_lag, max_frows] (0, 0, 0 without bit 2) */
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv,
                               int32_t n_primal, int32_t units, int32_t cols, int32_t rel, int32_t funits,
                               int32_t offload, int32_t* out, int64_t out_capacity, int64_t* out_words);

@@ -23,8 +23,16 @@ def _f32(x):
     return np.float32(x)
 
 
-def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, max_iter=None):
-    """Run the stream algorithm for a batch of <= 32 instances (float32)."""
+def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, max_iter=None, lag=None):
+    """Run the stream algorithm for a batch of <= 32 instances (float32).
+
+    A frontier-slot schedule (``sched["frontier_slots"] > 0``) runs the form
+    that schedule is built for: the work vector is a slot array, the
+    right-hand sides live in a vector R read through each forward chunk's
+    stage, the forward results in a vector Y read through each backward
+    chunk's stage, and the releases of a backward chunk run ``lag`` chunks
+    after it (the most a release may trail the sweep; default the schedule's
+    lag) -- so a slot freed too early shows up as a wrong result."""
     qp = plan.qdldl_plan
     rg = sched["ragged"]
     n, nnz_l = qp.n, qp.nnz_l
@@ -117,8 +125,13 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     oma = _f32(1.0) - alpha
     iters = plan.settings.max_iter if max_iter is None else max_iter
     nch = sched["n_chunks"]
-    X = np.full((n + 2, lanes), np.nan, dtype=np.float32)  # row n: the zero row, n + 1: trash
-    X[n] = 0.0
+    fr = int(sched.get("frontier_slots", 0)) > 0
+    zr = int(sched["frontier_slots"]) if fr else n  # the zero row (slot); the trash row follows
+    X = np.full((zr + 2, lanes), np.nan, dtype=np.float32)
+    X[zr] = 0.0
+    R = np.full((n, lanes), np.nan, dtype=np.float32)  # frontier: right-hand sides
+    Y = np.full((n, lanes), np.nan, dtype=np.float32)  # frontier: forward results
+    lag = (int(sched["frontier_lag"]) if fr else 1) if lag is None else lag
     meta_all = sched["meta"]
     fmeta_all = sched["fmeta"]
     nfc = sched["n_fchunks"]
@@ -129,7 +142,7 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         return all_[off : off + w]
 
     def xrow(byte_off):
-        assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= n + 1
+        assert byte_off % 128 == 0 and 0 <= byte_off // 128 <= zr + 1
         return byte_off // 128
 
     def run_units(m, nu, stage, backward, first_unit=0):
@@ -143,7 +156,8 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         units = m[off : off + (nu + NSENT) * KUW].reshape(nu + NSENT, KUW)
         ubase = int(units[0][6]) // 512  # stage position of the list's first unit
         for sent in units[nu:]:
-            assert np.all(sent[:5] == n * 128) and sent[5] == 0 and sent[6] == 0 and sent[7] == (n + 1) * 128
+            assert np.all(sent[:4] == zr * 128) and sent[4] == (0 if fr else n * 128)
+            assert sent[5] == 0 and sent[6] == 0 and sent[7] == (zr + 1) * 128
         nfl = stage.size
 
         def load(u):
@@ -153,13 +167,18 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             assert lo == ((ubase + u) * 512 if u < nu else 0)
             lv = stage[lo // 4 : lo // 4 + 128].reshape(lanes, 4).T.copy()  # [slot][lane]
             xs = [X[xrow(o)].copy() for o in src]
-            t = X[xrow(ctl[0])].copy()
+            if fr:  # t from the stage (right-hand-side block / forward-result block)
+                to = int(ctl[0])
+                assert to % 128 == 0 and to // 4 + 32 <= nfl
+                t = stage[to // 4 : to // 4 + 32].copy()
+            else:
+                t = X[xrow(ctl[0])].copy()
             d = None
             if backward:
                 doff = int(ctl[1]) >> DSHIFT
                 assert doff % 4 == 0 and doff // 4 + 32 <= nfl
                 d = stage[doff // 4 : doff // 4 + 32].copy()
-            if u < nu:
+            if u < nu and not fr:
                 assert xrow(ctl[3]) == (xrow(ctl[0]) if int(ctl[1]) & LAST else n + 1)
             return ctl, lv, xs, t, d
 
@@ -188,9 +207,14 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                     acc = acc - lv[3] * x3
                     res = acc
                 X[xrow(ctl[3])] = res
+                if fr and not backward and u < nu and fl & LAST:
+                    row = fl >> DSHIFT
+                    assert 0 <= row < n
+                    Y[row] = res  # the forward result, for the backward sweep's stage
                 prev = res
                 cur = nxt
 
+    pending = []  # deferred releases (frontier lag)
     items = [(0, nch - 1 - t) for t in range(nch)]
     for _ in range(iters):
         items += [(1, c) for c in range(nfc)] + [(2, c) for c in range(nch - 1, -1, -1)]
@@ -201,7 +225,13 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             assert nu == sched["fchunk_units"][ch] and nu <= sched["max_funits"]
             o0, o1 = sched["fchunk_off"][ch], sched["fchunk_off"][ch + 1]
             assert o1 - o0 == nu * 128 and o1 <= FL
-            run_units(fm, nu, Fs[o0:o1], backward=False)
+            stage = Fs[o0:o1]
+            if fr:  # the chunk's rows' right-hand sides follow its units
+                r0, r1 = int(fm[1]), int(fm[2])
+                assert 0 <= r0 < r1 <= n and r1 - r0 <= sched["max_frows"]
+                assert not np.isnan(R[r0:r1]).any(), "a right-hand side is read before its release"
+                stage = np.concatenate([stage, R[r0:r1].reshape(-1)])
+            run_units(fm, nu, stage, backward=False)
             continue
         m = block(meta_all, sched["meta_off"], sched["meta_words"], ch, sched["max_meta_words"])
         ns, ncols, nrel, c0, u0, nprim, nl, npre = (int(v) for v in m[:8])
@@ -220,6 +250,11 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
         o0, o1 = sched["chunk_off"][ch], sched["chunk_off"][ch + 1]
         assert o1 - o0 == nu * 128 + ncols * 32 and o1 <= BL
         stage = Lb[o0:o1]
+        if fr:
+            assert nl == 0 and npre == 0
+            if kind == 2:  # the chunk's columns' forward results follow its D^-1 rows
+                assert not np.isnan(Y[c0 : c0 + ncols]).any()
+                stage = np.concatenate([stage, Y[c0 : c0 + ncols].reshape(-1)])
         leaf_at, pre_at = ns + NSENT, ns + nl + 2 * NSENT
         if kind == 0:
             # the first-right-hand-side pass copies only the releaser's forward units
@@ -227,41 +262,60 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
             stage = np.full_like(stage, np.nan)
             p0, p1 = (ns + nl) * 128, (ns + nl + npre) * 128
             stage[p0:p1] = Lb[o0 + p0 : o0 + p1]
-        if kind == 2:
-            if ns:
-                run_units(m, ns, stage, backward=True)
-            if nl:
-                run_units(m, nl, stage, backward=True, first_unit=leaf_at)
+        def rhs_out(k, i, value):
+            """The next right-hand side: into R (frontier) or the work vector."""
+            if fr:
+                idx = int(recs[k, 3])
+                assert 0 <= idx < n
+                R[idx] = value
+            else:
+                X[i] = value
+
+        def releases(recs=recs, rel_i=rel_i, rel_rho=rel_rho, rel_rinv=rel_rinv, u0=u0, nprim=nprim, nrel=nrel):
             for k in range(nrel):
                 i = xrow(rel_i[k])
-                assert i < n
+                assert i < (zr if fr else n)
                 uu = u0 + k
                 sol = X[i].copy()
+                assert not np.isnan(sol).any()
                 if k < nprim:
                     xn = alpha * sol + oma * s0[uu]
                     s0[uu] = xn
-                    X[i] = sigma * xn - pp0[uu]
+                    out = sigma * xn - pp0[uu]
                 else:
                     rinv = rel_rinv[k]
                     zk, yk = s0[uu].copy(), s1[uu].copy()
                     rz = zk - rinv * yk
                     zt = rz + rinv * sol
-                    zr = alpha * zt + oma * zk
-                    zn = zr + rinv * yk
+                    zrel = alpha * zt + oma * zk
+                    zn = zrel + rinv * yk
                     zn = np.where(zn < pp0[uu], pp0[uu], zn)
                     zn = np.where(zn > pp1[uu], pp1[uu], zn)
-                    yn = yk + rel_rho[k] * (zr - zn)
+                    yn = yk + rel_rho[k] * (zrel - zn)
                     s0[uu], s1[uu] = zn, yn
-                    X[i] = zn - rinv * yn
+                    out = zn - rinv * yn
+                if fr:
+                    R[int(recs[k, 3])] = out
+                else:
+                    X[i] = out
+
+        if kind == 2:
+            if ns:
+                run_units(m, ns, stage, backward=True)
+            if nl:
+                run_units(m, nl, stage, backward=True, first_unit=leaf_at)
+            pending.append(releases)
+            # a release may trail the sweep by lag - 1 chunks; all are done before the forward sweep
+            while len(pending) > max(lag - 1, 0) or (ch == 0 and pending):
+                pending.pop(0)()
         else:
             for k in range(nrel):
-                i = xrow(rel_i[k])
-                assert i < n
+                i = -1 if fr else xrow(rel_i[k])
                 uu = u0 + k
-                X[i] = sigma * s0[uu] - pp0[uu] if k < nprim else s0[uu] - rel_rinv[k] * s1[uu]
+                rhs_out(k, i, sigma * s0[uu] - pp0[uu] if k < nprim else s0[uu] - rel_rinv[k] * s1[uu])
         if npre:
             run_units(m, npre, stage, backward=False, first_unit=pre_at)
-        assert X[n].max() == 0.0 and X[n].min() == 0.0
+        assert X[zr].max() == 0.0 and X[zr].min() == 0.0
     # ---- stream_to_state_kernel + unscale
     x = np.zeros((lanes, plan.n), np.float32)
     z = np.zeros((lanes, plan.m), np.float32)

@@ -1,0 +1,77 @@
+"""Frontier-slot schedules (host schedule of the next streaming-kernel form).
+
+The schedule renames the work-vector rows to slots that hold only what a
+sweep still reads; right-hand sides and forward results travel through the
+stages instead.  The CPU replay runs that form with every index bounds-checked
+and the releases of each backward chunk deferred by the schedule's lag (the
+most a release may trail the sweep): its iterates equal the oracle's bit for
+bit, cold and warm started, so no slot is reused while something still reads
+it.  The streaming kernel does not run this form yet.
+"""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from oracle import osqp_ref
+from warpmpc_b200 import problems
+from warpmpc_b200.schedule import stream_schedule
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import stream_sim  # noqa: E402
+
+FRONTIER = (16, 16, 12, 16, 4)
+
+
+@pytest.mark.parametrize("cls,iters", [(problems.SMALL, 4), (problems.CARTPOLE, 3),
+                                       (problems.MPCClass("q5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"), 3)],
+                         ids=["small", "cartpole", "quadrotor_n5"])
+@pytest.mark.parametrize("lag", [None, 1])
+def test_frontier_replay_bitexact(cls, iters, lag):
+    b = problems.make_batch(cls, 6, seed=31)
+    plan = problems.make_plan(b)
+    sched = stream_schedule(plan, targets=FRONTIER)
+    assert 0 < sched["frontier_slots"] < plan.qdldl_plan.n and sched["frontier_lag"] == 4
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters, lag=lag)
+    ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters)
+    for g, r in zip(got, ref[:3]):
+        np.testing.assert_array_equal(g, r)
+
+
+def test_frontier_replay_warm_start():
+    b = problems.make_batch(problems.SMALL, 8, seed=7)
+    plan = problems.make_plan(b)
+    sched = stream_schedule(plan, targets=FRONTIER)
+    x, z, y = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3)[:3]
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, x0=x, z0=z, y0=y, max_iter=3)
+    ref = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, x, z, y, max_iter=3)
+    for g, r in zip(got, ref[:3]):
+        np.testing.assert_array_equal(g, r)
+
+
+def test_frontier_slots_shrink_the_work_vector():
+    """Slots needed against rows for the benchmark patterns: the quadrotor's
+    work vector drops from 1358 rows to about 500."""
+    for cls, most in ((problems.SMALL, 0.6), (problems.CARTPOLE, 0.5), (problems.QUADROTOR, 0.45)):
+        plan = problems.make_plan(problems.make_batch(cls, 2, seed=0))
+        sched = stream_schedule(plan, targets=FRONTIER)
+        assert sched["frontier_slots"] <= most * plan.qdldl_plan.n, (cls.name, sched["frontier_slots"])
+
+
+def test_frontier_needs_no_offload():
+    plan = problems.make_plan(problems.make_batch(problems.SMALL, 2, seed=0))
+    with pytest.raises(NotImplementedError):
+        stream_schedule(plan, targets=(16, 16, 12, 16, 4 | 1))
+
+
+def test_frontier_replay_detects_releases_later_than_the_schedule_allows():
+    """Control: releases trailing the sweep by more chunks than the schedule
+    reserved slots for read reused slots, and the iterates change."""
+    b = problems.make_batch(problems.SMALL, 6, seed=31)
+    plan = problems.make_plan(b)
+    sched = stream_schedule(plan, targets=FRONTIER)
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3, lag=8)
+    ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3)
+    assert not all(np.array_equal(g, r) for g, r in zip(got, ref[:3]))

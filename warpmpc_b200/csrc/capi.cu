@@ -223,6 +223,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   t.rel = rel;
   t.funits = funits;
   t.offload = offload & 3;
+  t.frontier = (offload >> 2) & 1;  // bit 2: frontier-slot schedule
   if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
       !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
     return fail(WMPC_ERR_UNSUPPORTED, "%s", why.c_str());
@@ -241,6 +242,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   w.push_back(hs.dummy_units);
   app(hs.pad_boff); app(hs.pad_foff);
   app(hs.chunk_pre_u0); app(hs.chunk_pre_units);
+  w.push_back(hs.frontier_slots); w.push_back(hs.frontier_lag); w.push_back(hs.max_frows);
   *out_words = static_cast<int64_t>(w.size());
   if (!out) return WMPC_OK;
   if (out_capacity < static_cast<int64_t>(w.size())) return fail(WMPC_ERR_INVALID_ARGUMENT, "output buffer too small");

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -161,6 +162,179 @@ void push_sentinels(int zero_row, int trash_row, std::vector<int>* m) {
   }
 }
 
+// Units of one chunk kept for the frontier pass: where the chunk's unit meta
+// starts, its units in stage order, and its row (forward) or column
+// (backward) range.
+struct ChunkUnits {
+  int word0;  // first word of unit 0 in the meta vector
+  int lo, hi; // rows [lo, hi) (forward) or columns [lo, hi) (backward)
+  int nu;     // units (= meta words / kUnitWords before the sentinels)
+  int rel_word0 = -1, u0 = 0, nrel = 0;  // backward: release records
+  std::vector<UnitBuild> units;
+};
+
+// Slots for the values of one sweep phase.  A value gets a slot when the unit
+// that finishes it stores it and keeps it through its last read; the slot is
+// reusable two units later (a unit's operands are loaded before the previous
+// unit stores).  Values nothing reads later go to the trash slot.  Returns the
+// slot of every value (-1: none) and the number of slots used.
+std::vector<int> assign_slots(int n_values, const std::vector<int>& write_t, const std::vector<int>& free_after,
+                              int* n_slots) {
+  std::vector<int> by_time(n_values);
+  std::iota(by_time.begin(), by_time.end(), 0);
+  std::sort(by_time.begin(), by_time.end(), [&](int a, int b) { return write_t[a] < write_t[b]; });
+  std::vector<int> slot(n_values, -1);
+  std::priority_queue<int, std::vector<int>, std::greater<int>> free_slots;
+  using Pending = std::pair<int, int>;  // (reusable from time, slot)
+  std::priority_queue<Pending, std::vector<Pending>, std::greater<Pending>> pending;
+  int used = 0;
+  for (int v : by_time) {
+    if (write_t[v] < 0 || free_after[v] < 0) continue;  // never written, or never read after its store
+    while (!pending.empty() && pending.top().first <= write_t[v]) {
+      free_slots.push(pending.top().second);
+      pending.pop();
+    }
+    int sl;
+    if (free_slots.empty()) {
+      sl = used++;
+    } else {
+      sl = free_slots.top();
+      free_slots.pop();
+    }
+    slot[v] = sl;
+    pending.push({free_after[v] + 2, sl});
+  }
+  *n_slots = used;
+  return slot;
+}
+
+// Frontier mode: rename the work-vector rows of every unit and release record
+// to slots, so the work vector holds only what a sweep still reads.  The
+// right-hand sides move to a per-tile vector R read through each forward
+// chunk's stage (block of rows [lo, hi) after its units); the forward results
+// to a vector Y read through each backward chunk's stage (block of columns
+// [lo, hi) after the D^-1 rows).  Unit words: sources and store become slot
+// offsets, the target becomes the byte offset of `t` in the stage's L area,
+// and a forward unit's flags carry its row (its Y entry) in place of the D^-1
+// offset; release records carry the released index's slot and, in place of
+// the unscale factor, the index (its R entry).  Sentinels and no-op units read
+// stage offset 0.
+bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, const std::vector<ChunkUnits>& bwd,
+                          const std::vector<int>& order, HostStream* S, std::string* why) {
+  const int zero_row = n;
+  // ---- forward phase: values y_i, written by the last unit of row i
+  std::vector<int> f_write(n, -1), f_read(n, -1);
+  int tau = 0;
+  for (const ChunkUnits& c : fwd)
+    for (const UnitBuild& ub : c.units) {
+      for (int s2 = 0; s2 < 4; ++s2)
+        if (ub.src[s2] != zero_row) f_read[ub.src[s2]] = std::max(f_read[ub.src[s2]], tau);
+      if ((ub.flags & kUnitLast) && ub.target != zero_row) f_write[ub.target] = tau;
+      ++tau;
+    }
+  std::vector<int> f_free(n, -1);
+  for (int v = 0; v < n; ++v)
+    if (f_read[v] > f_write[v] && f_write[v] >= 0) f_free[v] = f_read[v];
+  int f_slots = 0;
+  const std::vector<int> fslot = assign_slots(n, f_write, f_free, &f_slots);
+  // ---- backward phase (chunks in sweep order: last chunk first): values x_j
+  std::vector<int> b_write(n, -1), b_read(n, -1), chunk_end;
+  tau = 0;
+  for (int k = static_cast<int>(bwd.size()) - 1; k >= 0; --k) {
+    for (const UnitBuild& ub : bwd[k].units) {
+      for (int s2 = 0; s2 < 4; ++s2)
+        if (ub.src[s2] != zero_row) b_read[ub.src[s2]] = std::max(b_read[ub.src[s2]], tau);
+      if ((ub.flags & kUnitLast) && ub.target != zero_row) b_write[ub.target] = tau;
+      ++tau;
+    }
+    chunk_end.push_back(tau - 1);
+  }
+  // a release may run until the sweep is `lag` chunks further (ring depth)
+  const int nb = static_cast<int>(bwd.size());
+  for (int p = 0; p < nb; ++p) {
+    const ChunkUnits& c = bwd[nb - 1 - p];
+    const int t_rel = chunk_end[std::min(nb - 1, p + lag - 1)];
+    for (int k = 0; k < c.nrel; ++k) {
+      const int i = order[c.u0 + k];
+      if (b_write[i] < 0 || b_write[i] > t_rel) {
+        *why = "frontier: a release precedes its column";
+        return false;
+      }
+      b_read[i] = std::max(b_read[i], t_rel);
+    }
+  }
+  std::vector<int> b_free(n, -1);
+  for (int v = 0; v < n; ++v)
+    if (b_write[v] >= 0) b_free[v] = std::max(b_read[v], b_write[v] + 1);
+  int b_slots = 0;
+  const std::vector<int> bslot = assign_slots(n, b_write, b_free, &b_slots);
+  const int F = std::max(f_slots, b_slots);
+  const int zs = F, ts = F + 1;
+  if (F + 2 > (1 << 20)) {
+    *why = "frontier: too many slots";
+    return false;
+  }
+  auto sentinel_words = [&](std::vector<int>& m, int w0) {
+    for (int k = 0; k < kUnitSentinels; ++k) {
+      int* w = &m[w0 + k * kUnitWords];
+      for (int s2 = 0; s2 < 4; ++s2) w[s2] = zs * 128;
+      w[4] = 0;
+      w[5] = 0;
+      w[6] = 0;
+      w[7] = ts * 128;
+    }
+  };
+  // ---- rewrite the forward meta
+  for (const ChunkUnits& c : fwd) {
+    for (int u = 0; u < c.nu; ++u) {
+      const UnitBuild& ub = c.units[u];
+      int* w = &S->fmeta[c.word0 + u * kUnitWords];
+      for (int s2 = 0; s2 < 4; ++s2) {
+        const int r = ub.src[s2];
+        if (r != zero_row && fslot[r] < 0) {
+          *why = "frontier: a forward read without a slot";
+          return false;
+        }
+        w[s2] = (r == zero_row ? zs : fslot[r]) * 128;
+      }
+      const bool real = ub.target != zero_row;
+      w[4] = real ? c.nu * 512 + (ub.target - c.lo) * 128 : 0;
+      w[5] = ub.flags | ((real ? ub.target : 0) << kUnitDoffShift);
+      const bool keep = (ub.flags & kUnitLast) && real && fslot[ub.target] >= 0;
+      w[7] = (keep ? fslot[ub.target] : ts) * 128;
+    }
+    sentinel_words(S->fmeta, c.word0 + c.nu * kUnitWords);
+  }
+  // ---- rewrite the backward meta and release records
+  for (const ChunkUnits& c : bwd) {
+    const int ncols = c.hi - c.lo;
+    for (int u = 0; u < c.nu; ++u) {
+      const UnitBuild& ub = c.units[u];
+      int* w = &S->meta[c.word0 + u * kUnitWords];
+      for (int s2 = 0; s2 < 4; ++s2) {
+        const int r = ub.src[s2];
+        if (r != zero_row && bslot[r] < 0) {
+          *why = "frontier: a backward read without a slot";
+          return false;
+        }
+        w[s2] = (r == zero_row ? zs : bslot[r]) * 128;
+      }
+      const bool real = ub.target != zero_row;
+      w[4] = real ? c.nu * 512 + ncols * 128 + (ub.target - c.lo) * 128 : 0;
+      w[7] = ((ub.flags & kUnitLast) && real ? bslot[ub.target] : ts) * 128;
+    }
+    for (int l = 0; l < 3; ++l) sentinel_words(S->meta, c.word0 + (c.nu + l * kUnitSentinels) * kUnitWords);
+    for (int k = 0; k < c.nrel; ++k) {
+      const int i = order[c.u0 + k];
+      S->meta[c.rel_word0 + 4 * k] = bslot[i] * 128;
+      S->meta[c.rel_word0 + 4 * k + 3] = i;
+    }
+  }
+  S->frontier_slots = F;
+  S->frontier_lag = lag;
+  return true;
+}
+
 }  // namespace
 
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
@@ -174,6 +348,11 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     *why = "bad stream targets";
     return false;
   }
+  if (t.frontier && (t.offload || t.frontier_lag < 1)) {
+    *why = "frontier mode needs offload 0 and a release lag of at least one chunk";
+    return false;
+  }
+  std::vector<ChunkUnits> fwd_units, bwd_units;  // frontier mode only
   // release column of every index: smallest column whose L entry lies in row i
   std::vector<int> rel_col(n);
   for (int i = 0; i < n; ++i) rel_col[i] = i;
@@ -360,6 +539,18 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     while (m.size() % 4) m.push_back(0);
     S.meta_off[ch] = static_cast<int>(S.meta.size());
     S.meta_words[ch] = static_cast<int>(m.size());
+    if (t.frontier) {
+      ChunkUnits cu;
+      cu.word0 = S.meta_off[ch] + kChunkHeader;
+      cu.lo = c0;
+      cu.hi = c1;
+      cu.nu = ns;
+      cu.rel_word0 = S.meta_off[ch] + kChunkHeader + (ns + nl + np + 3 * kUnitSentinels) * kUnitWords;
+      cu.u0 = u0;
+      cu.nrel = nrel;
+      cu.units = lists[0];
+      bwd_units.push_back(std::move(cu));
+    }
     S.max_meta_words = std::max(S.max_meta_words, static_cast<int>(m.size()));
     S.meta.insert(S.meta.end(), m.begin(), m.end());
     for (int li = 0; li < 3; ++li)
@@ -383,7 +574,9 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     }
   // ---- forward sweep (sweeper): rows in order (row-gather form), columns ascending in a row; pre rows excluded
   {
-    auto row_units = [&](int i) { return pre_row[i] ? 0 : (rcount[i] + 3) / 4; };
+    // (frontier mode: a row without entries gets one no-op unit that carries
+    // its right-hand side into its forward value)
+    auto row_units = [&](int i) { return pre_row[i] ? 0 : t.frontier && rcount[i] == 0 ? 1 : (rcount[i] + 3) / 4; };
     std::vector<int> fb{0};
     {
       int units = 0;
@@ -406,7 +599,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       for (int i = r0; i < r1; ++i) {
         const std::vector<int>& re = row_entries[i];
         const int cnt = static_cast<int>(re.size());
-        if (cnt == 0 || pre_row[i]) continue;
+        if ((cnt == 0 && !t.frontier) || pre_row[i]) continue;
         std::vector<int> slot_of;
         std::vector<UnitBuild> add = cut_units(cnt, true, i, zero_row, [&](int q) { return col_of[re[q]]; }, &slot_of);
         const int first = append_units(&units, std::move(add), 3, zero_row, &S.dummy_units);
@@ -415,7 +608,17 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       const int nu = static_cast<int>(units.size());
       if (nu == 0) continue;
       for (const auto& pe : placed) entry_foff[pe.first] = foff + (pe.second >> 2) * 128 + (pe.second & 3);
-      std::vector<int> m{nu, 0, 0, 0, 0, 0, 0, 0};
+      std::vector<int> m{nu, t.frontier ? r0 : 0, t.frontier ? r1 : 0, 0, 0, 0, 0, 0};
+      if (t.frontier) {
+        ChunkUnits cu;
+        cu.word0 = static_cast<int>(S.fmeta.size()) + kChunkHeader;
+        cu.lo = r0;
+        cu.hi = r1;
+        cu.nu = nu;
+        cu.units = units;
+        fwd_units.push_back(std::move(cu));
+        S.max_frows = std::max(S.max_frows, r1 - r0);
+      }
       for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
       push_sentinels(zero_row, trash_row, &m);
       S.fchunk_off.push_back(foff);
@@ -439,6 +642,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       *why = "forward stream misses an entry";
       return false;
     }
+  if (t.frontier && !build_frontier_slots(n, t.frontier_lag, fwd_units, bwd_units, order, &S, why)) return false;
   // factorization re-reads: the L entry every update reads, D^-1 of every step's column
   S.upd_pos.clear();
   S.step_doff.resize(hp.nnz_l);

@@ -217,6 +217,8 @@ struct StreamTargets {
   int units = 16, cols = 16, rel = 12;  // backward chunks
   int funits = 16;                      // forward chunks
   int offload = 0;                      // also give the releaser warp: 1 leaf columns, 2 pre rows (bits)
+  int frontier = 0;                     // frontier slots (see build_frontier_slots); needs offload 0
+  int frontier_lag = 4;                 // chunks a release may trail the sweep (the L ring depth)
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.
@@ -230,6 +232,10 @@ struct HostStream {
   int max_row_kv = 0;
   std::vector<int> u_perm, u_orig;
   int dummy_units = 0;
+  // frontier mode: work-vector slots (zero slot = frontier_slots, trash slot
+  // + 1), the release lag the slot reservations assume, the longest forward
+  // chunk in rows (its right-hand-side block in the stage)
+  int frontier_slots = 0, frontier_lag = 0, max_frows = 0;
   // host copies used by the OSQP side to lay out the state
   std::vector<int> u_of_perm;  // permuted index -> U index
 };

@@ -45,7 +45,7 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
 
     targets: (backward units, backward columns, backward releases, forward
     units) per chunk, and the offload bits (1: leaf columns, 2: rows reading
-    only leaf rows, solved by the releasing warp)."""
+    only leaf rows, solved by the releasing warp; 4: the frontier-slot form)."""
     qp = plan.qdldl_plan
     desc, keep, rg = _pattern_desc(qp)
     rho = native.f32(plan.rho_vec)
@@ -100,6 +100,9 @@ def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
     take("pad_foff", npf)
     take("chunk_pre_u0", n_chunks)
     take("chunk_pre_units", n_chunks)
+    fs, flag, mfr = (int(v) for v in buf[pos : pos + 3])
+    pos += 3
+    out.update({"frontier_slots": fs, "frontier_lag": flag, "max_frows": mfr})
     assert pos == buf.size
     out["ragged"] = rg
     return out
