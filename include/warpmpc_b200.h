@@ -209,6 +209,13 @@ typedef struct wmpc_osqp_batch {
  * (solve_with_factor), 0 when the call factors. */
 size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t mode, int32_t external_factor);
 
+/* Which streaming schedule the problem carries (no reference counterpart: the
+ * streaming kernel is this library's).  info[0]: 1 when persistent solves run
+ * the streaming kernel's schedule, 0 when they fall back; info[1]: work-vector
+ * slots of the frontier form (0: the plain form, one row per KKT index);
+ * info[2]: the KKT dimension; info[3]: the frontier form's release lag. */
+int wmpc_osqp_stream_info(const wmpc_osqp* osqp, int32_t info[4]);
+
 enum { WMPC_OSQP_PLAIN = 0, WMPC_OSQP_PERSISTENT = 1 };
 
 /* KKT assembly + numeric factorization.  Replaces CompiledOSQP.factor

@@ -1,0 +1,83 @@
+"""The streaming kernel's frontier form on the GPU vs the oracle.
+
+With ``WMPC_STREAM_FRONTIER=1`` a compiled problem carries the frontier-slot
+schedule: the work vector holds only what a sweep still reads, the
+right-hand sides and forward results travel through per-tile vectors and the
+stages.  Fixed-iteration solves then run that form; their iterates must equal
+the oracle's bit for bit (the arithmetic and its order are unchanged).  The
+quadrotor pattern uses 12-unit chunks so that two CTAs fit an SM.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import osqp_ref
+from warpmpc_b200 import problems
+from warpmpc_b200.jax_osqp import compile_osqp
+
+pytestmark = pytest.mark.gpu
+
+QUAD_KNOBS = {"WMPC_STREAM_UNITS": "12", "WMPC_STREAM_COLS": "12", "WMPC_STREAM_REL": "8",
+              "WMPC_STREAM_FUNITS": "12"}
+
+
+def _compile(monkeypatch, plan, knobs):
+    monkeypatch.setenv("WMPC_STREAM_FRONTIER", "1")
+    for k, v in knobs.items():
+        monkeypatch.setenv(k, v)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    info = comp.engine.stream_info()
+    assert info["streaming"] and 0 < info["frontier_slots"] < info["n"], info
+    return comp
+
+
+def _run(comp, b, warm=None):
+    import torch
+
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+    if warm is None:
+        out = comp.solve(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u))
+    else:
+        out = comp.solve_warm_start(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), *[t(w) for w in warm])
+    return [o.cpu().numpy() for o in out]
+
+
+@pytest.mark.parametrize("cls,batch,knobs", [(problems.SMALL, 9500, {}), (problems.CARTPOLE, 700, {}),
+                                             (problems.QUADROTOR, 4801, QUAD_KNOBS)],
+                         ids=["small", "cartpole", "quadrotor"])
+def test_frontier_form_bitexact(cuda_device, monkeypatch, cls, batch, knobs):
+    """Many tiles (two CTAs per SM where they fit), a partial last tile."""
+    from oracle.cpu_baseline import CpuOSQP
+
+    b = problems.make_batch(cls, batch, seed=23)
+    plan = problems.make_plan(b)
+    comp = _compile(monkeypatch, plan, knobs)
+    got = _run(comp, b)
+    ref = CpuOSQP(plan).solve(b.p_values, b.a_values, b.q, b.l, b.u)
+    for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r, err_msg=name)
+    assert not np.any(comp.engine.last_status.cpu().numpy() & 8)
+
+
+def test_frontier_form_warm_start(cuda_device, monkeypatch):
+    b = problems.make_batch(problems.CARTPOLE, 70, seed=4)
+    plan = problems.make_plan(b)
+    comp = _compile(monkeypatch, plan, {})
+    rng = np.random.default_rng(2)
+    warm = tuple((rng.standard_normal((70, k)) * 0.1).astype(np.float32) for k in (plan.n, plan.m, plan.m))
+    got = _run(comp, b, warm=warm)
+    ref = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, *warm)
+    for g, r in zip(got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r)
+
+
+def test_frontier_form_refuses_termination_checks(cuda_device, monkeypatch):
+    """The frontier form runs fixed iterations; a checked solve fails loudly."""
+    import torch
+
+    b = problems.make_batch(problems.SMALL, 40, seed=3)
+    plan = problems.make_plan(b)
+    comp = _compile(monkeypatch, plan, {})
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    with pytest.raises(Exception, match="fixed iterations"):
+        comp.engine.solve(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), check_termination=5)

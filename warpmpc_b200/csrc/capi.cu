@@ -531,6 +531,14 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (const char* v = getenv("WMPC_STREAM_FUNITS")) targets.funits = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_OFFLOAD")) targets.offload = atoi(v) & 3;
     if (targets.units <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.funits <= 0) targets = StreamTargets();
+    // opt-in: the frontier-slot form (fixed-iteration solves only; no releaser offload)
+    if (const char* v = getenv("WMPC_STREAM_FRONTIER")) {
+      if (atoi(v) > 0) {
+        targets.frontier = 1;
+        targets.offload = 0;
+        if (const char* lag = getenv("WMPC_STREAM_FRONTIER_LAG")) targets.frontier_lag = atoi(lag);
+      }
+    }
     // iterate-change unscale factors (original KKT order) for early termination
     std::vector<float> unscale(hp.n, 1.0f);
     for (int j = 0; j < n; ++j) unscale[j] = desc->scaling_d[j];
@@ -556,6 +564,9 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
       sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
       sp.max_row_kv = hs.max_row_kv;
+      sp.frontier_slots = hs.frontier_slots;
+      sp.frontier_lag = hs.frontier_lag;
+      sp.max_frows = hs.max_frows;
       sp.max_lstages = 12;
       sp.max_sstages = 6;
       if (const char* v = getenv("WMPC_STREAM_LSTAGES")) sp.max_lstages = atoi(v);
@@ -616,6 +627,15 @@ int wmpc_osqp_destroy(wmpc_osqp* osqp) {
   if (osqp->block) cudaFree(osqp->block);
   if (osqp->stream_block) cudaFree(osqp->stream_block);
   delete osqp;
+  return WMPC_OK;
+}
+
+int wmpc_osqp_stream_info(const wmpc_osqp* osqp, int32_t info[4]) {
+  if (!osqp || !info) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  info[0] = osqp->has_stream ? 1 : 0;
+  info[1] = osqp->has_stream ? osqp->sp.frontier_slots : 0;
+  info[2] = osqp->has_stream ? osqp->sp.n : 0;
+  info[3] = osqp->has_stream ? osqp->sp.frontier_lag : 0;
   return WMPC_OK;
 }
 

@@ -239,6 +239,8 @@ struct StreamJob {
   const float* fstream;
   float4* state;  // [tile][U][lane] ADMM state records
   float* pres;    // [tile][U][lane] scaled primal residual of each constraint
+  float* rhs;     // frontier form: [tile][n][lane] right-hand sides (release -> forward stage)
+  float* fwd;     // frontier form: [tile][n][lane] forward results (sweep -> backward stage)
   int* iters;     // [batch] iterations run (may be null)
   int n_tiles, max_iter, batch;
   int check_every;  // > 0: stop a tile once every lane's largest unscaled iterate change <= chg_eps
@@ -333,15 +335,17 @@ __device__ __forceinline__ void load_meta(const int4* __restrict__ mu, int u, Un
 }
 
 // lane_l: this lane's 16 bytes of unit 0 of the stage (lst + lane * 16)
+// tb: where the target offsets point (the work vector, or the stage's L area
+// in the frontier form), this lane's column
 template <bool kBackward>
 __device__ __forceinline__ void load_data(const unsigned char* lane_l, const unsigned char* lst,
-                                          const unsigned char* xb, int lane, UnitOps& r) {
+                                          const unsigned char* xb, const unsigned char* tb, int lane, UnitOps& r) {
   r.l = *reinterpret_cast<const float4*>(lane_l + r.ctl.z);
   r.x0 = *reinterpret_cast<const float*>(xb + r.src.x);
   r.x1 = *reinterpret_cast<const float*>(xb + r.src.y);
   r.x2 = *reinterpret_cast<const float*>(xb + r.src.z);
   r.x3 = *reinterpret_cast<const float*>(xb + r.src.w);
-  r.t = *reinterpret_cast<const float*>(xb + r.ctl.x);
+  r.t = *reinterpret_cast<const float*>(tb + r.ctl.x);
   if (kBackward) r.d = *reinterpret_cast<const float*>(lst + (r.ctl.y >> kUnitDoffShift) + lane * 4);
 }
 
@@ -355,7 +359,10 @@ __device__ __forceinline__ float select_flag(int flags, int mask, float a, float
 }
 
 // Forward unit: acc = (first ? rhs_i : acc) - L_i,c0 x_c0 - ... (ascending c)
-__device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, float& acc, float& prev) {
+// kFrontier: a row's last unit also writes the row's result to yt (the
+// forward-result vector, this lane's column; the row is in the flags word)
+template <bool kFrontier>
+__device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, float* yt, float& acc, float& prev) {
   const int fl = r.ctl.y;
   const float x3 = select_flag(fl, kUnitFwd, prev, r.x3);
   acc = select_flag(fl, kUnitFirst, r.t, acc);
@@ -364,6 +371,9 @@ __device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb
   acc = acc - r.l.z * r.x2;
   acc = acc - r.l.w * x3;
   *reinterpret_cast<float*>(xb + r.ctl.w) = acc;
+  if constexpr (kFrontier) {
+    if (fl & kUnitLast) yt[(fl >> kUnitDoffShift) * 32] = acc;
+  }
   prev = acc;
 }
 
@@ -387,26 +397,26 @@ __device__ __forceinline__ void backward_unit(const UnitOps& r, unsigned char* x
 // register sets in rotation, one exit test per three units).  The units past
 // nu are sentinels: computed when nu is not a multiple of 3, harmlessly (they
 // store to the trash row, and acc/prev are dead after the chunk).
-template <bool kBackward>
+template <bool kBackward, bool kFrontier = false>
 __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const unsigned char* lst, unsigned char* xb,
-                                          int lane, int nu) {
+                                          const unsigned char* tb, float* yt, int lane, int nu) {
   static_assert(kUnitGroup == 3 && kUnitSentinels >= 4, "loop shape and sentinel count disagree");
   const unsigned char* lane_l = lst + lane * 16;
   UnitOps A, B, C;
   float acc = 0.0f, prev = 0.0f;
   load_meta(mu, 0, A);
-  load_data<kBackward>(lane_l, lst, xb, lane, A);
+  load_data<kBackward>(lane_l, lst, xb, tb, lane, A);
   load_meta(mu, 1, B);
   for (int u = 0; u < nu; u += 3) {
     load_meta(mu, u + 2, C);
-    load_data<kBackward>(lane_l, lst, xb, lane, B);
-    if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit(A, xb, acc, prev);
+    load_data<kBackward>(lane_l, lst, xb, tb, lane, B);
+    if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit<kFrontier>(A, xb, yt, acc, prev);
     load_meta(mu, u + 3, A);
-    load_data<kBackward>(lane_l, lst, xb, lane, C);
-    if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit(B, xb, acc, prev);
+    load_data<kBackward>(lane_l, lst, xb, tb, lane, C);
+    if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit<kFrontier>(B, xb, yt, acc, prev);
     load_meta(mu, u + 4, B);
-    load_data<kBackward>(lane_l, lst, xb, lane, A);
-    if (kBackward) backward_unit(C, xb, acc, prev); else forward_unit(C, xb, acc, prev);
+    load_data<kBackward>(lane_l, lst, xb, tb, lane, A);
+    if (kBackward) backward_unit(C, xb, acc, prev); else forward_unit<kFrontier>(C, xb, yt, acc, prev);
   }
 }
 
@@ -456,13 +466,17 @@ struct RelParams {
 // this lane's largest unscaled iterate change / primal residual so far
 // (both are tracked, and lanes freeze, only when termination is checked:
 // kTrack; without it the update is the plain ADMM step).
-template <bool kCons, bool kTrack>
-__device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb,
+// kFrontier: the next right-hand side goes to rt (this lane's column of the
+// right-hand-side vector) at the index the record carries in its last word,
+// not back into the work vector.
+template <bool kCons, bool kTrack, bool kFrontier>
+__device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb, float* rt,
                                                  float4* stu, float* peu, float& chg, float& pres, bool frozen_in) {
+  static_assert(!(kTrack && kFrontier), "the frontier form's records carry indices, not unscale factors");
   const bool frozen = kTrack && frozen_in;
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
-    float* xi = reinterpret_cast<float*>(xb + g.o[j]);
+    float* xi = kFrontier ? rt + __float_as_int(g.f[j]) * 32 : reinterpret_cast<float*>(xb + g.o[j]);
     float2* out = reinterpret_cast<float2*>(stu + g.kk[j] * 32);
     if (!kCons) {
       const float xa = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
@@ -493,10 +507,10 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
   }
 }
 
-template <bool kCons, bool kTrack>
+template <bool kCons, bool kTrack, bool kFrontier>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
-                                             const RelParams& rp, unsigned char* xb, float4* stu, float* peu,
-                                             float& chg, float& pres, bool frozen) {
+                                             const RelParams& rp, unsigned char* xb, float* rt, float4* stu,
+                                             float* peu, float& chg, float& pres, bool frozen) {
   if (begin >= end) return;
   RelGroup a, b;
   load_rel_group<kTrack>(rel, begin, end, S, SE, xb, a);
@@ -504,11 +518,11 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + kRelGroup < end ? k + kRelGroup : end - 1;
     load_rel_group<kTrack>(rel, kb, end, S, SE, xb, b);
-    update_rel_group<kCons, kTrack>(a, rp, xb, stu, peu, chg, pres, frozen);
+    update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + kRelGroup >= end) break;
     const int ka = k + 2 * kRelGroup < end ? k + 2 * kRelGroup : end - 1;
     load_rel_group<kTrack>(rel, ka, end, S, SE, xb, a);
-    update_rel_group<kCons, kTrack>(b, rp, xb, stu, peu, chg, pres, frozen);
+    update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + 2 * kRelGroup >= end) break;
   }
 }
@@ -527,8 +541,16 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // half of every chunk's releases (the releaser is on the critical path with
 // the sweeper); the first releaser frees the stages and publishes rel_done
 // once both halves are done.
-template <bool kTrack>
+// kFrontier (fixed iterations only): X holds slots, not rows.  The releasers
+// write the right-hand sides to the per-tile vector rhs and the sweeper each
+// row's forward result to fwd; the producer copies a forward chunk's rows of
+// rhs, and a backward chunk's columns of fwd, into the stage behind its L
+// data, where the units read their targets.  Those copies wait for the writes:
+// a sweep's first forward chunk until every earlier item is released, its
+// first backward chunk until every earlier item is swept.
+template <bool kTrack, bool kFrontier>
 __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
+  static_assert(!(kTrack && kFrontier), "the frontier form runs fixed iterations");
   constexpr bool kSplit = !kTrack;
   extern __shared__ __align__(128) unsigned char smem[];
   const int lstage_bytes = a.meta_bytes + a.lbytes;
@@ -597,10 +619,28 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             pre_at = (uint32_t)__ldg(sp.chunk_pre_u0 + ch);
             lbytes = (uint32_t)__ldg(sp.chunk_pre_units + ch) * 512u;
           }
-          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes);
+          // frontier form: the rows' right-hand sides (forward) or the columns'
+          // forward results (backward), placed behind the L data
+          uint32_t xbytes = 0;
+          const float* xsrc = nullptr;
+          if constexpr (kFrontier) {
+            if (fwd) {
+              if (ch == 0 && !wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return false;
+              const int r0 = __ldg(sp.fmeta + moff + 1), r1 = __ldg(sp.fmeta + moff + 2);
+              xbytes = (uint32_t)(r1 - r0) * 128u;
+              xsrc = J.rhs + soff + (size_t)r0 * 32;
+            } else if (kind == kItemBwd) {
+              if (ch == sp.n_chunks - 1 && !wait_counter_bounded(sweep_done, issued_l, abort_flag, kWaitLimitNs))
+                return false;
+              xbytes = (uint32_t)__ldg(sp.chunk_cols + ch) * 128u;
+              xsrc = J.fwd + soff + (size_t)__ldg(sp.meta + moff + 3) * 32;
+            }
+          }
+          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes + xbytes);
           bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + moff, (uint32_t)mwords * 4u, lfull + lr.stage);
           if (lbytes)
             bulk_g2s(st + a.meta_bytes + pre_at * 512u, (fwd ? ft : bt) + loff + pre_at * 128u, lbytes, lfull + lr.stage);
+          if (kFrontier && xbytes) bulk_g2s(st + a.meta_bytes + lbytes, xsrc, xbytes, lfull + lr.stage);
           lr.advance(a.lstages);
           ++issued_l;
           if (!fwd) {
@@ -639,8 +679,11 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
     unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
     bool ok = true;
     for (int g = blockIdx.x; g < total_tiles && ok; g += gridDim.x) {
-      const StreamJob& J = a.job[job_of(a, g)];
+      const int c = job_of(a, g);
+      const StreamJob& J = a.job[c];
       const StreamPlan& sp = J.sp;
+      float* yt = nullptr;  // frontier form: this lane's column of the tile's forward results
+      if constexpr (kFrontier) yt = J.fwd + (size_t)(g - (c ? a.tile_end[c - 1] : 0)) * sp.n * 32 + lane;
       auto sweep = [&](int kind, int ch) -> bool {
         if (kind != kItemRel) {
           // a forward sweep needs every right-hand side of the previous pass
@@ -652,13 +695,16 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           const unsigned char* lst = stage + a.meta_bytes;
           const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
           const int nu = meta[0];
+          const unsigned char* tb = kFrontier ? lst + lane * 4 : xb;
           if (nu > 0) {
             if (kind == kItemFwd) {
-              run_units<false>(mu, lst, xb, lane, nu);  // forward substitution, row-gather form
+              run_units<false, kFrontier>(mu, lst, xb, tb, yt, lane, nu);  // forward substitution, row-gather form
             } else {
-              run_units<true>(mu, lst, xb, lane, nu);   // backward substitution, column form
+              run_units<true>(mu, lst, xb, tb, nullptr, lane, nu);         // backward substitution, column form
             }
           }
+          // the forward results written here are read back by bulk copies
+          if (kFrontier && kind == kItemFwd) fence_proxy_async_global();
           __syncwarp();
           if (lane == 0) {
             if (kind == kItemFwd) mbar_arrive(lempty + lr.stage);
@@ -693,7 +739,9 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       const int tile = g - (c ? a.tile_end[c - 1] : 0);
       const float sigma = J.sigma, alpha = J.alpha, oma = J.one_minus_alpha;
       // this class's zero row (read by padding slots); every earlier tile is done with X
-      if (rw == 0) X[n * 32 + lane] = 0.0f;
+      if (rw == 0) X[(kFrontier ? sp.frontier_slots : n) * 32 + lane] = 0.0f;
+      float* rt = nullptr;  // frontier form: this lane's column of the tile's right-hand sides
+      if constexpr (kFrontier) rt = J.rhs + (size_t)tile * n * 32 + lane;
       float4* stt = J.state + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
       float pres = 0.0f;  // this lane's largest unscaled primal residual in the current iteration
@@ -728,35 +776,38 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           share(0, nprim, pb, pe);
           share(nprim, nrel, cb, ce);
           // leaf columns (read by no other column): solved here, just before their release
-          if (rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, lane, nl);
+          if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, nullptr, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
+            // (frontier form: into rhs at the record's index)
             for (int k = pb; k < pe; ++k) {
+              const int4 r = rel[k];
               const float4 st = S[k * 32];
-              *reinterpret_cast<float*>(xb + rel[k].x) = sigma * st.x - st.z;
+              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = sigma * st.x - st.z;
             }
             for (int k = cb; k < ce; ++k) {
               const int4 r = rel[k];
               const float4 st = S[k * 32];
-              *reinterpret_cast<float*>(xb + r.x) = st.x - __int_as_float(r.z) * st.y;
+              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = st.x - __int_as_float(r.z) * st.y;
             }
+            if constexpr (kFrontier) fence_proxy_async_global();  // read back by bulk copies
           } else {
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false, kTrack>(rel, pb, pe, S, SE, rp, xb, stu, peu, chg, pres, frozen);
-            run_releases<true, kTrack>(rel, cb, ce, S, SE, rp, xb, stu, peu, chg, pres, frozen);
+            run_releases<false, kTrack, kFrontier>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen);
+            run_releases<true, kTrack, kFrontier>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
           }
           // forward rows whose entries all read leaf rows: their right-hand sides are now final
-          if (rw == 0 && np > 0) {
+          if (!kFrontier && rw == 0 && np > 0) {
             __syncwarp();
-            run_units<false>(mu_pre, lst, xb, lane, np);
+            run_units<false>(mu_pre, lst, xb, xb, nullptr, lane, np);
           }
           __syncwarp();
           if (rw == 1) {
@@ -838,14 +889,19 @@ RingSizes ring_sizes(const StreamPlan& sp, bool track) {
   RingSizes r;
   const int mw = sp.max_meta_words > sp.max_fmeta_words ? sp.max_meta_words : sp.max_fmeta_words;
   r.meta_bytes = ((mw * 4 + 127) / 128) * 128;
-  const int bl = sp.max_units * 512 + sp.max_cols * 128;
-  const int fl = sp.max_funits * 512;
+  // (frontier form: a backward stage also holds its columns' forward results,
+  // a forward stage its rows' right-hand sides)
+  const bool frontier = sp.frontier_slots > 0;
+  const int bl = sp.max_units * 512 + sp.max_cols * (frontier ? 256 : 128);
+  const int fl = sp.max_funits * 512 + (frontier ? sp.max_frows * 128 : 0);
   r.lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
   r.pres_off = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
   r.sbytes = r.pres_off + (track ? r.pres_off / 4 : 0);
-  r.x_rows = sp.n + 2;
+  r.x_rows = (frontier ? sp.frontier_slots : sp.n) + 2;
   r.lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
   r.smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
+  // the slots assume releases trail the sweep by at most frontier_lag chunks
+  if (frontier) r.lmax = std::min(r.lmax, sp.frontier_lag);
   return r;
 }
 
@@ -873,9 +929,11 @@ bool ring_config(const RingSizes& r, StreamLaunch* cfg, size_t limit = (size_t)k
 // (sized with the residuals: a pattern that fits this fits every launch)
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring_config(ring_sizes(sp, true), cfg); }
 
+// streams, state records, residuals (+ frontier form: right-hand sides and forward results)
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
-  return tiles * ((size_t)sp.blen + (size_t)sp.flen + 5 * 32 * (size_t)sp.n) + 64;
+  const size_t vectors = sp.frontier_slots > 0 ? 7 : 5;
+  return tiles * ((size_t)sp.blen + (size_t)sp.flen + vectors * 32 * (size_t)sp.n) + 64;
 }
 
 // Factorization into the streams and the state into its records (one class).
@@ -891,6 +949,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   float* fstream = bstream + (size_t)n_tiles * sp.blen;
   float4* state = reinterpret_cast<float4*>(fstream + (size_t)n_tiles * sp.flen);
   float* pres = reinterpret_cast<float*>(state + tl * sp.n);
+  float* rhs = sp.frontier_slots > 0 ? pres + tl * sp.n : nullptr;
+  float* fwd = sp.frontier_slots > 0 ? rhs + tl * sp.n : nullptr;
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
   if (!reuse_factor) {
     // L-batch sized so that every tile's warp is resident at once (all of a
@@ -918,6 +978,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   job->fstream = fstream;
   job->state = state;
   job->pres = pres;
+  job->rhs = rhs;
+  job->fwd = fwd;
   job->n_tiles = n_tiles;
   job->batch = batch;
   job->sigma = o.sigma;
@@ -940,6 +1002,12 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   double cost[kMaxStreamJobs];
   bool track = false;
   for (int i = 0; i < n_jobs; ++i) track = track || jobs[i].check_every > 0;
+  const bool frontier = jobs[0].sp.frontier_slots > 0;
+  for (int i = 0; i < n_jobs; ++i)
+    if ((jobs[i].sp.frontier_slots > 0) != frontier)
+      return fail(WMPC_ERR_UNSUPPORTED, "frontier-form and plain classes cannot share a launch");
+  if (frontier && track)
+    return fail(WMPC_ERR_UNSUPPORTED, "the frontier-form schedule runs fixed iterations (no termination checks)");
   for (int i = 0; i < n_jobs; ++i) {
     const RingSizes ri = ring_sizes(jobs[i].sp, track);
     r.meta_bytes = std::max(r.meta_bytes, ri.meta_bytes);
@@ -989,6 +1057,8 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     J.fstream = d.fstream;
     J.state = d.state;
     J.pres = d.pres;
+    J.rhs = d.rhs;
+    J.fwd = d.fwd;
     J.iters = d.iters;
     J.n_tiles = d.n_tiles;
     J.max_iter = d.max_iter;
@@ -1012,7 +1082,8 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.sbytes = cfg.sbytes;
   a.pres_off = cfg.pres_off;
   const int grid = total < ctas_per_sm * num_sms ? total : ctas_per_sm * num_sms;
-  auto kernel = track ? admm_stream_kernel<true> : admm_stream_kernel<false>;
+  auto kernel = track ? admm_stream_kernel<true, false>
+                      : (frontier ? admm_stream_kernel<false, true> : admm_stream_kernel<false, false>);
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   profile_mark_begin(s);
   kernel<<<grid, track ? 96 : 128, cfg.smem, s>>>(a);

@@ -335,6 +335,65 @@ bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, co
   return true;
 }
 
+// Every word the streaming kernel reads in the frontier form, checked against
+// what it addresses: slots inside the work vector (zero and trash slot
+// included), stage offsets inside the chunk's L area plus its right-hand-side
+// or forward-result block, rows, columns and released indices inside [0, n).
+bool check_frontier_tables(const HostStream& S, int n, std::string* why) {
+  const int F = S.frontier_slots;
+  auto bad = [&](const char* what, int ch) {
+    *why = std::string("frontier table check: ") + what + " (chunk " + std::to_string(ch) + ")";
+    return false;
+  };
+  auto slot_ok = [&](int w, int top) { return w >= 0 && w % 128 == 0 && w / 128 <= top; };
+  for (int ch = 0; ch < S.n_fchunks; ++ch) {
+    const int* m = &S.fmeta[S.fmeta_off[ch]];
+    const int nu = m[0], r0 = m[1], r1 = m[2];
+    if (nu != S.fchunk_units[ch] || nu < 1 || nu > S.max_funits) return bad("forward units", ch);
+    if (r0 < 0 || r1 <= r0 || r1 > n || r1 - r0 > S.max_frows) return bad("forward rows", ch);
+    if (S.fmeta_words[ch] < kChunkHeader + (nu + kUnitSentinels) * kUnitWords) return bad("forward meta size", ch);
+    const int area = nu * 512 + (r1 - r0) * 128;
+    for (int u = 0; u < nu + kUnitSentinels; ++u) {
+      const int* w = m + kChunkHeader + u * kUnitWords;
+      for (int s2 = 0; s2 < 4; ++s2)
+        if (!slot_ok(w[s2], F)) return bad("forward source slot", ch);
+      if (w[4] < 0 || w[4] % 128 != 0 || w[4] + 128 > area) return bad("forward right-hand-side offset", ch);
+      if (u < nu && (w[5] & kUnitLast) && ((w[5] >> kUnitDoffShift) < 0 || (w[5] >> kUnitDoffShift) >= n))
+        return bad("forward result row", ch);
+      if (u >= nu && (w[5] & kUnitLast)) return bad("sentinel flags", ch);
+      if (w[6] < 0 || w[6] % 512 != 0 || w[6] + 512 > nu * 512) return bad("forward L offset", ch);
+      if (!slot_ok(w[7], F + 1)) return bad("forward store slot", ch);
+    }
+  }
+  for (int ch = 0; ch < S.n_chunks; ++ch) {
+    const int* m = &S.meta[S.meta_off[ch]];
+    const int ns = m[0], ncols = m[1], nrel = m[2], c0 = m[3], u0 = m[4];
+    if (m[6] != 0 || m[7] != 0) return bad("releaser units", ch);
+    if (ns != S.chunk_units[ch] || ns < 0 || ns > S.max_units) return bad("backward units", ch);
+    if (ncols != S.chunk_cols[ch] || ncols < 0 || ncols > S.max_cols || c0 < 0 || c0 + ncols > n)
+      return bad("backward columns", ch);
+    if (nrel < 0 || nrel > S.max_rel || u0 < 0 || u0 + nrel > n) return bad("releases", ch);
+    const int rel0 = kChunkHeader + (ns + 3 * kUnitSentinels) * kUnitWords;
+    if (S.meta_words[ch] < rel0 + 4 * nrel) return bad("backward meta size", ch);
+    const int dend = ns * 512 + ncols * 128, area = dend + ncols * 128;
+    for (int u = 0; u < ns + kUnitSentinels; ++u) {
+      const int* w = m + kChunkHeader + u * kUnitWords;
+      for (int s2 = 0; s2 < 4; ++s2)
+        if (!slot_ok(w[s2], F)) return bad("backward source slot", ch);
+      if (w[4] < 0 || w[4] % 128 != 0 || (u < ns && w[4] + 128 > area)) return bad("backward forward-result offset", ch);
+      const int doff = w[5] >> kUnitDoffShift;
+      if (doff < 0 || doff % 128 != 0 || doff + 128 > (u < ns ? dend : 128)) return bad("backward D^-1 offset", ch);
+      if (w[6] < 0 || w[6] % 512 != 0 || (u < ns && w[6] + 512 > ns * 512)) return bad("backward L offset", ch);
+      if (!slot_ok(w[7], F + 1)) return bad("backward store slot", ch);
+    }
+    for (int k = 0; k < nrel; ++k) {
+      const int* r = m + rel0 + 4 * k;
+      if (!slot_ok(r[0], F - 1) || r[3] < 0 || r[3] >= n) return bad("release record", ch);
+    }
+  }
+  return true;
+}
+
 }  // namespace
 
 bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const float* rho_by_constraint,
@@ -643,6 +702,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       return false;
     }
   if (t.frontier && !build_frontier_slots(n, t.frontier_lag, fwd_units, bwd_units, order, &S, why)) return false;
+  if (t.frontier && !check_frontier_tables(S, n, why)) return false;
   // factorization re-reads: the L entry every update reads, D^-1 of every step's column
   S.upd_pos.clear();
   S.step_doff.resize(hp.nnz_l);

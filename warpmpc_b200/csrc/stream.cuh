@@ -48,6 +48,12 @@ constexpr int kChunkHeader = 8;
 // Forward chunk meta block: [0] nunits [1..7] 0, units, sentinels.
 // Stage L area: units (512 B each), then D^-1 of the chunk's columns (128 B each).
 // Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
+// Frontier form (frontier_slots > 0): the work vector rows are slots (zero
+// slot frontier_slots, trash slot + 1); a forward header carries its rows
+// [r0, r1) in words 1-2 and its stage the rows' right-hand sides after the
+// units; a backward stage carries its columns' forward results after the
+// D^-1 rows; unit targets are stage offsets, forward flags carry the row and
+// release records the released index in word 3.
 
 struct StreamPlan {
   int n;              // KKT dimension
@@ -90,6 +96,9 @@ struct StreamPlan {
   const int* u_orig;        // [n] U index -> original KKT index
   int max_row_nnz;
   int max_lstages, max_sstages;  // ring depth limits (tuning; defaults 12 and 6)
+  // frontier form: slots (0: the plain form), the release lag the slots
+  // assume (the L ring may be no deeper), the longest forward chunk in rows
+  int frontier_slots, frontier_lag, max_frows;
 };
 
 // ---- PTX helpers -----------------------------------------------------------
@@ -265,6 +274,8 @@ struct StreamJobDesc {
   const float* fstream = nullptr;
   float4* state = nullptr;
   float* pres = nullptr;
+  float* rhs = nullptr;   // frontier form: [tile][n][lane] right-hand sides
+  float* fwd = nullptr;   // frontier form: [tile][n][lane] forward results
   int* iters = nullptr;
   int n_tiles = 0, max_iter = 0, batch = 0, check_every = 0;
   float chg_eps = 0.0f, sigma = 0.0f, alpha = 0.0f, one_minus_alpha = 0.0f;

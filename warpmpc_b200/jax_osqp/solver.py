@@ -122,6 +122,16 @@ class OSQPEngine:
         self.last_iters = None
         self.last_status = None
 
+    def stream_info(self) -> dict:
+        """The streaming schedule this problem carries: ``streaming`` (persistent
+        solves run the streaming kernel), ``frontier_slots`` (work-vector slots
+        of the frontier form; 0 for the plain form), ``n`` (KKT dimension) and
+        ``frontier_lag``."""
+        info = (ctypes.c_int32 * 4)()
+        native.check(native.lib().wmpc_osqp_stream_info(self.dev.handle, info))
+        return {"streaming": bool(info[0]), "frontier_slots": int(info[1]), "n": int(info[2]),
+                "frontier_lag": int(info[3])}
+
     # -- argument normalisation -------------------------------------------------
     def _mat(self, values, width, name):
         t = _as_f32(values, self.device, name)

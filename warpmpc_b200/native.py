@@ -224,6 +224,7 @@ SIGNATURES = {
     "wmpc_osqp_create": (ctypes.c_int, [ctypes.POINTER(OsqpDesc), ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "wmpc_osqp_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "wmpc_osqp_workspace_bytes": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "wmpc_osqp_stream_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "wmpc_osqp_factor": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
