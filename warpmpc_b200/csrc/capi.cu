@@ -224,6 +224,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   t.funits = funits;
   t.offload = offload & 3;
   t.frontier = (offload >> 2) & 1;  // bit 2: frontier-slot schedule
+  if (offload >> 8) t.frontier_lag = offload >> 8;  // bits 8+: its release lag
   if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
       !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
     return fail(WMPC_ERR_UNSUPPORTED, "%s", why.c_str());
@@ -584,6 +585,9 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
       sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
       sk.add(hs.chunk_u0.data(), hs.chunk_u0.size(), &sp.chunk_u0);
+      sk.add(hs.chunk_c0.data(), hs.chunk_c0.size(), &sp.chunk_c0);
+      sk.add(hs.frow0.data(), hs.frow0.size(), &sp.frow0);
+      sk.add(hs.frows.data(), hs.frows.size(), &sp.frows);
       sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
       sk.add(hs.chunk_pre_u0.data(), hs.chunk_pre_u0.size(), &sp.chunk_pre_u0);
       sk.add(hs.chunk_pre_units.data(), hs.chunk_pre_units.size(), &sp.chunk_pre_units);

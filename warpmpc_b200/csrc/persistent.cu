@@ -601,46 +601,86 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         const float* bt = J.bstream + (size_t)tile * sp.blen;
         const float* ft = J.fstream + (size_t)tile * sp.flen;
         const size_t soff = (size_t)tile * n * 32;
+        // An item's copies: meta block, L data (first-right-hand-side pass: only
+        // the releaser's forward units), frontier form: the rows' right-hand
+        // sides (forward) or the columns' forward results (backward) behind
+        // the L data; backward and first-rhs items also the state records.
+        struct Copies {
+          int moff, mwords, loff, nrel, u0;
+          uint32_t lbytes, pre_at, xrow, xbytes;
+        };
+        auto describe = [&](int kind, int ch) {
+          Copies d;
+          const bool fwd = kind == kItemFwd;
+          d.moff = __ldg((fwd ? sp.fmeta_off : sp.meta_off) + ch);
+          d.mwords = __ldg((fwd ? sp.fmeta_words : sp.meta_words) + ch);
+          d.loff = __ldg((fwd ? sp.fchunk_off : sp.chunk_off) + ch);
+          d.nrel = 0;
+          d.u0 = 0;
+          d.pre_at = 0;
+          d.xrow = 0;
+          d.xbytes = 0;
+          if (fwd) {
+            d.lbytes = (uint32_t)__ldg(sp.fchunk_units + ch) * 512u;
+            if constexpr (kFrontier) {
+              d.xrow = (uint32_t)__ldg(sp.frow0 + ch);
+              d.xbytes = (uint32_t)__ldg(sp.frows + ch) * 128u;
+            }
+          } else {
+            d.nrel = __ldg(sp.chunk_nrel + ch);
+            d.u0 = __ldg(sp.chunk_u0 + ch);
+            if (kind == kItemBwd) {
+              const uint32_t cols = (uint32_t)__ldg(sp.chunk_cols + ch);
+              d.lbytes = (uint32_t)__ldg(sp.chunk_units + ch) * 512u + cols * 128u;
+              if constexpr (kFrontier) {
+                d.xrow = (uint32_t)__ldg(sp.chunk_c0 + ch);
+                d.xbytes = cols * 128u;
+              }
+            } else {
+              d.pre_at = (uint32_t)__ldg(sp.chunk_pre_u0 + ch);
+              d.lbytes = (uint32_t)__ldg(sp.chunk_pre_units + ch) * 512u;
+            }
+          }
+          return d;
+        };
+        // the next item's descriptors are loaded while this item waits and
+        // issues (one table round trip per item would otherwise pace the ring)
+        Copies ahead{};
+        int ahead_kind = -1, ahead_ch = -1;
         auto produce = [&](int kind, int ch) -> bool {
           const bool fwd = kind == kItemFwd;
-          const int moff = __ldg((fwd ? sp.fmeta_off : sp.meta_off) + ch);
-          const int mwords = __ldg((fwd ? sp.fmeta_words : sp.meta_words) + ch);
-          const int loff = __ldg((fwd ? sp.fchunk_off : sp.chunk_off) + ch);
-          uint32_t lbytes = 0;
-          if (fwd) lbytes = (uint32_t)__ldg(sp.fchunk_units + ch) * 512u;
-          if (kind == kItemBwd) lbytes = (uint32_t)__ldg(sp.chunk_units + ch) * 512u + (uint32_t)__ldg(sp.chunk_cols + ch) * 128u;
+          const Copies d = (kind == ahead_kind && ch == ahead_ch) ? ahead : describe(kind, ch);
+          if (fwd) {
+            ahead_kind = ch + 1 < sp.n_fchunks ? kItemFwd : kItemBwd;
+            ahead_ch = ch + 1 < sp.n_fchunks ? ch + 1 : sp.n_chunks - 1;
+          } else {
+            ahead_kind = ch > 0 ? kind : kItemFwd;
+            ahead_ch = ch > 0 ? ch - 1 : 0;
+          }
+          ahead = describe(ahead_kind, ahead_ch);
           if (issued_l >= (uint32_t)a.lstages &&
               !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
             return false;
           unsigned char* st = lring + (size_t)lr.stage * lstage_bytes;
-          // first-right-hand-side pass: only the releaser's forward units need coefficients
-          uint32_t pre_at = 0;
-          if (kind == kItemRel) {
-            pre_at = (uint32_t)__ldg(sp.chunk_pre_u0 + ch);
-            lbytes = (uint32_t)__ldg(sp.chunk_pre_units + ch) * 512u;
-          }
-          // frontier form: the rows' right-hand sides (forward) or the columns'
-          // forward results (backward), placed behind the L data
-          uint32_t xbytes = 0;
           const float* xsrc = nullptr;
           if constexpr (kFrontier) {
+            // those blocks are final once every earlier item is released
+            // (forward) or swept (backward)
             if (fwd) {
               if (ch == 0 && !wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return false;
-              const int r0 = __ldg(sp.fmeta + moff + 1), r1 = __ldg(sp.fmeta + moff + 2);
-              xbytes = (uint32_t)(r1 - r0) * 128u;
-              xsrc = J.rhs + soff + (size_t)r0 * 32;
+              xsrc = J.rhs + soff + (size_t)d.xrow * 32;
             } else if (kind == kItemBwd) {
               if (ch == sp.n_chunks - 1 && !wait_counter_bounded(sweep_done, issued_l, abort_flag, kWaitLimitNs))
                 return false;
-              xbytes = (uint32_t)__ldg(sp.chunk_cols + ch) * 128u;
-              xsrc = J.fwd + soff + (size_t)__ldg(sp.meta + moff + 3) * 32;
+              xsrc = J.fwd + soff + (size_t)d.xrow * 32;
             }
           }
-          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)mwords * 4u + lbytes + xbytes);
-          bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + moff, (uint32_t)mwords * 4u, lfull + lr.stage);
-          if (lbytes)
-            bulk_g2s(st + a.meta_bytes + pre_at * 512u, (fwd ? ft : bt) + loff + pre_at * 128u, lbytes, lfull + lr.stage);
-          if (kFrontier && xbytes) bulk_g2s(st + a.meta_bytes + lbytes, xsrc, xbytes, lfull + lr.stage);
+          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)d.mwords * 4u + d.lbytes + d.xbytes);
+          bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + d.moff, (uint32_t)d.mwords * 4u, lfull + lr.stage);
+          if (d.lbytes)
+            bulk_g2s(st + a.meta_bytes + d.pre_at * 512u, (fwd ? ft : bt) + d.loff + d.pre_at * 128u, d.lbytes,
+                     lfull + lr.stage);
+          if (kFrontier && d.xbytes) bulk_g2s(st + a.meta_bytes + d.lbytes, xsrc, d.xbytes, lfull + lr.stage);
           lr.advance(a.lstages);
           ++issued_l;
           if (!fwd) {
@@ -648,10 +688,10 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            const uint32_t nrel = (uint32_t)__ldg(sp.chunk_nrel + ch);
+            const uint32_t nrel = (uint32_t)d.nrel;
             mbar_arrive_expect_tx(sfull + sr.stage, nrel * (kTrack ? 640u : 512u));
             if (nrel) {
-              const size_t u = soff + (size_t)__ldg(sp.chunk_u0 + ch) * 32;
+              const size_t u = soff + (size_t)d.u0 * 32;
               bulk_g2s(ss, J.state + u, nrel * 512u, sfull + sr.stage);
               if constexpr (kTrack) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
             }
@@ -703,8 +743,10 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
               run_units<true>(mu, lst, xb, tb, nullptr, lane, nu);         // backward substitution, column form
             }
           }
-          // the forward results written here are read back by bulk copies
-          if (kFrontier && kind == kItemFwd) fence_proxy_async_global();
+          // the forward results are read back by bulk copies of the backward
+          // sweep, issued once sweep_done covers the last forward chunk (one
+          // fence per sweep: a fence waits for this thread's stores)
+          if (kFrontier && kind == kItemFwd && ch == sp.n_fchunks - 1) fence_proxy_async_global();
           __syncwarp();
           if (lane == 0) {
             if (kind == kItemFwd) mbar_arrive(lempty + lr.stage);
@@ -793,7 +835,8 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
               const float4 st = S[k * 32];
               *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = st.x - __int_as_float(r.z) * st.y;
             }
-            if constexpr (kFrontier) fence_proxy_async_global();  // read back by bulk copies
+            // read back by bulk copies once rel_done covers the pass's last chunk
+            if (kFrontier && ch == 0) fence_proxy_async_global();
           } else {
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
@@ -1085,6 +1128,9 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   auto kernel = track ? admm_stream_kernel<true, false>
                       : (frontier ? admm_stream_kernel<false, true> : admm_stream_kernel<false, false>);
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+  // all of the SM's unified memory as shared memory, so that two CTAs fit
+  WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
   profile_mark_begin(s);
   kernel<<<grid, track ? 96 : 128, cfg.smem, s>>>(a);
   profile_mark_end(s);

@@ -351,6 +351,7 @@ bool check_frontier_tables(const HostStream& S, int n, std::string* why) {
     const int nu = m[0], r0 = m[1], r1 = m[2];
     if (nu != S.fchunk_units[ch] || nu < 1 || nu > S.max_funits) return bad("forward units", ch);
     if (r0 < 0 || r1 <= r0 || r1 > n || r1 - r0 > S.max_frows) return bad("forward rows", ch);
+    if (S.frow0[ch] != r0 || S.frows[ch] != r1 - r0) return bad("forward row table", ch);
     if (S.fmeta_words[ch] < kChunkHeader + (nu + kUnitSentinels) * kUnitWords) return bad("forward meta size", ch);
     const int area = nu * 512 + (r1 - r0) * 128;
     for (int u = 0; u < nu + kUnitSentinels; ++u) {
@@ -370,7 +371,8 @@ bool check_frontier_tables(const HostStream& S, int n, std::string* why) {
     const int ns = m[0], ncols = m[1], nrel = m[2], c0 = m[3], u0 = m[4];
     if (m[6] != 0 || m[7] != 0) return bad("releaser units", ch);
     if (ns != S.chunk_units[ch] || ns < 0 || ns > S.max_units) return bad("backward units", ch);
-    if (ncols != S.chunk_cols[ch] || ncols < 0 || ncols > S.max_cols || c0 < 0 || c0 + ncols > n)
+    if (ncols != S.chunk_cols[ch] || ncols < 0 || ncols > S.max_cols || c0 < 0 || c0 + ncols > n ||
+        S.chunk_c0[ch] != c0)
       return bad("backward columns", ch);
     if (nrel < 0 || nrel > S.max_rel || u0 < 0 || u0 + nrel > n) return bad("releases", ch);
     const int rel0 = kChunkHeader + (ns + 3 * kUnitSentinels) * kUnitWords;
@@ -482,6 +484,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   S.chunk_units.resize(S.n_chunks);
   S.chunk_cols.resize(S.n_chunks);
   S.chunk_u0.resize(S.n_chunks);
+  S.chunk_c0.resize(S.n_chunks);
   S.chunk_nrel.resize(S.n_chunks);
   S.meta_off.resize(S.n_chunks);
   S.meta_words.resize(S.n_chunks);
@@ -544,6 +547,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
     S.chunk_pre_units.push_back(np);
     S.chunk_units[ch] = nu;
     S.chunk_cols[ch] = c1 - c0;
+    S.chunk_c0[ch] = c0;
     S.chunk_u0[ch] = u0;
     S.chunk_nrel[ch] = nrel;
     S.max_units = std::max(S.max_units, nu);
@@ -682,6 +686,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       push_sentinels(zero_row, trash_row, &m);
       S.fchunk_off.push_back(foff);
       S.fchunk_units.push_back(nu);
+      S.frow0.push_back(r0);
+      S.frows.push_back(r1 - r0);
       S.fmeta_off.push_back(static_cast<int>(S.fmeta.size()));
       S.fmeta_words.push_back(static_cast<int>(m.size()));
       S.max_fmeta_words = std::max(S.max_fmeta_words, static_cast<int>(m.size()));

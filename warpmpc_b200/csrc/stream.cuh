@@ -99,6 +99,9 @@ struct StreamPlan {
   // frontier form: slots (0: the plain form), the release lag the slots
   // assume (the L ring may be no deeper), the longest forward chunk in rows
   int frontier_slots, frontier_lag, max_frows;
+  const int* chunk_c0;  // [n_chunks] first column of a backward chunk (its forward-result block)
+  const int* frow0;     // [n_fchunks] first row of a forward chunk (its right-hand-side block)
+  const int* frows;     // [n_fchunks] its rows
 };
 
 // ---- PTX helpers -----------------------------------------------------------
@@ -227,7 +230,7 @@ struct StreamTargets {
   int funits = 16;                      // forward chunks
   int offload = 0;                      // also give the releaser warp: 1 leaf columns, 2 pre rows (bits)
   int frontier = 0;                     // frontier slots (see build_frontier_slots); needs offload 0
-  int frontier_lag = 4;                 // chunks a release may trail the sweep (the L ring depth)
+  int frontier_lag = 4;                 // chunks a release may trail the sweep (bounds the L ring depth)
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.
@@ -245,6 +248,7 @@ struct HostStream {
   // + 1), the release lag the slot reservations assume, the longest forward
   // chunk in rows (its right-hand-side block in the stage)
   int frontier_slots = 0, frontier_lag = 0, max_frows = 0;
+  std::vector<int> chunk_c0, frow0, frows;  // first column of a backward chunk; first row, rows of a forward chunk
   // host copies used by the OSQP side to lay out the state
   std::vector<int> u_of_perm;  // permuted index -> U index
 };
