@@ -6,7 +6,8 @@ stages instead.  The CPU replay runs that form with every index bounds-checked
 and the releases of each backward chunk deferred by the schedule's lag (the
 most a release may trail the sweep): its iterates equal the oracle's bit for
 bit, cold and warm started, so no slot is reused while something still reads
-it.  The streaming kernel does not run this form yet.
+it.  The streaming kernel runs this form when a problem is created with
+WMPC_STREAM_FRONTIER=1 (GPU parity in test_gpu_frontier.py).
 """
 
 import os

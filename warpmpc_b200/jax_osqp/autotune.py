@@ -4,7 +4,8 @@ The streaming kernel's schedule has a few free choices that do not change
 any result bit (every candidate runs the same arithmetic in the same order):
 how many units, columns and releases a backward chunk holds, how many units a
 forward chunk holds, which leaf work moves to the releaser warps, the ring
-depths and the CTAs per SM.  Which choice is fastest depends on the pattern
+depths, the CTAs per SM and (as a candidate knob, not a default candidate)
+the frontier-slot form.  Which choice is fastest depends on the pattern
 and the device, so ``autotune_stream`` times a list of candidates on a
 representative batch and returns the fastest, checking on the way that every
 candidate's iterates equal the first one's.  Results are cached per pattern
@@ -34,6 +35,10 @@ KNOBS = {
     "lstages": "WMPC_STREAM_LSTAGES",
     "sstages": "WMPC_STREAM_SSTAGES",
     "ctas": "WMPC_STREAM_CTAS",
+    # the frontier-slot form: fixed-iteration solves only (a problem compiled
+    # with it refuses solves that check termination), so not a default candidate
+    "frontier": "WMPC_STREAM_FRONTIER",
+    "frontier_lag": "WMPC_STREAM_FRONTIER_LAG",
 }
 
 DEFAULT_CANDIDATES = (
