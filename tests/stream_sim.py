@@ -29,8 +29,9 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
     A frontier-slot schedule (``sched["frontier_slots"] > 0``) runs the form
     that schedule is built for: the work vector is a slot array, the
     right-hand sides live in a vector R read through each forward chunk's
-    stage, the forward results in a vector Y read through each backward
-    chunk's stage, and the releases of a backward chunk run ``lag`` chunks
+    stage, the forward results (left by the forward units over their rows'
+    right-hand sides in the stage, then copied out) in a vector Y read through
+    each backward chunk's stage, and the releases of a backward chunk run ``lag`` chunks
     after it (the most a release may trail the sweep; default the schedule's
     lag) -- so a slot freed too early shows up as a wrong result."""
     qp = plan.qdldl_plan
@@ -207,10 +208,9 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                     acc = acc - lv[3] * x3
                     res = acc
                 X[xrow(ctl[3])] = res
-                if fr and not backward and u < nu and fl & LAST:
-                    row = fl >> DSHIFT
-                    assert 0 <= row < n
-                    Y[row] = res  # the forward result, for the backward sweep's stage
+                if fr and not backward:  # every unit also stores over its row's right-hand side in the stage
+                    to = int(ctl[0])
+                    stage[to // 4 : to // 4 + 32] = res
                 prev = res
                 cur = nxt
 
@@ -232,6 +232,8 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 assert not np.isnan(R[r0:r1]).any(), "a right-hand side is read before its release"
                 stage = np.concatenate([stage, R[r0:r1].reshape(-1)])
             run_units(fm, nu, stage, backward=False)
+            if fr:  # the second releaser copies the block (now the rows' forward results) to Y
+                Y[r0:r1] = stage[nu * 128 : nu * 128 + (r1 - r0) * 32].reshape(r1 - r0, lanes)
             continue
         m = block(meta_all, sched["meta_off"], sched["meta_words"], ch, sched["max_meta_words"])
         ns, ncols, nrel, c0, u0, nprim, nl, npre = (int(v) for v in m[:8])

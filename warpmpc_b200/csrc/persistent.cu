@@ -359,10 +359,13 @@ __device__ __forceinline__ float select_flag(int flags, int mask, float a, float
 }
 
 // Forward unit: acc = (first ? rhs_i : acc) - L_i,c0 x_c0 - ... (ascending c)
-// kFrontier: a row's last unit also writes the row's result to yt (the
-// forward-result vector, this lane's column; the row is in the flags word)
+// kFrontier: every unit also stores acc over its row's right-hand side in the
+// stage (tb + target offset: read only by this row's units, and only by the
+// first), so after the chunk that block holds the rows' forward results.
+// Sentinels store to offset 0 (unit 0's coefficients, no longer read).
 template <bool kFrontier>
-__device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, float* yt, float& acc, float& prev) {
+__device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb, const unsigned char* tb, float& acc,
+                                             float& prev) {
   const int fl = r.ctl.y;
   const float x3 = select_flag(fl, kUnitFwd, prev, r.x3);
   acc = select_flag(fl, kUnitFirst, r.t, acc);
@@ -371,9 +374,7 @@ __device__ __forceinline__ void forward_unit(const UnitOps& r, unsigned char* xb
   acc = acc - r.l.z * r.x2;
   acc = acc - r.l.w * x3;
   *reinterpret_cast<float*>(xb + r.ctl.w) = acc;
-  if constexpr (kFrontier) {
-    if (fl & kUnitLast) yt[(fl >> kUnitDoffShift) * 32] = acc;
-  }
+  if constexpr (kFrontier) *reinterpret_cast<float*>(const_cast<unsigned char*>(tb) + r.ctl.x) = acc;
   prev = acc;
 }
 
@@ -399,7 +400,7 @@ __device__ __forceinline__ void backward_unit(const UnitOps& r, unsigned char* x
 // store to the trash row, and acc/prev are dead after the chunk).
 template <bool kBackward, bool kFrontier = false>
 __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const unsigned char* lst, unsigned char* xb,
-                                          const unsigned char* tb, float* yt, int lane, int nu) {
+                                          const unsigned char* tb, int lane, int nu) {
   static_assert(kUnitGroup == 3 && kUnitSentinels >= 4, "loop shape and sentinel count disagree");
   const unsigned char* lane_l = lst + lane * 16;
   UnitOps A, B, C;
@@ -410,13 +411,13 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
   for (int u = 0; u < nu; u += 3) {
     load_meta(mu, u + 2, C);
     load_data<kBackward>(lane_l, lst, xb, tb, lane, B);
-    if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit<kFrontier>(A, xb, yt, acc, prev);
+    if (kBackward) backward_unit(A, xb, acc, prev); else forward_unit<kFrontier>(A, xb, tb, acc, prev);
     load_meta(mu, u + 3, A);
     load_data<kBackward>(lane_l, lst, xb, tb, lane, C);
-    if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit<kFrontier>(B, xb, yt, acc, prev);
+    if (kBackward) backward_unit(B, xb, acc, prev); else forward_unit<kFrontier>(B, xb, tb, acc, prev);
     load_meta(mu, u + 4, B);
     load_data<kBackward>(lane_l, lst, xb, tb, lane, A);
-    if (kBackward) backward_unit(C, xb, acc, prev); else forward_unit<kFrontier>(C, xb, yt, acc, prev);
+    if (kBackward) backward_unit(C, xb, acc, prev); else forward_unit<kFrontier>(C, xb, tb, acc, prev);
   }
 }
 
@@ -542,12 +543,14 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // the sweeper); the first releaser frees the stages and publishes rel_done
 // once both halves are done.
 // kFrontier (fixed iterations only): X holds slots, not rows.  The releasers
-// write the right-hand sides to the per-tile vector rhs and the sweeper each
-// row's forward result to fwd; the producer copies a forward chunk's rows of
-// rhs, and a backward chunk's columns of fwd, into the stage behind its L
-// data, where the units read their targets.  Those copies wait for the writes:
-// a sweep's first forward chunk until every earlier item is released, its
-// first backward chunk until every earlier item is swept.
+// write the right-hand sides to the per-tile vector rhs; the producer copies a
+// forward chunk's rows of rhs, and a backward chunk's columns of fwd, into the
+// stage behind its L data, where the units read their targets.  The sweeper
+// leaves each row's forward result over its right-hand side in the stage, and
+// the second releaser copies that block to fwd and frees the forward stage
+// (y_done).  The copies into stages wait for the writes: a sweep's first
+// forward chunk until every earlier item is released, its first backward
+// chunk until every earlier forward block is in fwd.
 template <bool kTrack, bool kFrontier>
 __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
   static_assert(!(kTrack && kFrontier), "the frontier form runs fixed iterations");
@@ -567,6 +570,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
   unsigned* rel_done = sweep_done + 1;
   volatile unsigned* stop_at = rel_done + 1;  // item index where a converged tile's items end
   unsigned* rel_done1 = rel_done + 2;         // items the second releaser finished (kSplit)
+  unsigned* y_done = rel_done + 3;            // frontier form: forward items whose results are in fwd
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
@@ -582,6 +586,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
     *rel_done = 0;
     *stop_at = 0xffffffffu;
     *rel_done1 = 0;
+    *y_done = 0;
     fence_mbarrier_init();
   }
   __syncthreads();
@@ -670,7 +675,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
               if (ch == 0 && !wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return false;
               xsrc = J.rhs + soff + (size_t)d.xrow * 32;
             } else if (kind == kItemBwd) {
-              if (ch == sp.n_chunks - 1 && !wait_counter_bounded(sweep_done, issued_l, abort_flag, kWaitLimitNs))
+              if (ch == sp.n_chunks - 1 && !wait_counter_bounded(y_done, issued_l, abort_flag, kWaitLimitNs))
                 return false;
               xsrc = J.fwd + soff + (size_t)d.xrow * 32;
             }
@@ -719,11 +724,8 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
     unsigned char* xb = smem + lane * 4;  // this lane's column of the work vector
     bool ok = true;
     for (int g = blockIdx.x; g < total_tiles && ok; g += gridDim.x) {
-      const int c = job_of(a, g);
-      const StreamJob& J = a.job[c];
+      const StreamJob& J = a.job[job_of(a, g)];
       const StreamPlan& sp = J.sp;
-      float* yt = nullptr;  // frontier form: this lane's column of the tile's forward results
-      if constexpr (kFrontier) yt = J.fwd + (size_t)(g - (c ? a.tile_end[c - 1] : 0)) * sp.n * 32 + lane;
       auto sweep = [&](int kind, int ch) -> bool {
         if (kind != kItemRel) {
           // a forward sweep needs every right-hand side of the previous pass
@@ -738,18 +740,16 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           const unsigned char* tb = kFrontier ? lst + lane * 4 : xb;
           if (nu > 0) {
             if (kind == kItemFwd) {
-              run_units<false, kFrontier>(mu, lst, xb, tb, yt, lane, nu);  // forward substitution, row-gather form
+              run_units<false, kFrontier>(mu, lst, xb, tb, lane, nu);  // forward substitution, row-gather form
             } else {
-              run_units<true>(mu, lst, xb, tb, nullptr, lane, nu);         // backward substitution, column form
+              run_units<true>(mu, lst, xb, tb, lane, nu);              // backward substitution, column form
             }
           }
-          // the forward results are read back by bulk copies of the backward
-          // sweep, issued once sweep_done covers the last forward chunk (one
-          // fence per sweep: a fence waits for this thread's stores)
-          if (kFrontier && kind == kItemFwd && ch == sp.n_fchunks - 1) fence_proxy_async_global();
           __syncwarp();
           if (lane == 0) {
-            if (kind == kItemFwd) mbar_arrive(lempty + lr.stage);
+            // (frontier form: the second releaser frees a forward stage once it
+            // has copied the stage's forward results out)
+            if (!kFrontier && kind == kItemFwd) mbar_arrive(lempty + lr.stage);
             st_release_cta(sweep_done, t + 1);
           }
           __syncwarp();
@@ -783,7 +783,11 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       // this class's zero row (read by padding slots); every earlier tile is done with X
       if (rw == 0) X[(kFrontier ? sp.frontier_slots : n) * 32 + lane] = 0.0f;
       float* rt = nullptr;  // frontier form: this lane's column of the tile's right-hand sides
-      if constexpr (kFrontier) rt = J.rhs + (size_t)tile * n * 32 + lane;
+      float* yt = nullptr;  // and of its forward results
+      if constexpr (kFrontier) {
+        rt = J.rhs + (size_t)tile * n * 32 + lane;
+        yt = J.fwd + (size_t)tile * n * 32 + lane;
+      }
       float4* stt = J.state + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
       float pres = 0.0f;  // this lane's largest unscaled primal residual in the current iteration
@@ -791,6 +795,25 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       int iters_run = 0, frozen_at = 0;
       bool stop = false, frozen = false;
       auto release = [&](int kind, int ch) -> bool {
+        if (kFrontier && kind == kItemFwd && rw == 1) {
+          // frontier form: copy the forward results the sweeper left in the
+          // chunk's stage (rows [r0, r1) of its header) to fwd, then free it
+          if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, kWaitLimitNs)) return false;
+          const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
+          const int* meta = reinterpret_cast<const int*>(stage);
+          const int nu = meta[0], r0 = meta[1], rows = meta[2] - meta[1];
+          const float* yb = reinterpret_cast<const float*>(stage + a.meta_bytes + nu * 512) + lane;
+          float* yg = yt + (size_t)r0 * 32;
+          for (int r = 0; r < rows; ++r) yg[r * 32] = yb[r * 32];
+          // read back by the backward sweep's bulk copies once y_done covers the last chunk
+          if (ch == sp.n_fchunks - 1) fence_proxy_async_global();
+          __syncwarp();
+          if (lane == 0) {
+            mbar_arrive(lempty + lr.stage);
+            st_release_cta(y_done, t + 1);
+          }
+          __syncwarp();
+        }
         if (kind != kItemFwd) {
           if (kind == kItemBwd) {
             // the chunk's columns are solved (and its stage is full)
@@ -818,7 +841,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           share(0, nprim, pb, pe);
           share(nprim, nrel, cb, ce);
           // leaf columns (read by no other column): solved here, just before their release
-          if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, nullptr, lane, nl);
+          if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
@@ -850,7 +873,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           // forward rows whose entries all read leaf rows: their right-hand sides are now final
           if (!kFrontier && rw == 0 && np > 0) {
             __syncwarp();
-            run_units<false>(mu_pre, lst, xb, xb, nullptr, lane, np);
+            run_units<false>(mu_pre, lst, xb, xb, lane, np);
           }
           __syncwarp();
           if (rw == 1) {
