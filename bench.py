@@ -141,13 +141,15 @@ def algorithmic_bytes_per_instance(plan, max_iter):
     return factor + max_iter * iteration, factor, iteration
 
 
-def measured_traffic(args, batch):
+def measured_traffic(args, batch, form="plain"):
     """DRAM bytes of one persistent-kernel launch at this batch, scaled from the
     ncu capture summarised in profiles/ (traffic grows with the instance count:
-    every tile streams the same bytes); None when no capture covers the config."""
+    every tile streams the same bytes); None when no capture covers the config
+    and schedule form (plain or frontier) the launch ran."""
     import re
 
-    path = os.path.join(ROOT, "profiles", f"admm_stream_kernel_{args.config}.md")
+    name = f"admm_stream_kernel_{args.config}.md" if form == "plain" else f"admm_stream_kernel_{form}_{args.config}.md"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
             m = re.search(r"^traffic_bytes_per_instance:\s*(\d+)", f.read(), re.M)
@@ -587,6 +589,9 @@ def main():
                                                     mode="plain", device=dev)
     eng = comp.engine
     B = b.batch
+    # the schedule form a fixed-iteration solve of this batch runs (frontier: two CTAs per SM)
+    n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    form = "frontier" if eng.stream_info()["frontier_slots"] > 0 and (B + 31) // 32 > n_sms else "plain"
     to_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     P, A, Q, L, U = (to_dev(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u))
     f32 = dict(dtype=torch.float32, device=dev)
@@ -670,7 +675,7 @@ def main():
     achieved = algo_bytes / (dom_ms_per_launch * 1e-3) / 1e9
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-        "traffic": measured_traffic(args, B), "kernel": "admm_stream_kernel",
+        "traffic": measured_traffic(args, B, form), "kernel": "admm_stream_kernel", "schedule": form,
         "kernel_ms": dom_ms_per_launch, "bytes_per_launch": algo_bytes,
         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
     }

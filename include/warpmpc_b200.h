@@ -212,8 +212,13 @@ size_t wmpc_osqp_workspace_bytes(const wmpc_osqp* osqp, int32_t batch, int32_t m
 /* Which streaming schedule the problem carries (no reference counterpart: the
  * streaming kernel is this library's).  info[0]: 1 when persistent solves run
  * the streaming kernel's schedule, 0 when they fall back; info[1]: work-vector
- * slots of the frontier form (0: the plain form, one row per KKT index);
- * info[2]: the KKT dimension; info[3]: the frontier form's release lag. */
+ * slots of the frontier form that fixed-iteration solves of more 32-instance
+ * tiles than SMs run (0: the plain form, one row per KKT index); info[2]: the
+ * KKT dimension; info[3]: the frontier form's release lag.  The frontier form
+ * is built when the problem is created with WMPC_STREAM_FRONTIER=1 (the only
+ * schedule) or =2, the default (beside the plain one, used where it lets two
+ * CTAs share an SM and the plain form does not); =0 builds only the plain
+ * form. */
 int wmpc_osqp_stream_info(const wmpc_osqp* osqp, int32_t info[4]);
 
 enum { WMPC_OSQP_PLAIN = 0, WMPC_OSQP_PERSISTENT = 1 };

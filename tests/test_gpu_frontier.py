@@ -81,3 +81,34 @@ def test_frontier_form_refuses_termination_checks(cuda_device, monkeypatch):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
     with pytest.raises(Exception, match="fixed iterations"):
         comp.engine.solve(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), check_termination=5)
+
+
+def test_frontier_beside_plain_schedule(cuda_device, monkeypatch):
+    """WMPC_STREAM_FRONTIER=2 (the default) builds both schedules.  Fixed-iteration solves of
+    more tiles than SMs run the frontier form where it fits two CTAs per SM and
+    the plain form does not (the quadrotor pattern); checked solves run the
+    plain form.  Iterates bit-exact against the oracle, and the checked solve
+    equal to a plain-only problem's."""
+    import torch
+    from oracle.cpu_baseline import CpuOSQP
+
+    b = problems.make_batch(problems.QUADROTOR, 4801, seed=29)
+    plan = problems.make_plan(b)
+    monkeypatch.setenv("WMPC_STREAM_FRONTIER", "2")
+    both = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    assert both.engine.stream_info()["frontier_slots"] > 0
+    monkeypatch.setenv("WMPC_STREAM_FRONTIER", "0")
+    plain = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    assert plain.engine.stream_info()["frontier_slots"] == 0
+    got = _run(both, b)
+    ref = CpuOSQP(plan).solve(b.p_values, b.a_values, b.q, b.l, b.u)
+    for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
+        np.testing.assert_array_equal(g, r, err_msg=name)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    args = [t(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u)]
+    checked = both.engine.solve(*args, check_termination=5)
+    iters_both = both.engine.last_iters.cpu().numpy()
+    want = plain.engine.solve(*args, check_termination=5)
+    for g, w in zip(checked, want):
+        np.testing.assert_array_equal(g.cpu().numpy(), w.cpu().numpy())
+    np.testing.assert_array_equal(iters_both, plain.engine.last_iters.cpu().numpy())

@@ -148,6 +148,90 @@ struct Packer {
   }
 };
 
+
+// One streaming schedule of an OSQP problem: compact factor tables, chunk
+// schedule and launch check, uploaded in one block.  False (why set) when the
+// pattern cannot use the streaming kernel in this form.
+bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, const wmpc_osqp_desc* desc,
+                       const std::vector<float>& unscale, StreamPlan* out, void** block, std::string* why) {
+  HostStream hs;
+  std::vector<int> init_slot, upd_ptr;
+  std::vector<unsigned short> upd_slot16;
+  int max_row = 0;
+  if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, why) ||
+      !build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, desc->n, &hs, why, unscale.data()))
+    return false;
+  StreamPlan sp{};
+  sp.n = hp.n;
+  sp.nnz_l = hp.nnz_l;
+  sp.n_chunks = hs.n_chunks;
+  sp.blen = hs.blen;
+  sp.max_units = hs.max_units;
+  sp.max_cols = hs.max_cols;
+  sp.max_rel = hs.max_rel;
+  sp.max_meta_words = hs.max_meta_words;
+  sp.max_row_nnz = max_row;
+  sp.n_fchunks = hs.n_fchunks;
+  sp.flen = hs.flen;
+  sp.max_funits = hs.max_funits;
+  sp.max_fmeta_words = hs.max_fmeta_words;
+  sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
+  sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
+  sp.max_row_kv = hs.max_row_kv;
+  sp.frontier_slots = hs.frontier_slots;
+  sp.frontier_lag = hs.frontier_lag;
+  sp.max_frows = hs.max_frows;
+  sp.max_lstages = 12;
+  sp.max_sstages = 6;
+  if (const char* v = getenv("WMPC_STREAM_LSTAGES")) sp.max_lstages = atoi(v);
+  if (const char* v = getenv("WMPC_STREAM_SSTAGES")) sp.max_sstages = atoi(v);
+  StreamLaunch cfg;
+  if (!stream_launch_config(sp, &cfg)) {
+    *why = "work vector and ring do not fit in shared memory";
+    return false;
+  }
+  std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
+  Packer sk;
+  sk.add(hs.chunk_off.data(), hs.chunk_off.size(), &sp.chunk_off);
+  sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
+  sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
+  sk.add(hs.chunk_u0.data(), hs.chunk_u0.size(), &sp.chunk_u0);
+  sk.add(hs.chunk_c0.data(), hs.chunk_c0.size(), &sp.chunk_c0);
+  sk.add(hs.frow0.data(), hs.frow0.size(), &sp.frow0);
+  sk.add(hs.frows.data(), hs.frows.size(), &sp.frows);
+  sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
+  sk.add(hs.chunk_pre_u0.data(), hs.chunk_pre_u0.size(), &sp.chunk_pre_u0);
+  sk.add(hs.chunk_pre_units.data(), hs.chunk_pre_units.size(), &sp.chunk_pre_units);
+  sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
+  sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
+  sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);
+  sk.add(init_slot.data(), init_slot.size(), &sp.init_slot);
+  sk.add(upd_ptr.data(), upd_ptr.size(), &sp.upd_ptr);
+  sk.add(upd_slot.data(), upd_slot.size(), &sp.upd_slot);
+  sk.add(hs.col_uoff.data(), hs.col_uoff.size(), &sp.col_uoff);
+  sk.add(hs.dinv_off.data(), hs.dinv_off.size(), &sp.dinv_off);
+  sk.add(hs.proc_boff.data(), hs.proc_boff.size(), &sp.proc_boff);
+  sk.add(hs.proc_foff.data(), hs.proc_foff.size(), &sp.proc_foff);
+  sk.add(hs.upd_pos.data(), hs.upd_pos.size(), &sp.upd_pos);
+  sk.add(hs.step_doff.data(), hs.step_doff.size(), &sp.step_doff);
+  sk.add(hs.pad_boff.data(), hs.pad_boff.size(), &sp.pad_boff);
+  sk.add(hs.pad_foff.data(), hs.pad_foff.size(), &sp.pad_foff);
+  sk.add(hs.u_perm.data(), hs.u_perm.size(), &sp.u_perm);
+  sk.add(hs.u_orig.data(), hs.u_orig.size(), &sp.u_orig);
+  sk.add(hs.fchunk_off.data(), hs.fchunk_off.size(), &sp.fchunk_off);
+  sk.add(hs.fchunk_units.data(), hs.fchunk_units.size(), &sp.fchunk_units);
+  sk.add(hs.fmeta_off.data(), hs.fmeta_off.size(), &sp.fmeta_off);
+  sk.add(hs.fmeta_words.data(), hs.fmeta_words.size(), &sp.fmeta_words);
+  sk.add(hs.fmeta.data(), hs.fmeta.size(), &sp.fmeta);
+  int* sblock = nullptr;
+  if (sk.upload(&sblock) != WMPC_OK) {
+    *why = g_last_error;
+    return false;
+  }
+  *block = sblock;
+  *out = sp;
+  return true;
+}
 }  // namespace
 }  // namespace wmpc
 
@@ -521,10 +605,6 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     hp.lp = kkt_plan->h_lp;
     hp.li = kkt_plan->h_li;
     hp.p = kkt_plan->h_p;
-    HostStream hs;
-    std::vector<int> init_slot, upd_ptr;
-    std::vector<unsigned short> upd_slot16;
-    int max_row = 0;
     StreamTargets targets;
     if (const char* v = getenv("WMPC_STREAM_UNITS")) targets.units = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_COLS")) targets.cols = atoi(v);
@@ -532,93 +612,26 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (const char* v = getenv("WMPC_STREAM_FUNITS")) targets.funits = atoi(v);
     if (const char* v = getenv("WMPC_STREAM_OFFLOAD")) targets.offload = atoi(v) & 3;
     if (targets.units <= 0 || targets.cols <= 0 || targets.rel <= 0 || targets.funits <= 0) targets = StreamTargets();
-    // opt-in: the frontier-slot form (fixed-iteration solves only; no releaser offload)
-    if (const char* v = getenv("WMPC_STREAM_FRONTIER")) {
-      if (atoi(v) > 0) {
-        targets.frontier = 1;
-        targets.offload = 0;
-        if (const char* lag = getenv("WMPC_STREAM_FRONTIER_LAG")) targets.frontier_lag = atoi(lag);
-      }
-    }
+    // the frontier-slot form (fixed-iteration solves only; no releaser offload):
+    // 0 none, 1 the only schedule, 2 (default) a second schedule beside the plain one
+    int frontier_mode = 2;
+    if (const char* v = getenv("WMPC_STREAM_FRONTIER")) frontier_mode = atoi(v);
+    StreamTargets ftargets = targets;
+    ftargets.frontier = 1;
+    ftargets.offload = 0;
+    if (const char* lag = getenv("WMPC_STREAM_FRONTIER_LAG")) ftargets.frontier_lag = atoi(lag);
     // iterate-change unscale factors (original KKT order) for early termination
     std::vector<float> unscale(hp.n, 1.0f);
     for (int j = 0; j < n; ++j) unscale[j] = desc->scaling_d[j];
     for (int r = 0; r < m; ++r) unscale[n + r] = std::max(desc->scaling_einv[r], desc->y_unscale[r]);
-    bool ok = build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot16, &max_row, &q->stream_why) &&
-              build_stream_schedule(hp, targets, desc->rho_vec, desc->rho_inv_vec, n, &hs, &q->stream_why,
-                                    unscale.data());
-    StreamPlan& sp = q->sp;
-    if (ok) {
-      sp.n = hp.n;
-      sp.nnz_l = hp.nnz_l;
-      sp.n_chunks = hs.n_chunks;
-      sp.blen = hs.blen;
-      sp.max_units = hs.max_units;
-      sp.max_cols = hs.max_cols;
-      sp.max_rel = hs.max_rel;
-      sp.max_meta_words = hs.max_meta_words;
-      sp.max_row_nnz = max_row;
-      sp.n_fchunks = hs.n_fchunks;
-      sp.flen = hs.flen;
-      sp.max_funits = hs.max_funits;
-      sp.max_fmeta_words = hs.max_fmeta_words;
-      sp.n_pad_b = static_cast<int>(hs.pad_boff.size());
-      sp.n_pad_f = static_cast<int>(hs.pad_foff.size());
-      sp.max_row_kv = hs.max_row_kv;
-      sp.frontier_slots = hs.frontier_slots;
-      sp.frontier_lag = hs.frontier_lag;
-      sp.max_frows = hs.max_frows;
-      sp.max_lstages = 12;
-      sp.max_sstages = 6;
-      if (const char* v = getenv("WMPC_STREAM_LSTAGES")) sp.max_lstages = atoi(v);
-      if (const char* v = getenv("WMPC_STREAM_SSTAGES")) sp.max_sstages = atoi(v);
-      StreamLaunch cfg;
-      if (!stream_launch_config(sp, &cfg)) {
-        ok = false;
-        q->stream_why = "work vector and ring do not fit in shared memory";
-      }
-    }
-    if (ok) {
-      std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
-      Packer sk;
-      sk.add(hs.chunk_off.data(), hs.chunk_off.size(), &sp.chunk_off);
-      sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
-      sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);
-      sk.add(hs.chunk_u0.data(), hs.chunk_u0.size(), &sp.chunk_u0);
-      sk.add(hs.chunk_c0.data(), hs.chunk_c0.size(), &sp.chunk_c0);
-      sk.add(hs.frow0.data(), hs.frow0.size(), &sp.frow0);
-      sk.add(hs.frows.data(), hs.frows.size(), &sp.frows);
-      sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
-      sk.add(hs.chunk_pre_u0.data(), hs.chunk_pre_u0.size(), &sp.chunk_pre_u0);
-      sk.add(hs.chunk_pre_units.data(), hs.chunk_pre_units.size(), &sp.chunk_pre_units);
-      sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
-      sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
-      sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);
-      sk.add(init_slot.data(), init_slot.size(), &sp.init_slot);
-      sk.add(upd_ptr.data(), upd_ptr.size(), &sp.upd_ptr);
-      sk.add(upd_slot.data(), upd_slot.size(), &sp.upd_slot);
-      sk.add(hs.col_uoff.data(), hs.col_uoff.size(), &sp.col_uoff);
-      sk.add(hs.dinv_off.data(), hs.dinv_off.size(), &sp.dinv_off);
-      sk.add(hs.proc_boff.data(), hs.proc_boff.size(), &sp.proc_boff);
-      sk.add(hs.proc_foff.data(), hs.proc_foff.size(), &sp.proc_foff);
-      sk.add(hs.upd_pos.data(), hs.upd_pos.size(), &sp.upd_pos);
-      sk.add(hs.step_doff.data(), hs.step_doff.size(), &sp.step_doff);
-      sk.add(hs.pad_boff.data(), hs.pad_boff.size(), &sp.pad_boff);
-      sk.add(hs.pad_foff.data(), hs.pad_foff.size(), &sp.pad_foff);
-      sk.add(hs.u_perm.data(), hs.u_perm.size(), &sp.u_perm);
-      sk.add(hs.u_orig.data(), hs.u_orig.size(), &sp.u_orig);
-      sk.add(hs.fchunk_off.data(), hs.fchunk_off.size(), &sp.fchunk_off);
-      sk.add(hs.fchunk_units.data(), hs.fchunk_units.size(), &sp.fchunk_units);
-      sk.add(hs.fmeta_off.data(), hs.fmeta_off.size(), &sp.fmeta_off);
-      sk.add(hs.fmeta_words.data(), hs.fmeta_words.size(), &sp.fmeta_words);
-      sk.add(hs.fmeta.data(), hs.fmeta.size(), &sp.fmeta);
-      int* sblock = nullptr;
-      if (sk.upload(&sblock) == WMPC_OK) {
-        q->stream_block = sblock;
-        q->has_stream = true;
-      } else {
-        q->stream_why = g_last_error;
-      }
+    q->has_stream = build_stream_plan(hp, frontier_mode == 1 ? ftargets : targets, desc, unscale, &q->sp,
+                                      &q->stream_block, &q->stream_why);
+    if (q->has_stream && frontier_mode == 2) {
+      std::string why;
+      q->has_frontier = build_stream_plan(hp, ftargets, desc, unscale, &q->spf, &q->stream_block_f, &why);
+      // worth it where it lets two CTAs share an SM and the plain form does not
+      q->frontier_pays = q->has_frontier && stream_fits_two_ctas(q->spf, kkt_plan->device) &&
+                         !stream_fits_two_ctas(q->sp, kkt_plan->device);
     }
   }
   *out = q;
@@ -630,16 +643,19 @@ int wmpc_osqp_destroy(wmpc_osqp* osqp) {
   DeviceGuard guard(osqp->device);
   if (osqp->block) cudaFree(osqp->block);
   if (osqp->stream_block) cudaFree(osqp->stream_block);
+  if (osqp->stream_block_f) cudaFree(osqp->stream_block_f);
   delete osqp;
   return WMPC_OK;
 }
 
 int wmpc_osqp_stream_info(const wmpc_osqp* osqp, int32_t info[4]) {
   if (!osqp || !info) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  // (the schedule a fixed-iteration solve of more tiles than SMs runs)
+  const wmpc::StreamPlan& sp = osqp->frontier_pays ? osqp->spf : osqp->sp;
   info[0] = osqp->has_stream ? 1 : 0;
-  info[1] = osqp->has_stream ? osqp->sp.frontier_slots : 0;
-  info[2] = osqp->has_stream ? osqp->sp.n : 0;
-  info[3] = osqp->has_stream ? osqp->sp.frontier_lag : 0;
+  info[1] = osqp->has_stream ? sp.frontier_slots : 0;
+  info[2] = osqp->has_stream ? sp.n : 0;
+  info[3] = osqp->has_stream ? sp.frontier_lag : 0;
   return WMPC_OK;
 }
 

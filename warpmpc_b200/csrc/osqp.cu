@@ -474,7 +474,9 @@ Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int m
     L.x = c.take((size_t)o.n * batch);
     L.z = c.take((size_t)o.m * batch);
     L.y = c.take((size_t)o.m * batch);
-    L.stream_ws = c.take(stream_workspace_floats(q->sp, batch));
+    // (either schedule a launch may pick)
+    L.stream_ws = c.take(std::max(stream_workspace_floats(q->sp, batch),
+                                  q->has_frontier ? stream_workspace_floats(q->spf, batch) : (size_t)0));
     L.stream_status = reinterpret_cast<int*>(c.take((size_t)((batch + 31) / 32) * 32));
     L.error_word = reinterpret_cast<int*>(c.take(4));
     *total = c.used;
@@ -605,16 +607,25 @@ int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_ba
   return WMPC_OK;
 }
 
-// Streaming solve, first half: inputs staged, factor, state records; fills `job`.
+// The schedule a fixed-iteration solve of `tiles` instance tiles runs alone:
+// the frontier form where it lets two CTAs share an SM and the plain form does
+// not, and the batch has tiles for both.  Checked solves run the plain form.
+static bool frontier_for(const wmpc_osqp& q, bool check, int tiles) {
+  return q.frontier_pays && !check && tiles > q.num_sms;
+}
+
+// Streaming solve, first half: inputs staged, factor, state records; fills
+// `job` (frontier: with the problem's frontier-form schedule).
 int stream_solve_begin(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
-                       StreamJobDesc* job, cudaStream_t s) {
+                       bool frontier, StreamJobDesc* job, cudaStream_t s) {
   const Osqp& o = q.dev;
   const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
   const int check = opt.check_termination > 0 ? opt.check_termination : 0;
   int rc;
   if ((rc = stage_inputs(o, opt, d, L, s))) return rc;
   WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
-  if ((rc = stream_begin(q.kkt_plan->pat, q.sp, o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, L.x, L.z, L.y,
+  if ((rc = stream_begin(q.kkt_plan->pat, frontier ? q.spf : q.sp, o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0,
+                         L.x, L.z, L.y,
                          L.qs, L.ls, L.us, opt.warm_start != 0, check > 0, L.stream_ws, L.stream_status, B,
                          q.num_sms, opt.reuse_factor != 0, job, s)))
     return rc;
@@ -638,7 +649,7 @@ int stream_solve_end(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmp
   const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
   const int check = opt.check_termination > 0 ? opt.check_termination : 0;
   int rc;
-  if ((rc = stream_end(q.sp, o, job, L.x, L.z, L.y, s))) return rc;
+  if ((rc = stream_end(job.sp, o, job, L.x, L.z, L.y, s))) return rc;
   State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
   residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
       o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B,
@@ -672,7 +683,8 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   int rc;
   if (L.streaming) {
     StreamJobDesc job;
-    if ((rc = stream_solve_begin(q, opt, d, L, &job, s))) return rc;
+    const bool frontier = frontier_for(q, opt.check_termination > 0, (B + 31) / 32);
+    if ((rc = stream_solve_begin(q, opt, d, L, frontier, &job, s))) return rc;
     if ((rc = stream_run(&job, 1, L.error_word, q.num_sms, s))) return rc;
     return stream_solve_end(q, opt, d, L, job, L.error_word, s);
   }
@@ -769,6 +781,13 @@ int osqp_solve_multi(const wmpc_osqp* const* qs, const wmpc_osqp_options* opts, 
   std::vector<StreamJobDesc> jobs(n);
   std::vector<int> active;
   int rc;
+  // one schedule form per launch: the frontier form only when every class
+  // would pick it for the launch's tiles
+  bool frontier = true;
+  int tiles = 0;
+  for (int i = 0; i < n; ++i) tiles += ds[i].batch > 0 ? (ds[i].batch + 31) / 32 : 0;
+  for (int i = 0; i < n; ++i)
+    if (ds[i].batch > 0) frontier = frontier && frontier_for(*qs[i], opts[i].check_termination > 0, tiles);
   for (int i = 0; i < n; ++i) {
     const wmpc_osqp& q = *qs[i];
     const wmpc_osqp_batch& d = ds[i];
@@ -782,7 +801,7 @@ int osqp_solve_multi(const wmpc_osqp* const* qs, const wmpc_osqp_options* opts, 
                  static_cast<char*>(ws[i]), &need, &q, true);
     if (ws[i] == nullptr || ws_bytes[i] < need)
       return fail(WMPC_ERR_WORKSPACE, "class %d needs %zu workspace bytes, got %zu", i, need, ws_bytes[i]);
-    if ((rc = stream_solve_begin(q, opts[i], d, L[i], &jobs[i], s))) return rc;
+    if ((rc = stream_solve_begin(q, opts[i], d, L[i], frontier, &jobs[i], s))) return rc;
     active.push_back(i);
   }
   if (active.empty()) return WMPC_OK;

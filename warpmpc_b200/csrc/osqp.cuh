@@ -51,5 +51,10 @@ struct wmpc_osqp {
   bool has_stream = false;
   wmpc::StreamPlan sp{};
   void* stream_block = nullptr;
+  // optional second schedule in the frontier-slot form (fixed iterations only)
+  bool has_frontier = false;
+  bool frontier_pays = false;  // it fits two CTAs per SM where sp does not
+  wmpc::StreamPlan spf{};
+  void* stream_block_f = nullptr;
   std::string stream_why;  // why the streaming path is unavailable (diagnostics)
 };

@@ -995,6 +995,32 @@ bool ring_config(const RingSizes& r, StreamLaunch* cfg, size_t limit = (size_t)k
 // (sized with the residuals: a pattern that fits this fits every launch)
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring_config(ring_sizes(sp, true), cfg); }
 
+namespace {
+
+// The two-CTA ring of a launch on device `dev` (-1: the current device): 4-stage
+// L and 3-stage S rings at most, half the SM's shared memory each (false when
+// the device cannot be queried).
+bool two_cta_config(const RingSizes& r, StreamLaunch* cfg, int dev = -1) {
+  int sm_bytes = 0, reserved = 0;
+  if ((dev < 0 && cudaGetDevice(&dev) != cudaSuccess) ||
+      cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  RingSizes r2 = r;
+  r2.lmax = std::min(r2.lmax, 4);
+  r2.smax = std::min(r2.smax, 3);
+  return ring_config(r2, cfg, (size_t)(sm_bytes / 2 - reserved));
+}
+
+}  // namespace
+
+bool stream_fits_two_ctas(const StreamPlan& sp, int device) {
+  StreamLaunch cfg;
+  return two_cta_config(ring_sizes(sp, false), &cfg, device);
+}
+
 // streams, state records, residuals (+ frontier form: right-hand sides and forward results)
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
@@ -1094,23 +1120,11 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   // stream does): small patterns, enough tiles for both.
   int ctas_per_sm = 1;
   {
-    int dev = 0, sm_bytes = 0, reserved = 0;
     const char* env = getenv("WMPC_STREAM_CTAS");
-    const bool allow = !(env && atoi(env) == 1);
-    if (allow && cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess) {
-      RingSizes r2 = r;
-      r2.lmax = std::min(r2.lmax, 4);
-      r2.smax = std::min(r2.smax, 3);
-      StreamLaunch cfg2;
-      const size_t half = (size_t)(sm_bytes / 2 - reserved);
-      if (ring_config(r2, &cfg2, half) && total_tiles_of(jobs, n_jobs) > num_sms) {
-        cfg = cfg2;
-        ctas_per_sm = 2;
-      }
-    } else {
-      (void)cudaGetLastError();
+    StreamLaunch cfg2;
+    if (!(env && atoi(env) == 1) && total_tiles_of(jobs, n_jobs) > num_sms && two_cta_config(r, &cfg2)) {
+      cfg = cfg2;
+      ctas_per_sm = 2;
     }
   }
   StreamArgs a{};

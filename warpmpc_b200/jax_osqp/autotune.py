@@ -35,8 +35,9 @@ KNOBS = {
     "lstages": "WMPC_STREAM_LSTAGES",
     "sstages": "WMPC_STREAM_SSTAGES",
     "ctas": "WMPC_STREAM_CTAS",
-    # the frontier-slot form: fixed-iteration solves only (a problem compiled
-    # with it refuses solves that check termination), so not a default candidate
+    # the frontier-slot form: 0 none, 1 the only schedule (a problem compiled
+    # so refuses solves that check termination), 2 (the library default)
+    # beside the plain one where it lets two CTAs share an SM
     "frontier": "WMPC_STREAM_FRONTIER",
     "frontier_lag": "WMPC_STREAM_FRONTIER_LAG",
 }
