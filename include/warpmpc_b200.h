@@ -274,7 +274,9 @@ int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_op
  * holds only the values a sweep still reads, in slots; right-hand sides and
  * forward results travel through the stages (what the streaming kernel runs
  * when a problem is created with WMPC_STREAM_FRONTIER=1); bits 8 and up, when
- * nonzero, set its release lag in chunks (default 4).  With out == NULL, *out_words receives the
+ * nonzero, set its release lag in chunks (default 4); bit 3 (with bit 2)
+ * copies each row without entries from the stage into its slot at its
+ * chunk's start instead of sweeping it as a unit.  With out == NULL, *out_words receives the
  * buffer size; otherwise out (capacity out_capacity int32 words) receives,
  * in order:
  *   [n_chunks, blen, max_units, max_cols, max_rel, max_meta_words, max_row_nnz, n_meta]

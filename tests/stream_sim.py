@@ -231,7 +231,16 @@ def replay(plan, sched, p_values, a_values, q, l, u, x0=None, z0=None, y0=None, 
                 assert 0 <= r0 < r1 <= n and r1 - r0 <= sched["max_frows"]
                 assert not np.isnan(R[r0:r1]).any(), "a right-hand side is read before its release"
                 stage = np.concatenate([stage, R[r0:r1].reshape(-1)])
-            run_units(fm, nu, stage, backward=False)
+            if fr:  # rows without entries: copied from the stage into their slots before the units
+                ncopy = int(fm[3])
+                c0 = KHDR + (nu + NSENT) * KUW
+                assert c0 % 2 == 0 and c0 + 2 * ncopy <= fm.size
+                for k in range(ncopy):
+                    src, dst = int(fm[c0 + 2 * k]), int(fm[c0 + 2 * k + 1])
+                    assert src % 128 == 0 and nu * 512 <= src and src // 4 + 32 <= stage.size
+                    X[xrow(dst)] = stage[src // 4 : src // 4 + 32]
+            if nu:
+                run_units(fm, nu, stage, backward=False)
             if fr:  # the second releaser copies the block (now the rows' forward results) to Y
                 Y[r0:r1] = stage[nu * 128 : nu * 128 + (r1 - r0) * 32].reshape(r1 - r0, lanes)
             continue

@@ -76,3 +76,31 @@ def test_frontier_replay_detects_releases_later_than_the_schedule_allows():
     got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3, lag=8)
     ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=3)
     assert not all(np.array_equal(g, r) for g, r in zip(got, ref[:3]))
+
+
+FRONTIER_COPIES = (16, 16, 12, 16, 4 | 8)
+
+
+@pytest.mark.parametrize("cls,iters", [(problems.SMALL, 4), (problems.CARTPOLE, 3),
+                                       (problems.MPCClass("q5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"), 3)],
+                         ids=["small", "cartpole", "quadrotor_n5"])
+def test_frontier_copies_replay_bitexact(cls, iters):
+    """Rows without entries copied from the stage into their slots at their
+    chunk's start (no unit swept for them): same bits as the oracle, cold and
+    warm, with the releases deferred by the schedule's lag; the forward
+    sweep has fewer units and no more slots than with copy units."""
+    b = problems.make_batch(cls, 6, seed=37)
+    plan = problems.make_plan(b)
+    sched = stream_schedule(plan, targets=FRONTIER_COPIES)
+    base = stream_schedule(plan, targets=FRONTIER)
+    assert int(np.sum(sched["fchunk_units"])) < int(np.sum(base["fchunk_units"]))
+    assert sched["frontier_slots"] <= base["frontier_slots"] + 2
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters)
+    ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters)
+    for g, r in zip(got, ref[:3]):
+        np.testing.assert_array_equal(g, r)
+    x, z, y = ref[:3]
+    got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, x0=x, z0=z, y0=y, max_iter=iters)
+    ref = osqp_ref.solve_warm_start(plan, b.p_values, b.a_values, b.q, b.l, b.u, x, z, y, max_iter=iters)
+    for g, r in zip(got, ref[:3]):
+        np.testing.assert_array_equal(g, r)

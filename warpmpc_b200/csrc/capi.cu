@@ -308,6 +308,7 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
   t.funits = funits;
   t.offload = offload & 3;
   t.frontier = (offload >> 2) & 1;  // bit 2: frontier-slot schedule
+  t.frontier_copies = (offload >> 3) & 1;  // bit 3: with chunk-start copies of rows without entries
   if (offload >> 8) t.frontier_lag = offload >> 8;  // bits 8+: its release lag
   if (!build_factor_tables(hp, &init_slot, &upd_ptr, &upd_slot, &max_row, &why) ||
       !build_stream_schedule(hp, t, rho, rhoinv, n_primal, &hs, &why))
@@ -620,6 +621,7 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     ftargets.frontier = 1;
     ftargets.offload = 0;
     if (const char* lag = getenv("WMPC_STREAM_FRONTIER_LAG")) ftargets.frontier_lag = atoi(lag);
+    if (const char* v = getenv("WMPC_STREAM_FRONTIER_COPIES")) ftargets.frontier_copies = atoi(v) > 0 ? 1 : 0;
     // iterate-change unscale factors (original KKT order) for early termination
     std::vector<float> unscale(hp.n, 1.0f);
     for (int j = 0; j < n; ++j) unscale[j] = desc->scaling_d[j];

@@ -738,6 +738,15 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           const int4* mu = reinterpret_cast<const int4*>(meta + kChunkHeader);
           const int nu = meta[0];
           const unsigned char* tb = kFrontier ? lst + lane * 4 : xb;
+          if (kFrontier && kind == kItemFwd) {
+            // rows without entries: their right-hand side is their forward value
+            const int ncopy = meta[3];
+            const int2* cp = reinterpret_cast<const int2*>(meta + kChunkHeader + (nu + kUnitSentinels) * kUnitWords);
+            for (int k = 0; k < ncopy; ++k) {
+              const int2 e = cp[k];
+              *reinterpret_cast<float*>(xb + e.y) = *reinterpret_cast<const float*>(tb + e.x);
+            }
+          }
           if (nu > 0) {
             if (kind == kItemFwd) {
               run_units<false, kFrontier>(mu, lst, xb, tb, lane, nu);  // forward substitution, row-gather form

@@ -171,15 +171,18 @@ struct ChunkUnits {
   int nu;     // units (= meta words / kUnitWords before the sentinels)
   int rel_word0 = -1, u0 = 0, nrel = 0;  // backward: release records
   std::vector<UnitBuild> units;
+  std::vector<int> copies;  // forward: rows without entries copied into their slots at chunk start
+  int copy_word0 = -1;      // their (stage offset, slot offset) pairs in the meta vector
 };
 
 // Slots for the values of one sweep phase.  A value gets a slot when the unit
 // that finishes it stores it and keeps it through its last read; the slot is
-// reusable two units later (a unit's operands are loaded before the previous
-// unit stores).  Values nothing reads later go to the trash slot.  Returns the
-// slot of every value (-1: none) and the number of slots used.
+// reusable `gap` time steps later (two units: a unit's operands are loaded
+// before the previous unit stores).  Values nothing reads later go to the
+// trash slot.  Returns the slot of every value (-1: none) and the number of
+// slots used.
 std::vector<int> assign_slots(int n_values, const std::vector<int>& write_t, const std::vector<int>& free_after,
-                              int* n_slots) {
+                              int* n_slots, int gap = 2) {
   std::vector<int> by_time(n_values);
   std::iota(by_time.begin(), by_time.end(), 0);
   std::sort(by_time.begin(), by_time.end(), [&](int a, int b) { return write_t[a] < write_t[b]; });
@@ -202,7 +205,7 @@ std::vector<int> assign_slots(int n_values, const std::vector<int>& write_t, con
       free_slots.pop();
     }
     slot[v] = sl;
-    pending.push({free_after[v] + 2, sl});
+    pending.push({free_after[v] + gap, sl});
   }
   *n_slots = used;
   return slot;
@@ -222,21 +225,25 @@ std::vector<int> assign_slots(int n_values, const std::vector<int>& write_t, con
 bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, const std::vector<ChunkUnits>& bwd,
                           const std::vector<int>& order, HostStream* S, std::string* why) {
   const int zero_row = n;
-  // ---- forward phase: values y_i, written by the last unit of row i
+  // ---- forward phase: values y_i, written by the last unit of row i, or (a
+  // row without entries) copied from the stage before its chunk's first unit.
+  // Time: unit k at 2k + 2, a chunk's copies at 2k + 1 (k its first unit).
   std::vector<int> f_write(n, -1), f_read(n, -1);
   int tau = 0;
-  for (const ChunkUnits& c : fwd)
+  for (const ChunkUnits& c : fwd) {
+    for (int row : c.copies) f_write[row] = 2 * tau + 1;
     for (const UnitBuild& ub : c.units) {
       for (int s2 = 0; s2 < 4; ++s2)
-        if (ub.src[s2] != zero_row) f_read[ub.src[s2]] = std::max(f_read[ub.src[s2]], tau);
-      if ((ub.flags & kUnitLast) && ub.target != zero_row) f_write[ub.target] = tau;
+        if (ub.src[s2] != zero_row) f_read[ub.src[s2]] = std::max(f_read[ub.src[s2]], 2 * tau + 2);
+      if ((ub.flags & kUnitLast) && ub.target != zero_row) f_write[ub.target] = 2 * tau + 2;
       ++tau;
     }
+  }
   std::vector<int> f_free(n, -1);
   for (int v = 0; v < n; ++v)
     if (f_read[v] > f_write[v] && f_write[v] >= 0) f_free[v] = f_read[v];
   int f_slots = 0;
-  const std::vector<int> fslot = assign_slots(n, f_write, f_free, &f_slots);
+  const std::vector<int> fslot = assign_slots(n, f_write, f_free, &f_slots, 4);
   // ---- backward phase (chunks in sweep order: last chunk first): values x_j
   std::vector<int> b_write(n, -1), b_read(n, -1), chunk_end;
   tau = 0;
@@ -304,6 +311,11 @@ bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, co
       w[7] = (keep ? fslot[ub.target] : ts) * 128;
     }
     sentinel_words(S->fmeta, c.word0 + c.nu * kUnitWords);
+    for (size_t k = 0; k < c.copies.size(); ++k) {
+      const int row = c.copies[k];
+      S->fmeta[c.copy_word0 + 2 * k] = c.nu * 512 + (row - c.lo) * 128;
+      S->fmeta[c.copy_word0 + 2 * k + 1] = (fslot[row] >= 0 ? fslot[row] : ts) * 128;
+    }
   }
   // ---- rewrite the backward meta and release records
   for (const ChunkUnits& c : bwd) {
@@ -348,13 +360,19 @@ bool check_frontier_tables(const HostStream& S, int n, std::string* why) {
   auto slot_ok = [&](int w, int top) { return w >= 0 && w % 128 == 0 && w / 128 <= top; };
   for (int ch = 0; ch < S.n_fchunks; ++ch) {
     const int* m = &S.fmeta[S.fmeta_off[ch]];
-    const int nu = m[0], r0 = m[1], r1 = m[2];
-    if (nu != S.fchunk_units[ch] || nu < 1 || nu > S.max_funits) return bad("forward units", ch);
+    const int nu = m[0], r0 = m[1], r1 = m[2], ncopy = m[3];
+    if (nu != S.fchunk_units[ch] || nu < 0 || nu > S.max_funits || ncopy < 0 || nu + ncopy < 1)
+      return bad("forward units", ch);
     if (r0 < 0 || r1 <= r0 || r1 > n || r1 - r0 > S.max_frows) return bad("forward rows", ch);
     if (S.frow0[ch] != r0 || S.frows[ch] != r1 - r0) return bad("forward row table", ch);
-    if (S.fmeta_words[ch] < kChunkHeader + (nu + kUnitSentinels) * kUnitWords) return bad("forward meta size", ch);
+    const int copy0 = kChunkHeader + (nu + kUnitSentinels) * kUnitWords;
+    if (S.fmeta_words[ch] < copy0 + 2 * ncopy) return bad("forward meta size", ch);
     const int area = nu * 512 + (r1 - r0) * 128;
-    for (int u = 0; u < nu + kUnitSentinels; ++u) {
+    for (int k = 0; k < ncopy; ++k) {
+      const int src = m[copy0 + 2 * k], dst = m[copy0 + 2 * k + 1];
+      if (src < nu * 512 || src % 128 != 0 || src + 128 > area || !slot_ok(dst, F + 1)) return bad("forward copy", ch);
+    }
+    for (int u = 0; u < (nu > 0 ? nu + kUnitSentinels : 0); ++u) {
       const int* w = m + kChunkHeader + u * kUnitWords;
       for (int s2 = 0; s2 < 4; ++s2)
         if (!slot_ok(w[s2], F)) return bad("forward source slot", ch);
@@ -407,6 +425,10 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   S = HostStream();
   if (t.units <= 0 || t.cols <= 0 || t.rel <= 0 || t.funits <= 0) {
     *why = "bad stream targets";
+    return false;
+  }
+  if (t.frontier_copies && !t.frontier) {
+    *why = "frontier copies need the frontier form";
     return false;
   }
   if (t.frontier && (t.offload || t.frontier_lag < 1)) {
@@ -638,7 +660,8 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
   // ---- forward sweep (sweeper): rows in order (row-gather form), columns ascending in a row; pre rows excluded
   {
     // (frontier mode: a row without entries gets one no-op unit that carries
-    // its right-hand side into its forward value)
+    // its right-hand side into its forward value, or with frontier_copies a
+    // copy from the stage into its slot at chunk start, sized here as a unit)
     auto row_units = [&](int i) { return pre_row[i] ? 0 : t.frontier && rcount[i] == 0 ? 1 : (rcount[i] + 3) / 4; };
     std::vector<int> fb{0};
     {
@@ -659,19 +682,31 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       const int r0 = fb[k], r1 = fb[k + 1];
       std::vector<UnitBuild> units;
       std::vector<std::pair<int, int>> placed;
+      std::vector<int> copies;
       for (int i = r0; i < r1; ++i) {
         const std::vector<int>& re = row_entries[i];
         const int cnt = static_cast<int>(re.size());
         if ((cnt == 0 && !t.frontier) || pre_row[i]) continue;
+        if (cnt == 0 && t.frontier_copies) {
+          copies.push_back(i);
+          continue;
+        }
         std::vector<int> slot_of;
         std::vector<UnitBuild> add = cut_units(cnt, true, i, zero_row, [&](int q) { return col_of[re[q]]; }, &slot_of);
         const int first = append_units(&units, std::move(add), 3, zero_row, &S.dummy_units);
         for (int q = 0; q < cnt; ++q) placed.emplace_back(re[q], first * 4 + slot_of[q]);
       }
       const int nu = static_cast<int>(units.size());
-      if (nu == 0) continue;
+      const int ncopy = static_cast<int>(copies.size());
+      if (nu == 0 && ncopy == 0) continue;
       for (const auto& pe : placed) entry_foff[pe.first] = foff + (pe.second >> 2) * 128 + (pe.second & 3);
-      std::vector<int> m{nu, t.frontier ? r0 : 0, t.frontier ? r1 : 0, 0, 0, 0, 0, 0};
+      std::vector<int> m{nu, t.frontier ? r0 : 0, t.frontier ? r1 : 0, ncopy, 0, 0, 0, 0};
+      for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
+      push_sentinels(zero_row, trash_row, &m);
+      // frontier copies: (stage offset of the row's right-hand side, slot offset) pairs
+      const int copy_word0 = static_cast<int>(S.fmeta.size() + m.size());
+      for (int k = 0; k < 2 * ncopy; ++k) m.push_back(0);
+      while (m.size() % 4) m.push_back(0);
       if (t.frontier) {
         ChunkUnits cu;
         cu.word0 = static_cast<int>(S.fmeta.size()) + kChunkHeader;
@@ -679,11 +714,11 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
         cu.hi = r1;
         cu.nu = nu;
         cu.units = units;
+        cu.copies = copies;
+        cu.copy_word0 = copy_word0;
         fwd_units.push_back(std::move(cu));
         S.max_frows = std::max(S.max_frows, r1 - r0);
       }
-      for (int u = 0; u < nu; ++u) push_unit_meta(units[u], u, trash_row, &m);
-      push_sentinels(zero_row, trash_row, &m);
       S.fchunk_off.push_back(foff);
       S.fchunk_units.push_back(nu);
       S.frow0.push_back(r0);

@@ -50,8 +50,9 @@ constexpr int kChunkHeader = 8;
 // Work vector rows: 0..n-1 the KKT indices, n a zero row, n + 1 a trash row.
 // Frontier form (frontier_slots > 0): the work vector rows are slots (zero
 // slot frontier_slots, trash slot + 1); a forward header carries its rows
-// [r0, r1) in words 1-2 and its stage the rows' right-hand sides after the
-// units; a backward stage carries its columns' forward results after the
+// [r0, r1) in words 1-2 and in word 3 the number of (stage offset, slot
+// offset) copy pairs after the sentinels, and its stage the rows' right-hand
+// sides after the units; a backward stage carries its columns' forward results after the
 // D^-1 rows; unit targets are stage offsets, forward flags carry the row and
 // release records the released index in word 3.
 
@@ -231,6 +232,7 @@ struct StreamTargets {
   int offload = 0;                      // also give the releaser warp: 1 leaf columns, 2 pre rows (bits)
   int frontier = 0;                     // frontier slots (see build_frontier_slots); needs offload 0
   int frontier_lag = 4;                 // chunks a release may trail the sweep (bounds the L ring depth)
+  int frontier_copies = 0;              // frontier: rows without entries copied into slots, not swept as units
 };
 
 // Host result: every array of StreamPlan, to be uploaded by the plan.
