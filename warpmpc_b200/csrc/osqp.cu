@@ -609,9 +609,11 @@ int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_ba
 
 // The schedule a fixed-iteration solve of `tiles` instance tiles runs alone:
 // the frontier form where it lets two CTAs share an SM and the plain form does
-// not, and the batch has tiles for both.  Checked solves run the plain form.
+// not, and the batch has tiles for both (and one CTA per SM is not forced:
+// WMPC_STREAM_CTAS=1).  Checked solves run the plain form.
 static bool frontier_for(const wmpc_osqp& q, bool check, int tiles) {
-  return q.frontier_pays && !check && tiles > q.num_sms;
+  const char* ctas = getenv("WMPC_STREAM_CTAS");
+  return q.frontier_pays && !check && tiles > q.num_sms && !(ctas && atoi(ctas) == 1);
 }
 
 // Streaming solve, first half: inputs staged, factor, state records; fills
