@@ -631,9 +631,9 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     if (q->has_stream && frontier_mode == 2) {
       std::string why;
       q->has_frontier = build_stream_plan(hp, ftargets, desc, unscale, &q->spf, &q->stream_block_f, &why);
-      // worth it where it lets two CTAs share an SM and the plain form does not
-      q->frontier_pays = q->has_frontier && stream_fits_two_ctas(q->spf, kkt_plan->device) &&
-                         !stream_fits_two_ctas(q->sp, kkt_plan->device);
+      // worth it where it lets more CTAs share an SM than the plain form
+      q->frontier_pays = q->has_frontier &&
+                         stream_max_ctas(q->spf, kkt_plan->device) > stream_max_ctas(q->sp, kkt_plan->device);
     }
   }
   *out = q;

@@ -1006,10 +1006,10 @@ bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg) { return ring
 
 namespace {
 
-// The two-CTA ring of a launch on device `dev` (-1: the current device): 4-stage
-// L and 3-stage S rings at most, half the SM's shared memory each (false when
-// the device cannot be queried).
-bool two_cta_config(const RingSizes& r, StreamLaunch* cfg, int dev = -1) {
+// The ring of a launch with k CTAs per SM on device `dev` (-1: the current
+// device): 4-stage L and 3-stage S rings at most, 1/k of the SM's shared
+// memory each (false when the device cannot be queried).
+bool multi_cta_config(const RingSizes& r, int k, StreamLaunch* cfg, int dev = -1) {
   int sm_bytes = 0, reserved = 0;
   if ((dev < 0 && cudaGetDevice(&dev) != cudaSuccess) ||
       cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
@@ -1020,14 +1020,28 @@ bool two_cta_config(const RingSizes& r, StreamLaunch* cfg, int dev = -1) {
   RingSizes r2 = r;
   r2.lmax = std::min(r2.lmax, 4);
   r2.smax = std::min(r2.smax, 3);
-  return ring_config(r2, cfg, (size_t)(sm_bytes / 2 - reserved));
+  return ring_config(r2, cfg, (size_t)(sm_bytes / k - reserved));
+}
+
+// Most CTAs per SM a launch may use: 1 when WMPC_STREAM_CTAS=1, else
+// WMPC_STREAM_MAX_CTAS (2 to 4; default 2).
+int ctas_limit() {
+  const char* one = getenv("WMPC_STREAM_CTAS");
+  if (one && atoi(one) == 1) return 1;
+  const char* v = getenv("WMPC_STREAM_MAX_CTAS");
+  const int k = v ? atoi(v) : 2;
+  return k < 1 ? 1 : (k > 4 ? 4 : k);
 }
 
 }  // namespace
 
-bool stream_fits_two_ctas(const StreamPlan& sp, int device) {
-  StreamLaunch cfg;
-  return two_cta_config(ring_sizes(sp, false), &cfg, device);
+int stream_max_ctas(const StreamPlan& sp, int device) {
+  const RingSizes r = ring_sizes(sp, false);
+  for (int k = ctas_limit(); k >= 2; --k) {
+    StreamLaunch cfg;
+    if (multi_cta_config(r, k, &cfg, device)) return k;
+  }
+  return 1;
 }
 
 // streams, state records, residuals (+ frontier form: right-hand sides and forward results)
@@ -1124,16 +1138,19 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   std::sort(order, order + n_jobs, [&](int x, int y) { return cost[x] > cost[y]; });
   StreamLaunch cfg;
   if (!ring_config(r, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "these classes do not fit one launch's shared memory");
-  // Two CTAs (two sweepers) per SM when both fit with 4-stage L and 3-stage S
-  // rings (the ring depth does not limit the sweep; the sweeper's instruction
-  // stream does): small patterns, enough tiles for both.
+  // k CTAs (k sweepers) per SM when k fit with 4-stage L and 3-stage S rings
+  // (the ring depth does not limit the sweep; the sweeper's instruction stream
+  // does) and there are more tiles than k - 1 per SM: small patterns.
   int ctas_per_sm = 1;
   {
-    const char* env = getenv("WMPC_STREAM_CTAS");
-    StreamLaunch cfg2;
-    if (!(env && atoi(env) == 1) && total_tiles_of(jobs, n_jobs) > num_sms && two_cta_config(r, &cfg2)) {
-      cfg = cfg2;
-      ctas_per_sm = 2;
+    const int tiles = total_tiles_of(jobs, n_jobs);
+    for (int k = ctas_limit(); k >= 2; --k) {
+      StreamLaunch cfgk;
+      if (tiles > (k - 1) * num_sms && multi_cta_config(r, k, &cfgk)) {
+        cfg = cfgk;
+        ctas_per_sm = k;
+        break;
+      }
     }
   }
   StreamArgs a{};

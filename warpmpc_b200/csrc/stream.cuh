@@ -269,8 +269,9 @@ struct StreamLaunch {
   size_t smem;
 };
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
-// whether two CTAs of a fixed-iteration launch of this plan fit one SM of `device`
-bool stream_fits_two_ctas(const StreamPlan& sp, int device);
+// most CTAs of a fixed-iteration launch of this plan that fit one SM of `device`
+// (within the launch limit: 2 unless WMPC_STREAM_MAX_CTAS allows up to 4)
+int stream_max_ctas(const StreamPlan& sp, int device);
 size_t stream_workspace_floats(const StreamPlan& sp, int batch);
 
 // One class of a streaming launch (host view): its plan, stream buffers and
