@@ -214,14 +214,14 @@ std::vector<int> assign_slots(int n_values, const std::vector<int>& write_t, con
 // Frontier mode: rename the work-vector rows of every unit and release record
 // to slots, so the work vector holds only what a sweep still reads.  The
 // right-hand sides move to a per-tile vector R read through each forward
-// chunk's stage (block of rows [lo, hi) after its units); the forward results
-// to a vector Y read through each backward chunk's stage (block of columns
-// [lo, hi) after the D^-1 rows).  Unit words: sources and store become slot
-// offsets, the target becomes the byte offset of `t` in the stage's L area,
-// and a forward unit's flags carry its row (its Y entry) in place of the D^-1
-// offset; release records carry the released index's slot and, in place of
-// the unscale factor, the index (its R entry).  Sentinels and no-op units read
-// stage offset 0.
+// chunk's stage (block of rows [lo, hi) after its units, where the units also
+// leave the rows' forward results); the forward results to a vector Y read
+// through each backward chunk's stage (block of columns [lo, hi) after the
+// D^-1 rows).  Unit words: sources and store become slot offsets, the target
+// becomes the byte offset of `t` in the stage's L area (a forward unit has no
+// D^-1 offset: its flags word is the flags alone); release records carry the
+// released index's slot and, in place of the unscale factor, the index (its R
+// entry).  Sentinels and no-op units read stage offset 0.
 bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, const std::vector<ChunkUnits>& bwd,
                           const std::vector<int>& order, HostStream* S, std::string* why) {
   const int zero_row = n;
@@ -306,7 +306,7 @@ bool build_frontier_slots(int n, int lag, const std::vector<ChunkUnits>& fwd, co
       }
       const bool real = ub.target != zero_row;
       w[4] = real ? c.nu * 512 + (ub.target - c.lo) * 128 : 0;
-      w[5] = ub.flags | ((real ? ub.target : 0) << kUnitDoffShift);
+      w[5] = ub.flags;
       const bool keep = (ub.flags & kUnitLast) && real && fslot[ub.target] >= 0;
       w[7] = (keep ? fslot[ub.target] : ts) * 128;
     }
@@ -377,9 +377,7 @@ bool check_frontier_tables(const HostStream& S, int n, std::string* why) {
       for (int s2 = 0; s2 < 4; ++s2)
         if (!slot_ok(w[s2], F)) return bad("forward source slot", ch);
       if (w[4] < 0 || w[4] % 128 != 0 || w[4] + 128 > area) return bad("forward right-hand-side offset", ch);
-      if (u < nu && (w[5] & kUnitLast) && ((w[5] >> kUnitDoffShift) < 0 || (w[5] >> kUnitDoffShift) >= n))
-        return bad("forward result row", ch);
-      if (u >= nu && (w[5] & kUnitLast)) return bad("sentinel flags", ch);
+      if ((w[5] >> kUnitDoffShift) != 0 || (u >= nu && (w[5] & kUnitLast))) return bad("forward flags", ch);
       if (w[6] < 0 || w[6] % 512 != 0 || w[6] + 512 > nu * 512) return bad("forward L offset", ch);
       if (!slot_ok(w[7], F + 1)) return bad("forward store slot", ch);
     }

@@ -53,8 +53,8 @@ constexpr int kChunkHeader = 8;
 // [r0, r1) in words 1-2 and in word 3 the number of (stage offset, slot
 // offset) copy pairs after the sentinels, and its stage the rows' right-hand
 // sides after the units; a backward stage carries its columns' forward results after the
-// D^-1 rows; unit targets are stage offsets, forward flags carry the row and
-// release records the released index in word 3.
+// D^-1 rows; unit targets are stage offsets and release records carry the
+// released index in word 3.
 
 struct StreamPlan {
   int n;              // KKT dimension
