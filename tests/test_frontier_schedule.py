@@ -106,11 +106,13 @@ def test_frontier_copies_replay_bitexact(cls, iters):
         np.testing.assert_array_equal(g, r)
 
 
-@pytest.mark.parametrize("copies", [False, True], ids=["copy_units", "copy_lists"])
-def test_frontier_replay_random_patterns(copies):
+@pytest.mark.parametrize("bits", [0, 3, 4, 4 | 8], ids=["plain", "plain_offload", "frontier", "frontier_copies"])
+def test_schedule_replay_random_patterns(bits):
     """Random sparse QPs (box, equality, one-sided and free rows) under small
-    chunk targets, so that most rows sit near a chunk edge: the frontier
-    replay equals the oracle bit for bit on every pattern."""
+    chunk targets, so that most rows sit near a chunk edge: the replay of the
+    plain form (with and without releaser offload) and of the frontier form
+    (copy units or copy lists) equals the oracle bit for bit on every
+    pattern."""
     import scipy.sparse as sps
 
     from warpmpc_b200.jax_osqp import OSQPSettings
@@ -130,7 +132,7 @@ def test_frontier_replay_random_patterns(copies):
         u = np.where(kind == 2, 1e30, np.where(kind == 1, l, l + rng.uniform(0.1, 2.0, m)))
         u = np.where(kind == 3, 1e30, u)
         plan = build_osqp_plan(p, a, l, u, OSQPSettings(rho=0.1, sigma=1e-6, alpha=1.6, max_iter=4, rho_is_vec=True))
-        targets = (4, 4, 3, 4, 4 | (8 if copies else 0))
+        targets = (4, 4, 3, 4, bits)
         sched = stream_schedule(plan, targets=targets)
         B = 5
         f32 = np.float32
