@@ -20,9 +20,11 @@ reference's *own* ``_symperm_upper``/``_qdldl_etree``/``_build_numeric_program``
 so ``build_qdldl_plan``'s cross-checks pass.  The AMD permutation itself is
 therefore not pinned by this import (the qdldl package is absent).
 
-It reads the reference tree at import time, so it only works where the
-reference checkout exists (this development container); golden fixtures made
-with it are committed under ``tests/golden``.
+It reads the reference tree at import time, so it only works where a
+reference checkout exists and the environment variable
+``WARPMPC_REFERENCE_ROOT`` names it (there is no default location); golden
+fixtures made with it are committed under ``tests/golden``, and the live
+comparisons in the tests skip when the variable is unset.
 """
 
 from __future__ import annotations
@@ -34,7 +36,7 @@ import types
 import numpy as np
 import scipy.sparse as sp
 
-REFERENCE_ROOT = os.environ.get("WARPMPC_REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("WARPMPC_REFERENCE_ROOT", "")
 
 # Callable (upper_csc) -> permutation array.  Set before calling
 # build_qdldl_plan / build_osqp_plan through the reference.
@@ -44,7 +46,7 @@ _loaded = None
 
 
 def available() -> bool:
-    return os.path.isdir(os.path.join(REFERENCE_ROOT, "warpmpc"))
+    return bool(REFERENCE_ROOT) and os.path.isdir(os.path.join(REFERENCE_ROOT, "warpmpc"))
 
 
 def _identity_decorator(fn=None, *args, **kwargs):
@@ -116,7 +118,15 @@ def _install_stubs() -> None:
     # casadi: only named in annotations and stage-compilation code paths the
     # planners do not run (warpmpc/jax_sqp/casadi_stage.py)
     casadi = types.ModuleType("casadi")
-    casadi.__getattr__ = lambda name: type(name, (), {})
+
+    def _casadi_attr(name):
+        # module metadata (__file__, __spec__, ...) stays absent, so tools
+        # that walk sys.modules (inspect) are not handed a placeholder class
+        if name.startswith("__"):
+            raise AttributeError(name)
+        return type(name, (), {})
+
+    casadi.__getattr__ = _casadi_attr
     sys.modules.setdefault("casadi", casadi)
 
 

@@ -1,7 +1,8 @@
 """Generate the golden planner fixtures from the reference's own code.
 
-Run in a checkout that has the reference tree (default /root/reference, or
-WARPMPC_REFERENCE_ROOT):  python tests/golden/make_golden.py
+Run where the reference tree exists, naming it in WARPMPC_REFERENCE_ROOT
+(this script falls back to /root/reference, where the development container
+mounts it):  WARPMPC_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py
 
 The reference's NumPy/SciPy planners are imported through the oracle's
 placeholder-module shim (oracle/ref_import.py).  The AMD permutation comes
@@ -22,6 +23,7 @@ import scipy.sparse as sp
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+os.environ.setdefault("WARPMPC_REFERENCE_ROOT", "/root/reference")
 
 from oracle import ref_import  # noqa: E402
 from warpmpc_b200 import problems  # noqa: E402
@@ -144,6 +146,17 @@ def main():
         b = problems.make_batch(cls, 1, seed=7)
         _save_osqp(f"mpc_{cls.name}", ns, b.p_matrix0, b.a_matrix0, b.l[0].astype(float), b.u[0].astype(float),
                    dict(problems.DEFAULT_SETTINGS), q=b.q[0].astype(float))
+    # the plans the bench solves: the quadrotor class from the headline
+    # workload's instance 0 (seed 1000), and the two mixed-batch classes no
+    # other fixture covers (instance 0 of their seeds 4000 + k)
+    b = problems.make_batch(problems.QUADROTOR, 1, seed=1000)
+    _save_osqp("mpc_quadrotor", ns, b.p_matrix0, b.a_matrix0, b.l[0].astype(float), b.u[0].astype(float),
+               dict(problems.DEFAULT_SETTINGS), q=b.q[0].astype(float))
+    for k, cls in enumerate(problems.MIXED_CLASSES):
+        if cls.name in ("small-n40", "quad-n20"):
+            b = problems.make_batch(cls, 1, seed=4000 + k)
+            _save_osqp(f"mpc_{cls.name}", ns, b.p_matrix0, b.a_matrix0, b.l[0].astype(float), b.u[0].astype(float),
+                       dict(problems.DEFAULT_SETTINGS, max_iter=50), q=b.q[0].astype(float))
     _save_sqp("small", problems.SMALL)
     _save_sqp("quadrotor_n5", problems.MPCClass("quadrotor-n5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"))
     print("fixtures written to", HERE)
