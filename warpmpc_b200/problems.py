@@ -141,43 +141,133 @@ class MPCBatch:
         return int(self.q.shape[0])
 
 
-def make_batch(cls: MPCClass, batch: int, seed: int = 0, dtype=np.float32) -> MPCBatch:
-    """Seeded batch of ``batch`` instances of class ``cls``."""
+@dataclass
+class MPCParams:
+    """The per-instance draws a batch is made of: dynamics ``A`` (B, nx, nx),
+    ``B`` (B, nx, nu), cost diagonals ``qd`` (B, nx) and ``rd`` (B, nu), the
+    initial state ``x0`` (B, nx) and the state reference ``x_ref`` (B, nx).
+    Arrays are NumPy or torch (``qp_from_params`` is differentiable in torch)."""
+
+    cls: MPCClass
+    a: object
+    b: object
+    qd: object
+    rd: object
+    x0: object
+    x_ref: object
+
+
+def draw_params(cls: MPCClass, batch: int, seed: int = 0) -> MPCParams:
+    """The seeded float64 draws of ``make_batch(cls, batch, seed)``, in its order."""
     rng = np.random.default_rng(seed)
-    nx, nu, N = cls.nx, cls.nu, cls.horizon
     a, b = _draw_dynamics(cls, rng, batch)
-    qd = rng.uniform(1.0, 10.0, size=(batch, nx))
-    rd = rng.uniform(0.1, 1.0, size=(batch, nu))
-    x0 = rng.uniform(-cls.x0_max, cls.x0_max, size=(batch, nx))
-    x_ref = rng.uniform(-0.5, 0.5, size=(batch, nx))
-    sources = np.concatenate(
-        [qd, rd, a.reshape(batch, -1), b.reshape(batch, -1), -np.ones((batch, 1)), np.ones((batch, 1))], axis=1
-    )
+    qd = rng.uniform(1.0, 10.0, size=(batch, cls.nx))
+    rd = rng.uniform(0.1, 1.0, size=(batch, cls.nu))
+    x0 = rng.uniform(-cls.x0_max, cls.x0_max, size=(batch, cls.nx))
+    x_ref = rng.uniform(-0.5, 0.5, size=(batch, cls.nx))
+    return MPCParams(cls, a, b, qd, rd, x0, x_ref)
+
+
+def qp_from_params(params: MPCParams):
+    """(p_values, a_values, q, l, u) of the instances' QPs, computed with the
+    array module of ``params`` (NumPy float64, or torch so that gradients flow
+    back to the draws: diag Q enters P and q, diag R enters P, x0 enters the
+    first nx rows of l and u)."""
+    cls = params.cls
+    nx, nu, N = cls.nx, cls.nu, cls.horizon
+    is_torch = not isinstance(params.qd, np.ndarray)
+    if is_torch:
+        import torch
+
+        cat, tile = torch.cat, lambda t, reps: t.repeat(*reps)
+        ones = lambda rows, val: torch.full((rows, 1), val, dtype=params.qd.dtype, device=params.qd.device)  # noqa: E731
+        const = lambda arr: torch.as_tensor(arr, dtype=params.qd.dtype, device=params.qd.device)  # noqa: E731
+        idx = lambda arr: torch.as_tensor(arr, dtype=torch.long, device=params.qd.device)  # noqa: E731
+    else:
+        cat, tile = (lambda xs, dim: np.concatenate(xs, axis=dim)), np.tile
+        ones = lambda rows, val: np.full((rows, 1), val)  # noqa: E731
+        const = idx = lambda arr: arr  # noqa: E731
+    batch = params.qd.shape[0]
+    sources = cat([params.qd, params.rd, params.a.reshape(batch, -1), params.b.reshape(batch, -1), ones(batch, -1.0),
+                   ones(batch, 1.0)], 1)
     p_ids, a_ids = _pattern_with_ids(cls)
     p_upper = sp.triu(p_ids, format="csc")
     p_upper.sum_duplicates(); p_upper.sort_indices()
-    p_values = sources[:, np.asarray(p_upper.data, dtype=np.int64) - 1]
-    a_values = sources[:, np.asarray(a_ids.data, dtype=np.int64) - 1]
+    p_values = sources[:, idx(np.asarray(p_upper.data, dtype=np.int64) - 1)]
+    a_values = sources[:, idx(np.asarray(a_ids.data, dtype=np.int64) - 1)]
     nvar = (N + 1) * nx + N * nu
-    q = np.zeros((batch, nvar))
-    qx = -(qd * x_ref)
-    q[:, : (N + 1) * nx] = np.tile(qx, (1, N + 1))
     m = (N + 1) * nx + nvar
-    l = np.empty((batch, m))
-    u = np.empty((batch, m))
-    l[:, :nx] = -x0
-    u[:, :nx] = -x0
-    l[:, nx : (N + 1) * nx] = 0.0
-    u[:, nx : (N + 1) * nx] = 0.0
+    qx = -(params.qd * params.x_ref)
+    q = cat([tile(qx, (1, N + 1)), const(np.zeros((batch, N * nu)))], 1)
     box_lo = np.concatenate([np.full((N + 1) * nx, -cls.x_max), np.full(N * nu, -cls.u_max)])
-    l[:, (N + 1) * nx :] = box_lo[None, :]
-    u[:, (N + 1) * nx :] = -box_lo[None, :]
+    lo_rest = np.concatenate([np.zeros(N * nx), box_lo])
+    l = cat([-params.x0, const(np.broadcast_to(lo_rest, (batch, m - nx)).copy())], 1)
+    hi_rest = np.concatenate([np.zeros(N * nx), -box_lo])
+    u = cat([-params.x0, const(np.broadcast_to(hi_rest, (batch, m - nx)).copy())], 1)
+    return p_values, a_values, q, l, u
+
+
+class ClosedLoop:
+    """Advances a batch's MPC instances one step in closed loop: every
+    instance applies its first planned input, x0 <- A x0 + B u0 with its own
+    (A, B), clipped inside the state box, and the new x0 is written into the
+    first nx rows of l and u (l = u = -x0), so the next solve is a new QP.
+
+    ``advance`` works on device tensors with torch operations (no host
+    synchronisation: it can sit inside a captured CUDA graph);
+    ``advance_host`` does the same on NumPy/host arrays."""
+
+    def __init__(self, cls: MPCClass, params: MPCParams, device=None):
+        self.cls = cls
+        self.ui = (cls.horizon + 1) * cls.nx
+        self.a_np = np.asarray(params.a, dtype=np.float32)
+        self.b_np = np.asarray(params.b, dtype=np.float32)
+        self.x0_np = np.asarray(params.x0, dtype=np.float32).copy()
+        self.bound = np.float32(0.999 * cls.x_max)
+        if device is not None:
+            import torch
+
+            self.a = torch.from_numpy(self.a_np).to(device)
+            self.b = torch.from_numpy(self.b_np).to(device)
+            self.x0 = torch.from_numpy(self.x0_np).to(device)
+
+    def advance(self, x, l, u):
+        """x: (B, n) solution on the device; l, u: (B, m) device tensors updated in place."""
+        import torch
+
+        nx, nu = self.cls.nx, self.cls.nu
+        u0 = x[:, self.ui : self.ui + nu]
+        nxt = torch.bmm(self.a, self.x0[:, :, None])[:, :, 0] + torch.bmm(self.b, u0[:, :, None])[:, :, 0]
+        self.x0.copy_(nxt.clamp_(-float(self.bound), float(self.bound)))
+        l[:, :nx] = -self.x0
+        u[:, :nx] = -self.x0
+
+    def advance_host(self, x, l, u):
+        """NumPy (or host tensor) version of ``advance``."""
+        nx, nu = self.cls.nx, self.cls.nu
+        x = np.asarray(x)
+        u0 = x[:, self.ui : self.ui + nu]
+        nxt = np.einsum("bij,bj->bi", self.a_np, self.x0_np) + np.einsum("bij,bj->bi", self.b_np, u0)
+        self.x0_np[:] = np.clip(nxt, -self.bound, self.bound)
+        l = np.asarray(l)
+        u = np.asarray(u)
+        l[:, :nx] = -self.x0_np
+        u[:, :nx] = -self.x0_np
+
+
+def make_batch(cls: MPCClass, batch: int, seed: int = 0, dtype=np.float32) -> MPCBatch:
+    """Seeded batch of ``batch`` instances of class ``cls``."""
+    params = draw_params(cls, batch, seed)
+    p_values, a_values, q, l, u = qp_from_params(params)
+    p_ids, a_ids = _pattern_with_ids(cls)
+    p_upper = sp.triu(p_ids, format="csc")
+    p_upper.sum_duplicates(); p_upper.sort_indices()
     p0 = sp.csc_matrix((p_values[0], p_upper.indices, p_upper.indptr), shape=p_upper.shape)
     a0 = sp.csc_matrix((a_values[0], a_ids.indices, a_ids.indptr), shape=a_ids.shape)
     return MPCBatch(
         cls=cls, p_matrix0=p0, a_matrix0=a0,
         p_values=p_values.astype(dtype), a_values=a_values.astype(dtype),
-        q=q.astype(dtype), l=l.astype(dtype), u=u.astype(dtype), x0=x0.astype(dtype),
+        q=q.astype(dtype), l=l.astype(dtype), u=u.astype(dtype), x0=params.x0.astype(dtype),
     )
 
 
