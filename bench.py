@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--no-line-search", action="store_true", help="skip the SQP line-search step timing")
     ap.add_argument("--no-assembly", action="store_true", help="skip the SQP QP assembly timing")
     ap.add_argument("--no-sqp", action="store_true", help="skip the SQP step timing")
+    ap.add_argument("--no-sqp4", action="store_true", help="skip the nonlinear quadrotor SQP timing")
+    ap.add_argument("--sqp4-batch", type=int, default=262144, help="instances of the nonlinear SQP leg")
     return ap.parse_args()
 
 
@@ -131,9 +133,10 @@ class ClockSampler:
 def algorithmic_bytes_per_instance(plan, max_iter):
     """Roofline bytes of one persistent solve of one instance (float32).
 
-    factor: KKT values read + L, D, D^-1 written; each ADMM iteration: L read
-    twice (forward and backward sweep) + D^-1 read.  Index tables are shared
-    by all instances and amortised to zero.
+    factor (factor_stream_kernel): KKT values read + L, D, D^-1 written; each
+    ADMM iteration (admm_stream_kernel): L read twice (forward and backward
+    sweep) + D^-1 read.  Index tables are shared by all instances and
+    amortised to zero.  Returns (whole solve, factor, one iteration).
     """
     qp = plan.qdldl_plan
     factor = 4 * (plan.nnz_kkt + qp.nnz_l + 2 * qp.n)
@@ -141,14 +144,14 @@ def algorithmic_bytes_per_instance(plan, max_iter):
     return factor + max_iter * iteration, factor, iteration
 
 
-def measured_traffic(args, batch, form="plain"):
-    """DRAM bytes of one persistent-kernel launch at this batch, scaled from the
-    ncu capture summarised in profiles/ (traffic grows with the instance count:
+def measured_traffic(args, batch, form="plain", kernel="admm_stream_kernel"):
+    """DRAM bytes of one launch of `kernel` at this batch, scaled from the ncu
+    capture summarised in profiles/ (traffic grows with the instance count:
     every tile streams the same bytes); None when no capture covers the config
     and schedule form (plain or frontier) the launch ran."""
     import re
 
-    name = f"admm_stream_kernel_{args.config}.md" if form == "plain" else f"admm_stream_kernel_{form}_{args.config}.md"
+    name = f"{kernel}_{args.config}.md" if form == "plain" else f"{kernel}_{form}_{args.config}.md"
     path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
@@ -193,9 +196,11 @@ def barrier(world):
         multirank.barrier(_env(world))
 
 
-def cpu_baseline(plan, batch_np, args, cores=None):
-    """Oracle C restatement on the host cores: warm-started step on a bounded sample."""
+def cpu_baseline(plan, batch_np, args, cls, seed, cores=None):
+    """Oracle C restatement on the host cores: one closed-loop warm-started
+    step on a bounded sample (cold solve, state advanced by u0, timed warm solve)."""
     from oracle.cpu_baseline import CpuOSQP
+    from warpmpc_b200 import problems
 
     cpu = CpuOSQP(plan)
     cores = cores or os.cpu_count() or 1
@@ -208,9 +213,14 @@ def cpu_baseline(plan, batch_np, args, cores=None):
     per = (time.perf_counter() - t0) / probe
     sample = int(min(b.batch, max(probe, args.cpu_seconds / 2 / max(per, 1e-9))))
     sl = slice(0, sample)
-    x, z, y, *_ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], b.l[sl], b.u[sl], threads=cores)
+    params = problems.draw_params(cls, b.batch, seed)
+    loop = problems.ClosedLoop(cls, problems.MPCParams(cls, *[getattr(params, k)[sl] for k in
+                                                            ("a", "b", "qd", "rd", "x0", "x_ref")]))
+    lo, hi = b.l[sl].copy(), b.u[sl].copy()
+    x, z, y, *_ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], lo, hi, threads=cores)
+    loop.advance_host(x, lo, hi)
     t0 = time.perf_counter()
-    _, _, _, prim, dual, _ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], b.l[sl], b.u[sl], warm=(x, z, y),
+    _, _, _, prim, dual, _ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], lo, hi, warm=(x, z, y),
                                        threads=cores)
     dt = time.perf_counter() - t0
     ok = float(np.mean((prim <= RES_TOL) & (dual <= RES_TOL)))
@@ -219,7 +229,7 @@ def cpu_baseline(plan, batch_np, args, cores=None):
         "unit": "solves/s",
         "cores": cpu.threads_used,
         "kind": "port",
-        "sample": f"{sample} instances of the same workload, one warm-started step (second of two), "
+        "sample": f"{sample} instances of the same workload, one closed-loop warm-started step (second of two), "
                   f"{plan.settings.max_iter} ADMM iterations, C restatement (oracle/c/osqp_cpu.c), "
                   f"{cpu.threads_used} threads; {ok:.3f} of the sample at res<=1e-3",
         "seconds": dt,
@@ -249,12 +259,17 @@ def run_reference(args):
     budget = 150.0 / max(1, args.steps + args.warmup)  # whole run within a few minutes
     sample = int(min(b.batch, max(probe, budget / max(per, 1e-9))))
     sl = slice(0, sample)
+    params = problems.draw_params(cls, args.batch, 1000)
+    loop = problems.ClosedLoop(cls, problems.MPCParams(cls, *[getattr(params, k)[sl] for k in
+                                                            ("a", "b", "qd", "rd", "x0", "x_ref")]))
+    lo, hi = b.l[sl].copy(), b.u[sl].copy()
     warm = None
     times, fracs = [], []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        x, z, y, prim, dual, _ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], b.l[sl], b.u[sl], warm=warm,
+        x, z, y, prim, dual, _ = cpu.solve(b.p_values[sl], b.a_values[sl], b.q[sl], lo, hi, warm=warm,
                                            threads=cores)
+        loop.advance_host(x, lo, hi)  # the instances' next states: the next step is a new QP
         dt = time.perf_counter() - t0
         warm = (x, z, y)
         if step >= args.warmup:
@@ -491,14 +506,80 @@ def sqp_timing(args, dev, world):
     }
 
 
+def nonlinear_sqp_timing(args, dev, world):
+    """Nonlinear SQP: the rigid-body quadrotor (12 states, 4 motor thrusts,
+    RK4 dt = 0.02, N = 40) over args.sqp4_batch instances per GPU, 5 SQP
+    iterations with the filter line search, 25 ADMM iterations per QP (warm
+    started from the previous QP), the whole solve replayed from a CUDA
+    graph; then the same solve followed by the gradient of ||u0 - u_target||^2
+    with respect to x0 and the cost weights through the last QP (adjoint on
+    the kept factorization), also graphed.  Reports instance-solves/s, the
+    residual of the dynamics after the iterations and (forward + adjoint) /
+    forward."""
+    import torch
+
+    from warpmpc_b200 import multirank, quadrotor_sqp as qs
+
+    B, horizon = args.sqp4_batch, 40
+    data = qs.make_data(B, seed=multirank.instance_seed(7000, multirank.rank_env().rank))
+    w = qs.QuadrotorSQP(horizon, data, dev, iterations=5, max_iter=25)
+    u_target = torch.full((B, qs.NU), qs.U_HOVER, device=dev)
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        w.solve()
+        zf, rf = w.solve(keep_factor=True)
+        w.gradient(zf, rf, u_target)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    torch.cuda.synchronize()
+    g_fwd, g_fb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g_fwd):
+        z_out, _ = w.solve()
+    with torch.cuda.graph(g_fb, pool=g_fwd.pool()):
+        z_fb, r_fb = w.solve(keep_factor=True)
+        grads = w.gradient(z_fb, r_fb, u_target)
+
+    def timed(graph, reps):
+        graph.replay()
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / reps, world)
+
+    reps = max(1, min(args.steps, 3))
+    fwd_ms = timed(g_fwd, reps)
+    fb_ms = timed(g_fb, reps)
+    c, gv, lo, up = w.sqp.evaluate_nlp(z_out, w.x0)
+    viol = (torch.clamp(lo - gv, min=0) + torch.clamp(gv - up, min=0)).abs().amax(dim=1)
+    finite = bool(torch.isfinite(grads[0]).all() and torch.isfinite(grads[1]).all() and torch.isfinite(grads[2]).all())
+    del g_fwd, g_fb
+    return {
+        "workload": f"nonlinear quadrotor MPC (12 states, 4 thrusts, RK4 dt=0.02) N={horizon}, {B} instances/GPU, "
+                    "5 SQP iterations x 25 ADMM iterations, filter line search, one CUDA graph",
+        "ms_per_solve": fwd_ms, "instance_solves_per_s": B / (fwd_ms * 1e-3),
+        "kkt_dim": int(w.plan.osqp_plan.qdldl_plan.n), "nnz_l": int(w.plan.osqp_plan.qdldl_plan.nnz_l),
+        "max_violation_median": float(viol.median()), "frac_violation_le_1e-3": float((viol <= 1e-3).float().mean()),
+        "fwd_adjoint_ms": fb_ms, "fwd_bwd_over_fwd": fb_ms / fwd_ms, "gradients_finite": finite,
+        "gradient_wrt": "x0 (12), Q diagonal (12), R diagonal (4)",
+    }
+
+
 def mixed_timing(args, dev, world):
     """Mixed-size batch: args.mixed_batch instances spread over four linear MPC
     classes (nx, nu, N) = (4, 2, 10), (4, 2, 40), (12, 4, 20), (12, 4, 30),
     one multi-class persistent launch per step (wmpc_osqp_solve_persistent),
     at most 50 ADMM iterations with early exit (an instance stops once its
-    iterate stops changing by more than 1e-3; SOLVED from exact residuals),
-    warm-started closed loop.  Also times the same launch with a fixed 50
-    iterations.  Value: instances at primal/dual residual <= 1e-3 per second."""
+    primal residual and iterate change are at most 1e-3; SOLVED from exact
+    residuals), in a closed MPC loop (every step each instance applies its u0
+    and the next QP starts from its new state, warm-started from the previous
+    solution), the whole step replayed from a CUDA graph.  Also times the same
+    loop with a fixed 50 iterations.  Value: instances at primal/dual residual
+    <= 1e-3 per second."""
     import torch
 
     from warpmpc_b200 import multirank, problems
@@ -507,33 +588,64 @@ def mixed_timing(args, dev, world):
     classes = problems.MIXED_CLASSES
     per = max(1, args.mixed_batch // len(classes))
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    items = []
+    engines, data = [], []
     for k, cls in enumerate(classes):
         settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 50})
         plan = problems.make_plan(problems.make_batch(cls, 1, seed=4000 + k), settings)
-        b = problems.make_batch(cls, per, seed=multirank.instance_seed(4000 + 10 * k, multirank.rank_env().rank))
+        seed = multirank.instance_seed(4000 + 10 * k, multirank.rank_env().rank)
+        b = problems.make_batch(cls, per, seed=seed)
         comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
-        items.append([comp.engine, t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), None])
-
-    def step(check):
-        outs = solve_classes([tuple(it) for it in items], check_termination=check)
-        for it, o in zip(items, outs):
-            it[6] = (o[0], o[1], o[2])
-        return outs
+        engines.append(comp.engine)
+        data.append((cls, seed, b))
 
     res = {}
     for label, check in (("early_exit", 1), ("fixed50", 0)):
-        for it in items:
-            it[6] = None
-        for _ in range(max(3, args.warmup)):
-            step(check)
+        # every label starts the loop from the same initial states
+        items, loops = [], []
+        for eng, (cls, seed, b) in zip(engines, data):
+            items.append([eng, t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), None])
+            loops.append(problems.ClosedLoop(cls, problems.draw_params(cls, per, seed), device=dev))
+        outs0 = solve_classes([tuple(it) for it in items], check_termination=check)  # cold start
+        warm = [tuple(o[k].clone() for k in range(3)) for o in outs0]
+        for it, w, lp, o in zip(items, warm, loops, outs0):
+            it[6] = w
+            lp.advance(o[0], it[4], it[5])
+
+        def step():
+            outs = solve_classes([tuple(it) for it in items], check_termination=check)
+            for it, o, lp in zip(items, outs, loops):
+                for k in range(3):
+                    it[6][k].copy_(o[k])
+                lp.advance(o[0], it[4], it[5])
+            return outs
+
+        s = torch.cuda.Stream(dev)
+        s.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(s):
+            for _ in range(max(3, args.warmup)):
+                step()
+        torch.cuda.current_stream(dev).wait_stream(s)
+        torch.cuda.synchronize()
+        graph = None
+        try:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                outs = step()
+        except Exception as exc:  # report, do not hide
+            print(f"[bench] mixed: CUDA graph capture failed, timing eager launches: {exc!r}", file=sys.stderr)
+            graph = None
+        run = graph.replay if graph is not None else step
+        for _ in range(2):
+            r = run()
+            outs = r if graph is None else outs
         torch.cuda.synchronize()
         barrier(world)
         steps = max(1, min(args.steps, 5))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(steps):
-            outs = step(check)
+            r = run()
+            outs = r if graph is None else outs
         e1.record()
         torch.cuda.synchronize()
         ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
@@ -544,10 +656,13 @@ def mixed_timing(args, dev, world):
             "ms_per_step": ms,
             "converged_fraction": ok / (per * len(classes)),
             "mean_iters": {cls.name: float(o[6].float().mean().item()) for cls, o in zip(classes, outs)},
+            "graphed": graph is not None,
         }
+        del graph
     return {
         "workload": f"{per * len(classes)} instances/GPU over 4 linear MPC classes "
-                    "(4,2,10) (4,2,40) (12,4,20) (12,4,30), warm-started closed loop, <= 50 ADMM iterations",
+                    "(4,2,10) (4,2,40) (12,4,20) (12,4,30), closed MPC loop (state advanced by u0 every step, "
+                    "warm-started), <= 50 ADMM iterations, one persistent launch per step, CUDA graph",
         "unit": "solves/s",
         **res,
     }
@@ -579,7 +694,8 @@ def main():
     world, rank, local = dist_setup(args)
     dev = torch.device("cuda", local)
     cls = get_class(args.config)
-    b = problems.make_batch(cls, args.batch, seed=multirank.instance_seed(1000, rank))
+    seed = multirank.instance_seed(1000, rank)
+    b = problems.make_batch(cls, args.batch, seed=seed)
     b0 = problems.make_batch(cls, 1, seed=1000)  # plan from the same instance 0 on every rank
     plan = problems.make_plan(b0)
     if world > 1:
@@ -589,9 +705,6 @@ def main():
                                                     mode="plain", device=dev)
     eng = comp.engine
     B = b.batch
-    # the schedule form a fixed-iteration solve of this batch runs (frontier: two CTAs per SM)
-    n_sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    form = "frontier" if eng.stream_info()["frontier_slots"] > 0 and (B + 31) // 32 > n_sms else "plain"
     to_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     P, A, Q, L, U = (to_dev(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u))
     f32 = dict(dtype=torch.float32, device=dev)
@@ -599,9 +712,13 @@ def main():
            torch.empty(B, **f32), torch.empty(B, **f32), torch.empty(B, **f32),
            torch.empty(B, dtype=torch.int32, device=dev), torch.empty(B, dtype=torch.int32, device=dev)]
     warm = (out[0], out[1], out[2])
+    # closed MPC loop: after every solve each instance applies its u0 and the
+    # next step's QP starts from the instance's new state (l = u = -x0 rows)
+    loop = problems.ClosedLoop(cls, problems.draw_params(cls, args.batch, seed), device=dev)
 
     def step():
         eng.solve(P, A, Q, L, U, warm=warm, out=out)
+        loop.advance(out[0], L, U)
 
     # cold solve to seed the warm start, then warm-up steps
     eng.solve(P, A, Q, L, U, out=out)
@@ -657,14 +774,25 @@ def main():
     step()
     dom_ms, dom_n, launches_step = native.profile_end()
     torch.cuda.synchronize()
-    # dominant kernel timed alone over the timed-region workload (eager, same inputs)
-    native.profile_begin()
+    # the schedule form, CTAs per SM and grid of the step's streaming launch, as the library ran it
+    launch = native.stream_last_launch()
+    form = launch["form"] or "plain"
+    # dominant kernel (admm_stream_kernel) and the factorization kernel
+    # (factor_stream_kernel) each timed alone over the timed-region workload
+    # (eager, same inputs; the library's event pair around each launch, on its stream)
+    native.profile_begin(native.PROFILE_DOMINANT)
     for _ in range(args.steps):
         step()
     dom_ms, dom_n, _ = native.profile_end()
+    native.profile_begin(native.PROFILE_FACTOR)
+    for _ in range(args.steps):
+        step()
+    fac_ms, fac_n, _ = native.profile_end()
     dom_ms_per_launch = dom_ms / max(dom_n, 1)
+    fac_ms_per_launch = fac_ms / max(fac_n, 1)
     per_inst, fac_b, it_b = algorithmic_bytes_per_instance(plan, plan.settings.max_iter)
-    algo_bytes = per_inst * B
+    admm_bytes = plan.settings.max_iter * it_b * B  # what admm_stream_kernel alone must move
+    factor_bytes = fac_b * B                         # what factor_stream_kernel alone must move
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -672,12 +800,23 @@ def main():
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = algo_bytes / (dom_ms_per_launch * 1e-3) / 1e9
+    peak_source = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = admm_bytes / (dom_ms_per_launch * 1e-3) / 1e9
+    fac_achieved = factor_bytes / (fac_ms_per_launch * 1e-3) / 1e9 if fac_n else None
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": measured_traffic(args, B, form), "kernel": "admm_stream_kernel", "schedule": form,
-        "kernel_ms": dom_ms_per_launch, "bytes_per_launch": algo_bytes,
-        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+        "ctas_per_sm": launch["ctas_per_sm"], "kernel_ms": dom_ms_per_launch, "launches_timed": dom_n,
+        "bytes_per_launch": admm_bytes,
+        "bytes_rule": f"{plan.settings.max_iter} iterations x 4 (2 nnz(L) + n) per instance",
+        "peak_source": peak_source,
+        "factor": {
+            "kernel": "factor_stream_kernel", "kernel_ms": fac_ms_per_launch, "launches_timed": fac_n,
+            "bytes_per_launch": factor_bytes, "bytes_rule": "4 (nnz(KKT) + nnz(L) + 2 n) per instance",
+            "achieved": fac_achieved, "peak": peak, "unit": "GB/s",
+            "frac": (fac_achieved / peak) if fac_achieved else None,
+            "traffic": measured_traffic(args, B, "plain", "factor_stream_kernel"),
+        },
     }
 
     # ---- plain per-call drop-in ------------------------------------------------------
@@ -705,16 +844,22 @@ def main():
     e2e = None
     if not args.no_e2e:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
-        hP, hA, hQ, hL, hU = (pin(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u))
+        hP, hA, hQ = (pin(v) for v in (b.p_values, b.a_values, b.q))
+        # the loop continues from the device loop's current states (l, u rows and x0)
+        hL, hU = L.cpu().pin_memory(), U.cpu().pin_memory()
         hx, hz, hy = (torch.empty(tuple(t.shape), dtype=torch.float32).pin_memory() for t in out[:3])
         hx.copy_(out[0].cpu()); hz.copy_(out[1].cpu()); hy.copy_(out[2].cpu())
         hres = [torch.empty(B, dtype=torch.float32).pin_memory() for _ in range(3)]
         h2d = sum(t.numel() * 4 for t in (hP, hA, hQ, hL, hU, hx, hz, hy))
         d2h = sum(t.numel() * 4 for t in (hx, hz, hy, *hres))
+        hloop = problems.ClosedLoop(cls, problems.draw_params(cls, args.batch, seed))
+        hloop.x0_np[:] = loop.x0.cpu().numpy()
 
         def e2e_step():
-            # host in, host out: the engine copies slices in and out on two streams while it solves
+            # host in, host out: the engine copies slices in and out on two streams while it solves;
+            # then the host applies u0 and writes the instances' next states into l and u
             comp.engine.solve_host(hP, hA, hQ, hL, hU, warm=(hx, hz, hy), out=(hx, hz, hy, *hres))
+            hloop.advance_host(hx.numpy(), hL.numpy(), hU.numpy())
 
         e2e_step()
         torch.cuda.synchronize()
@@ -759,9 +904,13 @@ def main():
     if not args.no_sqp:
         sqp = side_leg("sqp step", lambda: sqp_timing(args, dev, world))
 
+    sqp4 = None
+    if not args.no_sqp4:
+        sqp4 = side_leg("nonlinear sqp", lambda: nonlinear_sqp_timing(args, dev, world))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(plan, b, args)
+        cpu = cpu_baseline(plan, b, args, cls, seed)
 
     graphed = graph is not None
     del graph  # release the graph before tearing anything down
@@ -790,6 +939,7 @@ def main():
             "line_search": line_search,
             "assembly": assembly,
             "sqp_step": sqp,
+            "nonlinear_sqp": sqp4,
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,

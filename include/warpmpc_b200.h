@@ -168,6 +168,13 @@ typedef struct wmpc_osqp_desc {
   const float* scaling_einv;  /* [m] 1/E        */
   const float* y_scale;       /* [m] c/E        */
   const float* y_unscale;     /* [m] E/c        */
+  /* rho adaptation (optional; NULL disables it for this problem): each
+   * constraint's rho class (-1 loose: rho_min, 0 inequality: rho,
+   * 1 equality: 1e3 rho, as solver.py:164-183 assigns them), the KKT slot
+   * of each constraint's -1/rho diagonal entry, and the plan's scalar rho. */
+  const int32_t* rho_type;    /* [m] */
+  const int32_t* rho_to_kkt;  /* [m] */
+  float rho;
 } wmpc_osqp_desc;
 
 typedef struct wmpc_osqp wmpc_osqp;
@@ -185,6 +192,14 @@ typedef struct wmpc_osqp_options {
   int32_t reuse_factor;      /* 1: the workspace already holds the factor of
                                 these P/A values from a previous call with the
                                 same workspace, batch and mode: skip it       */
+  int32_t adaptive_rho_interval; /* > 0: every this many iterations each
+                                instance re-estimates its rho from its scaled
+                                residuals (OSQP's rule, Stellato et al. 2020,
+                                sec. 5.2) and, when the estimate is more than
+                                adaptive_rho_tolerance times away, takes it and
+                                refactors (plain mode; the reference has no
+                                rho adaptation: solver.py:587-588) */
+  float adaptive_rho_tolerance;
 } wmpc_osqp_options;
 
 /* Batched problem data, batch-major.  p_values [pb x nnz_p], a_values
@@ -202,6 +217,9 @@ typedef struct wmpc_osqp_batch {
   float* x; float* z; float* y;
   float* prim_res; float* dual_res; float* obj;
   int32_t* iters; int32_t* status;
+  /* rho adaptation outputs (may be NULL): each instance's final scalar rho
+   * and how many times it changed (one refactorization each) */
+  float* rho; int32_t* rho_updates;
 } wmpc_osqp_batch;
 
 /* Device workspace bytes for `batch` instances.  mode: WMPC_OSQP_PLAIN or
@@ -290,6 +308,43 @@ int wmpc_osqp_solve_persistent(const wmpc_osqp* const* osqps, const wmpc_osqp_op
  *   [n_pad_b, n_pad_f, dummy_units] pad_boff[n_pad_b] pad_foff[n_pad_f]
  *   chunk_pre_u0[n_chunks] chunk_pre_units[n_chunks]
  *   [frontier_slots, frontier_lag, max_frows] (0, 0, 0 without bit 2) */
+/* ------------------------------------------------------------------ */
+/* Stage model of the nonlinear SQP workload (a rigid-body quadrotor). */
+/* No counterpart in the reference, whose stage functions and their   */
+/* derivatives come from CasADi (warpmpc/jax_sqp/casadi_stage.py:     */
+/* 66-189; CasADi is absent here).  State x = [p (3), roll/pitch/yaw  */
+/* (3), v (3, world), w (3, body rates)], input u = 4 motor thrusts:  */
+/*   p' = v;  eta' = W(eta) w;  v' = (sum f)/m R(eta) e3 - g e3;      */
+/*   w' = J^-1 (tau - w x J w),  J = diag(jx, jy, jz),                */
+/*   tau = (arm (-f1 - f2 + f3 + f4), arm (-f1 + f2 + f3 - f4),       */
+/*          yaw_coef (-f1 + f2 - f3 + f4)),                           */
+/* discretised with one classical RK4 step of length dt.              */
+typedef struct wmpc_quadrotor_model {
+  float mass, jx, jy, jz, arm, yaw_coef, gravity;
+} wmpc_quadrotor_model;
+
+/* For every stage k < n_stages and instance b: F(x_k, u_k) of the stage
+ * variables z[b * z_stride + 16 k + (0..11 | 12..15)] (batch-major z of the
+ * SQP, stage blocks of 16) into x_next[(k * batch + b) * 12 + i] and, when
+ * jac is not NULL, the dynamics rows' Jacobian entries of g = x_next - F
+ * into jac[(k * batch + b) * 126 + e] in wmpc_quadrotor_jac_pattern's order
+ * (forward-mode derivatives, float32).  Stream-ordered, launch only. */
+int wmpc_quadrotor_rk4(const wmpc_quadrotor_model* model, const float* z, int64_t z_stride, int32_t batch,
+                       int32_t n_stages, float dt, float* x_next, float* jac, wmpc_stream_t stream);
+/* The entry order of those 126 entries: row_ptr[13] (entries of row r at
+ * [row_ptr[r], row_ptr[r + 1])) and cols[126] (0..15 = [x, u] of the stage,
+ * 16 + r = x_next,r).  Host only. */
+int wmpc_quadrotor_jac_pattern(int32_t* cols, int32_t* row_ptr);
+
+/* Host-only query of the chunk tables the per-call solve (wmpc_solve) uses
+ * for its TMA-fed kernel (for CPU-side checks; no counterpart in the
+ * reference).  out = [n_chunks, table_words, tables[table_words],
+ * desc[8 n_chunks]]; each chunk's table is {columns C, entries E, c0, e0,
+ * C column ends relative to e0, E row byte offsets (row * 128)} padded to 4
+ * words, its desc {table word offset, table words, e0, c0, E, C, 0, 0}.
+ * WMPC_ERR_UNSUPPORTED when a column has more than 64 entries (the solve
+ * then runs the one-lane kernel).  With out = NULL only *out_words is set. */
+int wmpc_solve_tables_host(const wmpc_pattern_desc* desc, int32_t* out, int64_t out_capacity, int64_t* out_words);
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv,
                               int32_t n_primal, int32_t units, int32_t cols, int32_t rel, int32_t funits,
                               int32_t offload, int32_t* out, int64_t out_capacity, int64_t* out_words);
@@ -302,6 +357,15 @@ int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, c
  * waits for the recorded events and returns the summed device time. */
 int wmpc_profile_begin(void);
 int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* total_launches);
+/* Which launches the event pairs bracket: 0 (default) the dominant kernel
+ * as above, 1 the factorization kernels (the streaming factorization of
+ * the persistent path, the per-call factorization).  No counterpart in the
+ * reference. */
+int wmpc_profile_select(int32_t channel);
+/* The last streaming ADMM launch of this process (no counterpart in the
+ * reference): info = {schedule form (0 none yet, 1 plain, 2 frontier),
+ * CTAs per SM, grid size, dynamic shared memory bytes}. */
+int wmpc_stream_last_launch(int32_t info[4]);
 /* Kernels launched by this library since load (or the last profile_begin). */
 int64_t wmpc_launch_count(void);
 

@@ -196,14 +196,23 @@ def test_two_ctas_per_sm_small_class_bitexact(cuda_device, monkeypatch):
     b = problems.make_batch(problems.SMALL, 9500, seed=13)  # 297 tiles > 148 SMs
     plan = problems.make_plan(b)
     comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    from warpmpc_b200 import native
+
     got = _run(comp, b)
+    assert native.stream_last_launch()["ctas_per_sm"] == 2
     ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u)
     for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
         np.testing.assert_array_equal(g, r, err_msg=name)
+    # the CTA limit is a per-problem setting, fixed when the problem is created
     monkeypatch.setenv("WMPC_STREAM_CTAS", "1")
-    one = _run(comp, b)
+    comp1 = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    one = _run(comp1, b)
+    assert native.stream_last_launch()["ctas_per_sm"] == 1
     for g, o in zip(got[:3], one[:3]):
         np.testing.assert_array_equal(g, o)
+    assert native.stream_last_launch()["ctas_per_sm"] == 1
+    _run(comp, b)  # created before the setting: still two
+    assert native.stream_last_launch()["ctas_per_sm"] == 2
 
 
 def test_autotune_stream_candidates_agree(cuda_device, tmp_path):

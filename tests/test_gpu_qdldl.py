@@ -104,3 +104,29 @@ def test_empty_batch_and_bad_shapes(cuda_device):
         comp.factor(torch.zeros((plan.nnz_a + 1, 3)))
     with pytest.raises(TypeError):
         comp.factor(torch.zeros((plan.nnz_a, 3), dtype=torch.float64))
+
+
+@pytest.mark.parametrize("cls", [problems.SMALL, problems.QUADROTOR], ids=lambda c: c.name)
+def test_tma_solve_many_tiles(cuda_device, monkeypatch, cls):
+    """The TMA-fed solve (batch a multiple of 4, one factor per instance) over
+    many tiles per CTA and a partial last tile: bit-identical to the
+    one-lane-per-instance kernel (WMPC_SOLVE_STREAM_OFF=1) and to the oracle."""
+    import torch
+
+    from oracle import osqp_ref
+
+    batch = 148 * 32 * 2 + 28  # more tiles than CTAs, last tile 28 lanes wide
+    b = problems.make_batch(cls, batch, seed=8)
+    plan = problems.make_plan(b)
+    qp = plan.qdldl_plan
+    comp = compile_qdldl_variant(qp, np.float32, backend="cuda", transpose_work=True)
+    vals = np.ascontiguousarray(osqp_ref.assemble_kkt_values(plan, b.p_values, b.a_values).T)
+    lx, d, dinv = comp.factor(torch.from_numpy(vals).cuda())
+    rhs = torch.from_numpy(np.random.default_rng(4).standard_normal((qp.n, batch)).astype(np.float32)).cuda()
+    x_tma = comp.solve(lx, dinv, rhs).cpu().numpy()
+    monkeypatch.setenv("WMPC_SOLVE_STREAM_OFF", "1")
+    x_one = comp.solve(lx, dinv, rhs).cpu().numpy()
+    np.testing.assert_array_equal(x_tma, x_one)
+    sl = slice(batch - 64, batch)  # the oracle on the last two tiles (the partial one included)
+    want = qdldl_ref.solve(qp, lx.cpu().numpy()[:, sl], dinv.cpu().numpy()[:, sl], rhs.cpu().numpy()[:, sl])
+    np.testing.assert_array_equal(x_tma[:, sl], want)

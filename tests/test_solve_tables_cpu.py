@@ -1,0 +1,89 @@
+"""CPU replay of the TMA-fed per-call solve kernel (solve_stream.cu) over the
+chunk tables the library builds (wmpc_solve_tables_host): every item's
+copies and every work-vector index are checked against the kernel's buffer
+sizes, and the replayed arithmetic (float32, the kernel's order) must equal
+the oracle's serial solve bit for bit."""
+
+import numpy as np
+import pytest
+
+from oracle import qdldl_ref
+from warpmpc_b200 import problems, schedule
+
+# the kernel's constants (solve_stream.cu)
+BOX, CHUNK_ENTRIES, CHUNK_COLS, RHS_ROWS, TABLE_BYTES = 32, 64, 32, 96, 512
+DATA_ROWS = CHUNK_ENTRIES + CHUNK_COLS
+
+
+def replay(qp, tab, lx, dinv, rhs):
+    """One instance column at a time (lanes are independent); float32 throughout."""
+    n, nnz_l = qp.n, qp.nnz_l
+    T, D = tab["tables"], tab["desc"]
+    f32 = np.float32
+    X = np.zeros(n, dtype=f32)
+    # rhs items: boxes of 32 rows inside the data area, rows past n zero-filled
+    for k in range((n + RHS_ROWS - 1) // RHS_ROWS):
+        r0 = k * RHS_ROWS
+        rows = min(RHS_ROWS, n - r0)
+        assert ((rows + BOX - 1) // BOX) * BOX <= DATA_ROWS
+        for r in range(rows):
+            X[qp.pinv[r0 + r]] = rhs[r0 + r]
+
+    def chunk(k, backward):
+        toff, words, e0, c0, E, C = (int(v) for v in D[k, :6])
+        assert toff % 4 == 0 and words % 4 == 0 and words * 4 <= TABLE_BYTES
+        assert 0 < C <= CHUNK_COLS and 0 <= E <= CHUNK_ENTRIES
+        t = T[toff : toff + words]
+        assert t[0] == C and t[1] == E and t[2] == c0 and t[3] == e0
+        assert ((E + BOX - 1) // BOX) * BOX <= CHUNK_ENTRIES
+        if backward:
+            assert ((C + BOX - 1) // BOX) * BOX + CHUNK_ENTRIES <= DATA_ROWS
+        cend = t[4 : 4 + C]
+        roff = t[4 + C : 4 + C + E]
+        assert np.all(roff % 128 == 0) and np.all(roff // 128 < n) and np.all(roff >= 0)
+        assert np.all(np.diff(np.concatenate([[0], cend])) >= 0) and (C == 0 or cend[-1] == E)
+        L = np.zeros(((E + BOX - 1) // BOX) * BOX, dtype=f32)
+        L[:E] = lx[e0 : e0 + E]  # rows past nnz_l would be zero-filled by the copy
+        return c0, C, cend, roff // 128, L
+
+    nch = D.shape[0]
+    for k in range(nch):
+        c0, C, cend, rows, L = chunk(k, False)
+        b = 0
+        for j in range(C):
+            e = int(cend[j])
+            if e > b:
+                val = X[c0 + j]
+                for q in range(b, e):
+                    X[rows[q]] = f32(X[rows[q]] - f32(L[q] * val))
+            b = e
+    for k in range(nch - 1, -1, -1):
+        c0, C, cend, rows, L = chunk(k, True)
+        for j in range(C - 1, -1, -1):
+            b = int(cend[j - 1]) if j > 0 else 0
+            e = int(cend[j])
+            corr = f32(0.0)
+            for q in range(b, e):
+                corr = f32(corr + f32(L[q] * X[rows[q]]))
+            X[c0 + j] = f32(f32(X[c0 + j] * dinv[c0 + j]) - corr)
+    # chunks cover every column exactly once, in order
+    assert np.array_equal(np.concatenate([np.arange(d[3], d[3] + d[5]) for d in D]), np.arange(n))
+    return X[qp.pinv]
+
+
+@pytest.mark.parametrize("cls", [problems.SMALL, problems.CARTPOLE, problems.QUADROTOR], ids=lambda c: c.name)
+def test_solve_stream_replay_matches_oracle(cls):
+    from oracle import osqp_ref
+
+    b = problems.make_batch(cls, 2, seed=21)
+    plan = problems.make_plan(b)
+    qp = plan.qdldl_plan
+    tab = schedule.solve_tables(qp)
+    kkt = osqp_ref.assemble_kkt_values(plan, b.p_values, b.a_values)  # (B, nnz_kkt) original order
+    rng = np.random.default_rng(3)
+    for i in range(2):
+        lx, d, dinv = qdldl_ref.factor(qp, kkt[i : i + 1].T.astype(np.float32))
+        rhs = rng.standard_normal((qp.n, 1)).astype(np.float32)
+        want = qdldl_ref.solve(qp, lx, dinv, rhs)[:, 0]
+        got = replay(qp, tab, lx[:, 0], dinv[:, 0], rhs[:, 0])
+        np.testing.assert_array_equal(got, want)

@@ -43,13 +43,16 @@ std::atomic<long long> g_launches{0};
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
 size_t g_prof_used = 0;
 bool g_prof_open = false;
+int g_prof_channel = kProfileDominant;
+std::mutex g_launch_mu;
+int g_last_launch[4] = {0, 0, 0, 0};
 }  // namespace
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-void profile_mark_begin(cudaStream_t s) {
+void profile_mark_begin(cudaStream_t s, int channel) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
-  if (!g_prof_on) return;
+  if (!g_prof_on || channel != g_prof_channel) return;
   if (g_prof_used == g_prof_events.size()) {
     cudaEvent_t a, b;
     if (cudaEventCreate(&a) != cudaSuccess) return;
@@ -60,12 +63,20 @@ void profile_mark_begin(cudaStream_t s) {
   g_prof_open = true;
 }
 
-void profile_mark_end(cudaStream_t s) {
+void profile_mark_end(cudaStream_t s, int channel) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
-  if (!g_prof_on || !g_prof_open) return;
+  if (!g_prof_on || !g_prof_open || channel != g_prof_channel) return;
   cudaEventRecord(g_prof_events[g_prof_used].second, s);
   ++g_prof_used;
   g_prof_open = false;
+}
+
+void record_stream_launch(int form, int ctas_per_sm, int grid, int smem_bytes) {
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  g_last_launch[0] = form;
+  g_last_launch[1] = ctas_per_sm;
+  g_last_launch[2] = grid;
+  g_last_launch[3] = smem_bytes;
 }
 
 size_t osqp_workspace_bytes(const wmpc_osqp& q, int batch, int pb, int ab, int mode, bool external);
@@ -252,6 +263,20 @@ int wmpc_profile_begin(void) {
   return WMPC_OK;
 }
 
+int wmpc_profile_select(int32_t channel) {
+  if (channel < 0 || channel > 1) return fail(WMPC_ERR_INVALID_ARGUMENT, "profile channel %d (0 or 1)", channel);
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_channel = channel;
+  return WMPC_OK;
+}
+
+int wmpc_stream_last_launch(int32_t info[4]) {
+  if (!info) return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  for (int i = 0; i < 4; ++i) info[i] = g_last_launch[i];
+  return WMPC_OK;
+}
+
 int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* total_launches) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   double total = 0.0;
@@ -274,6 +299,26 @@ int wmpc_profile_end(float* dominant_ms, int32_t* dominant_launches, int64_t* to
 }
 
 int64_t wmpc_launch_count(void) { return g_launches.load(); }
+
+int wmpc_solve_tables_host(const wmpc_pattern_desc* desc, int32_t* out, int64_t out_capacity, int64_t* out_words) {
+  if (!desc || !out_words || !desc->lp || (desc->nnz_l > 0 && !desc->li))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "null argument");
+  const int n = desc->n, nnz_l = desc->nnz_l;
+  if (n <= 0 || nnz_l <= 0) return fail(WMPC_ERR_INVALID_ARGUMENT, "bad sizes");
+  std::vector<int> tables, sdesc;
+  if (!build_solve_tables(n, std::vector<int>(desc->lp, desc->lp + n + 1), std::vector<int>(desc->li, desc->li + nnz_l),
+                          &tables, &sdesc))
+    return fail(WMPC_ERR_UNSUPPORTED, "a column has more entries than a solve chunk holds");
+  std::vector<int> w{static_cast<int>(sdesc.size() / 8), static_cast<int>(tables.size())};
+  w.insert(w.end(), tables.begin(), tables.end());
+  w.insert(w.end(), sdesc.begin(), sdesc.end());
+  *out_words = static_cast<int64_t>(w.size());
+  if (out) {
+    if (out_capacity < *out_words) return fail(WMPC_ERR_INVALID_ARGUMENT, "output capacity too small");
+    std::memcpy(out, w.data(), w.size() * sizeof(int32_t));
+  }
+  return WMPC_OK;
+}
 
 int wmpc_stream_schedule_host(const wmpc_pattern_desc* desc, const float* rho, const float* rhoinv, int32_t n_primal,
                               int32_t units, int32_t cols, int32_t rel, int32_t funits, int32_t offload,
@@ -397,6 +442,14 @@ int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out)
   pk.add(desc->li, nnz_l, &pat.li);
   pk.add(desc->p, n, &pat.p);
   pk.add(desc->pinv, n, &pat.pinv);
+  // chunk tables of the TMA-fed per-call solve (when every column fits a chunk)
+  std::vector<int> solve_tables, solve_desc;
+  if (nnz_l > 0 && build_solve_tables(n, std::vector<int>(desc->lp, desc->lp + n + 1),
+                                      std::vector<int>(desc->li, desc->li + nnz_l), &solve_tables, &solve_desc)) {
+    pk.add(solve_tables.data(), solve_tables.size(), &plan->solve_tables);
+    pk.add(solve_desc.data(), solve_desc.size(), &plan->solve_desc);
+    plan->solve_chunks = (int)solve_desc.size() / 8;
+  }
   int rc = pk.upload(&plan->table_block);
   if (rc) {
     delete plan;
@@ -466,8 +519,8 @@ int wmpc_solve(const wmpc_plan* plan, const float* lx, const float* dinv, int32_
   if (factor_bstride != 0 && factor_bstride != 1) return fail(WMPC_ERR_INVALID_ARGUMENT, "factor_bstride must be 0 or 1");
   DeviceGuard guard(plan->device);
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", plan->device);
-  return launch_solve(plan->pat, lx, dinv, factor_bstride, rhs, x, batch, workspace, workspace_bytes,
-                      static_cast<cudaStream_t>(stream));
+  return launch_solve_plan(*plan, lx, dinv, factor_bstride, rhs, x, batch, workspace, workspace_bytes,
+                           static_cast<cudaStream_t>(stream));
 }
 
 int wmpc_factor_solve(const wmpc_plan* plan, const float* values, int64_t values_ld, int32_t values_bstride,
@@ -546,6 +599,7 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", kkt_plan->device);
   auto* q = new wmpc_osqp();
   q->device = kkt_plan->device;
+  q->ctas_limit = stream_ctas_limit_setting();
   q->kkt_plan = kkt_plan;
   Osqp& o = q->dev;
   o.n = n;
@@ -583,6 +637,24 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
   pk.addf(desc->y_unscale, m, &o.y_unscale);
   pk.add(p_up_rows.data(), np, &q->p_upper_rows);
   pk.add(p_up_cols.data(), np, &q->p_upper_cols);
+  // rho adaptation: each constraint's rho class and, per KKT slot, the
+  // constraint whose -1/rho it holds (-1: none)
+  std::vector<int32_t> kkt_rho_row;
+  if (desc->rho_type && desc->rho_to_kkt && m > 0) {
+    kkt_rho_row.assign(nk, -1);
+    for (int r = 0; r < m; ++r) {
+      const int slot = desc->rho_to_kkt[r];
+      const int t = desc->rho_type[r];
+      if (slot < 0 || slot >= nk || kkt_src[slot] >= 0 || kkt_rho_row[slot] >= 0 || t < -1 || t > 1) {
+        delete q;
+        return fail(WMPC_ERR_INVALID_ARGUMENT, "bad rho_to_kkt/rho_type entry for constraint %d", r);
+      }
+      kkt_rho_row[slot] = r;
+    }
+    pk.add(desc->rho_type, m, &o.rho_type);
+    pk.add(kkt_rho_row.data(), nk, &o.kkt_rho_row);
+    o.rho0 = desc->rho;
+  }
   int* block = nullptr;
   int rc = pk.upload(&block);
   if (rc) {
@@ -633,7 +705,8 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
       q->has_frontier = build_stream_plan(hp, ftargets, desc, unscale, &q->spf, &q->stream_block_f, &why);
       // worth it where it lets more CTAs share an SM than the plain form
       q->frontier_pays = q->has_frontier &&
-                         stream_max_ctas(q->spf, kkt_plan->device) > stream_max_ctas(q->sp, kkt_plan->device);
+                         stream_max_ctas(q->spf, kkt_plan->device, q->ctas_limit) >
+                             stream_max_ctas(q->sp, kkt_plan->device, q->ctas_limit);
     }
   }
   *out = q;

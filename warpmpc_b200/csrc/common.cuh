@@ -24,10 +24,16 @@ namespace wmpc {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 
-// Launch accounting and dominant-kernel timing (wmpc_profile_begin/end).
+// Launch accounting and per-channel kernel timing (wmpc_profile_begin/end):
+// marks of the channel selected by wmpc_profile_select record event pairs,
+// the others are ignored.
+constexpr int kProfileDominant = 0;  // the step's dominant kernel (ADMM sweeps, per-call solves, ...)
+constexpr int kProfileFactor = 1;    // factorization kernels
 void count_launch();
-void profile_mark_begin(cudaStream_t s);
-void profile_mark_end(cudaStream_t s);
+void profile_mark_begin(cudaStream_t s, int channel = kProfileDominant);
+void profile_mark_end(cudaStream_t s, int channel = kProfileDominant);
+// The last streaming ADMM launch (wmpc_stream_last_launch).
+void record_stream_launch(int form, int ctas_per_sm, int grid, int smem_bytes);
 
 #define WMPC_CUDA_TRY(expr)                                                              \
   do {                                                                                   \
@@ -104,6 +110,10 @@ struct wmpc_plan {
   wmpc::Pattern pat{};
   int* table_block = nullptr;  // single device allocation holding every table
   size_t table_ints = 0;
+  // chunk index tables of the TMA-fed per-call solve (null: not applicable)
+  const int* solve_tables = nullptr;
+  const int* solve_desc = nullptr;  // two int4 per chunk
+  int solve_chunks = 0;
   // host copies of the ragged program (inputs of the streaming schedule)
   std::vector<int> h_init_ptr, h_init_rows, h_proc_ptr, h_proc_cols, h_proc_offsets, h_proc_lidx, h_lp, h_li, h_p;
 };

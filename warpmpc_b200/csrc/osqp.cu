@@ -123,20 +123,35 @@ __device__ __forceinline__ float clip_nan(float v, float lo, float hi) {
   return (t > hi) ? hi : t;
 }
 
+// Per-(constraint, instance) rho and 1/rho ([m][batch]) when rho adapts per
+// instance; null pointers: the plan's vector.
+struct RhoRows {
+  const float* rho = nullptr;
+  const float* rinv = nullptr;
+};
+
+__device__ __forceinline__ float rho_at(const Osqp& o, const RhoRows& rr, int r, long long k) {
+  return rr.rho ? rr.rho[k] : __ldg(o.rho + r);
+}
+__device__ __forceinline__ float rinv_at(const Osqp& o, const RhoRows& rr, int r, long long k) {
+  return rr.rinv ? rr.rinv[k] : __ldg(o.rho_inv + r);
+}
+
 // rhs entry of KKT index `orig` (original, un-permuted numbering)
-__device__ __forceinline__ float rhs_entry(const Osqp& o, const State& st, int orig, int b) {
+__device__ __forceinline__ float rhs_entry(const Osqp& o, const State& st, int orig, int b, const RhoRows& rr = {}) {
   if (orig < o.n) {
     const long long k = (long long)orig * st.ld + b;
     return o.sigma * st.x[k] - st.qs[k];
   }
   const int r = orig - o.n;
   const long long k = (long long)r * st.ld + b;
-  return st.z[k] - __ldg(o.rho_inv + r) * st.y[k];
+  return st.z[k] - rinv_at(o, rr, r, k) * st.y[k];
 }
 
 // ADMM update of KKT index `orig` given the solve output `sol`
 // (solver.py:813-819); returns the next iteration's rhs entry.
-__device__ __forceinline__ float admm_update(const Osqp& o, const State& st, int orig, int b, float sol) {
+__device__ __forceinline__ float admm_update(const Osqp& o, const State& st, int orig, int b, float sol,
+                                             const RhoRows& rr = {}) {
   if (orig < o.n) {
     const long long k = (long long)orig * st.ld + b;
     const float x = st.x[k];
@@ -146,30 +161,143 @@ __device__ __forceinline__ float admm_update(const Osqp& o, const State& st, int
   }
   const int r = orig - o.n;
   const long long k = (long long)r * st.ld + b;
-  const float rinv = __ldg(o.rho_inv + r);
+  const float rinv = rinv_at(o, rr, r, k);
   const float z = st.z[k], y = st.y[k];
   const float rz = z - rinv * y;
   const float zt = rz + rinv * sol;
   const float zr = o.alpha * zt + o.one_minus_alpha * z;
   const float zn = clip_nan(zr + rinv * y, st.ls[k], st.us[k]);
-  const float yn = y + __ldg(o.rho + r) * (zr - zn);
+  const float yn = y + rho_at(o, rr, r, k) * (zr - zn);
   st.z[k] = zn;
   st.y[k] = yn;
   return zn - rinv * yn;
 }
 
-__global__ void admm_first_rhs_kernel(Osqp o, State st, float* __restrict__ rhs, int batch) {
+__global__ void admm_first_rhs_kernel(Osqp o, State st, float* __restrict__ rhs, int batch, RhoRows rr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
-  for (int i = blockIdx.y; i < o.nk; i += gridDim.y) rhs[(long long)i * batch + b] = rhs_entry(o, st, i, b);
+  for (int i = blockIdx.y; i < o.nk; i += gridDim.y) rhs[(long long)i * batch + b] = rhs_entry(o, st, i, b, rr);
 }
 
-__global__ void admm_update_kernel(Osqp o, State st, float* __restrict__ rhs, int batch) {
+__global__ void admm_update_kernel(Osqp o, State st, float* __restrict__ rhs, int batch, RhoRows rr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= batch) return;
   for (int i = blockIdx.y; i < o.nk; i += gridDim.y) {
     const long long k = (long long)i * batch + b;
-    rhs[k] = admm_update(o, st, i, b, rhs[k]);
+    rhs[k] = admm_update(o, st, i, b, rhs[k], rr);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// rho adaptation (per instance, plain mode).  No counterpart in the reference
+// (solver.py:587-588 rejects adaptive_rho); the rule is OSQP's (Stellato et
+// al. 2020, "OSQP: an operator splitting solver for quadratic programs",
+// sec. 5.2), on the scaled iterate:
+//   r_p = |A x - z|_inf / (max(|A x|_inf, |z|_inf) + 1e-10)
+//   r_d = |P x + q + A^T y|_inf / (max(|P x|_inf, |A^T y|_inf, |q|_inf) + 1e-10)
+//   rho' = clamp(rho sqrt(r_p / (r_d + 1e-10)), 1e-6, 1e6)
+// taken when rho' > tol rho or rho' < rho / tol; the rho vector then follows
+// the plan's classes (loose rows 1e-6, equality rows 1e3 rho', others rho')
+// and 1/rho is one float32 division per row.  Sums run in the oracle's order
+// (A x and P x by rows, A^T y by columns, entries in storage order).
+// ---------------------------------------------------------------------------
+
+__global__ void rho_init_kernel(Osqp o, float* __restrict__ rho_row, float* __restrict__ rinv_row,
+                                float* __restrict__ rho_b, int* __restrict__ count, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  for (int r = blockIdx.y; r < o.m; r += gridDim.y) {
+    const long long k = (long long)r * batch + b;
+    rho_row[k] = __ldg(o.rho + r);
+    rinv_row[k] = __ldg(o.rho_inv + r);
+  }
+  if (blockIdx.y == 0) {
+    rho_b[b] = o.rho0;
+    count[b] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(128) rho_update_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
+                                                         const float* __restrict__ aT, long long lda, int sba, State st,
+                                                         float* __restrict__ rho_row, float* __restrict__ rinv_row,
+                                                         float* __restrict__ rho_b, int* __restrict__ changed,
+                                                         int* __restrict__ count, float tol, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
+  auto xs = [&](int j) { return st.x[(long long)j * st.ld + b]; };
+  auto as = [&](int e) { return in.a(e) * __ldg(o.a_scale + e); };
+  float prim = 0.f, axn = 0.f, zn = 0.f;
+  for (int row = 0; row < o.m; ++row) {
+    float ax = 0.0f;
+    const int e0 = __ldg(o.a_row_ptr + row), e1 = __ldg(o.a_row_ptr + row + 1);
+    for (int t = e0; t < e1; ++t) {
+      const int e = __ldg(o.a_row_ent + t);
+      ax = ax + as(e) * xs(__ldg(o.a_cols + e));
+    }
+    const float z = st.z[(long long)row * st.ld + b];
+    prim = fmaxf(prim, fabsf(ax - z));
+    axn = fmaxf(axn, fabsf(ax));
+    zn = fmaxf(zn, fabsf(z));
+  }
+  float dual = 0.f, pxn = 0.f, atyn = 0.f, qn = 0.f;
+  for (int j = 0; j < o.n; ++j) {
+    float px = 0.0f;
+    const int f0 = __ldg(o.pf_row_ptr + j), f1 = __ldg(o.pf_row_ptr + j + 1);
+    for (int t = f0; t < f1; ++t) {
+      const int v = __ldg(o.pf_val + t);
+      px = px + (in.p(v) * __ldg(o.p_scale + v)) * xs(__ldg(o.pf_col + t));
+    }
+    float aty = 0.0f;
+    const int c0 = __ldg(o.a_col_ptr + j), c1 = __ldg(o.a_col_ptr + j + 1);
+    for (int e = c0; e < c1; ++e) aty = aty + as(e) * st.y[(long long)__ldg(o.a_rows + e) * st.ld + b];
+    const float qj = st.qs[(long long)j * st.ld + b];
+    dual = fmaxf(dual, fabsf(px + qj + aty));
+    pxn = fmaxf(pxn, fabsf(px));
+    atyn = fmaxf(atyn, fabsf(aty));
+    qn = fmaxf(qn, fabsf(qj));
+  }
+  const float rp = prim / (fmaxf(axn, zn) + 1e-10f);
+  const float rd = dual / (fmaxf(fmaxf(pxn, atyn), qn) + 1e-10f);
+  const float rho = rho_b[b];
+  float est = rho * sqrtf(rp / (rd + 1e-10f));
+  est = fminf(fmaxf(est, 1e-6f), 1e6f);
+  const bool take = est > rho * tol || est < rho / tol;
+  changed[b] = take ? 1 : 0;
+  if (!take) return;
+  rho_b[b] = est;
+  count[b] += 1;
+  for (int r = 0; r < o.m; ++r) {
+    const int t = __ldg(o.rho_type + r);
+    const float v = t < 0 ? 1e-6f : (t > 0 ? 1e3f * est : est);
+    const long long k = (long long)r * batch + b;
+    rho_row[k] = v;
+    rinv_row[k] = 1.0f / v;
+  }
+}
+
+// The rho outputs of a plain-mode solve: each instance's final rho and rho
+// changes (without adaptation: the plan's rho and 0).
+__global__ void rho_report_kernel(const float* __restrict__ rho_b, const int* __restrict__ count, float rho0,
+                                  float* __restrict__ rho_out, int* __restrict__ count_out, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  if (rho_out) rho_out[b] = rho_b ? rho_b[b] : rho0;
+  if (count_out) count_out[b] = count ? count[b] : 0;
+}
+
+// KKT values with each instance's own -1/rho entries (only the instances
+// marked in `only`, when given).
+__global__ void assemble_kkt_rho_kernel(Osqp o, const float* __restrict__ pT, long long ldp, int sbp,
+                                        const float* __restrict__ aT, long long lda, int sba,
+                                        const float* __restrict__ rinv_row, const int* __restrict__ only,
+                                        float* __restrict__ kkt, int batch) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch || (only && !only[b])) return;
+  InstanceData in{pT + (long long)b * sbp, ldp, aT + (long long)b * sba, lda};
+  for (int s = blockIdx.y; s < o.nnz_kkt; s += gridDim.y) {
+    const int r = __ldg(o.kkt_rho_row + s);
+    kkt[(long long)s * batch + b] = r >= 0 ? -rinv_row[(long long)r * batch + b] : kkt_value(o, in, s);
   }
 }
 
@@ -450,6 +578,9 @@ struct Carve {
 
 struct Layout {
   float *pT, *aT, *qs, *ls, *us, *qT, *x, *z, *y, *kkt, *lx, *d, *dinv, *rhs, *scratch;
+  float *rho_row, *rinv_row, *rho_b;  // plain mode: per-instance rho vectors and scalar (rho adaptation)
+  int* rho_changed;                   // [batch] 1 where the last estimate changed rho
+  int* rho_count;                     // [batch] rho changes so far
   size_t scratch_bytes;
   bool factor_separately;  // factor with the per-call kernels before iterating
   bool streaming;          // persistent mode on the TMA-fed streaming kernel
@@ -460,7 +591,7 @@ struct Layout {
 
 // Workspace carve-up.  `external`: the caller supplies the factorization.
 Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int mode, bool external, char* base,
-             size_t* total, const wmpc_osqp* q = nullptr, bool use_stream = false) {
+             size_t* total, const wmpc_osqp* q = nullptr, bool use_stream = false, bool per_instance_factor = false) {
   Carve c{base};
   Layout L{};
   if (use_stream && q && q->has_stream && mode == WMPC_OSQP_PERSISTENT && !external) {
@@ -482,7 +613,8 @@ Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int m
     *total = c.used;
     return L;
   }
-  const int kb = pb > ab ? pb : ab;  // KKT (factor) batch
+  // KKT (factor) batch: one factor per instance when rho adapts per instance
+  const int kb = per_instance_factor ? batch : (pb > ab ? pb : ab);
   L.pT = c.take((size_t)o.nnz_p * pb);
   L.aT = c.take((size_t)o.nnz_a * ab);
   L.qT = c.take((size_t)o.n * batch);
@@ -506,6 +638,11 @@ Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int m
   }
   if (mode == WMPC_OSQP_PLAIN) {
     L.rhs = c.take((size_t)o.nk * batch);
+    L.rho_row = c.take((size_t)o.m * batch);
+    L.rinv_row = c.take((size_t)o.m * batch);
+    L.rho_b = c.take((size_t)batch);
+    L.rho_changed = reinterpret_cast<int*>(c.take((size_t)batch));
+    L.rho_count = reinterpret_cast<int*>(c.take((size_t)batch));
     size_t s2 = solve_workspace_bytes(pat, batch);
     scratch = scratch > s2 ? scratch : s2;
   } else {
@@ -608,12 +745,13 @@ int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_ba
 }
 
 // The schedule a fixed-iteration solve of `tiles` instance tiles runs alone:
-// the frontier form where it lets two CTAs share an SM and the plain form does
-// not, and the batch has tiles for both (and one CTA per SM is not forced:
-// WMPC_STREAM_CTAS=1).  Checked solves run the plain form.
+// the frontier form where this batch's launch of it would put more CTAs on
+// an SM than the plain form's (both counts under the problem's CTA limit,
+// which the launch uses too).  Checked solves run the plain form.
 static bool frontier_for(const wmpc_osqp& q, bool check, int tiles) {
-  const char* ctas = getenv("WMPC_STREAM_CTAS");
-  return q.frontier_pays && !check && tiles > q.num_sms && !(ctas && atoi(ctas) == 1);
+  if (!q.has_frontier || check) return false;
+  return stream_ctas_for(q.spf, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit) >
+         stream_ctas_for(q.sp, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit);
 }
 
 // Streaming solve, first half: inputs staged, factor, state records; fills
@@ -639,6 +777,7 @@ int stream_solve_begin(const wmpc_osqp& q, const wmpc_osqp_options& opt, const w
   // the final iterate.
   job->max_iter = opt.max_iter;
   job->check_every = check;
+  job->ctas_limit = q.ctas_limit;
   job->chg_eps = opt.eps_abs;
   job->iters = check ? d.iters : nullptr;
   return WMPC_OK;
@@ -678,8 +817,19 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if (B <= 0) return WMPC_OK;
   const int pb = d.p_batch, ab = d.a_batch;
   const bool external = lx_ext != nullptr;
+  const bool adaptive = opt.adaptive_rho_interval > 0;
+  if (adaptive) {
+    if (mode != WMPC_OSQP_PLAIN) return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation runs in plain mode");
+    if (external || opt.reuse_factor)
+      return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation refactors: it cannot start from a given factorization");
+    if (!o.rho_type || !o.kkt_rho_row)
+      return fail(WMPC_ERR_UNSUPPORTED, "the problem was created without the rho adaptation tables");
+    if (!(opt.adaptive_rho_tolerance >= 1.0f))
+      return fail(WMPC_ERR_INVALID_ARGUMENT, "adaptive_rho_tolerance must be at least 1");
+  }
   size_t need = 0;
-  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need, &q, stream_eligible(q, &opt));
+  Layout L = carve(o, pat, B, pb, ab, mode, external, static_cast<char*>(ws), &need, &q, stream_eligible(q, &opt),
+                   adaptive);
   if (ws == nullptr || ws_bytes < need)
     return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
   int rc;
@@ -700,7 +850,19 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   const float* lx = lx_ext;
   const float* dinv = dinv_ext;
   int fb = fb_ext;
-  if (!external && L.factor_separately) {
+  dim3 rgrid(ceil_div(B, 128), o.m > 0 ? (o.m < 2048 ? o.m : 2048) : 1);
+  dim3 kgrid(ceil_div(B, 128), o.nnz_kkt < 4096 ? o.nnz_kkt : 4096);
+  if (adaptive) {
+    // one factor per instance, each instance's rho vector starting at the plan's
+    rho_init_kernel<<<rgrid, 128, 0, s>>>(o, L.rho_row, L.rinv_row, L.rho_b, L.rho_count, B);
+    WMPC_LAUNCH_CHECK();
+    assemble_kkt_rho_kernel<<<kgrid, 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, L.rinv_row, nullptr, L.kkt, B);
+    WMPC_LAUNCH_CHECK();
+    if ((rc = launch_factor(pat, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s))) return rc;
+    lx = L.lx;
+    dinv = L.dinv;
+    fb = B;
+  } else if (!external && L.factor_separately) {
     if (!opt.reuse_factor &&
         (rc = assemble_and_factor(o, pat, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch, L.scratch_bytes, s)))
       return rc;
@@ -713,14 +875,37 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if (mode == WMPC_OSQP_PLAIN) {
     const int fstride = fb > 1 ? 1 : 0;
     dim3 egrid(ceil_div(B, 128), o.nk < 2048 ? o.nk : 2048);
-    admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
+    const RhoRows rr = adaptive ? RhoRows{L.rho_row, L.rinv_row} : RhoRows{};
+    admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B, rr);
     WMPC_LAUNCH_CHECK();
     for (int it = 0; it < opt.max_iter; ++it) {
       profile_mark_begin(s);
-      rc = launch_solve(pat, lx, dinv, fstride, L.rhs, L.rhs, B, L.scratch, L.scratch_bytes, s);
+      rc = launch_solve_plan(*q.kkt_plan, lx, dinv, fstride, L.rhs, L.rhs, B, L.scratch, L.scratch_bytes, s);
       profile_mark_end(s);
       if (rc) return rc;
-      admm_update_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B);
+      admm_update_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B, rr);
+      WMPC_LAUNCH_CHECK();
+      if (adaptive && (it + 1) % opt.adaptive_rho_interval == 0 && it + 1 < opt.max_iter) {
+        // new rho estimates; the instances whose rho changed refactor, and
+        // every instance's next right-hand side is formed with its rho
+        rho_update_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.rho_row,
+                                                           L.rinv_row, L.rho_b, L.rho_changed, L.rho_count,
+                                                           opt.adaptive_rho_tolerance, B);
+        WMPC_LAUNCH_CHECK();
+        assemble_kkt_rho_kernel<<<kgrid, 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, L.rinv_row, L.rho_changed,
+                                                      L.kkt, B);
+        WMPC_LAUNCH_CHECK();
+        if ((rc = launch_factor(pat, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s,
+                                L.rho_changed)))
+          return rc;
+        admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B, rr);
+        WMPC_LAUNCH_CHECK();
+      }
+    }
+    if (d.rho || d.rho_updates) {
+      rho_report_kernel<<<ceil_div(B, 256), 256, 0, s>>>(adaptive ? L.rho_b : nullptr,
+                                                         adaptive ? L.rho_count : nullptr, o.rho0, d.rho,
+                                                         d.rho_updates, B);
       WMPC_LAUNCH_CHECK();
     }
     residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(

@@ -36,6 +36,10 @@ struct Osqp {
   const float* scaling_einv;  // [m]
   const float* y_scale;       // [m]
   const float* y_unscale;     // [m]
+  // rho adaptation (null when the problem was created without its tables)
+  const int* rho_type;        // [m] -1 loose, 0 inequality, 1 equality
+  const int* kkt_rho_row;     // [nnz_kkt] constraint of a -1/rho slot, else -1
+  float rho0;                 // the plan's scalar rho
 };
 
 }  // namespace wmpc
@@ -48,6 +52,7 @@ struct wmpc_osqp {
   void* block = nullptr;  // single device allocation holding every table
   const int* p_upper_rows = nullptr;  // [nnz_p] row of every stored upper entry of P
   const int* p_upper_cols = nullptr;  // [nnz_p]
+  int ctas_limit = 2;  // most CTAs per SM of a streaming launch (the environment's setting at creation)
   bool has_stream = false;
   wmpc::StreamPlan sp{};
   void* stream_block = nullptr;

@@ -264,6 +264,7 @@ struct StreamArgs {
   int lbytes;       // per L stage L area
   int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes of records (+ 4 of residuals)
   int pres_off;     // byte offset of the residuals in an S stage (end of the records)
+  unsigned long long wait_limit_ns;  // give-up time of every handshake wait (the drain keeps kWaitLimitNs)
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
 
@@ -275,7 +276,11 @@ __device__ __forceinline__ int job_of(const StreamArgs& a, int g) {
 
 enum : int { kItemRel = 0, kItemFwd = 1, kItemBwd = 2 };
 
-constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: a healthy wait is microseconds
+// 2 s: a healthy wait is microseconds.  The default give-up time of the
+// warps' handshake waits (WMPC_STREAM_WAIT_LIMIT_NS overrides it per launch,
+// so that a test can make them run out), and always the time the abort
+// drain gives the bulk copies already issued (those always complete).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
 
 // ring position: stage index and the parity of the lap
 struct Ring {
@@ -664,7 +669,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           }
           ahead = describe(ahead_kind, ahead_ch);
           if (issued_l >= (uint32_t)a.lstages &&
-              !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, kWaitLimitNs))
+              !mbar_wait_bounded(lempty + lr.stage, lr.phase ^ 1u, abort_flag, a.wait_limit_ns))
             return false;
           unsigned char* st = lring + (size_t)lr.stage * lstage_bytes;
           const float* xsrc = nullptr;
@@ -672,10 +677,10 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             // those blocks are final once every earlier item is released
             // (forward) or swept (backward)
             if (fwd) {
-              if (ch == 0 && !wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return false;
+              if (ch == 0 && !wait_counter_bounded(rel_done, issued_l, abort_flag, a.wait_limit_ns)) return false;
               xsrc = J.rhs + soff + (size_t)d.xrow * 32;
             } else if (kind == kItemBwd) {
-              if (ch == sp.n_chunks - 1 && !wait_counter_bounded(y_done, issued_l, abort_flag, kWaitLimitNs))
+              if (ch == sp.n_chunks - 1 && !wait_counter_bounded(y_done, issued_l, abort_flag, a.wait_limit_ns))
                 return false;
               xsrc = J.fwd + soff + (size_t)d.xrow * 32;
             }
@@ -690,7 +695,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           ++issued_l;
           if (!fwd) {
             if (issued_s >= (uint32_t)a.sstages &&
-                !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, kWaitLimitNs))
+                !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, a.wait_limit_ns))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
             const uint32_t nrel = (uint32_t)d.nrel;
@@ -708,7 +713,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         // before a checked iteration: wait until the releaser has decided
         auto cont = [&](int it) -> int {
           if (!check_point(J.check_every, it)) return 1;
-          if (!wait_counter_bounded(rel_done, issued_l, abort_flag, kWaitLimitNs)) return -1;
+          if (!wait_counter_bounded(rel_done, issued_l, abort_flag, a.wait_limit_ns)) return -1;
           return *stop_at == issued_l ? 0 : 1;
         };
         if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, produce, cont)) {
@@ -729,9 +734,9 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       auto sweep = [&](int kind, int ch) -> bool {
         if (kind != kItemRel) {
           // a forward sweep needs every right-hand side of the previous pass
-          if (kind == kItemFwd && ch == 0 && !wait_counter_bounded(rel_done, t, abort_flag, kWaitLimitNs))
+          if (kind == kItemFwd && ch == 0 && !wait_counter_bounded(rel_done, t, abort_flag, a.wait_limit_ns))
             return false;
-          if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) return false;
+          if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, a.wait_limit_ns)) return false;
           const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
           const int* meta = reinterpret_cast<const int*>(stage);
           const unsigned char* lst = stage + a.meta_bytes;
@@ -769,7 +774,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       };
       auto cont = [&](int it) -> int {
         if (!check_point(J.check_every, it)) return 1;
-        if (!wait_counter_bounded(rel_done, t, abort_flag, kWaitLimitNs)) return -1;
+        if (!wait_counter_bounded(rel_done, t, abort_flag, a.wait_limit_ns)) return -1;
         return *stop_at == t ? 0 : 1;
       };
       if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, sweep, cont)) ok = false;
@@ -807,7 +812,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         if (kFrontier && kind == kItemFwd && rw == 1) {
           // frontier form: copy the forward results the sweeper left in the
           // chunk's stage (rows [r0, r1) of its header) to fwd, then free it
-          if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, kWaitLimitNs)) return false;
+          if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, a.wait_limit_ns)) return false;
           const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
           const int* meta = reinterpret_cast<const int*>(stage);
           const int nu = meta[0], r0 = meta[1], rows = meta[2] - meta[1];
@@ -826,8 +831,8 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         if (kind != kItemFwd) {
           if (kind == kItemBwd) {
             // the chunk's columns are solved (and its stage is full)
-            if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, kWaitLimitNs)) return false;
-          } else if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, kWaitLimitNs)) {
+            if (!wait_counter_bounded(sweep_done, t + 1, abort_flag, a.wait_limit_ns)) return false;
+          } else if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, a.wait_limit_ns)) {
             return false;
           }
           const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
@@ -851,7 +856,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           share(nprim, nrel, cb, ce);
           // leaf columns (read by no other column): solved here, just before their release
           if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
-          if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, kWaitLimitNs)) return false;
+          if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, a.wait_limit_ns)) return false;
           const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
@@ -889,7 +894,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             if (lane == 0) st_release_cta(rel_done1, t + 1);
           } else {
             // both halves done before the stages are freed
-            if (kSplit && !wait_counter_bounded(rel_done1, t + 1, abort_flag, kWaitLimitNs)) return false;
+            if (kSplit && !wait_counter_bounded(rel_done1, t + 1, abort_flag, a.wait_limit_ns)) return false;
             if (lane == 0) {
               mbar_arrive(sempty + sr.stage);
               mbar_arrive(lempty + lr.stage);
@@ -1023,9 +1028,11 @@ bool multi_cta_config(const RingSizes& r, int k, StreamLaunch* cfg, int dev = -1
   return ring_config(r2, cfg, (size_t)(sm_bytes / k - reserved));
 }
 
+}  // namespace
+
 // Most CTAs per SM a launch may use: 1 when WMPC_STREAM_CTAS=1, else
-// WMPC_STREAM_MAX_CTAS (2 to 4; default 2).
-int ctas_limit() {
+// WMPC_STREAM_MAX_CTAS (2 to 4; default 2).  Read when a problem is created.
+int stream_ctas_limit_setting() {
   const char* one = getenv("WMPC_STREAM_CTAS");
   if (one && atoi(one) == 1) return 1;
   const char* v = getenv("WMPC_STREAM_MAX_CTAS");
@@ -1033,16 +1040,51 @@ int ctas_limit() {
   return k < 1 ? 1 : (k > 4 ? 4 : k);
 }
 
+namespace {
+
+// Whether k CTAs of `kernel` (threads each, smem bytes of dynamic shared
+// memory, the SM's unified memory carved out as shared memory) are resident
+// on one SM at once: shared memory alone does not decide it, registers count too.
+bool ctas_resident(const void* kernel, int threads, size_t smem, int k) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return blocks >= k;
+}
+
+// The fixed-iteration kernel instance of a schedule form.
+const void* fixed_iteration_kernel(bool frontier) {
+  return frontier ? reinterpret_cast<const void*>(admm_stream_kernel<false, true>)
+                  : reinterpret_cast<const void*>(admm_stream_kernel<false, false>);
+}
+
 }  // namespace
 
-int stream_max_ctas(const StreamPlan& sp, int device) {
+int stream_max_ctas(const StreamPlan& sp, int device, int limit) {
   const RingSizes r = ring_sizes(sp, false);
-  for (int k = ctas_limit(); k >= 2; --k) {
+  for (int k = limit; k >= 2; --k) {
     StreamLaunch cfg;
-    if (multi_cta_config(r, k, &cfg, device)) return k;
+    if (multi_cta_config(r, k, &cfg, device) &&
+        ctas_resident(fixed_iteration_kernel(sp.frontier_slots > 0), 128, cfg.smem, k))
+      return k;
   }
   return 1;
 }
+
+int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit) {
+  for (int k = stream_max_ctas(sp, device, limit); k >= 2; --k)
+    if (tiles > (k - 1) * num_sms) return k;
+  return 1;
+}
+
 
 // streams, state records, residuals (+ frontier form: right-hand sides and forward results)
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
@@ -1078,8 +1120,10 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
     const size_t smem = (size_t)warps * factor_warp_words(sp, lbatch) * sizeof(float);
     if (smem > (size_t)kMaxSmemBytes) return fail(WMPC_ERR_UNSUPPORTED, "factor rows too long for shared memory");
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    profile_mark_begin(s, kProfileFactor);
     factor_stream_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, s>>>(pat, sp, o, in, bstream, fstream, status,
                                                                             n_tiles, batch, lbatch);
+    profile_mark_end(s, kProfileFactor);
     WMPC_LAUNCH_CHECK();
   }
   {
@@ -1144,9 +1188,14 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   int ctas_per_sm = 1;
   {
     const int tiles = total_tiles_of(jobs, n_jobs);
-    for (int k = ctas_limit(); k >= 2; --k) {
+    const void* kfn = track ? reinterpret_cast<const void*>(admm_stream_kernel<true, false>)
+                            : fixed_iteration_kernel(frontier);
+    int limit = jobs[0].ctas_limit;
+    for (int i = 1; i < n_jobs; ++i) limit = std::min(limit, jobs[i].ctas_limit);
+    for (int k = limit; k >= 2; --k) {
       StreamLaunch cfgk;
-      if (tiles > (k - 1) * num_sms && multi_cta_config(r, k, &cfgk)) {
+      if (tiles > (k - 1) * num_sms && multi_cta_config(r, k, &cfgk) &&
+          ctas_resident(kfn, track ? 96 : 128, cfgk.smem, k)) {
         cfg = cfgk;
         ctas_per_sm = k;
         break;
@@ -1187,6 +1236,11 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.lbytes = cfg.lbytes;
   a.sbytes = cfg.sbytes;
   a.pres_off = cfg.pres_off;
+  a.wait_limit_ns = kWaitLimitNs;
+  if (const char* v = getenv("WMPC_STREAM_WAIT_LIMIT_NS")) {
+    const long long ns = atoll(v);
+    if (ns > 0) a.wait_limit_ns = (unsigned long long)ns;
+  }
   const int grid = total < ctas_per_sm * num_sms ? total : ctas_per_sm * num_sms;
   auto kernel = track ? admm_stream_kernel<true, false>
                       : (frontier ? admm_stream_kernel<false, true> : admm_stream_kernel<false, false>);
@@ -1197,6 +1251,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   profile_mark_begin(s);
   kernel<<<grid, track ? 96 : 128, cfg.smem, s>>>(a);
   profile_mark_end(s);
+  record_stream_launch(frontier ? 2 : 1, ctas_per_sm, grid, (int)cfg.smem);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
 }

@@ -24,10 +24,10 @@ namespace wmpc {
 template <bool kSmem>
 __global__ void __launch_bounds__(256) factor_kernel(Pattern pat, const float* __restrict__ values,
                                                      long long ldv, int bstride, float* lx, float* d,
-                                                     float* dinv, float* yglob, int batch) {
+                                                     float* dinv, float* yglob, int batch, const int* only) {
   extern __shared__ float smem[];
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= batch) return;
+  if (b >= batch || (only && !only[b])) return;
   LaneVec y = kSmem ? LaneVec{smem + threadIdx.x, (long long)blockDim.x}
                     : LaneVec{yglob + b, (long long)batch};
   const float* vb = values + (long long)b * bstride;
@@ -69,7 +69,7 @@ size_t solve_workspace_bytes(const Pattern& pat, int batch) {
 }
 
 int launch_factor(const Pattern& pat, const float* values, long long ldv, int bstride, float* lx,
-                  float* d, float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream) {
+                  float* d, float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream, const int* only) {
   if (batch <= 0) return WMPC_OK;
   const int lanes = smem_lanes_for_rows(pat.n);
   if (lanes >= 32) {
@@ -77,14 +77,18 @@ int launch_factor(const Pattern& pat, const float* values, long long ldv, int bs
     const size_t smem = (size_t)4 * pat.n * threads;
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
+    profile_mark_begin(stream, kProfileFactor);
     factor_kernel<true><<<ceil_div(batch, threads), threads, smem, stream>>>(pat, values, ldv, bstride, lx,
-                                                                             d, dinv, nullptr, batch);
+                                                                             d, dinv, nullptr, batch, only);
+    profile_mark_end(stream, kProfileFactor);
   } else {
     const size_t need = factor_workspace_bytes(pat, batch);
     if (ws == nullptr || ws_bytes < need)
       return fail(WMPC_ERR_WORKSPACE, "factor needs %zu workspace bytes, got %zu", need, ws_bytes);
+    profile_mark_begin(stream, kProfileFactor);
     factor_kernel<false><<<ceil_div(batch, 128), 128, 0, stream>>>(pat, values, ldv, bstride, lx, d, dinv,
-                                                                  static_cast<float*>(ws), batch);
+                                                                  static_cast<float*>(ws), batch, only);
+    profile_mark_end(stream, kProfileFactor);
   }
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;

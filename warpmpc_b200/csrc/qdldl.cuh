@@ -2,6 +2,8 @@
 // kernels (qdldl.cu) and the fused OSQP kernels (osqp.cu).
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace wmpc {
@@ -66,11 +68,26 @@ __device__ __forceinline__ void ldl_solve_permuted(const Pattern& pat, const flo
   }
 }
 
+bool build_solve_tables(int n, const std::vector<int>& lp, const std::vector<int>& li, std::vector<int>* tables,
+                        std::vector<int>* desc);
 size_t factor_workspace_bytes(const Pattern& pat, int batch);
 size_t solve_workspace_bytes(const Pattern& pat, int batch);
+// only (optional, [batch]): factor just the instances marked nonzero
 int launch_factor(const Pattern& pat, const float* values, long long ldv, int bstride, float* lx,
-                  float* d, float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream);
+                  float* d, float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream,
+                  const int* only = nullptr);
 int launch_solve(const Pattern& pat, const float* lx, const float* dinv, int fstride, const float* rhs,
                  float* x, int batch, void* ws, size_t ws_bytes, cudaStream_t stream);
+int launch_solve_stream(const wmpc_plan& plan, const float* lx, const float* dinv, int fstride, const float* rhs,
+                        float* x, int batch, cudaStream_t s, bool* applied);
+// The per-call solve of a plan: the TMA-fed kernel where it applies, else the
+// one-lane-per-instance kernel (same results bit for bit).
+inline int launch_solve_plan(const wmpc_plan& plan, const float* lx, const float* dinv, int fstride,
+                             const float* rhs, float* x, int batch, void* ws, size_t ws_bytes, cudaStream_t stream) {
+  bool applied = false;
+  const int rc = launch_solve_stream(plan, lx, dinv, fstride, rhs, x, batch, stream, &applied);
+  if (rc || applied) return rc;
+  return launch_solve(plan.pat, lx, dinv, fstride, rhs, x, batch, ws, ws_bytes, stream);
+}
 
 }  // namespace wmpc

@@ -158,8 +158,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
                                                   uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t start = global_timer_ns();
+  // suspend for at most 20 us between checks, or the whole limit when shorter
+  const uint32_t hint = limit_ns < 20000ull ? (uint32_t)limit_ns : 20000u;
   for (;;) {
-    if (mbar_try_wait_suspend(bar, parity, 20000u)) return true;
+    if (mbar_try_wait_suspend(bar, parity, hint)) return true;
     if (abort && *abort) return false;
     if (global_timer_ns() - start > limit_ns) return false;
   }
@@ -271,7 +273,13 @@ struct StreamLaunch {
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
 // most CTAs of a fixed-iteration launch of this plan that fit one SM of `device`
 // (within the launch limit: 2 unless WMPC_STREAM_MAX_CTAS allows up to 4)
-int stream_max_ctas(const StreamPlan& sp, int device);
+int stream_max_ctas(const StreamPlan& sp, int device, int limit);
+// the CTAs-per-SM limit of the environment (WMPC_STREAM_CTAS=1: one;
+// WMPC_STREAM_MAX_CTAS: 2 to 4; default 2), fixed per problem at creation
+int stream_ctas_limit_setting();
+// CTAs per SM a fixed-iteration launch of `tiles` tiles of this plan runs
+// with (k only when there are more than k - 1 tiles per SM)
+int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit);
 size_t stream_workspace_floats(const StreamPlan& sp, int batch);
 
 // One class of a streaming launch (host view): its plan, stream buffers and
@@ -288,6 +296,7 @@ struct StreamJobDesc {
   int* iters = nullptr;
   int n_tiles = 0, max_iter = 0, batch = 0, check_every = 0;
   float chg_eps = 0.0f, sigma = 0.0f, alpha = 0.0f, one_minus_alpha = 0.0f;
+  int ctas_limit = 2;  // most CTAs per SM this class's problem allows (a launch takes the smallest)
 };
 
 }  // namespace wmpc

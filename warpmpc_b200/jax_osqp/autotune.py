@@ -11,10 +11,11 @@ representative batch and returns the fastest, checking on the way that every
 candidate's iterates equal the first one's.  Results are cached per pattern
 digest and device name.
 
-The knobs are the library's process-wide schedule settings, so tuning and
-``apply`` set them in the environment of this process: the chunking, offload
-and ring knobs are read when a compiled problem is created, ``ctas`` at every
-solve -- keep ``apply(best)`` around both, or set the knobs for the process.
+The knobs are the library's schedule settings, read from the environment
+when a compiled problem is created (each problem keeps the values it was
+created with), so tuning and ``apply`` set them in the environment of this
+process around the creation; ``compile_osqp(..., schedule=best)`` does the
+same for one problem.
 """
 
 from __future__ import annotations
@@ -40,6 +41,12 @@ KNOBS = {
     # beside the plain one where it lets two CTAs share an SM
     "frontier": "WMPC_STREAM_FRONTIER",
     "frontier_lag": "WMPC_STREAM_FRONTIER_LAG",
+    # most CTAs per SM a fixed-iteration launch may use (2 to 4; capped by
+    # what is resident on an SM: shared memory and registers)
+    "max_ctas": "WMPC_STREAM_MAX_CTAS",
+    # frontier form: rows without L entries copied into their slots from a
+    # per-chunk list instead of being swept as units
+    "frontier_copies": "WMPC_STREAM_FRONTIER_COPIES",
 }
 
 DEFAULT_CANDIDATES = (

@@ -290,8 +290,8 @@ def build_osqp_plan(
     settings = OSQPSettings() if settings is None else settings
     if settings.scaling < 0:
         raise ValueError("settings.scaling must be nonnegative")
-    if settings.adaptive_rho:
-        raise NotImplementedError("the fixed-pattern OSQP solver expects adaptive_rho=False")
+    if settings.adaptive_rho and (settings.adaptive_rho_interval < 1 or settings.adaptive_rho_tolerance < 1.0):
+        raise ValueError("adaptive_rho needs adaptive_rho_interval >= 1 and adaptive_rho_tolerance >= 1")
     if settings.polishing:
         raise NotImplementedError("the fixed-pattern OSQP solver expects polishing=False")
 

@@ -79,13 +79,15 @@ class DeviceOSQP:
             "scaling_einv": native.f32(plan.scaling_einv),
             "y_scale": native.f32(plan.y_scale),
             "y_unscale": native.f32(plan.y_unscale),
+            "rho_type": native.i32(plan.constr_type),
+            "rho_to_kkt": native.i32(plan.rho_to_kkt),
         }
         kw = {}
         for k, v in keep.items():
             kw[k] = native.ptr_f32(v) if v.dtype == np.float32 else native.ptr_i32(v)
         desc = native.OsqpDesc(
             n=plan.n, m=plan.m, nnz_p=plan.nnz_p, nnz_a=plan.nnz_a, nnz_kkt=plan.nnz_kkt,
-            sigma=np.float32(s.sigma), alpha=np.float32(s.alpha),
+            sigma=np.float32(s.sigma), alpha=np.float32(s.alpha), rho=np.float32(s.rho),
             nnz_p_full=int(plan.p_full_rows.size), **kw,
         )
         handle = ctypes.c_void_p()
@@ -110,17 +112,23 @@ _MODES = {"plain": native.WMPC_OSQP_PLAIN, "persistent": native.WMPC_OSQP_PERSIS
 
 
 class OSQPEngine:
-    """Host-side driver of ``wmpc_osqp_factor`` / ``wmpc_osqp_solve``."""
+    """Host-side driver of ``wmpc_osqp_factor`` / ``wmpc_osqp_solve``.
+
+    A plan with ``settings.adaptive_rho`` runs the per-call ("plain")
+    kernels whatever ``mode`` asks: the persistent kernels keep one rho
+    vector per pattern, rho adaptation needs one per instance."""
 
     def __init__(self, plan: FixedOSQPPlan, device=None, mode: str = "persistent", kkt_plan: DevicePlan | None = None):
         if mode not in _MODES:
             raise ValueError(f"unknown mode {mode!r}; expected one of {sorted(_MODES)}")
         self.plan = plan
-        self.mode = mode
+        self.mode = "plain" if plan.settings.adaptive_rho else mode
         self.dev = DeviceOSQP(plan, device, kkt_plan=kkt_plan)
         self.device = self.dev.torch_device
         self.last_iters = None
         self.last_status = None
+        self.last_rho = None
+        self.last_rho_updates = None
 
     def stream_info(self) -> dict:
         """The streaming schedule this problem carries: ``streaming`` (persistent
@@ -221,6 +229,8 @@ class OSQPEngine:
             max_iter=int(s.max_iter if max_iter is None else max_iter),
             check_termination=int(s.check_termination if check_termination is None else check_termination),
             eps_abs=np.float32(s.eps_abs), eps_rel=np.float32(s.eps_rel), warm_start=1 if warm is not None else 0,
+            adaptive_rho_interval=int(s.adaptive_rho_interval) if s.adaptive_rho else 0,
+            adaptive_rho_tolerance=np.float32(s.adaptive_rho_tolerance),
         )
         return data, opts, keep, (x, z, y, prim, dual, obj, iters, status), batch
 
@@ -258,6 +268,14 @@ class OSQPEngine:
             ws, wsb = _workspace(lib.wmpc_osqp_adjoint_workspace_bytes(self.dev.handle, batch, mode_id), dev)
         else:
             ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext), dev)
+        if pl.settings.adaptive_rho:
+            # each instance's final rho and number of rho changes (refactorizations)
+            import torch
+
+            rho_out = torch.empty(batch, dtype=torch.float32, device=dev)
+            upd_out = torch.empty(batch, dtype=torch.int32, device=dev)
+            data.rho, data.rho_updates = rho_out.data_ptr(), upd_out.data_ptr()
+            self.last_rho, self.last_rho_updates = rho_out, upd_out
         native.check(lib.wmpc_osqp_solve(self.dev.handle, ctypes.byref(opts), ctypes.byref(data), lx_p, dinv_p, fb,
                                          mode_id, native.tensor_ptr(ws), wsb, native.current_stream_handle(dev)))
         self.last_iters = iters
@@ -458,6 +476,7 @@ def compile_osqp(
     mode: str = "persistent",
     device=None,
     adjoint_iters: int | None = None,
+    schedule: dict | None = None,
 ) -> CompiledOSQP:
     """Compile fixed-pattern batched OSQP iterations (solver.py:685-1492).
 
@@ -466,10 +485,24 @@ def compile_osqp(
     adjoint that re-uses the forward factor; ``adjoint_iters`` sets its ADMM
     iterations (default ``settings.max_iter``).  ``derivative_refinement_iters``
     is accepted for signature compatibility (the reference's refinement of a
-    separately factored adjoint system does not exist here).
+    separately factored adjoint system does not exist here).  ``schedule``:
+    streaming-schedule knobs for this problem (``autotune.KNOBS`` names, e.g.
+    the ``best`` of ``autotune_stream``), fixed when the problem is created.
     """
 
     import torch
+
+    if schedule:
+        from .autotune import apply
+
+        with apply(schedule):
+            return compile_osqp(plan, dtype, qdldl_backend=qdldl_backend, qdldl_factor_backend=qdldl_factor_backend,
+                                qdldl_solve_backend=qdldl_solve_backend, transpose_work=transpose_work,
+                                segmented=segmented, segment_budget=segment_budget, segment_strategy=segment_strategy,
+                                level_scheduled_solve=level_scheduled_solve,
+                                level_scheduled_solve_threshold=level_scheduled_solve_threshold,
+                                derivatives=derivatives, derivative_refinement_iters=derivative_refinement_iters,
+                                mode=mode, device=device, adjoint_iters=adjoint_iters)
 
     qdldl = compile_qdldl_variant(
         plan.qdldl_plan,

@@ -81,6 +81,12 @@ class OSQPSettings:
     check_termination: int = 0
     warm_starting: bool = False
     polishing: bool = False
+    # rho adaptation (no counterpart in the reference, which rejects
+    # adaptive_rho): with adaptive_rho, every adaptive_rho_interval iterations
+    # each instance re-estimates rho from its scaled residuals and refactors
+    # when the estimate is more than adaptive_rho_tolerance times away
+    adaptive_rho_interval: int = 25
+    adaptive_rho_tolerance: float = 5.0
 
 
 class OSQPWarmStart(NamedTuple):

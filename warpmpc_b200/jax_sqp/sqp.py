@@ -78,20 +78,21 @@ class SparseMPCSQP:
         r = self.values.assemble(self.values.pack(self.evaluate(z, params, True)))
         return r.cost, r.g, r.constraint_l, r.constraint_u
 
-    def solve_qp(self, z, params, warm) -> SQPSolveResult:
-        """_solve_qp_with_state_jit (sparse_mpc.py:954-976): the QP at z, warm-started."""
+    def solve_qp(self, z, params, warm, keep_factor: bool = False) -> SQPSolveResult:
+        """_solve_qp_with_state_jit (sparse_mpc.py:954-976): the QP at z, warm-started.
+        keep_factor: the QP engine keeps the factorization for an adjoint."""
         lin = self.linearize(z, params)
         x, qz, qy, prim, dual, obj = self.qp.engine.solve(lin.p_values, lin.a_values, lin.q, lin.l, lin.u,
-                                                          warm=warm)
+                                                          warm=warm, keep_factor=keep_factor)
         return SQPSolveResult(x, qz, qy, prim, dual, obj, lin)
 
-    def line_search_step(self, z, params, warm) -> SQPLineSearchStepResult:
+    def line_search_step(self, z, params, warm, keep_factor: bool = False) -> SQPLineSearchStepResult:
         """_line_search_step_with_state_jit (sparse_mpc.py:997-1053)."""
         import torch
 
         from .line_search import constraint_violation
 
-        solve = self.solve_qp(z, params, warm)
+        solve = self.solve_qp(z, params, warm, keep_factor)
         d = solve.direction
         costs, viols = [], []
         for step in self._steps_host:

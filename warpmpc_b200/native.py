@@ -31,6 +31,7 @@ STATUS_MAX_ITER = 0
 STATUS_SOLVED = 1
 STATUS_NONFINITE = 2
 STATUS_ZERO_PIVOT = 4
+STATUS_KERNEL_ABORT = 8
 
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -55,6 +56,12 @@ class PatternDesc(ctypes.Structure):
         ("p", _i32p),
         ("pinv", _i32p),
     ]
+
+
+class QuadrotorModel(ctypes.Structure):
+    """wmpc_quadrotor_model: the rigid-body model's constants."""
+
+    _fields_ = [(k, ctypes.c_float) for k in ("mass", "jx", "jy", "jz", "arm", "yaw_coef", "gravity")]
 
 
 class OsqpDesc(ctypes.Structure):
@@ -87,6 +94,9 @@ class OsqpDesc(ctypes.Structure):
         ("scaling_einv", _f32p),
         ("y_scale", _f32p),
         ("y_unscale", _f32p),
+        ("rho_type", _i32p),
+        ("rho_to_kkt", _i32p),
+        ("rho", ctypes.c_float),
     ]
 
 
@@ -98,6 +108,8 @@ class OsqpOptions(ctypes.Structure):
         ("eps_rel", ctypes.c_float),
         ("warm_start", ctypes.c_int32),
         ("reuse_factor", ctypes.c_int32),
+        ("adaptive_rho_interval", ctypes.c_int32),
+        ("adaptive_rho_tolerance", ctypes.c_float),
     ]
 
 
@@ -145,6 +157,8 @@ class OsqpBatch(ctypes.Structure):
         ("obj", ctypes.c_void_p),
         ("iters", ctypes.c_void_p),
         ("status", ctypes.c_void_p),
+        ("rho", ctypes.c_void_p),
+        ("rho_updates", ctypes.c_void_p),
     ]
 
 
@@ -246,6 +260,12 @@ SIGNATURES = {
         [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(OsqpOptions), ctypes.POINTER(OsqpBatch), ctypes.c_int32,
          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p],
     ),
+    "wmpc_quadrotor_rk4": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                          ctypes.c_int32, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
+    "wmpc_quadrotor_jac_pattern": (ctypes.c_int, [_i32p, _i32p]),
+    "wmpc_solve_tables_host": (ctypes.c_int, [ctypes.POINTER(PatternDesc), _i32p, ctypes.c_int64,
+                                              ctypes.POINTER(ctypes.c_int64)]),
     "wmpc_stream_schedule_host": (
         ctypes.c_int,
         [ctypes.POINTER(PatternDesc), _f32p, _f32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
@@ -275,6 +295,8 @@ SIGNATURES = {
         [ctypes.POINTER(SqpAssembleDims)] + [ctypes.c_void_p] * 14 + [ctypes.c_void_p],
     ),
     "wmpc_profile_begin": (ctypes.c_int, []),
+    "wmpc_profile_select": (ctypes.c_int, [ctypes.c_int32]),
+    "wmpc_stream_last_launch": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "wmpc_profile_end": (ctypes.c_int, [ctypes.POINTER(ctypes.c_float), _i32p, ctypes.POINTER(ctypes.c_int64)]),
     "wmpc_launch_count": (ctypes.c_int64, []),
     "wmpc_last_error_string": (ctypes.c_char_p, []),
@@ -383,7 +405,14 @@ def env_flag(name: str, default: str = "0") -> bool:
     return os.environ.get(name, default) not in ("0", "", "false", "False")
 
 
-def profile_begin() -> None:
+PROFILE_DOMINANT = 0
+PROFILE_FACTOR = 1
+
+
+def profile_begin(channel: int = PROFILE_DOMINANT) -> None:
+    """Start timing the launches of one channel: the dominant kernel (0) or
+    the factorization kernels (1)."""
+    check(lib().wmpc_profile_select(channel))
     check(lib().wmpc_profile_begin())
 
 
@@ -393,4 +422,13 @@ def profile_end() -> tuple[float, int, int]:
     n = ctypes.c_int32()
     total = ctypes.c_int64()
     check(lib().wmpc_profile_end(ctypes.byref(ms), ctypes.byref(n), ctypes.byref(total)))
+    check(lib().wmpc_profile_select(PROFILE_DOMINANT))
     return float(ms.value), int(n.value), int(total.value)
+
+
+def stream_last_launch() -> dict:
+    """The last streaming ADMM launch: schedule form, CTAs per SM, grid, shared memory."""
+    info = (ctypes.c_int32 * 4)()
+    check(lib().wmpc_stream_last_launch(info))
+    return {"form": {0: None, 1: "plain", 2: "frontier"}.get(int(info[0])), "ctas_per_sm": int(info[1]),
+            "grid": int(info[2]), "smem_bytes": int(info[3])}

@@ -40,6 +40,20 @@ def _pattern_desc(qp):
     return desc, arrays, rg
 
 
+def solve_tables(qdldl_plan) -> dict:
+    """Chunk tables of the TMA-fed per-call solve for a QDLDL plan
+    (``wmpc_solve_tables_host``): ``tables`` (int32 words) and ``desc``
+    (n_chunks x 8: table word offset, words, e0, c0, entries, columns, 0, 0)."""
+    desc, keep, _ = _pattern_desc(qdldl_plan)
+    lib = native.lib()
+    words = ctypes.c_int64()
+    native.check(lib.wmpc_solve_tables_host(ctypes.byref(desc), None, 0, ctypes.byref(words)))
+    buf = np.empty(words.value, dtype=np.int32)
+    native.check(lib.wmpc_solve_tables_host(ctypes.byref(desc), native.ptr_i32(buf), buf.size, ctypes.byref(words)))
+    n_chunks, tw = int(buf[0]), int(buf[1])
+    return {"tables": buf[2 : 2 + tw].copy(), "desc": buf[2 + tw : 2 + tw + 8 * n_chunks].reshape(n_chunks, 8).copy()}
+
+
 def stream_schedule(plan, targets=DEFAULT_TARGETS) -> dict:
     """Schedule of an OSQP plan (rho per constraint) as NumPy arrays.
 
