@@ -822,23 +822,52 @@ def main():
     # ---- plain per-call drop-in ------------------------------------------------------
     plain_res = None
     if plain is not None:
+        # the same closed loop, continued from the persistent loop's current states
         pe = plain.engine
         pout = [t.clone() for t in out]
         pwarm = (pout[0], pout[1], pout[2])
-        pe.solve(P, A, Q, L, U, warm=pwarm, out=pout)
+        PL, PU = L.clone(), U.clone()
+        ploop = problems.ClosedLoop(cls, problems.draw_params(cls, args.batch, seed), device=dev)
+        ploop.x0.copy_(loop.x0)
+
+        def pstep():
+            pe.solve(P, A, Q, PL, PU, warm=pwarm, out=pout)
+            ploop.advance(pout[0], PL, PU)
+
+        pstep()
         torch.cuda.synchronize()
         barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         psteps = max(1, min(args.steps, 5))
         e0.record()
         for _ in range(psteps):
-            pe.solve(P, A, Q, L, U, warm=pwarm, out=pout)
+            pstep()
         e1.record()
         torch.cuda.synchronize()
         pms = max_over_ranks(e0.elapsed_time(e1) / psteps, world)
         pfrac = float(np.mean((pout[3].cpu().numpy() <= RES_TOL) & (pout[4].cpu().numpy() <= RES_TOL)))
-        plain_res = {"value": multirank.sum_over_ranks(pfrac * B, multirank.rank_env(), dev) / (pms * 1e-3), "ms_per_step": pms, "converged_fraction": pfrac,
-                     "steps": psteps}
+        # the per-call kernels of one plain step, each timed by the library's event pairs
+        native.profile_begin(native.PROFILE_DOMINANT)
+        pstep()
+        s_ms, s_n, _ = native.profile_end()
+        native.profile_begin(native.PROFILE_FACTOR)
+        pstep()
+        f_ms, f_n, _ = native.profile_end()
+        qp = plan.qdldl_plan
+        solve_bytes = 4 * (2 * qp.nnz_l + 3 * qp.n) * B
+        solve_ms = s_ms / max(s_n, 1)
+        fac_ms = f_ms / max(f_n, 1)
+        plain_res = {"value": multirank.sum_over_ranks(pfrac * B, multirank.rank_env(), dev) / (pms * 1e-3),
+                     "ms_per_step": pms, "converged_fraction": pfrac, "steps": psteps,
+                     "solve_kernel": {"ms_per_launch": solve_ms, "launches_per_step": s_n,
+                                      "bytes_per_launch": solve_bytes,
+                                      "bytes_rule": "4 (2 nnz(L) + 3 n) per instance (L twice, D^-1, rhs in, x out)",
+                                      "achieved_gbs": solve_bytes / (solve_ms * 1e-3) / 1e9,
+                                      "frac": solve_bytes / (solve_ms * 1e-3) / 1e9 / roofline["peak"]},
+                     "factor_kernel": {"ms_per_launch": fac_ms, "launches_per_step": f_n,
+                                       "bytes_per_launch": fac_b * B, "bytes_rule": "4 (nnz(KKT) + nnz(L) + 2 n)",
+                                       "achieved_gbs": fac_b * B / (fac_ms * 1e-3) / 1e9 if f_n else None,
+                                       "frac": (fac_b * B / (fac_ms * 1e-3) / 1e9 / roofline["peak"]) if f_n else None}}
 
     # ---- end to end through the public API with pinned host buffers --------------------
     e2e = None

@@ -87,3 +87,59 @@ def test_solve_stream_replay_matches_oracle(cls):
         want = qdldl_ref.solve(qp, lx, dinv, rhs)[:, 0]
         got = replay(qp, tab, lx[:, 0], dinv[:, 0], rhs[:, 0])
         np.testing.assert_array_equal(got, want)
+
+
+def replay_factor(qp, sched, kkt):
+    """The staged per-call factorization (factor_rows_kernel) for one
+    instance: compact accumulator slots from the library's tables, L re-reads
+    by position lp[c] + q, float32 in the kernel's order."""
+    rg = sched["ragged"]
+    pp, ip = np.asarray(rg["proc_ptr"]), np.asarray(rg["init_ptr"])
+    pcols, poff, plidx = np.asarray(rg["proc_cols"]), np.asarray(rg["proc_offsets"]), np.asarray(rg["proc_lidx"])
+    init_pos = np.asarray(rg["init_pos"])
+    init_slot, upd_ptr, upd_slot = (np.asarray(sched[k]) for k in ("init_slot", "upd_ptr", "upd_slot"))
+    n, f32 = qp.n, np.float32
+    lx = np.full(qp.nnz_l, np.nan, dtype=f32)
+    dinv = np.full(n, np.nan, dtype=f32)
+    d = np.zeros(n, dtype=f32)
+    for k in range(n):
+        p0, p1, i0, i1 = pp[k], pp[k + 1], ip[k], ip[k + 1]
+        ys = np.zeros(p1 - p0, dtype=f32)
+        dk = f32(kkt[qp.perm_to_orig[qp.diag_pos[k]]])
+        for e in range(i0, i1):
+            s = init_slot[e]
+            assert 0 <= s < p1 - p0
+            ys[s] = f32(ys[s] + f32(kkt[qp.perm_to_orig[init_pos[e]]]))
+        u = upd_ptr[p0]
+        for e in range(p0, p1):
+            c = pcols[e]
+            val = ys[e - p0]
+            for q in range(poff[e]):
+                lid = qp.lp[c] + q
+                assert lid < qp.lp[c + 1] and not np.isnan(lx[lid])  # written by an earlier row
+                ys[upd_slot[u]] = f32(ys[upd_slot[u]] - f32(lx[lid] * val))
+                u += 1
+            assert not np.isnan(dinv[c])
+            lval = f32(val * dinv[c])
+            lx[plidx[e]] = lval
+            dk = f32(dk - f32(val * lval))
+        assert u == upd_ptr[p1]
+        d[k] = dk
+        dinv[k] = f32(f32(1.0) / dk)
+    return lx, d, dinv
+
+
+@pytest.mark.parametrize("cls", [problems.SMALL, problems.QUADROTOR], ids=lambda c: c.name)
+def test_staged_factor_replay_matches_oracle(cls):
+    from oracle import osqp_ref
+
+    b = problems.make_batch(cls, 1, seed=23)
+    plan = problems.make_plan(b)
+    qp = plan.qdldl_plan
+    sched = schedule.stream_schedule(plan)
+    kkt = osqp_ref.assemble_kkt_values(plan, b.p_values, b.a_values)[0].astype(np.float32)
+    lx, d, dinv = replay_factor(qp, sched, kkt)
+    lx_o, d_o, dinv_o = qdldl_ref.factor(qp, kkt[:, None])
+    np.testing.assert_array_equal(lx, lx_o[:, 0])
+    np.testing.assert_array_equal(d, d_o[:, 0])
+    np.testing.assert_array_equal(dinv, dinv_o[:, 0])

@@ -84,7 +84,7 @@ size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, in
 size_t osqp_adjoint_extra_bytes(const Osqp& o, int batch);
 int osqp_adjoint(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_adjoint_batch& a, int mode,
                  void* ws, size_t ws_bytes, cudaStream_t s);
-int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
+int osqp_factor(const Osqp& o, const wmpc_plan& plan, const float* p_values, int pb, const float* a_values, int ab,
                 float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s);
 int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
                const float* lx_ext, const float* dinv_ext, int fb_ext, int mode, void* ws, size_t ws_bytes,
@@ -442,6 +442,39 @@ int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out)
   pk.add(desc->li, nnz_l, &pat.li);
   pk.add(desc->p, n, &pat.p);
   pk.add(desc->pinv, n, &pat.pinv);
+  // compact-accumulator tables of the staged per-call factorization
+  std::vector<int> fac_init_slot, fac_upd_ptr, fac_upd_slot, fac_upd_lidx;
+  {
+    HostPattern hp;
+    hp.n = n;
+    hp.nnz_a = nnz_a;
+    hp.nnz_l = nnz_l;
+    hp.init_ptr.assign(desc->init_ptr, desc->init_ptr + n + 1);
+    hp.init_rows.assign(desc->init_rows, desc->init_rows + n_init);
+    hp.proc_ptr.assign(desc->proc_ptr, desc->proc_ptr + n + 1);
+    hp.proc_cols.assign(desc->proc_cols, desc->proc_cols + nnz_l);
+    hp.proc_offsets.assign(desc->proc_offsets, desc->proc_offsets + nnz_l);
+    hp.proc_lidx.assign(desc->proc_lidx, desc->proc_lidx + nnz_l);
+    hp.lp.assign(desc->lp, desc->lp + n + 1);
+    hp.li.assign(desc->li, desc->li + nnz_l);
+    std::vector<unsigned short> slot16;
+    std::string why;
+    int max_row = 0;
+    if (nnz_l > 0 && build_factor_tables(hp, &fac_init_slot, &fac_upd_ptr, &slot16, &max_row, &why)) {
+      fac_upd_slot.assign(slot16.begin(), slot16.end());
+      for (int k = 0; k < n; ++k)
+        for (int e = hp.proc_ptr[k]; e < hp.proc_ptr[k + 1]; ++e)
+          for (int q = 0; q < hp.proc_offsets[e]; ++q) fac_upd_lidx.push_back(hp.lp[hp.proc_cols[e]] + q);
+      int max_kv = 0;
+      for (int k = 0; k < n; ++k) max_kv = std::max(max_kv, 1 + hp.init_ptr[k + 1] - hp.init_ptr[k]);
+      pk.add(fac_init_slot.data(), fac_init_slot.size(), &plan->fac_init_slot);
+      pk.add(fac_upd_ptr.data(), fac_upd_ptr.size(), &plan->fac_upd_ptr);
+      pk.add(fac_upd_slot.data(), fac_upd_slot.size(), &plan->fac_upd_slot);
+      pk.add(fac_upd_lidx.data(), fac_upd_lidx.size(), &plan->fac_upd_lidx);
+      plan->fac_max_row = std::max(max_row, 1);
+      plan->fac_max_kv = max_kv;
+    }
+  }
   // chunk tables of the TMA-fed per-call solve (when every column fits a chunk)
   std::vector<int> solve_tables, solve_desc;
   if (nnz_l > 0 && build_solve_tables(n, std::vector<int>(desc->lp, desc->lp + n + 1),
@@ -506,7 +539,7 @@ int wmpc_factor(const wmpc_plan* plan, const float* values, int64_t values_ld, i
     return fail(WMPC_ERR_INVALID_ARGUMENT, "values_ld/values_bstride inconsistent with batch");
   DeviceGuard guard(plan->device);
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", plan->device);
-  return launch_factor(plan->pat, values, values_ld, values_bstride, lx, d, dinv, batch, workspace,
+  return launch_factor_plan(*plan, values, values_ld, values_bstride, lx, d, dinv, batch, workspace,
                        workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
@@ -774,7 +807,7 @@ int wmpc_osqp_factor(const wmpc_osqp* osqp, const float* p_values, int32_t p_bat
     return fail(WMPC_ERR_INVALID_ARGUMENT, "p_batch/a_batch must be positive and equal unless one is 1");
   DeviceGuard guard(osqp->device);
   if (!guard.ok) return fail(WMPC_ERR_CUDA, "cannot select device %d", osqp->device);
-  return osqp_factor(osqp->dev, osqp->kkt_plan->pat, p_values, p_batch, a_values, a_batch, lx, d, dinv, workspace,
+  return osqp_factor(osqp->dev, *osqp->kkt_plan, p_values, p_batch, a_values, a_batch, lx, d, dinv, workspace,
                      workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 

@@ -114,6 +114,15 @@ struct wmpc_plan {
   const int* solve_tables = nullptr;
   const int* solve_desc = nullptr;  // two int4 per chunk
   int solve_chunks = 0;
+  // compact-accumulator tables of the staged per-call factorization (null:
+  // the one-lane kernel factors): slot of each initial entry in its row's
+  // reach, per program entry its range of updates, per update its target
+  // slot and the L entry it re-reads
+  const int* fac_init_slot = nullptr;
+  const int* fac_upd_ptr = nullptr;
+  const int* fac_upd_slot = nullptr;
+  const int* fac_upd_lidx = nullptr;
+  int fac_max_row = 0, fac_max_kv = 0;
   // host copies of the ragged program (inputs of the streaming schedule)
   std::vector<int> h_init_ptr, h_init_rows, h_proc_ptr, h_proc_cols, h_proc_offsets, h_proc_lidx, h_lp, h_li, h_p;
 };

@@ -655,14 +655,14 @@ Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int m
   return L;
 }
 
-int assemble_and_factor(const Osqp& o, const Pattern& pat, const float* pT, int pb, const float* aT, int ab,
+int assemble_and_factor(const Osqp& o, const wmpc_plan& plan, const float* pT, int pb, const float* aT, int ab,
                         float* kkt, float* lx, float* d, float* dinv, void* scratch, size_t scratch_bytes,
                         cudaStream_t s) {
   const int kb = pb > ab ? pb : ab;
   dim3 grid(ceil_div(kb, 128), o.nnz_kkt < 4096 ? o.nnz_kkt : 4096);
   assemble_kkt_kernel<<<grid, 128, 0, s>>>(o, pT, pb, pb > 1 ? 1 : 0, aT, ab, ab > 1 ? 1 : 0, kkt, kb);
   WMPC_LAUNCH_CHECK();
-  return launch_factor(pat, kkt, kb, 1, lx, d, dinv, kb, scratch, scratch_bytes, s);
+  return launch_factor_plan(plan, kkt, kb, 1, lx, d, dinv, kb, scratch, scratch_bytes, s);
 }
 
 }  // namespace
@@ -699,8 +699,9 @@ size_t osqp_factor_workspace_bytes(const Osqp& o, const Pattern& pat, int pb, in
   return c.used;
 }
 
-int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb, const float* a_values, int ab,
+int osqp_factor(const Osqp& o, const wmpc_plan& plan, const float* p_values, int pb, const float* a_values, int ab,
                 float* lx, float* d, float* dinv, void* ws, size_t ws_bytes, cudaStream_t s) {
+  const Pattern& pat = plan.pat;
   const int kb = pb > ab ? pb : ab;
   const size_t need = osqp_factor_workspace_bytes(o, pat, pb, ab);
   if (ws == nullptr || ws_bytes < need)
@@ -714,7 +715,7 @@ int osqp_factor(const Osqp& o, const Pattern& pat, const float* p_values, int pb
   int rc;
   if ((rc = transpose_in(p_values, o.nnz_p, pb, o.nnz_p, nullptr, pT, pb, s))) return rc;
   if ((rc = transpose_in(a_values, o.nnz_a, ab, o.nnz_a, nullptr, aT, ab, s))) return rc;
-  return assemble_and_factor(o, pat, pT, pb, aT, ab, kkt, lx, d, dinv, scratch, f, s);
+  return assemble_and_factor(o, plan, pT, pb, aT, ab, kkt, lx, d, dinv, scratch, f, s);
 }
 
 namespace {
@@ -858,13 +859,15 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
     WMPC_LAUNCH_CHECK();
     assemble_kkt_rho_kernel<<<kgrid, 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, L.rinv_row, nullptr, L.kkt, B);
     WMPC_LAUNCH_CHECK();
-    if ((rc = launch_factor(pat, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s))) return rc;
+    if ((rc = launch_factor_plan(*q.kkt_plan, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s)))
+      return rc;
     lx = L.lx;
     dinv = L.dinv;
     fb = B;
   } else if (!external && L.factor_separately) {
     if (!opt.reuse_factor &&
-        (rc = assemble_and_factor(o, pat, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch, L.scratch_bytes, s)))
+        (rc = assemble_and_factor(o, *q.kkt_plan, L.pT, pb, L.aT, ab, L.kkt, L.lx, L.d, L.dinv, L.scratch,
+                                  L.scratch_bytes, s)))
       return rc;
     lx = L.lx;
     dinv = L.dinv;
@@ -895,7 +898,7 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
         assemble_kkt_rho_kernel<<<kgrid, 128, 0, s>>>(o, L.pT, ldp, sbp, L.aT, lda, sba, L.rinv_row, L.rho_changed,
                                                       L.kkt, B);
         WMPC_LAUNCH_CHECK();
-        if ((rc = launch_factor(pat, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s,
+        if ((rc = launch_factor_plan(*q.kkt_plan, L.kkt, B, 1, L.lx, L.d, L.dinv, B, L.scratch, L.scratch_bytes, s,
                                 L.rho_changed)))
           return rc;
         admm_first_rhs_kernel<<<egrid, 128, 0, s>>>(o, st, L.rhs, B, rr);

@@ -47,16 +47,6 @@ __host__ __device__ inline int factor_warp_words(const StreamPlan& sp, int lbatc
   return (2 * r + lbatch + sp.max_row_kv) * 32 + lbatch + 3 * r;
 }
 
-// KKT value of original slot idx from its staged raw input: the base value
-// (src < 0), P entry src scaled plus sigma on the diagonal, or A entry
-// src - nnz_p scaled (solver.py:764-776).
-__device__ __forceinline__ float staged_kkt_value(const Osqp& o, int idx, float raw) {
-  const int src = __ldg(o.kkt_src + idx);
-  if (src < 0) return __ldg(o.kkt_base + idx);
-  if (src < o.nnz_p) return raw * __ldg(o.p_scale + src) + __ldg(o.p_diag_sigma + src);
-  return raw * __ldg(o.a_scale + (src - o.nnz_p));
-}
-
 __device__ __forceinline__ int row_kkt_index(const Pattern& pat, int k, int i0, int j) {
   return __ldg(pat.perm_to_orig + (j == 0 ? __ldg(pat.diag_pos + k) : __ldg(pat.init_pos + i0 + j - 1)));
 }
@@ -68,12 +58,58 @@ __device__ __forceinline__ int row_kkt_index(const Pattern& pat, int k, int i0, 
 // the row's own arithmetic, so each row first stages them into shared memory
 // with asynchronous copies (one round trip per `lbatch` L entries), then
 // runs the program on shared memory.
-// Stage the L re-reads of updates [ub, ue): values per lane, slots warp-shared
-// (copied by all lanes in turn).
+// Index words are read by the 32 lanes in parallel (one word each, 32 at a
+// time) and broadcast with shuffles: a uniform load per word would put one
+// L2 round trip per word on the row's critical path (the tables do not stay
+// in the L1 left beside the shared memory).
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// Stage the L re-reads of updates [ub, ue): values per lane (each lane its
+// own instance's entry), slots warp-shared.
 __device__ __forceinline__ void stage_updates(const StreamPlan& sp, const float* Lu, float* lst, int* slot_w, int lane,
                                               int ub, int ue) {
-  for (int u = ub; u < ue; ++u) cp_async4(lst + (u - ub) * 32, Lu + __ldg(sp.upd_pos + u));
-  for (int u = ub + lane; u < ue; u += 32) cp_async4(slot_w + (u - ub), sp.upd_slot + u);
+  for (int base = ub; base < ue; base += 32) {
+    const int u = base + lane;
+    const int pos = u < ue ? __ldg(sp.upd_pos + u) : 0;
+    if (u < ue) cp_async4(slot_w + (u - ub), sp.upd_slot + u);
+    const int cnt = ue - base < 32 ? ue - base : 32;
+    for (int j = 0; j < cnt; ++j) cp_async4(lst + (base + j - ub) * 32, Lu + __shfl_sync(kFullMask, pos, j));
+  }
+}
+
+// How KKT input j of row k (original slot idx) is formed from its staged raw
+// input (solver.py:764-776): kind 0 the base value `add`, 1 a P entry
+// raw * p_scale + sigma-on-the-diagonal (`add`), 2 an A entry raw * a_scale;
+// src the P/A entry (-1: base).
+struct KktInput {
+  int kind, src;
+  float scale, add;
+};
+
+__device__ __forceinline__ KktInput kkt_input(const Osqp& o, const Pattern& pat, int k, int i0, int j) {
+  const int idx = row_kkt_index(pat, k, i0, j);
+  KktInput r;
+  r.src = __ldg(o.kkt_src + idx);
+  if (r.src < 0) {
+    r.kind = 0;
+    r.scale = 0.0f;
+    r.add = __ldg(o.kkt_base + idx);
+  } else if (r.src < o.nnz_p) {
+    r.kind = 1;
+    r.scale = __ldg(o.p_scale + r.src);
+    r.add = __ldg(o.p_diag_sigma + r.src);
+  } else {
+    r.kind = 2;
+    r.scale = __ldg(o.a_scale + (r.src - o.nnz_p));
+    r.add = 0.0f;
+  }
+  return r;
+}
+
+__device__ __forceinline__ float kkt_input_value(int kind, float scale, float add, float raw) {
+  if (kind == 0) return add;
+  if (kind == 1) return raw * scale + add;
+  return raw * scale;
 }
 
 __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
@@ -105,33 +141,77 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
   const float* ain = in.aT + (long long)bb * in.sba;
   const int n = pat.n;
   bool bad = false;
+  // the table pointers of the next row, loaded one row ahead
+  int n_p0 = __ldg(pat.proc_ptr), n_p1 = __ldg(pat.proc_ptr + 1);
+  int n_i0 = __ldg(pat.init_ptr), n_i1 = __ldg(pat.init_ptr + 1);
+  int n_ub = __ldg(sp.upd_ptr + n_p0), n_uend = __ldg(sp.upd_ptr + n_p1), n_doff = __ldg(sp.dinv_off);
   for (int k = 0; k < n; ++k) {
-    const int p0 = __ldg(pat.proc_ptr + k), p1 = __ldg(pat.proc_ptr + k + 1);
-    const int i0 = __ldg(pat.init_ptr + k), i1 = __ldg(pat.init_ptr + k + 1);
-    const int u_end = __ldg(sp.upd_ptr + p1);
-    int ub = __ldg(sp.upd_ptr + p0);
+    const int p0 = n_p0, p1 = n_p1, i0 = n_i0, i1 = n_i1, u_end = n_uend, doff_k = n_doff;
+    int ub = n_ub;
     int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+    const int nkv = 1 + i1 - i0;
     // stage this row's reads: KKT inputs, D^-1 of its steps, step tables, L re-reads
-    for (int j = 0; j < 1 + i1 - i0; ++j) {
-      const int src = __ldg(o.kkt_src + row_kkt_index(pat, k, i0, j));
-      if (src >= 0)
-        cp_async4(kst + j * 32, src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
+    // (lane j resolves KKT input j: its source and how its value is formed)
+    // (inputs past the first 32 are resolved again, 32 at a time, when used)
+    auto input_of = [&](int j) {
+      KktInput r{0, -1, 0.0f, 0.0f};
+      if (j < nkv) r = kkt_input(o, pat, k, i0, j);
+      return r;
+    };
+    const KktInput kin = input_of(lane);
+    for (int base = 0; base < nkv; base += 32) {
+      const KktInput kc = base == 0 ? kin : input_of(base + lane);
+      const int cnt = nkv - base < 32 ? nkv - base : 32;
+      for (int j = 0; j < cnt; ++j) {
+        const int src = __shfl_sync(kFullMask, kc.src, j);
+        if (src >= 0)
+          cp_async4(kst + (base + j) * 32,
+                    src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
+      }
     }
-    for (int e = p0; e < p1; ++e) cp_async4(dst + (e - p0) * 32, Ld + __ldg(sp.step_doff + e));
-    for (int e = p0 + lane; e < p1; e += 32) {
-      cp_async4(off_w + (e - p0), pat.proc_offsets + e);
-      cp_async4(boff_w + (e - p0), sp.proc_boff + e);
-      cp_async4(foff_w + (e - p0), sp.proc_foff + e);
+    for (int base = p0; base < p1; base += 32) {
+      const int e = base + lane;
+      const int doff = e < p1 ? __ldg(sp.step_doff + e) : 0;
+      if (e < p1) {
+        cp_async4(off_w + (e - p0), pat.proc_offsets + e);
+        cp_async4(boff_w + (e - p0), sp.proc_boff + e);
+        cp_async4(foff_w + (e - p0), sp.proc_foff + e);
+      }
+      const int cnt = p1 - base < 32 ? p1 - base : 32;
+      for (int j = 0; j < cnt; ++j) cp_async4(dst + (base + j - p0) * 32, Ld + __shfl_sync(kFullMask, doff, j));
     }
     stage_updates(sp, Lu, lst, slot_w, lane, ub, ue);
+    // the next row's table pointers while the copies are in flight
+    if (k + 1 < n) {
+      n_p0 = p1;
+      n_p1 = __ldg(pat.proc_ptr + k + 2);
+      n_i0 = i1;
+      n_i1 = __ldg(pat.init_ptr + k + 2);
+      n_ub = u_end;
+      n_uend = __ldg(sp.upd_ptr + n_p1);
+      n_doff = __ldg(sp.dinv_off + k + 1);
+    }
     cp_async_wait_all();
     __syncwarp();
-    // the row program
+    // the row program (the reference's order: diagonal input, then the
+    // initial entries in order, then the steps)
     for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
-    float dk = staged_kkt_value(o, row_kkt_index(pat, k, i0, 0), kst[0]);
-    for (int e = i0; e < i1; ++e) {
-      const int s = __ldg(sp.init_slot + e);
-      ys[s * 32] = ys[s * 32] + staged_kkt_value(o, row_kkt_index(pat, k, i0, 1 + e - i0), kst[(1 + e - i0) * 32]);
+    float dk = 0.0f;
+    for (int base = 0; base < nkv; base += 32) {
+      const KktInput kc = base == 0 ? kin : input_of(base + lane);
+      const int jl = base + lane;
+      const int islot = (jl > 0 && jl < nkv) ? __ldg(sp.init_slot + i0 + jl - 1) : 0;
+      const int cnt = nkv - base < 32 ? nkv - base : 32;
+      for (int jj = 0; jj < cnt; ++jj) {
+        const float v = kkt_input_value(__shfl_sync(kFullMask, kc.kind, jj), __shfl_sync(kFullMask, kc.scale, jj),
+                                        __shfl_sync(kFullMask, kc.add, jj), kst[(base + jj) * 32]);
+        const int s = __shfl_sync(kFullMask, islot, jj);
+        if (base + jj == 0) {
+          dk = v;
+        } else {
+          ys[s * 32] = ys[s * 32] + v;
+        }
+      }
     }
     int u = ub;
     for (int e = 0; e < p1 - p0; ++e) {
@@ -157,7 +237,7 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     }
     const float di = 1.0f / dk;
     bad |= !(di != 0.0f) || !isfinite(di);
-    Ld[__ldg(sp.dinv_off + k)] = di;
+    Ld[doff_k] = di;
     __syncwarp();  // the warp-shared tables are restaged by the next row
   }
   for (int i = 0; i < sp.n_pad_b; ++i) Lu[__ldg(sp.pad_boff + i)] = 0.0f;

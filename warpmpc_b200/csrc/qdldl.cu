@@ -14,6 +14,7 @@
 // NumPy-restated order.
 #include "common.cuh"
 #include "qdldl.cuh"
+#include "stream.cuh"
 
 namespace wmpc {
 
@@ -33,6 +34,136 @@ __global__ void __launch_bounds__(256) factor_kernel(Pattern pat, const float* _
   const float* vb = values + (long long)b * bstride;
   auto val_at = [&](int slot) -> float { return vb[(long long)__ldg(pat.perm_to_orig + slot) * ldv]; };
   factor_instance(pat, val_at, y, lx, batch, d, dinv, batch, b);
+}
+
+// Staged factorization: one warp per 32-instance tile, the row's reach kept
+// in a compact accumulator (one shared-memory slot per reach position instead
+// of a dense n-vector), and every value a row reads from memory -- its KKT
+// inputs, D^-1 of its steps' columns, the L entries of those columns above
+// the row -- brought into shared memory with 4-byte asynchronous copies
+// before the row's arithmetic (one round trip per `lbatch` L entries).  The
+// index words behind those copies are read by the 32 lanes in parallel and
+// broadcast with shuffles.  Same operation order as factor_instance (the
+// reference's row program), so the same bits.  Lanes past the batch factor a
+// copy of the last instance; with `only`, lanes of unmarked instances compute
+// and store nothing of theirs.
+struct FactorTables {
+  const int* init_slot;
+  const int* upd_ptr;
+  const int* upd_slot;
+  const int* upd_lidx;
+  int max_row, max_kv;
+};
+
+// per-warp shared memory in 4-byte words: ys, staged D^-1 [max_row] and L
+// re-reads [lbatch] and KKT inputs [max_kv] per lane; update slots [lbatch],
+// step offsets, L positions and columns [3 max_row] shared by the warp
+__host__ __device__ inline int factor_rows_words(int max_row, int max_kv, int lbatch) {
+  return (2 * max_row + lbatch + max_kv) * 32 + lbatch + 3 * max_row;
+}
+
+constexpr unsigned kLanes = 0xffffffffu;
+
+__global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTables ft, const float* __restrict__ values,
+                                                         long long ldv, int bstride, float* lx, float* d, float* dinv,
+                                                         int batch, int n_tiles, int lbatch, const int* only) {
+  extern __shared__ float fsm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tile = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (tile >= n_tiles) return;
+  const int b = tile * 32 + lane;
+  const int bb = b < batch ? b : batch - 1;
+  const bool keep = b < batch && (only == nullptr || only[b] != 0);
+  float* wbase = fsm + (size_t)warp * factor_rows_words(ft.max_row, ft.max_kv, lbatch);
+  float* ys = wbase + lane;
+  float* dst = ys + ft.max_row * 32;
+  float* lst = dst + ft.max_row * 32;
+  float* kst = lst + lbatch * 32;
+  int* slot_w = reinterpret_cast<int*>(wbase + (2 * ft.max_row + lbatch + ft.max_kv) * 32);
+  int* off_w = slot_w + lbatch;
+  int* lid_w = off_w + ft.max_row;
+  const float* vb = values + (long long)bb * bstride;
+  const int n = pat.n;
+  auto stage_updates = [&](int ub, int ue) {
+    for (int base = ub; base < ue; base += 32) {
+      const int u = base + lane;
+      const int lid = u < ue ? __ldg(ft.upd_lidx + u) : 0;
+      if (u < ue) cp_async4(slot_w + (u - ub), ft.upd_slot + u);
+      const int cnt = ue - base < 32 ? ue - base : 32;
+      for (int j = 0; j < cnt; ++j)
+        cp_async4(lst + (base + j - ub) * 32, lx + (long long)__shfl_sync(kLanes, lid, j) * batch + bb);
+    }
+  };
+  for (int k = 0; k < n; ++k) {
+    const int p0 = __ldg(pat.proc_ptr + k), p1 = __ldg(pat.proc_ptr + k + 1);
+    const int i0 = __ldg(pat.init_ptr + k), i1 = __ldg(pat.init_ptr + k + 1);
+    const int u_end = __ldg(ft.upd_ptr + p1);
+    int ub = __ldg(ft.upd_ptr + p0);
+    int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+    const int nkv = 1 + i1 - i0;
+    // KKT inputs (original slot of input j: the diagonal, then the initial entries)
+    auto orig_of = [&](int j) {
+      if (j >= nkv) return 0;
+      return __ldg(pat.perm_to_orig + (j == 0 ? __ldg(pat.diag_pos + k) : __ldg(pat.init_pos + i0 + j - 1)));
+    };
+    for (int base = 0; base < nkv; base += 32) {
+      const int orig = orig_of(base + lane);
+      const int cnt = nkv - base < 32 ? nkv - base : 32;
+      for (int j = 0; j < cnt; ++j)
+        cp_async4(kst + (base + j) * 32, vb + (long long)__shfl_sync(kLanes, orig, j) * ldv);
+    }
+    // D^-1 of the steps' columns, and the step tables
+    for (int base = p0; base < p1; base += 32) {
+      const int e = base + lane;
+      const int col = e < p1 ? __ldg(pat.proc_cols + e) : 0;
+      if (e < p1) {
+        cp_async4(off_w + (e - p0), pat.proc_offsets + e);
+        cp_async4(lid_w + (e - p0), pat.proc_lidx + e);
+      }
+      const int cnt = p1 - base < 32 ? p1 - base : 32;
+      for (int j = 0; j < cnt; ++j)
+        cp_async4(dst + (base + j - p0) * 32, dinv + (long long)__shfl_sync(kLanes, col, j) * batch + bb);
+    }
+    stage_updates(ub, ue);
+    cp_async_wait_all();
+    __syncwarp();
+    for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
+    float dk = kst[0];
+    for (int base = 0; base < nkv - 1; base += 32) {
+      const int e = i0 + base + lane;
+      const int slot = e < i1 ? __ldg(ft.init_slot + e) : 0;
+      const int cnt = nkv - 1 - base < 32 ? nkv - 1 - base : 32;
+      for (int j = 0; j < cnt; ++j) {
+        const int sl = __shfl_sync(kLanes, slot, j);
+        ys[sl * 32] = ys[sl * 32] + kst[(1 + base + j) * 32];
+      }
+    }
+    int u = ub;
+    for (int e = 0; e < p1 - p0; ++e) {
+      const int off = off_w[e];
+      const float val = ys[e * 32];
+      for (int q = 0; q < off; ++q, ++u) {
+        if (u == ue) {  // next batch of this row's L re-reads
+          __syncwarp();
+          ub = ue;
+          ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+          stage_updates(ub, ue);
+          cp_async_wait_all();
+          __syncwarp();
+        }
+        const int su = slot_w[u - ub];
+        ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
+      }
+      const float lval = val * dst[e * 32];
+      if (keep) lx[(long long)lid_w[e] * batch + b] = lval;
+      dk = dk - val * lval;
+    }
+    if (keep) {
+      d[(long long)k * batch + b] = dk;
+      dinv[(long long)k * batch + b] = 1.0f / dk;
+    }
+    __syncwarp();  // the warp-shared tables are restaged by the next row
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -92,6 +223,39 @@ int launch_factor(const Pattern& pat, const float* values, long long ldv, int bs
   }
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
+}
+
+int launch_factor_plan(const wmpc_plan& plan, const float* values, long long ldv, int bstride, float* lx, float* d,
+                       float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream, const int* only) {
+  if (batch <= 0) return WMPC_OK;
+  const Pattern& pat = plan.pat;
+  if (plan.fac_upd_ptr && !env_disabled("WMPC_FACTOR_STAGED_OFF")) {
+    int num_sms = 0;
+    if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, plan.device) != cudaSuccess) {
+      (void)cudaGetLastError();
+      num_sms = 148;
+    }
+    const int warps = 2;
+    const int n_tiles = (batch + 31) / 32;
+    // L-batch sized so that every tile's warp can be resident at once
+    const int per_sm = (n_tiles + num_sms - 1) / num_sms;
+    const int budget = (200 * 1024 / 4) / (per_sm > 0 ? per_sm : 1);
+    int lbatch = (budget - factor_rows_words(plan.fac_max_row, plan.fac_max_kv, 0)) / 33;
+    lbatch = lbatch < 8 ? 8 : (lbatch > 128 ? 128 : lbatch);
+    const size_t smem = (size_t)warps * factor_rows_words(plan.fac_max_row, plan.fac_max_kv, lbatch) * sizeof(float);
+    if (smem <= (size_t)kMaxSmemBytes) {
+      WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const FactorTables ft{plan.fac_init_slot, plan.fac_upd_ptr, plan.fac_upd_slot, plan.fac_upd_lidx,
+                            plan.fac_max_row, plan.fac_max_kv};
+      profile_mark_begin(stream, kProfileFactor);
+      factor_rows_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, stream>>>(pat, ft, values, ldv, bstride, lx, d,
+                                                                               dinv, batch, n_tiles, lbatch, only);
+      profile_mark_end(stream, kProfileFactor);
+      WMPC_LAUNCH_CHECK();
+      return WMPC_OK;
+    }
+  }
+  return launch_factor(pat, values, ldv, bstride, lx, d, dinv, batch, ws, ws_bytes, stream, only);
 }
 
 int launch_solve(const Pattern& pat, const float* lx, const float* dinv, int fstride, const float* rhs,

@@ -76,6 +76,11 @@ size_t solve_workspace_bytes(const Pattern& pat, int batch);
 int launch_factor(const Pattern& pat, const float* values, long long ldv, int bstride, float* lx,
                   float* d, float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream,
                   const int* only = nullptr);
+// The per-call factorization of a plan: the staged kernel where the plan has
+// its tables (and its shared memory fits), else the one-lane kernel (same bits).
+int launch_factor_plan(const wmpc_plan& plan, const float* values, long long ldv, int bstride, float* lx, float* d,
+                       float* dinv, int batch, void* ws, size_t ws_bytes, cudaStream_t stream,
+                       const int* only = nullptr);
 int launch_solve(const Pattern& pat, const float* lx, const float* dinv, int fstride, const float* rhs,
                  float* x, int batch, void* ws, size_t ws_bytes, cudaStream_t stream);
 int launch_solve_stream(const wmpc_plan& plan, const float* lx, const float* dinv, int fstride, const float* rhs,
