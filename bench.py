@@ -65,6 +65,7 @@ def parse_args():
     ap.add_argument("--no-assembly", action="store_true", help="skip the SQP QP assembly timing")
     ap.add_argument("--no-sqp", action="store_true", help="skip the SQP step timing")
     ap.add_argument("--no-sqp4", action="store_true", help="skip the nonlinear quadrotor SQP timing")
+    ap.add_argument("--no-tune", action="store_true", help="library default schedules (no autotuning)")
     ap.add_argument("--sqp4-batch", type=int, default=262144, help="instances of the nonlinear SQP leg")
     return ap.parse_args()
 
@@ -588,15 +589,18 @@ def mixed_timing(args, dev, world):
     classes = problems.MIXED_CLASSES
     per = max(1, args.mixed_batch // len(classes))
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    engines, data = [], []
+    engines, data, schedules = [], [], {}
     for k, cls in enumerate(classes):
         settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 50})
         plan = problems.make_plan(problems.make_batch(cls, 1, seed=4000 + k), settings)
         seed = multirank.instance_seed(4000 + 10 * k, multirank.rank_env().rank)
         b = problems.make_batch(cls, per, seed=seed)
-        comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
+        best, _ = tuned_schedule(args, plan, b, dev, max_instances=per)
+        comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev,
+                            schedule=best)
         engines.append(comp.engine)
         data.append((cls, seed, b))
+        schedules[cls.name] = best
 
     res = {}
     for label, check in (("early_exit", 1), ("fixed50", 0)):
@@ -664,8 +668,33 @@ def mixed_timing(args, dev, world):
                     "(4,2,10) (4,2,40) (12,4,20) (12,4,30), closed MPC loop (state advanced by u0 every step, "
                     "warm-started), <= 50 ADMM iterations, one persistent launch per step, CUDA graph",
         "unit": "solves/s",
+        "schedule_per_class": schedules,
         **res,
     }
+
+
+# schedule candidates the bench's tuner times for each problem (the library
+# defaults first); every candidate must reproduce the first one's iterates
+TUNE_CANDIDATES = ({}, {"frontier_copies": 1}, {"max_ctas": 3}, {"units": 12, "cols": 12, "rel": 10, "funits": 12})
+
+
+def tuned_schedule(args, plan, batch_np, dev, max_instances=32768):
+    """The fastest schedule of this pattern on this device (autotune_stream,
+    timed on up to max_instances of the workload's instances, cached per
+    pattern and device for the process), or {} with --no-tune."""
+    if args.no_tune:
+        return {}, None
+    from warpmpc_b200.jax_osqp.autotune import autotune_stream
+
+    sl = slice(0, min(batch_np.batch, max_instances))
+    try:
+        r = autotune_stream(plan, batch_np.p_values[sl], batch_np.a_values[sl], batch_np.q[sl], batch_np.l[sl],
+                            batch_np.u[sl], candidates=TUNE_CANDIDATES, repeats=2, device=dev,
+                            cache_path=os.path.join("/tmp", "wmpc_bench_tune.json"))
+    except Exception as exc:  # report, do not hide: the defaults run instead
+        print(f"[bench] schedule tuning failed, library defaults used: {exc!r}", file=sys.stderr)
+        return {}, None
+    return r.best, [[c, round(ms, 3)] for c, ms in r.timings_ms]
 
 
 def config_dict(args, cls, plan, batch):
@@ -700,7 +729,9 @@ def main():
     plan = problems.make_plan(b0)
     if world > 1:
         multirank.check_plans_agree(plan, multirank.rank_env(), dev)
-    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
+    schedule, tune_timings = tuned_schedule(args, plan, b, dev)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev,
+                        schedule=schedule)
     plain = None if args.no_plain else compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True,
                                                     mode="plain", device=dev)
     eng = comp.engine
@@ -807,7 +838,7 @@ def main():
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": measured_traffic(args, B, form), "kernel": "admm_stream_kernel", "schedule": form,
         "ctas_per_sm": launch["ctas_per_sm"], "kernel_ms": dom_ms_per_launch, "launches_timed": dom_n,
-        "bytes_per_launch": admm_bytes,
+        "bytes_per_launch": admm_bytes, "tuned_schedule": schedule, "tune_timings_ms": tune_timings,
         "bytes_rule": f"{plan.settings.max_iter} iterations x 4 (2 nnz(L) + n) per instance",
         "peak_source": peak_source,
         "factor": {

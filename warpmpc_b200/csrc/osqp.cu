@@ -1053,14 +1053,14 @@ __global__ void adjoint_matrix_kernel(Osqp o, const int* __restrict__ p_rows, co
                                       const float* __restrict__ y, const float* __restrict__ mu,
                                       const int* __restrict__ tau, float* __restrict__ dp, float* __restrict__ da,
                                       int batch) {
-  const int b = blockIdx.y;
+  const int b = blockIdx.x;  // one instance per x block (batches beyond 65535 instances fit grid x)
   if (b >= batch) return;
   const float* wb = w + (size_t)b * o.n;
   const float* xb = x + (size_t)b * o.n;
   const float* yb = y + (size_t)b * o.m;
   const float* mb = mu + (size_t)b * o.m;
   const int* tb = tau + (size_t)b * o.m;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < o.nnz_p + o.nnz_a; k += gridDim.x * blockDim.x) {
+  for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < o.nnz_p + o.nnz_a; k += gridDim.y * blockDim.x) {
     if (k < o.nnz_p) {
       const int i = __ldg(p_rows + k), j = __ldg(p_cols + k);
       dp[(size_t)b * o.nnz_p + k] = 0.5f * (wb[i] * xb[j] + wb[j] * xb[i]);
@@ -1131,7 +1131,7 @@ int osqp_adjoint(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_os
   WMPC_LAUNCH_CHECK();
   if (a.dp || a.da) {
     if (!a.dp || !a.da) return fail(WMPC_ERR_INVALID_ARGUMENT, "dp and da go together");
-    dim3 grid(ceil_div(o.nnz_p + o.nnz_a, 256) < 64 ? ceil_div(o.nnz_p + o.nnz_a, 256) : 64, B);
+    dim3 grid(B, ceil_div(o.nnz_p + o.nnz_a, 256) < 64 ? ceil_div(o.nnz_p + o.nnz_a, 256) : 64);
     adjoint_matrix_kernel<<<grid, 256, 0, s>>>(o, q.p_upper_rows, q.p_upper_cols, a.dq, a.x, a.y, mu, tau, a.dp,
                                                a.da, B);
     WMPC_LAUNCH_CHECK();
