@@ -355,7 +355,9 @@ def gradient_timing(args, dev, world):
         bwd_ms += e[1].elapsed_time(e[2]) / reps
     fwd_ms = max_over_ranks(fwd_ms, world)
     bwd_ms = max_over_ranks(bwd_ms, world)
+    accuracy = gradient_accuracy(plan.settings.max_iter, dev)
     return {
+        "accuracy_vs_fd64": accuracy,
         "workload": f"linear {cls.name} MPC nx={cls.nx} nu={cls.nu} N={cls.horizon}, {b.batch} instances/GPU, "
                     f"loss ||u0 - u_target||^2, forward {plan.settings.max_iter} + adjoint {plan.settings.max_iter} ADMM iterations",
         "fwd_ms": fwd_ms,
@@ -363,6 +365,43 @@ def gradient_timing(args, dev, world):
         "ratio": (fwd_ms + bwd_ms) / fwd_ms,
         "refactorizations_in_backward": 0,
     }
+
+
+def gradient_accuracy(iters, dev):
+    """The timed gradient's error at the same settings (forward and adjoint
+    `iters` ADMM iterations) on the 256 instances of the FP64 central-difference
+    fixture tests/golden/adjoint_fd_cartpole.npz (converged float64 QP
+    solves): per instance max |g - g_fd| / max(|g_fd|_inf, 1e-3) over diag Q,
+    diag R and x0, split by whether the forward solve met residual <= 1e-3."""
+    import torch
+
+    from warpmpc_b200 import problems
+    from warpmpc_b200.jax_osqp import compile_osqp
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "adjoint_fd_cartpole.npz"))
+    cls = problems.CARTPOLE
+    n_inst = int(g["fd_grad"].shape[0])
+    params = problems.draw_params(cls, n_inst, int(g["seed"]))
+    plan = problems.make_plan(problems.make_batch(cls, 1, int(g["seed"])))
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev,
+                        derivatives=True, adjoint_iters=iters)
+    leaves = {k: torch.from_numpy(getattr(params, k)).float().to(dev).requires_grad_(k in ("qd", "rd", "x0"))
+              for k in ("a", "b", "qd", "rd", "x0", "x_ref")}
+    p, a, q, l, u = (t.contiguous() for t in problems.qp_from_params(problems.MPCParams(cls, **leaves)))
+    x, z, y, prim, dual, obj = comp.solve(p, a, q, l, u)
+    ui = (cls.horizon + 1) * cls.nx
+    ut = torch.from_numpy(np.random.default_rng(int(g["target_seed"])).standard_normal((n_inst, cls.nu))).float().to(dev)
+    ((x[:, ui : ui + cls.nu] - ut) ** 2).sum().backward()
+    grad = torch.cat([leaves["qd"].grad, leaves["rd"].grad, leaves["x0"].grad], 1).cpu().numpy().astype(np.float64)
+    fd = g["fd_grad"]
+    rel = np.max(np.abs(grad - fd), axis=1) / np.maximum(np.max(np.abs(fd), axis=1), 1e-3)
+    conv = ((prim <= RES_TOL) & (dual <= RES_TOL)).cpu().numpy()
+    out = {"instances": int(g["converged"].sum()), "iterations": iters}
+    for name, sel in (("all", g["converged"]), ("forward_at_res_1e-3", g["converged"] & conv)):
+        r = rel[sel]
+        out[name] = {"count": int(sel.sum()), "median": float(np.median(r)), "p90": float(np.percentile(r, 90)),
+                     "frac_le_1e-2": float(np.mean(r <= 1e-2))} if r.size else {"count": 0}
+    return out
 
 
 def line_search_timing(args, dev, world, plan, hbm_peak, peak_source):

@@ -13,7 +13,7 @@ import pytest
 
 from oracle import osqp_ref
 from warpmpc_b200 import problems
-from warpmpc_b200.jax_osqp import compile_osqp
+from warpmpc_b200.jax_osqp import OSQPSettings, compile_osqp
 
 pytestmark = pytest.mark.gpu
 
@@ -71,24 +71,45 @@ def test_frontier_form_warm_start(cuda_device, monkeypatch):
         np.testing.assert_array_equal(g, r)
 
 
-def test_frontier_form_refuses_termination_checks(cuda_device, monkeypatch):
-    """The frontier form runs fixed iterations; a checked solve fails loudly."""
+@pytest.mark.parametrize("cls,batch", [(problems.SMALL, 40), (problems.CARTPOLE, 300)], ids=["small", "cartpole"])
+def test_frontier_form_termination_checks(cuda_device, monkeypatch, cls, batch):
+    """Checked solves in the frontier form (unscale factors from the index
+    table, the second releaser following the stop decisions): the same
+    iterates, iteration counts and status as the plain form's checked solve,
+    cold and warm."""
     import torch
 
-    b = problems.make_batch(problems.SMALL, 40, seed=3)
-    plan = problems.make_plan(b)
+    from warpmpc_b200 import native
+
+    b = problems.make_batch(cls, batch, seed=3)
+    plan = problems.make_plan(b, OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 60}))
     comp = _compile(monkeypatch, plan, {})
+    monkeypatch.setenv("WMPC_STREAM_FRONTIER", "0")
+    plain = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
-    with pytest.raises(Exception, match="fixed iterations"):
-        comp.engine.solve(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), check_termination=5)
+    args = [t(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u)]
+    rng = np.random.default_rng(8)
+    for warm in (None, tuple(t(rng.standard_normal((batch, k)).astype(np.float32) * 0.1)
+                             for k in (plan.n, plan.m, plan.m))):
+        got = comp.engine.solve(*args, warm=warm, check_termination=5)
+        assert native.stream_last_launch()["form"] == "frontier"
+        iters = comp.engine.last_iters.cpu().numpy()
+        status = comp.engine.last_status.cpu().numpy()
+        want = plain.engine.solve(*args, warm=warm, check_termination=5)
+        assert native.stream_last_launch()["form"] == "plain"
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g.cpu().numpy(), w.cpu().numpy())
+        np.testing.assert_array_equal(iters, plain.engine.last_iters.cpu().numpy())
+        np.testing.assert_array_equal(status, plain.engine.last_status.cpu().numpy())
+        assert iters.min() < 60  # some instances stopped early
 
 
 def test_frontier_beside_plain_schedule(cuda_device, monkeypatch):
-    """WMPC_STREAM_FRONTIER=2 (the default) builds both schedules.  Fixed-iteration solves of
+    """WMPC_STREAM_FRONTIER=2 (the default) builds both schedules.  Solves of
     more tiles than SMs run the frontier form where it fits two CTAs per SM and
-    the plain form does not (the quadrotor pattern); checked solves run the
-    plain form.  Iterates bit-exact against the oracle, and the checked solve
-    equal to a plain-only problem's."""
+    the plain form does not (the quadrotor pattern), checked solves included.
+    Iterates bit-exact against the oracle, and the checked solve equal to a
+    plain-only problem's, iteration counts included."""
     import torch
     from oracle.cpu_baseline import CpuOSQP
 

@@ -202,7 +202,10 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
     return false;
   }
   std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
+  std::vector<float> unscale_perm(hp.n, 1.0f);
+  for (int i = 0; i < hp.n; ++i) unscale_perm[i] = unscale[hp.p[i]];
   Packer sk;
+  sk.addf(unscale_perm.data(), unscale_perm.size(), &sp.unscale_perm);
   sk.add(hs.chunk_off.data(), hs.chunk_off.size(), &sp.chunk_off);
   sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
   sk.add(hs.chunk_cols.data(), hs.chunk_cols.size(), &sp.chunk_cols);

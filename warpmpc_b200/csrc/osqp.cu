@@ -745,14 +745,14 @@ int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_ba
   return WMPC_OK;
 }
 
-// The schedule a fixed-iteration solve of `tiles` instance tiles runs alone:
-// the frontier form where this batch's launch of it would put more CTAs on
-// an SM than the plain form's (both counts under the problem's CTA limit,
-// which the launch uses too).  Checked solves run the plain form.
+// The schedule a solve of `tiles` instance tiles runs alone: the frontier form
+// where this batch's launch of it would put more CTAs on an SM than the plain
+// form's (both counts under the problem's CTA limit, which the launch uses
+// too, and sized with the residual records of a checked solve).
 static bool frontier_for(const wmpc_osqp& q, bool check, int tiles) {
-  if (!q.has_frontier || check) return false;
-  return stream_ctas_for(q.spf, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit) >
-         stream_ctas_for(q.sp, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit);
+  if (!q.has_frontier) return false;
+  return stream_ctas_for(q.spf, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit, check) >
+         stream_ctas_for(q.sp, q.kkt_plan->device, tiles, q.num_sms, q.ctas_limit, check);
 }
 
 // Streaming solve, first half: inputs staged, factor, state records; fills

@@ -516,14 +516,17 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 constexpr int kRelGroup = 2;  // releases per group (groups of 4 measured 3.5 % slower: register pressure)
 
 struct RelGroup {
-  int o[kRelGroup], kk[kRelGroup];
+  int o[kRelGroup], kk[kRelGroup], ix[kRelGroup];
   float x[kRelGroup], rho[kRelGroup], rinv[kRelGroup], f[kRelGroup], e[kRelGroup];
   float4 st[kRelGroup];
 };
 
-template <bool kTrack>
+// A record's last word: the released index's unscale factor (plain form) or
+// the index itself (frontier form, whose unscale factors come from
+// unscale_perm when termination is checked).
+template <bool kTrack, bool kFrontier>
 __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
-                                               const unsigned char* xb, RelGroup& g) {
+                                               const unsigned char* xb, const float* unscale_perm, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
     const int kk = (k + j < end) ? k + j : k;
@@ -532,7 +535,13 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
     g.o[j] = r.x;
     g.rho[j] = __int_as_float(r.y);
     g.rinv[j] = __int_as_float(r.z);
-    g.f[j] = __int_as_float(r.w);
+    if constexpr (kFrontier) {
+      g.ix[j] = r.w;
+      g.f[j] = kTrack ? __ldg(unscale_perm + r.w) : 1.0f;
+    } else {
+      g.ix[j] = 0;
+      g.f[j] = __int_as_float(r.w);
+    }
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
     g.st[j] = S[kk * 32];
     if constexpr (kTrack) g.e[j] = SE[kk * 32];
@@ -558,11 +567,10 @@ struct RelParams {
 template <bool kCons, bool kTrack, bool kFrontier>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb, float* rt,
                                                  float4* stu, float* peu, float& chg, float& pres, bool frozen_in) {
-  static_assert(!(kTrack && kFrontier), "the frontier form's records carry indices, not unscale factors");
   const bool frozen = kTrack && frozen_in;
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
-    float* xi = kFrontier ? rt + __float_as_int(g.f[j]) * 32 : reinterpret_cast<float*>(xb + g.o[j]);
+    float* xi = kFrontier ? rt + g.ix[j] * 32 : reinterpret_cast<float*>(xb + g.o[j]);
     float2* out = reinterpret_cast<float2*>(stu + g.kk[j] * 32);
     if (!kCons) {
       const float xa = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
@@ -596,18 +604,19 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
 template <bool kCons, bool kTrack, bool kFrontier>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
                                              const RelParams& rp, unsigned char* xb, float* rt, float4* stu,
-                                             float* peu, float& chg, float& pres, bool frozen) {
+                                             float* peu, float& chg, float& pres, bool frozen,
+                                             const float* unscale_perm) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kTrack>(rel, begin, end, S, SE, xb, a);
+  load_rel_group<kTrack, kFrontier>(rel, begin, end, S, SE, xb, unscale_perm, a);
   for (int k = begin;; k += 2 * kRelGroup) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + kRelGroup < end ? k + kRelGroup : end - 1;
-    load_rel_group<kTrack>(rel, kb, end, S, SE, xb, b);
+    load_rel_group<kTrack, kFrontier>(rel, kb, end, S, SE, xb, unscale_perm, b);
     update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + kRelGroup >= end) break;
     const int ka = k + 2 * kRelGroup < end ? k + 2 * kRelGroup : end - 1;
-    load_rel_group<kTrack>(rel, ka, end, S, SE, xb, a);
+    load_rel_group<kTrack, kFrontier>(rel, ka, end, S, SE, xb, unscale_perm, a);
     update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + 2 * kRelGroup >= end) break;
   }
@@ -627,7 +636,10 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // half of every chunk's releases (the releaser is on the critical path with
 // the sweeper); the first releaser frees the stages and publishes rel_done
 // once both halves are done.
-// kFrontier (fixed iterations only): X holds slots, not rows.  The releasers
+// kFrontier: X holds slots, not rows (with termination checks too: the
+// second releaser then only copies forward results and follows the first
+// releaser's stop decisions, and the unscale factors come from unscale_perm,
+// since the records carry indices).  The releasers
 // write the right-hand sides to the per-tile vector rhs; the producer copies a
 // forward chunk's rows of rhs, and a backward chunk's columns of fwd, into the
 // stage behind its L data, where the units read their targets.  The sweeper
@@ -638,8 +650,7 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // chunk until every earlier forward block is in fwd.
 template <bool kTrack, bool kFrontier>
 __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
-  static_assert(!(kTrack && kFrontier), "the frontier form runs fixed iterations");
-  constexpr bool kSplit = !kTrack;
+  constexpr bool kSplit = !kTrack;  // the second releaser takes half of the releases (fixed iterations)
   extern __shared__ __align__(128) unsigned char smem[];
   const int lstage_bytes = a.meta_bytes + a.lbytes;
   const int total_tiles = a.tile_end[a.n_jobs - 1];
@@ -958,8 +969,10 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false, kTrack, kFrontier>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen);
-            run_releases<true, kTrack, kFrontier>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen);
+            run_releases<false, kTrack, kFrontier>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+                                                   sp.unscale_perm);
+            run_releases<true, kTrack, kFrontier>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+                                                  sp.unscale_perm);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -1008,7 +1021,13 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         ++t;
         return true;
       };
-      auto cont = [&](int it) -> int { (void)it; return stop ? 0 : 1; };
+      auto cont = [&](int it) -> int {
+        if (rw == 0) return stop ? 0 : 1;
+        // the second releaser (frontier form) follows the first one's decision
+        if (!check_point(J.check_every, it)) return 1;
+        if (!wait_counter_bounded(rel_done, t, abort_flag, a.wait_limit_ns)) return -1;
+        return *stop_at == t ? 0 : 1;
+      };
       if (!traverse(sp.n_chunks, sp.n_fchunks, J.max_iter, release, cont)) ok = false;
       if (ok && rw == 0 && J.iters && tile * 32 + lane < J.batch)
         J.iters[tile * 32 + lane] = frozen ? frozen_at : iters_run;
@@ -1140,27 +1159,34 @@ bool ctas_resident(const void* kernel, int threads, size_t smem, int k) {
   return blocks >= k;
 }
 
-// The fixed-iteration kernel instance of a schedule form.
-const void* fixed_iteration_kernel(bool frontier) {
+// The kernel instance of a schedule form, with or without termination checks,
+// and its threads (four warps; three for the plain form's checked instance,
+// which has no second releaser).
+const void* stream_kernel_of(bool frontier, bool track) {
+  if (track)
+    return frontier ? reinterpret_cast<const void*>(admm_stream_kernel<true, true>)
+                    : reinterpret_cast<const void*>(admm_stream_kernel<true, false>);
   return frontier ? reinterpret_cast<const void*>(admm_stream_kernel<false, true>)
                   : reinterpret_cast<const void*>(admm_stream_kernel<false, false>);
 }
+int stream_threads_of(bool frontier, bool track) { return track && !frontier ? 96 : 128; }
 
 }  // namespace
 
-int stream_max_ctas(const StreamPlan& sp, int device, int limit) {
-  const RingSizes r = ring_sizes(sp, false);
+int stream_max_ctas(const StreamPlan& sp, int device, int limit, bool track) {
+  const RingSizes r = ring_sizes(sp, track);
+  const bool frontier = sp.frontier_slots > 0;
   for (int k = limit; k >= 2; --k) {
     StreamLaunch cfg;
     if (multi_cta_config(r, k, &cfg, device) &&
-        ctas_resident(fixed_iteration_kernel(sp.frontier_slots > 0), 128, cfg.smem, k))
+        ctas_resident(stream_kernel_of(frontier, track), stream_threads_of(frontier, track), cfg.smem, k))
       return k;
   }
   return 1;
 }
 
-int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit) {
-  for (int k = stream_max_ctas(sp, device, limit); k >= 2; --k)
+int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit, bool track) {
+  for (int k = stream_max_ctas(sp, device, limit, track); k >= 2; --k)
     if (tiles > (k - 1) * num_sms) return k;
   return 1;
 }
@@ -1245,8 +1271,6 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   for (int i = 0; i < n_jobs; ++i)
     if ((jobs[i].sp.frontier_slots > 0) != frontier)
       return fail(WMPC_ERR_UNSUPPORTED, "frontier-form and plain classes cannot share a launch");
-  if (frontier && track)
-    return fail(WMPC_ERR_UNSUPPORTED, "the frontier-form schedule runs fixed iterations (no termination checks)");
   for (int i = 0; i < n_jobs; ++i) {
     const RingSizes ri = ring_sizes(jobs[i].sp, track);
     r.meta_bytes = std::max(r.meta_bytes, ri.meta_bytes);
@@ -1268,14 +1292,13 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   int ctas_per_sm = 1;
   {
     const int tiles = total_tiles_of(jobs, n_jobs);
-    const void* kfn = track ? reinterpret_cast<const void*>(admm_stream_kernel<true, false>)
-                            : fixed_iteration_kernel(frontier);
+    const void* kfn = stream_kernel_of(frontier, track);
     int limit = jobs[0].ctas_limit;
     for (int i = 1; i < n_jobs; ++i) limit = std::min(limit, jobs[i].ctas_limit);
     for (int k = limit; k >= 2; --k) {
       StreamLaunch cfgk;
       if (tiles > (k - 1) * num_sms && multi_cta_config(r, k, &cfgk) &&
-          ctas_resident(kfn, track ? 96 : 128, cfgk.smem, k)) {
+          ctas_resident(kfn, stream_threads_of(frontier, track), cfgk.smem, k)) {
         cfg = cfgk;
         ctas_per_sm = k;
         break;
@@ -1322,14 +1345,14 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     if (ns > 0) a.wait_limit_ns = (unsigned long long)ns;
   }
   const int grid = total < ctas_per_sm * num_sms ? total : ctas_per_sm * num_sms;
-  auto kernel = track ? admm_stream_kernel<true, false>
+  auto kernel = track ? (frontier ? admm_stream_kernel<true, true> : admm_stream_kernel<true, false>)
                       : (frontier ? admm_stream_kernel<false, true> : admm_stream_kernel<false, false>);
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   // all of the SM's unified memory as shared memory, so that two CTAs fit
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared));
   profile_mark_begin(s);
-  kernel<<<grid, track ? 96 : 128, cfg.smem, s>>>(a);
+  kernel<<<grid, stream_threads_of(frontier, track), cfg.smem, s>>>(a);
   profile_mark_end(s);
   record_stream_launch(frontier ? 2 : 1, ctas_per_sm, grid, (int)cfg.smem);
   WMPC_LAUNCH_CHECK();

@@ -103,6 +103,9 @@ struct StreamPlan {
   const int* chunk_c0;  // [n_chunks] first column of a backward chunk (its forward-result block)
   const int* frow0;     // [n_fchunks] first row of a forward chunk (its right-hand-side block)
   const int* frows;     // [n_fchunks] its rows
+  // frontier form with termination checks: the unscale factor of each
+  // permuted KKT index (the plain form's records carry it in their last word)
+  const float* unscale_perm;  // [n]
 };
 
 // ---- PTX helpers -----------------------------------------------------------
@@ -273,13 +276,14 @@ struct StreamLaunch {
 bool stream_launch_config(const StreamPlan& sp, StreamLaunch* cfg);
 // most CTAs of a fixed-iteration launch of this plan that fit one SM of `device`
 // (within the launch limit: 2 unless WMPC_STREAM_MAX_CTAS allows up to 4)
-int stream_max_ctas(const StreamPlan& sp, int device, int limit);
+// (track: a launch that checks termination, whose S stages also carry residuals)
+int stream_max_ctas(const StreamPlan& sp, int device, int limit, bool track = false);
 // the CTAs-per-SM limit of the environment (WMPC_STREAM_CTAS=1: one;
 // WMPC_STREAM_MAX_CTAS: 2 to 4; default 2), fixed per problem at creation
 int stream_ctas_limit_setting();
 // CTAs per SM a fixed-iteration launch of `tiles` tiles of this plan runs
 // with (k only when there are more than k - 1 tiles per SM)
-int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit);
+int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, int limit, bool track = false);
 size_t stream_workspace_floats(const StreamPlan& sp, int batch);
 
 // One class of a streaming launch (host view): its plan, stream buffers and
