@@ -132,3 +132,19 @@ def test_solve_with_objective_cotangent_and_shared_matrices(cuda_device):
     assert p.grad.shape == p.shape and a.grad.shape == a.shape
     # d obj / d q = x at the optimum (envelope theorem)
     np.testing.assert_allclose(q.grad.cpu().numpy(), x.detach().cpu().numpy(), rtol=2e-3, atol=2e-3)
+
+
+def test_adjoint_residual_optional(cuda_device):
+    """The differential QP's residual is formed only on request; the
+    gradients are the same bits either way."""
+    b, plan, comp = _setup(problems.SMALL, 12, seed=71, iters=40)
+    eng = comp.engine
+    args = [_t(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u)]
+    x, z, y, *_ = eng.solve(*args, keep_factor=True)
+    dx = _t(np.random.default_rng(3).standard_normal((12, plan.n)).astype(np.float32))
+    plain = eng.adjoint(eng.last_workspace, args[0], args[1], args[3], args[4], x, z, y, dx, None)
+    assert eng.last_adjoint_residual is None
+    with_res = eng.adjoint(eng.last_workspace, args[0], args[1], args[3], args[4], x, z, y, dx, None, residual=True)
+    for a, c in zip(plain, with_res):
+        np.testing.assert_array_equal(a.cpu().numpy(), c.cpu().numpy())
+    assert np.all(np.isfinite(eng.last_adjoint_residual.cpu().numpy()))

@@ -484,6 +484,31 @@ __global__ void __launch_bounds__(32 * kResParts) residual_kernel(
   }
 }
 
+// The final iterate's unscaling alone (no residual outputs requested): x,
+// z, y back to the problem's units and the status from the kernels' words.
+__global__ void __launch_bounds__(32 * kResParts) unscale_state_kernel(Osqp o, State st, int* status,
+                                                                     const int* status_in, const int* abort_word,
+                                                                     int batch) {
+  const int lane = threadIdx.x, part = threadIdx.y;
+  const int b = blockIdx.x * 32 + lane;
+  if (b >= batch) return;
+  for (int j = part; j < o.n; j += kResParts) {
+    const long long k = (long long)j * st.ld + b;
+    st.x[k] = st.x[k] * __ldg(o.scaling_d + j);
+  }
+  for (int r = part; r < o.m; r += kResParts) {
+    const long long k = (long long)r * st.ld + b;
+    st.z[k] = st.z[k] * __ldg(o.scaling_einv + r);
+    st.y[k] = st.y[k] * __ldg(o.y_unscale + r);
+  }
+  if (status && part == 0) {
+    int v = WMPC_STATUS_MAX_ITER;
+    if (status_in) v |= status_in[b];
+    if (abort_word && *abort_word) v |= WMPC_STATUS_KERNEL_ABORT;
+    status[b] = v;
+  }
+}
+
 __global__ void fill_int_kernel(int* out, int value, int count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < count) out[i] = value;
@@ -722,13 +747,24 @@ namespace {
 
 // Batch-major inputs -> symbolic-major, scaled where the reference scales;
 // the starting iterate (warm start, or zero).
+// Residual outputs requested (or termination checked): the final residuals
+// need P, A and the unscaled q in the workspace.
+static bool residuals_wanted(const wmpc_osqp_options& opt, const wmpc_osqp_batch& d) {
+  return d.prim_res || d.dual_res || d.obj || opt.check_termination > 0;
+}
+
+// P and A are staged when the solve factors or forms residuals (a solve that
+// reuses its factor without residual outputs -- the adjoint's -- skips them).
 int stage_inputs(const Osqp& o, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
                  cudaStream_t s) {
   const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
+  const bool sums = residuals_wanted(opt, d);
   int rc;
-  if ((rc = transpose_in(d.p_values, o.nnz_p, pb, o.nnz_p, nullptr, L.pT, pb, s))) return rc;
-  if ((rc = transpose_in(d.a_values, o.nnz_a, ab, o.nnz_a, nullptr, L.aT, ab, s))) return rc;
-  if ((rc = transpose_in(d.q, o.n, B, o.n, nullptr, L.qT, B, s))) return rc;
+  if (!opt.reuse_factor || sums) {
+    if ((rc = transpose_in(d.p_values, o.nnz_p, pb, o.nnz_p, nullptr, L.pT, pb, s))) return rc;
+    if ((rc = transpose_in(d.a_values, o.nnz_a, ab, o.nnz_a, nullptr, L.aT, ab, s))) return rc;
+  }
+  if (sums && (rc = transpose_in(d.q, o.n, B, o.n, nullptr, L.qT, B, s))) return rc;
   if ((rc = transpose_in(d.q, o.n, B, o.n, o.q_scale, L.qs, B, s))) return rc;
   if ((rc = transpose_in(d.l, o.m, B, o.m, o.scaling_e, L.ls, B, s))) return rc;
   if ((rc = transpose_in(d.u, o.m, B, o.m, o.scaling_e, L.us, B, s))) return rc;
@@ -793,9 +829,13 @@ int stream_solve_end(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmp
   int rc;
   if ((rc = stream_end(job.sp, o, job, L.x, L.z, L.y, s))) return rc;
   State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
-  residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
-      o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B,
-      L.stream_status, error_word, check ? opt.eps_abs : -1.0f, opt.eps_rel);
+  if (residuals_wanted(opt, d)) {
+    residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
+        o, L.pT, pb, pb > 1 ? 1 : 0, L.aT, ab, ab > 1 ? 1 : 0, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B,
+        L.stream_status, error_word, check ? opt.eps_abs : -1.0f, opt.eps_rel);
+  } else {
+    unscale_state_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(o, st, d.status, L.stream_status, error_word, B);
+  }
   WMPC_LAUNCH_CHECK();
   if (d.iters && !check) {
     fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
@@ -818,6 +858,8 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if (B <= 0) return WMPC_OK;
   const int pb = d.p_batch, ab = d.a_batch;
   const bool external = lx_ext != nullptr;
+  if ((d.prim_res || d.dual_res || d.obj || opt.check_termination > 0) && !(d.prim_res && d.dual_res && d.obj))
+    return fail(WMPC_ERR_INVALID_ARGUMENT, "prim_res, dual_res and obj go together (and with termination checks)");
   const bool adaptive = opt.adaptive_rho_interval > 0;
   if (adaptive) {
     if (mode != WMPC_OSQP_PLAIN) return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation runs in plain mode");
@@ -911,9 +953,13 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
                                                          d.rho_updates, B);
       WMPC_LAUNCH_CHECK();
     }
-    residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
-        o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B, nullptr, nullptr,
-        -1.0f, 0.0f);
+    if (residuals_wanted(opt, d)) {
+      residual_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(
+          o, L.pT, ldp, sbp, L.aT, lda, sba, st, L.qT, d.prim_res, d.dual_res, d.obj, d.status, B, nullptr, nullptr,
+          -1.0f, 0.0f);
+    } else {
+      unscale_state_kernel<<<ceil_div(B, 32), dim3(32, kResParts), 0, s>>>(o, st, d.status, nullptr, nullptr, B);
+    }
     WMPC_LAUNCH_CHECK();
     if (d.iters) {
       fill_int_kernel<<<ceil_div(B, 256), 256, 0, s>>>(d.iters, opt.max_iter, B);
@@ -1117,9 +1163,10 @@ int osqp_adjoint(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_os
   d.x = a.dq;  // w
   d.z = zd;
   d.y = mu;
-  d.prim_res = a.adj_prim_res ? a.adj_prim_res : misc;
-  d.dual_res = misc + B;
-  d.obj = misc + 2 * B;
+  // residuals of the differential QP only when asked for (they need P and A staged)
+  d.prim_res = a.adj_prim_res;
+  d.dual_res = a.adj_prim_res ? misc + B : nullptr;
+  d.obj = a.adj_prim_res ? misc + 2 * B : nullptr;
   d.iters = reinterpret_cast<int*>(misc + 3 * B);
   d.status = reinterpret_cast<int*>(misc + 4 * B);
   wmpc_osqp_options ao = opt;

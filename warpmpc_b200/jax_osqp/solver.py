@@ -415,11 +415,13 @@ class OSQPEngine:
         self.last_status = status_h
         return out
 
-    def adjoint(self, workspace, p_values, a_values, l, u, x, z, y, dx, dy=None, max_iter=None):
+    def adjoint(self, workspace, p_values, a_values, l, u, x, z, y, dx, dy=None, max_iter=None, residual=False):
         """Reverse-mode derivatives on the factor kept by ``solve(keep_factor=True)``.
 
         Returns ``(dq, dl, du, dp, da)`` per instance (``dp``/``da`` batch-major
-        on P's upper pattern and A's pattern).
+        on P's upper pattern and A's pattern).  ``residual=True`` also forms
+        the differential QP's primal residual (``last_adjoint_residual``),
+        which costs a pass over P and A.
         """
         import torch
 
@@ -441,7 +443,7 @@ class OSQPEngine:
         du = torch.empty((batch, pl.m), dtype=torch.float32, device=dev)
         dp = torch.empty((batch, pl.nnz_p), dtype=torch.float32, device=dev)
         da = torch.empty((batch, pl.nnz_a), dtype=torch.float32, device=dev)
-        res = torch.empty(batch, dtype=torch.float32, device=dev)
+        res = torch.empty(batch, dtype=torch.float32, device=dev) if residual else None
         s = pl.settings
         opts = native.OsqpOptions(max_iter=int(s.max_iter if max_iter is None else max_iter), check_termination=check,
                                   eps_abs=np.float32(s.eps_abs), eps_rel=np.float32(s.eps_rel), warm_start=0,
@@ -450,7 +452,8 @@ class OSQPEngine:
             batch=batch, p_values=p.data_ptr(), p_batch=int(p.shape[0]), a_values=a.data_ptr(),
             a_batch=int(a.shape[0]), l=lm.data_ptr(), u=um.data_ptr(), x=x.data_ptr(), z=z.data_ptr(),
             y=y.data_ptr(), dx=dxm.data_ptr(), dy=None if dym is None else dym.data_ptr(), dq=dq.data_ptr(),
-            dl=dl.data_ptr(), du=du.data_ptr(), dp=dp.data_ptr(), da=da.data_ptr(), adj_prim_res=res.data_ptr(),
+            dl=dl.data_ptr(), du=du.data_ptr(), dp=dp.data_ptr(), da=da.data_ptr(),
+            adj_prim_res=res.data_ptr() if residual else None,
         )
         native.check(native.lib().wmpc_osqp_adjoint(self.dev.handle, ctypes.byref(opts), ctypes.byref(data), mode_id,
                                                     native.tensor_ptr(ws), wsb, native.current_stream_handle(dev)))
