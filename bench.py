@@ -26,6 +26,7 @@ host cores instead (the reference's own JAX/Warp code cannot run here).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -306,11 +307,17 @@ def run_reference(args):
     return 0
 
 
+ADJOINT_ITERS = (15, 20, 25)  # adjoint ADMM iteration counts the gradient leg times
+
+
 def gradient_timing(args, dev, world):
     """(forward + adjoint) / forward on nx=4, nu=1, N=50, 16384 instances.
 
-    Forward: persistent solve that keeps its factor; backward: the adjoint on
-    that factor (25 ADMM iterations, cotangent of ||u0 - u_target||^2).
+    Forward: persistent solve (25 ADMM iterations) that keeps its factor;
+    backward: the adjoint on that factor (cotangent of ||u0 - u_target||^2),
+    timed at each adjoint iteration count of ADJOINT_ITERS, each with its
+    accuracy against the FP64 finite-difference fixture.  `ratio` is the
+    count equal to the forward's (25).
     """
     import torch
 
@@ -331,44 +338,53 @@ def gradient_timing(args, dev, world):
     def fwd():
         return eng.solve(P, A, Q, L, U, keep_factor=True)
 
-    def bwd(out):
+    def bwd(out, iters):
         x, z, y = out[0], out[1], out[2]
         dx = torch.zeros_like(x)
         dx[:, ui : ui + cls.nu] = 2.0 * (x[:, ui : ui + cls.nu] - u_target)
-        return eng.adjoint(eng.last_workspace, P, A, L, U, x, z, y, dx, None)
+        return eng.adjoint(eng.last_workspace, P, A, L, U, x, z, y, dx, None, max_iter=iters)
 
-    for _ in range(3):
-        o = fwd()
-        bwd(o)
-    torch.cuda.synchronize()
-    reps = 5
-    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    fwd_ms = bwd_ms = 0.0
-    for _ in range(reps):
-        e[0].record()
-        o = fwd()
-        e[1].record()
-        bwd(o)
-        e[2].record()
+    fwd_iters = plan.settings.max_iter
+    by_iters = {}
+    fwd_runs = []
+    for k in ADJOINT_ITERS:
+        for _ in range(3):
+            o = fwd()
+            bwd(o, k)
         torch.cuda.synchronize()
-        fwd_ms += e[0].elapsed_time(e[1]) / reps
-        bwd_ms += e[1].elapsed_time(e[2]) / reps
-    fwd_ms = max_over_ranks(fwd_ms, world)
-    bwd_ms = max_over_ranks(bwd_ms, world)
-    accuracy = gradient_accuracy(plan.settings.max_iter, dev)
+        reps = 5
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        fwd_ms = bwd_ms = 0.0
+        for _ in range(reps):
+            e[0].record()
+            o = fwd()
+            e[1].record()
+            bwd(o, k)
+            e[2].record()
+            torch.cuda.synchronize()
+            fwd_ms += e[0].elapsed_time(e[1]) / reps
+            bwd_ms += e[1].elapsed_time(e[2]) / reps
+        fwd_ms = max_over_ranks(fwd_ms, world)
+        bwd_ms = max_over_ranks(bwd_ms, world)
+        fwd_runs.append(fwd_ms)
+        by_iters[str(k)] = {"adjoint_ms": bwd_ms, "fwd_ms": fwd_ms, "ratio": (fwd_ms + bwd_ms) / fwd_ms,
+                            "accuracy_vs_fd64": gradient_accuracy(k, dev)}
+    main = by_iters.get(str(fwd_iters)) or by_iters[str(ADJOINT_ITERS[-1])]
     return {
-        "accuracy_vs_fd64": accuracy,
+        "accuracy_vs_fd64": main["accuracy_vs_fd64"],
         "workload": f"linear {cls.name} MPC nx={cls.nx} nu={cls.nu} N={cls.horizon}, {b.batch} instances/GPU, "
-                    f"loss ||u0 - u_target||^2, forward {plan.settings.max_iter} + adjoint {plan.settings.max_iter} ADMM iterations",
-        "fwd_ms": fwd_ms,
-        "adjoint_ms": bwd_ms,
-        "ratio": (fwd_ms + bwd_ms) / fwd_ms,
+                    f"loss ||u0 - u_target||^2, forward {fwd_iters} ADMM iterations, adjoint {fwd_iters} "
+                    f"(and {', '.join(str(k) for k in ADJOINT_ITERS)} in by_adjoint_iterations)",
+        "fwd_ms": main["fwd_ms"],
+        "adjoint_ms": main["adjoint_ms"],
+        "ratio": main["ratio"],
+        "by_adjoint_iterations": by_iters,
         "refactorizations_in_backward": 0,
     }
 
 
 def gradient_accuracy(iters, dev):
-    """The timed gradient's error at the same settings (forward and adjoint
+    """The timed gradient's error at the same settings (forward 25 and adjoint
     `iters` ADMM iterations) on the 256 instances of the FP64 central-difference
     fixture tests/golden/adjoint_fd_cartpole.npz (converged float64 QP
     solves): per instance max |g - g_fd| / max(|g_fd|_inf, 1e-3) over diag Q,
@@ -396,7 +412,8 @@ def gradient_accuracy(iters, dev):
     fd = g["fd_grad"]
     rel = np.max(np.abs(grad - fd), axis=1) / np.maximum(np.max(np.abs(fd), axis=1), 1e-3)
     conv = ((prim <= RES_TOL) & (dual <= RES_TOL)).cpu().numpy()
-    out = {"instances": int(g["converged"].sum()), "iterations": iters}
+    out = {"instances": int(g["converged"].sum()), "forward_iterations": plan.settings.max_iter,
+           "adjoint_iterations": iters}
     for name, sel in (("all", g["converged"]), ("forward_at_res_1e-3", g["converged"] & conv)):
         r = rel[sel]
         out[name] = {"count": int(sel.sum()), "median": float(np.median(r)), "p90": float(np.percentile(r, 90)),
@@ -572,9 +589,17 @@ def nonlinear_sqp_timing(args, dev, world):
         w.gradient(zf, rf, u_target)
     torch.cuda.current_stream(dev).wait_stream(s)
     torch.cuda.synchronize()
+    # the warm-up's kept factorization (tens of GB at this batch) and cached
+    # blocks go back to the device before the graphs allocate their own
+    del zf, rf
+    w.sqp.qp.engine.last_workspace = None
+    gc.collect()
+    torch.cuda.empty_cache()
     g_fwd, g_fb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
     with torch.cuda.graph(g_fwd):
         z_out, _ = w.solve()
+    gc.collect()
+    torch.cuda.empty_cache()
     with torch.cuda.graph(g_fb, pool=g_fwd.pool()):
         z_fb, r_fb = w.solve(keep_factor=True)
         grads = w.gradient(z_fb, r_fb, u_target)
@@ -975,15 +1000,32 @@ def main():
         e2e = {"value": multirank.sum_over_ranks(efrac * B, multirank.rank_env(), dev) / (ems * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
 
+    # the headline legs are done: release their device memory (graph pool, engines,
+    # workspaces, inputs) so that the larger side legs (262,144 nonlinear SQP
+    # instances) start from an empty device
+    graphed = graph is not None
+    del graph, run_step, step
+    del comp, eng, plain, P, A, Q, L, U, out, warm, loop
+    if plain_res is not None:
+        del pe, pout, pwarm, PL, PU, ploop, pstep
+    if e2e is not None:
+        del e2e_step
+    gc.collect()
+    torch.cuda.empty_cache()
+
     # ---- forward + adjoint vs forward (cartpole-like class, loss on u0) ------------------
     def side_leg(name, fn):
         """A secondary measurement: its failure is reported in its field and on
-        stderr, not allowed to take the headline line down with it."""
+        stderr, not allowed to take the headline line down with it.  Each leg's
+        device memory is returned to the device before the next one."""
         try:
             return fn()
         except Exception as exc:  # report, do not hide
             print(f"[bench] {name} measurement failed: {exc!r}", file=sys.stderr)
             return {"error": repr(exc)[:300]}
+        finally:
+            gc.collect()
+            torch.cuda.empty_cache()
 
     grad = None
     if not args.no_grad:
@@ -1011,8 +1053,6 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(plan, b, args, cls, seed)
 
-    graphed = graph is not None
-    del graph  # release the graph before tearing anything down
     if rank == 0:
         line = {
             "metric": METRIC,

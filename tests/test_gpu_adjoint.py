@@ -148,3 +148,70 @@ def test_adjoint_residual_optional(cuda_device):
     for a, c in zip(plain, with_res):
         np.testing.assert_array_equal(a.cpu().numpy(), c.cpu().numpy())
     assert np.all(np.isfinite(eng.last_adjoint_residual.cpu().numpy()))
+
+
+def test_gradient_at_benchmark_settings(cuda_device):
+    """The gradient the bench times: cart-pole class (nx=4, nu=1, N=50), 25
+    forward and 25 adjoint ADMM iterations, loss ||u0 - u_target||^2, d/d
+    (diag Q, diag R, x0) through torch autograd, on the 256 instances of the
+    FP64 central-difference fixture (converged float64 QP solves, step 1e-6).
+
+    25 forward iterations leave most of these instances unconverged, and an
+    unconverged iterate's active set is not the converged one, so the error
+    against the FP64 derivative is bounded here (1) on the instances whose
+    forward solve met residual <= 1e-3 and (2) as a median over all; (3) the
+    adjoint alone is checked against the exact active-set derivative of the
+    same forward iterate (float64), and (4) against the restated reference
+    gradient path on that iterate (looser: the reference's eps-regularized
+    augmented solve is itself off by up to a few percent)."""
+    import os
+
+    import torch
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "adjoint_fd_cartpole.npz"))
+    cls = problems.CARTPOLE
+    n_inst = int(g["fd_grad"].shape[0])
+    params = problems.draw_params(cls, n_inst, int(g["seed"]))
+    plan = problems.make_plan(problems.make_batch(cls, 1, int(g["seed"])))
+    assert plan.settings.max_iter == 25
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent",
+                        derivatives=True, adjoint_iters=25)
+    leaves = {k: torch.from_numpy(getattr(params, k)).float().cuda().requires_grad_(k in ("qd", "rd", "x0"))
+              for k in ("a", "b", "qd", "rd", "x0", "x_ref")}
+    p, a, q, l, u = (t.contiguous() for t in problems.qp_from_params(problems.MPCParams(cls, **leaves)))
+    x, z, y, prim, dual, obj = comp.solve(p, a, q, l, u)
+    ui = (cls.horizon + 1) * cls.nx
+    ut = torch.from_numpy(np.random.default_rng(int(g["target_seed"])).standard_normal((n_inst, cls.nu))).float().cuda()
+    ((x[:, ui : ui + cls.nu] - ut) ** 2).sum().backward()
+    grad = torch.cat([leaves["qd"].grad, leaves["rd"].grad, leaves["x0"].grad], 1).cpu().numpy().astype(np.float64)
+    fd = g["fd_grad"]
+    assert np.all(np.isfinite(grad))
+    rel = np.max(np.abs(grad - fd), axis=1) / np.maximum(np.max(np.abs(fd), axis=1), 1e-3)
+    conv = ((prim <= 1e-3) & (dual <= 1e-3)).cpu().numpy() & g["converged"]
+    assert conv.sum() >= 16, int(conv.sum())
+    # (1) forward-converged instances (measured: median 2.8e-5, 90 % within 1e-2)
+    assert np.median(rel[conv]) < 2e-4, np.median(rel[conv])
+    assert np.mean(rel[conv] <= 1e-2) >= 0.8, np.mean(rel[conv] <= 1e-2)
+    # (2) all fixture instances (measured: median 1.6e-4)
+    assert np.median(rel[g["converged"]]) < 1e-3, np.median(rel[g["converged"]])
+    # (3) + (4) the adjoint on the same forward iterate, first 32 instances
+    eng = comp.engine
+    pv, av, qv, lv, uv = (t.detach().contiguous() for t in (p, a, q, l, u))
+    xs, zs, ys, *_ = eng.solve(pv, av, qv, lv, uv, keep_factor=True)
+    dx = torch.zeros_like(xs)
+    dx[:, ui : ui + cls.nu] = 2.0 * (xs[:, ui : ui + cls.nu] - ut)
+    got = [t.cpu().numpy() for t in eng.adjoint(eng.last_workspace, pv, av, lv, uv, xs, zs, ys, dx, None)]
+    X, Z, Y = (t.cpu().numpy().astype(np.float64) for t in (xs, zs, ys))
+    PV, AV, LV, UV, DX = (t.cpu().numpy().astype(np.float64) for t in (pv, av, lv, uv, dx))
+    exact_err, ref_err = [], []
+    for i in range(32):
+        ex = adjoint_ref.active_set_adjoint(plan, PV[i], AV[i], LV[i], UV[i], X[i], Z[i], Y[i], DX[i], np.zeros(plan.m))
+        if np.max(np.abs(ex[0])) < 1e-6:
+            continue  # no cotangent reaches this instance's variables
+        exact_err.append(_rel(got[0][i], ex[0]))
+        rf = adjoint_ref.adjoint(plan, PV[i], AV[i], LV[i], UV[i], X[i], Y[i], DX[i], np.zeros(plan.m))
+        ref_err.append(_rel(got[0][i], rf[0]))
+    assert len(exact_err) >= 16
+    # measured: median 4.6e-5 against the exact adjoint
+    assert np.median(exact_err) < 5e-4, np.median(exact_err)
+    assert np.median(ref_err) < 5e-2, np.median(ref_err)

@@ -202,6 +202,13 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
     return false;
   }
   std::vector<int> upd_slot(upd_slot16.begin(), upd_slot16.end());
+  // factorization rows: {p0, p1, i0, i1}, {first update, update end, D^-1 offset, first KKT input}
+  std::vector<int> row_info;
+  row_info.reserve(8 * (size_t)hp.n);
+  for (int k = 0; k < hp.n; ++k) {
+    const int p0 = hp.proc_ptr[k], p1 = hp.proc_ptr[k + 1], i0 = hp.init_ptr[k], i1 = hp.init_ptr[k + 1];
+    row_info.insert(row_info.end(), {p0, p1, i0, i1, upd_ptr[p0], upd_ptr[p1], hs.dinv_off[k], k + i0});
+  }
   std::vector<float> unscale_perm(hp.n, 1.0f);
   for (int i = 0; i < hp.n; ++i) unscale_perm[i] = unscale[hp.p[i]];
   Packer sk;
@@ -219,6 +226,7 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
   sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);
   sk.add(hs.meta_words.data(), hs.meta_words.size(), &sp.meta_words);
   sk.add(hs.meta.data(), hs.meta.size(), &sp.meta);
+  sk.add(row_info.data(), row_info.size(), reinterpret_cast<const int**>(&sp.row_info));
   sk.add(init_slot.data(), init_slot.size(), &sp.init_slot);
   sk.add(upd_ptr.data(), upd_ptr.size(), &sp.upd_ptr);
   sk.add(upd_slot.data(), upd_slot.size(), &sp.upd_slot);
@@ -474,6 +482,18 @@ int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out)
       pk.add(fac_upd_ptr.data(), fac_upd_ptr.size(), &plan->fac_upd_ptr);
       pk.add(fac_upd_slot.data(), fac_upd_slot.size(), &plan->fac_upd_slot);
       pk.add(fac_upd_lidx.data(), fac_upd_lidx.size(), &plan->fac_upd_lidx);
+      // rows read ahead: {p0, p1, i0, i1}, {first update, update end, first input, 0}; per input its KKT slot
+      std::vector<int> row_info, kin_slot;
+      row_info.reserve(8 * (size_t)n);
+      kin_slot.reserve((size_t)n + n_init);
+      for (int k = 0; k < n; ++k) {
+        const int p0 = hp.proc_ptr[k], p1 = hp.proc_ptr[k + 1], i0 = hp.init_ptr[k], i1 = hp.init_ptr[k + 1];
+        row_info.insert(row_info.end(), {p0, p1, i0, i1, fac_upd_ptr[p0], fac_upd_ptr[p1], k + i0, 0});
+        kin_slot.push_back(desc->perm_to_orig[desc->diag_pos[k]]);
+        for (int e = i0; e < i1; ++e) kin_slot.push_back(desc->perm_to_orig[desc->init_pos[e]]);
+      }
+      pk.add(row_info.data(), row_info.size(), reinterpret_cast<const int**>(&plan->fac_row_info));
+      pk.add(kin_slot.data(), kin_slot.size(), &plan->fac_kin_slot);
       plan->fac_max_row = std::max(max_row, 1);
       plan->fac_max_kv = max_kv;
     }
@@ -501,6 +521,9 @@ int wmpc_plan_create(const wmpc_pattern_desc* desc, int device, wmpc_plan** out)
   plan->h_lp.assign(desc->lp, desc->lp + n + 1);
   plan->h_li.assign(desc->li, desc->li + nnz_l);
   plan->h_p.assign(desc->p, desc->p + n);
+  plan->h_perm_to_orig.assign(desc->perm_to_orig, desc->perm_to_orig + nnz_a);
+  plan->h_diag_pos.assign(desc->diag_pos, desc->diag_pos + n);
+  plan->h_init_pos.assign(desc->init_pos, desc->init_pos + n_init);
   *out = plan;
   return WMPC_OK;
 }
@@ -673,6 +696,38 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
   pk.addf(desc->y_unscale, m, &o.y_unscale);
   pk.add(p_up_rows.data(), np, &q->p_upper_rows);
   pk.add(p_up_cols.data(), np, &q->p_upper_cols);
+  // the factorization rows' KKT inputs in row-program order, resolved
+  {
+    const wmpc_plan& kp = *kkt_plan;
+    const int nkkt = n + m;
+    std::vector<int32_t> kin;
+    kin.reserve(4 * ((size_t)nkkt + kp.h_init_pos.size()));
+    auto put = [&](int slot) {
+      const int idx = kp.h_perm_to_orig[slot];
+      const int src = kkt_src[idx];
+      float scale = 0.0f, add = 0.0f;
+      int kind = 0;
+      if (src < 0) {
+        add = desc->kkt_base[idx];
+      } else if (src < np) {
+        kind = 1;
+        scale = desc->p_scale[src];
+        add = desc->p_diag_sigma[src];
+      } else {
+        kind = 2;
+        scale = desc->a_scale[src - np];
+      }
+      int32_t sb, ab;
+      std::memcpy(&sb, &scale, 4);
+      std::memcpy(&ab, &add, 4);
+      kin.insert(kin.end(), {src < 0 ? -1 : src, kind, sb, ab});
+    };
+    for (int k = 0; k < nkkt; ++k) {
+      put(kp.h_diag_pos[k]);
+      for (int e = kp.h_init_ptr[k]; e < kp.h_init_ptr[k + 1]; ++e) put(kp.h_init_pos[e]);
+    }
+    pk.add(kin.data(), kin.size(), reinterpret_cast<const int**>(&o.kin_desc));
+  }
   // rho adaptation: each constraint's rho class and, per KKT slot, the
   // constraint whose -1/rho it holds (-1: none)
   std::vector<int32_t> kkt_rho_row;

@@ -122,7 +122,11 @@ struct wmpc_plan {
   const int* fac_upd_ptr = nullptr;
   const int* fac_upd_slot = nullptr;
   const int* fac_upd_lidx = nullptr;
+  const int4* fac_row_info = nullptr;  // per row {p0, p1, i0, i1}, {first update, update end, first input, 0}
+  const int* fac_kin_slot = nullptr;   // per row, per KKT input: its original KKT slot
   int fac_max_row = 0, fac_max_kv = 0;
   // host copies of the ragged program (inputs of the streaming schedule)
   std::vector<int> h_init_ptr, h_init_rows, h_proc_ptr, h_proc_cols, h_proc_offsets, h_proc_lidx, h_lp, h_li, h_p;
+  // host copies of the KKT-slot tables (inputs of the factorization's row descriptors)
+  std::vector<int> h_perm_to_orig, h_diag_pos, h_init_pos;
 };

@@ -14,6 +14,11 @@ struct Osqp {
   // scaled: kkt_src[s] = -1 (base), j (P entry j) or nnz_p + j (A entry j).
   const float* kkt_base;
   const int* kkt_src;
+  // per factorization row, per KKT input in row-program order (the diagonal,
+  // then the row's initial entries): {P/A entry or -1, kind (0 base value,
+  // 1 P entry, 2 A entry), scale bits, add bits} -- the row's inputs of
+  // kkt_base / kkt_src / p_scale / p_diag_sigma / a_scale resolved
+  const int4* kin_desc;       // [n + m + initial entries]
   const float* p_scale;       // [nnz_p]
   const float* p_diag_sigma;  // [nnz_p]
   const float* a_scale;       // [nnz_a]

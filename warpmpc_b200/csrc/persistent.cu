@@ -39,16 +39,13 @@ struct OsqpInputs {
 
 // Per-warp shared memory of the factorization, in 4-byte words: per lane
 // (x 32) ys [max_row_nnz] (compact accumulator), staged D^-1 of the row's
-// steps [max_row_nnz], staged L re-reads [lbatch], staged raw KKT inputs
-// [max_row_kv]; shared by the warp: update slots [lbatch] and per-step
-// update counts, backward- and forward-stream offsets [3 x max_row_nnz].
+// steps [max_row_nnz], staged L re-reads [lbatch], staged raw KKT inputs of
+// this row and of the next [2 x max_row_kv]; shared by the warp: update
+// slots [lbatch] and per-step update counts, backward- and forward-stream
+// offsets [3 x max_row_nnz].
 __host__ __device__ inline int factor_warp_words(const StreamPlan& sp, int lbatch) {
   const int r = sp.max_row_nnz > 0 ? sp.max_row_nnz : 1;
-  return (2 * r + lbatch + sp.max_row_kv) * 32 + lbatch + 3 * r;
-}
-
-__device__ __forceinline__ int row_kkt_index(const Pattern& pat, int k, int i0, int j) {
-  return __ldg(pat.perm_to_orig + (j == 0 ? __ldg(pat.diag_pos + k) : __ldg(pat.init_pos + i0 + j - 1)));
+  return (2 * r + lbatch + 2 * sp.max_row_kv) * 32 + lbatch + 3 * r;
 }
 
 // Up-looking LDL^T (QDLDL row program, warp_backend.py:41-101), one lane per
@@ -56,60 +53,103 @@ __device__ __forceinline__ int row_kkt_index(const Pattern& pat, int k, int i0, 
 // KKT inputs, D^-1 of the columns it eliminates with, and the L entries of
 // those columns above the row (written by earlier rows) -- is independent of
 // the row's own arithmetic, so each row first stages them into shared memory
-// with asynchronous copies (one round trip per `lbatch` L entries), then
-// runs the program on shared memory.
+// with asynchronous copies, then runs the program on shared memory.
+// The copies' addresses come from index words read ahead, so that a row
+// waits for one round trip (its staged values) and no chain of table reads:
+// the row's ranges two rows ahead (row_info), the next row's per-lane words
+// (KKT input descriptors, D^-1 offsets of its steps, positions of its first
+// L re-reads) one row ahead, the next row's raw KKT inputs (they depend on
+// no factor value) copied one row ahead into a second buffer, and the
+// positions of a row's next L re-read batch while the current one is used.
 // Index words are read by the 32 lanes in parallel (one word each, 32 at a
-// time) and broadcast with shuffles: a uniform load per word would put one
-// L2 round trip per word on the row's critical path (the tables do not stay
-// in the L1 left beside the shared memory).
+// time) and broadcast with shuffles.
 constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int kPosRegs = 4;  // L re-read positions per lane: 32 x kPosRegs >= lbatch (at most 128)
 
-// Stage the L re-reads of updates [ub, ue): values per lane (each lane its
-// own instance's entry), slots warp-shared.
-__device__ __forceinline__ void stage_updates(const StreamPlan& sp, const float* Lu, float* lst, int* slot_w, int lane,
-                                              int ub, int ue) {
-  for (int base = ub; base < ue; base += 32) {
-    const int u = base + lane;
-    const int pos = u < ue ? __ldg(sp.upd_pos + u) : 0;
-    if (u < ue) cp_async4(slot_w + (u - ub), sp.upd_slot + u);
-    const int cnt = ue - base < 32 ? ue - base : 32;
-    for (int j = 0; j < cnt; ++j) cp_async4(lst + (base + j - ub) * 32, Lu + __shfl_sync(kFullMask, pos, j));
-  }
-}
-
-// How KKT input j of row k (original slot idx) is formed from its staged raw
-// input (solver.py:764-776): kind 0 the base value `add`, 1 a P entry
-// raw * p_scale + sigma-on-the-diagonal (`add`), 2 an A entry raw * a_scale;
-// src the P/A entry (-1: base).
-struct KktInput {
-  int kind, src;
-  float scale, add;
+struct PosBatch {
+  int v[kPosRegs];
 };
 
-__device__ __forceinline__ KktInput kkt_input(const Osqp& o, const Pattern& pat, int k, int i0, int j) {
-  const int idx = row_kkt_index(pat, k, i0, j);
-  KktInput r;
-  r.src = __ldg(o.kkt_src + idx);
-  if (r.src < 0) {
-    r.kind = 0;
-    r.scale = 0.0f;
-    r.add = __ldg(o.kkt_base + idx);
-  } else if (r.src < o.nnz_p) {
-    r.kind = 1;
-    r.scale = __ldg(o.p_scale + r.src);
-    r.add = __ldg(o.p_diag_sigma + r.src);
-  } else {
-    r.kind = 2;
-    r.scale = __ldg(o.a_scale + (r.src - o.nnz_p));
-    r.add = 0.0f;
+// positions of updates [ub, ue), lane holding update ub + lane + 32 i
+__device__ __forceinline__ void load_positions(const StreamPlan& sp, int ub, int ue, int lane, PosBatch& p) {
+#pragma unroll
+  for (int i = 0; i < kPosRegs; ++i) {
+    const int u = ub + lane + 32 * i;
+    p.v[i] = u < ue ? __ldg(sp.upd_pos + u) : 0;
   }
-  return r;
 }
 
+// Stage the L re-reads of updates [ub, ue) (ue - ub <= 32 kPosRegs): values
+// per lane (each lane its own instance's entry), slots warp-shared.
+__device__ __forceinline__ void stage_updates(const StreamPlan& sp, const float* Lu, float* lst, int* slot_w, int lane,
+                                              int ub, int ue, const PosBatch& p) {
+#pragma unroll
+  for (int i = 0; i < kPosRegs; ++i) {
+    const int base = ub + 32 * i;
+    if (base >= ue) break;
+    const int u = base + lane;
+    if (u < ue) cp_async4(slot_w + (u - ub), sp.upd_slot + u);
+    const int cnt = ue - base < 32 ? ue - base : 32;
+    for (int j = 0; j < cnt; ++j) cp_async4(lst + (base + j - ub) * 32, Lu + __shfl_sync(kFullMask, p.v[i], j));
+  }
+}
+
+// How KKT input j of a row is formed from its staged raw input
+// (solver.py:764-776), one descriptor per input in row-program order (the
+// diagonal, then the row's initial entries): x the P/A entry (-1: none),
+// y kind (0 the base value `add`, 1 a P entry raw * p_scale +
+// sigma-on-the-diagonal `add`, 2 an A entry raw * a_scale), z scale bits,
+// w add bits.
 __device__ __forceinline__ float kkt_input_value(int kind, float scale, float add, float raw) {
   if (kind == 0) return add;
   if (kind == 1) return raw * scale + add;
   return raw * scale;
+}
+
+__device__ __forceinline__ int4 kin_desc_of(const Osqp& o, int base, int j, int nkv) {
+  return j < nkv ? __ldg(o.kin_desc + base + j) : make_int4(-1, 0, 0, 0);
+}
+
+// the raw KKT inputs [first, nkv) of a row (descriptor of input first + lane in d)
+__device__ __forceinline__ void copy_kkt_inputs(const Osqp& o, const OsqpInputs& in, const float* pin,
+                                                const float* ain, float* kst, int first, int nkv, int4 d) {
+  const int cnt = nkv - first < 32 ? nkv - first : 32;
+  for (int j = 0; j < cnt; ++j) {
+    const int src = __shfl_sync(kFullMask, d.x, j);
+    if (src >= 0)
+      cp_async4(kst + (first + j) * 32,
+                src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
+  }
+}
+
+// A row's ranges: a = {p0, p1, i0, i1} (program steps, initial entries),
+// b = {ub, uend, doff, kin base} (updates, D^-1 offset of the row, first
+// KKT input descriptor).
+struct FacRow {
+  int4 a, b;
+};
+
+// the per-lane words of a row read ahead
+struct FacRowWords {
+  int4 kin;      // descriptor of KKT input `lane`
+  int sdoff;     // D^-1 offset of step p0 + lane
+  PosBatch pos;  // positions of the first L re-read batch
+};
+
+__device__ __forceinline__ FacRow load_fac_row(const StreamPlan& sp, int k) {
+  FacRow r;
+  r.a = __ldg(sp.row_info + 2 * k);
+  r.b = __ldg(sp.row_info + 2 * k + 1);
+  return r;
+}
+
+__device__ __forceinline__ void load_row_words(const Osqp& o, const StreamPlan& sp, const FacRow& r, int lbatch,
+                                               int lane, FacRowWords& w) {
+  const int p0 = r.a.x, p1 = r.a.y, nkv = 1 + r.a.w - r.a.z;
+  w.kin = kin_desc_of(o, r.b.w, lane, nkv);
+  w.sdoff = p0 + lane < p1 ? __ldg(sp.step_doff + p0 + lane) : 0;
+  const int ub = r.b.x, uend = r.b.y;
+  load_positions(sp, ub, ub + lbatch < uend ? ub + lbatch : uend, lane, w.pos);
 }
 
 __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
@@ -124,12 +164,14 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
   const int b = tile * 32 + lane;
   const int bb = b < batch ? b : batch - 1;  // padding lanes factor a copy of the last instance
   const int rmax = sp.max_row_nnz > 0 ? sp.max_row_nnz : 1;
+  const int kvmax = sp.max_row_kv;
   float* wbase = fsm + (size_t)warp * factor_warp_words(sp, lbatch);
   float* ys = wbase + lane;
   float* dst = ys + rmax * 32;
   float* lst = dst + rmax * 32;
-  float* kst = lst + lbatch * 32;
-  int* slot_w = reinterpret_cast<int*>(wbase + (2 * rmax + lbatch + sp.max_row_kv) * 32);  // warp-shared
+  float* kst = lst + lbatch * 32;        // raw KKT inputs of this row
+  float* kst_next = kst + kvmax * 32;    // and of the next
+  int* slot_w = reinterpret_cast<int*>(wbase + (2 * rmax + lbatch + 2 * kvmax) * 32);  // warp-shared
   int* off_w = slot_w + lbatch;
   int* boff_w = off_w + rmax;
   int* foff_w = boff_w + rmax;
@@ -141,37 +183,31 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
   const float* ain = in.aT + (long long)bb * in.sba;
   const int n = pat.n;
   bool bad = false;
-  // the table pointers of the next row, loaded one row ahead
-  int n_p0 = __ldg(pat.proc_ptr), n_p1 = __ldg(pat.proc_ptr + 1);
-  int n_i0 = __ldg(pat.init_ptr), n_i1 = __ldg(pat.init_ptr + 1);
-  int n_ub = __ldg(sp.upd_ptr + n_p0), n_uend = __ldg(sp.upd_ptr + n_p1), n_doff = __ldg(sp.dinv_off);
+  // row 0's ranges and words, row 1's ranges, row 0's raw inputs
+  FacRow cur = load_fac_row(sp, 0);
+  FacRow nxt = n > 1 ? load_fac_row(sp, 1) : cur;
+  FacRowWords wc;
+  load_row_words(o, sp, cur, lbatch, lane, wc);
+  copy_kkt_inputs(o, in, pin, ain, kst, 0, 1 + cur.a.w - cur.a.z, wc.kin);
+  cp_async_commit();
   for (int k = 0; k < n; ++k) {
-    const int p0 = n_p0, p1 = n_p1, i0 = n_i0, i1 = n_i1, u_end = n_uend, doff_k = n_doff;
-    int ub = n_ub;
-    int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+    const int p0 = cur.a.x, p1 = cur.a.y, i0 = cur.a.z, i1 = cur.a.w;
+    const int u_end = cur.b.y, doff_k = cur.b.z, kbase = cur.b.w;
     const int nkv = 1 + i1 - i0;
-    // stage this row's reads: KKT inputs, D^-1 of its steps, step tables, L re-reads
-    // (lane j resolves KKT input j: its source and how its value is formed)
-    // (inputs past the first 32 are resolved again, 32 at a time, when used)
-    auto input_of = [&](int j) {
-      KktInput r{0, -1, 0.0f, 0.0f};
-      if (j < nkv) r = kkt_input(o, pat, k, i0, j);
-      return r;
-    };
-    const KktInput kin = input_of(lane);
-    for (int base = 0; base < nkv; base += 32) {
-      const KktInput kc = base == 0 ? kin : input_of(base + lane);
-      const int cnt = nkv - base < 32 ? nkv - base : 32;
-      for (int j = 0; j < cnt; ++j) {
-        const int src = __shfl_sync(kFullMask, kc.src, j);
-        if (src >= 0)
-          cp_async4(kst + (base + j) * 32,
-                    src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
-      }
-    }
+    int ub = cur.b.x;
+    int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
+    // reads ahead: the ranges of row k + 2, the words of row k + 1
+    FacRow nn = nxt;
+    if (k + 2 < n) nn = load_fac_row(sp, k + 2);
+    FacRowWords wn = wc;
+    if (k + 1 < n) load_row_words(o, sp, nxt, lbatch, lane, wn);
+    // stage this row's reads: raw inputs past the first 32, D^-1 of its
+    // steps, step tables, the first batch of L re-reads
+    for (int base = 32; base < nkv; base += 32)
+      copy_kkt_inputs(o, in, pin, ain, kst, base, nkv, kin_desc_of(o, kbase, base + lane, nkv));
     for (int base = p0; base < p1; base += 32) {
       const int e = base + lane;
-      const int doff = e < p1 ? __ldg(sp.step_doff + e) : 0;
+      const int doff = base == p0 ? wc.sdoff : (e < p1 ? __ldg(sp.step_doff + e) : 0);
       if (e < p1) {
         cp_async4(off_w + (e - p0), pat.proc_offsets + e);
         cp_async4(boff_w + (e - p0), sp.proc_boff + e);
@@ -180,31 +216,29 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
       const int cnt = p1 - base < 32 ? p1 - base : 32;
       for (int j = 0; j < cnt; ++j) cp_async4(dst + (base + j - p0) * 32, Ld + __shfl_sync(kFullMask, doff, j));
     }
-    stage_updates(sp, Lu, lst, slot_w, lane, ub, ue);
-    // the next row's table pointers while the copies are in flight
-    if (k + 1 < n) {
-      n_p0 = p1;
-      n_p1 = __ldg(pat.proc_ptr + k + 2);
-      n_i0 = i1;
-      n_i1 = __ldg(pat.init_ptr + k + 2);
-      n_ub = u_end;
-      n_uend = __ldg(sp.upd_ptr + n_p1);
-      n_doff = __ldg(sp.dinv_off + k + 1);
-    }
-    cp_async_wait_all();
+    stage_updates(sp, Lu, lst, slot_w, lane, ub, ue, wc.pos);
+    cp_async_commit();
+    // the positions of the row's next L re-read batch, if any
+    PosBatch pnext;
+    load_positions(sp, ue, ue + lbatch < u_end ? ue + lbatch : u_end, lane, pnext);
+    // the next row's raw inputs into the other buffer (they depend on no factor value)
+    if (k + 1 < n) copy_kkt_inputs(o, in, pin, ain, kst_next, 0, 1 + nxt.a.w - nxt.a.z, wn.kin);
+    cp_async_commit();
+    cp_async_wait_group<1>();  // everything but the next row's inputs
     __syncwarp();
     // the row program (the reference's order: diagonal input, then the
     // initial entries in order, then the steps)
     for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
     float dk = 0.0f;
     for (int base = 0; base < nkv; base += 32) {
-      const KktInput kc = base == 0 ? kin : input_of(base + lane);
+      const int4 kc = base == 0 ? wc.kin : kin_desc_of(o, kbase, base + lane, nkv);
       const int jl = base + lane;
       const int islot = (jl > 0 && jl < nkv) ? __ldg(sp.init_slot + i0 + jl - 1) : 0;
       const int cnt = nkv - base < 32 ? nkv - base : 32;
       for (int jj = 0; jj < cnt; ++jj) {
-        const float v = kkt_input_value(__shfl_sync(kFullMask, kc.kind, jj), __shfl_sync(kFullMask, kc.scale, jj),
-                                        __shfl_sync(kFullMask, kc.add, jj), kst[(base + jj) * 32]);
+        const float v = kkt_input_value(__shfl_sync(kFullMask, kc.y, jj),
+                                        __int_as_float(__shfl_sync(kFullMask, kc.z, jj)),
+                                        __int_as_float(__shfl_sync(kFullMask, kc.w, jj)), kst[(base + jj) * 32]);
         const int s = __shfl_sync(kFullMask, islot, jj);
         if (base + jj == 0) {
           dk = v;
@@ -222,7 +256,8 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
           __syncwarp();
           ub = ue;
           ue = ub + lbatch < u_end ? ub + lbatch : u_end;
-          stage_updates(sp, Lu, lst, slot_w, lane, ub, ue);
+          stage_updates(sp, Lu, lst, slot_w, lane, ub, ue, pnext);
+          load_positions(sp, ue, ue + lbatch < u_end ? ue + lbatch : u_end, lane, pnext);
           cp_async_wait_all();
           __syncwarp();
         }
@@ -239,7 +274,14 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     bad |= !(di != 0.0f) || !isfinite(di);
     Ld[doff_k] = di;
     __syncwarp();  // the warp-shared tables are restaged by the next row
+    cur = nxt;
+    nxt = nn;
+    wc = wn;
+    float* t = kst;
+    kst = kst_next;
+    kst_next = t;
   }
+  cp_async_wait_all();
   for (int i = 0; i < sp.n_pad_b; ++i) Lu[__ldg(sp.pad_boff + i)] = 0.0f;
   for (int i = 0; i < sp.n_pad_f; ++i) F[__ldg(sp.pad_foff + i)] = 0.0f;
   if (status) status[b] = bad ? WMPC_STATUS_ZERO_PIVOT : 0;

@@ -41,28 +41,63 @@ __global__ void __launch_bounds__(256) factor_kernel(Pattern pat, const float* _
 // of a dense n-vector), and every value a row reads from memory -- its KKT
 // inputs, D^-1 of its steps' columns, the L entries of those columns above
 // the row -- brought into shared memory with 4-byte asynchronous copies
-// before the row's arithmetic (one round trip per `lbatch` L entries).  The
-// index words behind those copies are read by the 32 lanes in parallel and
-// broadcast with shuffles.  Same operation order as factor_instance (the
-// reference's row program), so the same bits.  Lanes past the batch factor a
-// copy of the last instance; with `only`, lanes of unmarked instances compute
-// and store nothing of theirs.
+// before the row's arithmetic.  The copies' addresses come from index words
+// read ahead (a row's ranges two rows ahead, its per-lane words -- KKT slots
+// of its inputs, columns of its steps, positions of its first L re-reads --
+// one row ahead, the positions of a row's next L re-read batch while the
+// current one is used), and a row's KKT inputs, which depend on no factor
+// value, are copied one row ahead into a second buffer: a row waits for one
+// round trip per L re-read batch and no chain of table reads.  Index words
+// are read by the 32 lanes in parallel and broadcast with shuffles.  Same
+// operation order as factor_instance (the reference's row program), so the
+// same bits.  Lanes past the batch factor a copy of the last instance; with
+// `only`, lanes of unmarked instances compute and store nothing of theirs.
 struct FactorTables {
   const int* init_slot;
   const int* upd_ptr;
   const int* upd_slot;
   const int* upd_lidx;
+  const int4* row_info;  // [2 n] {p0, p1, i0, i1}, {first update, update end, first input, 0}
+  const int* kin_slot;   // per row, per KKT input (diagonal, then initial entries): original KKT slot
   int max_row, max_kv;
 };
 
 // per-warp shared memory in 4-byte words: ys, staged D^-1 [max_row] and L
-// re-reads [lbatch] and KKT inputs [max_kv] per lane; update slots [lbatch],
-// step offsets, L positions and columns [3 max_row] shared by the warp
+// re-reads [lbatch] and KKT inputs of this row and the next [2 max_kv] per
+// lane; update slots [lbatch], step offsets, L positions and columns
+// [3 max_row] shared by the warp
 __host__ __device__ inline int factor_rows_words(int max_row, int max_kv, int lbatch) {
-  return (2 * max_row + lbatch + max_kv) * 32 + lbatch + 3 * max_row;
+  return (2 * max_row + lbatch + 2 * max_kv) * 32 + lbatch + 3 * max_row;
 }
 
 constexpr unsigned kLanes = 0xffffffffu;
+constexpr int kRowPosRegs = 4;  // L re-read positions per lane: 32 x kRowPosRegs >= lbatch (at most 128)
+
+struct RowPos {
+  int v[kRowPosRegs];
+};
+
+struct RowWords {
+  int kin;  // KKT slot of input `lane`
+  int col;  // column of step p0 + lane
+  RowPos pos;
+};
+
+__device__ __forceinline__ void row_positions(const FactorTables& ft, int ub, int ue, int lane, RowPos& p) {
+#pragma unroll
+  for (int i = 0; i < kRowPosRegs; ++i) {
+    const int u = ub + lane + 32 * i;
+    p.v[i] = u < ue ? __ldg(ft.upd_lidx + u) : 0;
+  }
+}
+
+__device__ __forceinline__ void row_words(const Pattern& pat, const FactorTables& ft, int4 a, int4 b, int lbatch,
+                                          int lane, RowWords& w) {
+  const int nkv = 1 + a.w - a.z;
+  w.kin = lane < nkv ? __ldg(ft.kin_slot + b.z + lane) : 0;
+  w.col = a.x + lane < a.y ? __ldg(pat.proc_cols + a.x + lane) : 0;
+  row_positions(ft, b.x, b.x + lbatch < b.y ? b.x + lbatch : b.y, lane, w.pos);
+}
 
 __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTables ft, const float* __restrict__ values,
                                                          long long ldv, int bstride, float* lx, float* d, float* dinv,
@@ -79,43 +114,56 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
   float* dst = ys + ft.max_row * 32;
   float* lst = dst + ft.max_row * 32;
   float* kst = lst + lbatch * 32;
-  int* slot_w = reinterpret_cast<int*>(wbase + (2 * ft.max_row + lbatch + ft.max_kv) * 32);
+  float* kst_next = kst + ft.max_kv * 32;
+  int* slot_w = reinterpret_cast<int*>(wbase + (2 * ft.max_row + lbatch + 2 * ft.max_kv) * 32);
   int* off_w = slot_w + lbatch;
   int* lid_w = off_w + ft.max_row;
   const float* vb = values + (long long)bb * bstride;
   const int n = pat.n;
-  auto stage_updates = [&](int ub, int ue) {
-    for (int base = ub; base < ue; base += 32) {
+  // L re-reads of updates [ub, ue) (positions of ub + lane + 32 i in p)
+  auto stage_updates = [&](int ub, int ue, const RowPos& p) {
+#pragma unroll
+    for (int i = 0; i < kRowPosRegs; ++i) {
+      const int base = ub + 32 * i;
+      if (base >= ue) break;
       const int u = base + lane;
-      const int lid = u < ue ? __ldg(ft.upd_lidx + u) : 0;
       if (u < ue) cp_async4(slot_w + (u - ub), ft.upd_slot + u);
       const int cnt = ue - base < 32 ? ue - base : 32;
       for (int j = 0; j < cnt; ++j)
-        cp_async4(lst + (base + j - ub) * 32, lx + (long long)__shfl_sync(kLanes, lid, j) * batch + bb);
+        cp_async4(lst + (base + j - ub) * 32, lx + (long long)__shfl_sync(kLanes, p.v[i], j) * batch + bb);
     }
   };
+  // KKT inputs [first, nkv) of a row (slot of input first + lane in slot)
+  auto copy_inputs = [&](float* dstk, int first, int nkv, int slot) {
+    const int cnt = nkv - first < 32 ? nkv - first : 32;
+    for (int j = 0; j < cnt; ++j) cp_async4(dstk + (first + j) * 32, vb + (long long)__shfl_sync(kLanes, slot, j) * ldv);
+  };
+  int4 ca = __ldg(ft.row_info), cb = __ldg(ft.row_info + 1);
+  int4 na = n > 1 ? __ldg(ft.row_info + 2) : ca, nb = n > 1 ? __ldg(ft.row_info + 3) : cb;
+  RowWords wc;
+  row_words(pat, ft, ca, cb, lbatch, lane, wc);
+  copy_inputs(kst, 0, 1 + ca.w - ca.z, wc.kin);
+  cp_async_commit();
   for (int k = 0; k < n; ++k) {
-    const int p0 = __ldg(pat.proc_ptr + k), p1 = __ldg(pat.proc_ptr + k + 1);
-    const int i0 = __ldg(pat.init_ptr + k), i1 = __ldg(pat.init_ptr + k + 1);
-    const int u_end = __ldg(ft.upd_ptr + p1);
-    int ub = __ldg(ft.upd_ptr + p0);
+    const int p0 = ca.x, p1 = ca.y, i0 = ca.z, i1 = ca.w;
+    const int u_end = cb.y, kbase = cb.z;
+    int ub = cb.x;
     int ue = ub + lbatch < u_end ? ub + lbatch : u_end;
     const int nkv = 1 + i1 - i0;
-    // KKT inputs (original slot of input j: the diagonal, then the initial entries)
-    auto orig_of = [&](int j) {
-      if (j >= nkv) return 0;
-      return __ldg(pat.perm_to_orig + (j == 0 ? __ldg(pat.diag_pos + k) : __ldg(pat.init_pos + i0 + j - 1)));
-    };
-    for (int base = 0; base < nkv; base += 32) {
-      const int orig = orig_of(base + lane);
-      const int cnt = nkv - base < 32 ? nkv - base : 32;
-      for (int j = 0; j < cnt; ++j)
-        cp_async4(kst + (base + j) * 32, vb + (long long)__shfl_sync(kLanes, orig, j) * ldv);
+    // reads ahead: the ranges of row k + 2, the words of row k + 1
+    int4 nna = na, nnb = nb;
+    if (k + 2 < n) {
+      nna = __ldg(ft.row_info + 2 * (k + 2));
+      nnb = __ldg(ft.row_info + 2 * (k + 2) + 1);
     }
-    // D^-1 of the steps' columns, and the step tables
+    RowWords wn = wc;
+    if (k + 1 < n) row_words(pat, ft, na, nb, lbatch, lane, wn);
+    // KKT inputs past the first 32, D^-1 of the steps' columns, the step tables, the first L batch
+    for (int base = 32; base < nkv; base += 32)
+      copy_inputs(kst, base, nkv, base + lane < nkv ? __ldg(ft.kin_slot + kbase + base + lane) : 0);
     for (int base = p0; base < p1; base += 32) {
       const int e = base + lane;
-      const int col = e < p1 ? __ldg(pat.proc_cols + e) : 0;
+      const int col = base == p0 ? wc.col : (e < p1 ? __ldg(pat.proc_cols + e) : 0);
       if (e < p1) {
         cp_async4(off_w + (e - p0), pat.proc_offsets + e);
         cp_async4(lid_w + (e - p0), pat.proc_lidx + e);
@@ -124,8 +172,13 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
       for (int j = 0; j < cnt; ++j)
         cp_async4(dst + (base + j - p0) * 32, dinv + (long long)__shfl_sync(kLanes, col, j) * batch + bb);
     }
-    stage_updates(ub, ue);
-    cp_async_wait_all();
+    stage_updates(ub, ue, wc.pos);
+    cp_async_commit();
+    RowPos pnext;
+    row_positions(ft, ue, ue + lbatch < u_end ? ue + lbatch : u_end, lane, pnext);
+    if (k + 1 < n) copy_inputs(kst_next, 0, 1 + na.w - na.z, wn.kin);
+    cp_async_commit();
+    cp_async_wait_group<1>();  // everything but the next row's inputs
     __syncwarp();
     for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
     float dk = kst[0];
@@ -147,7 +200,8 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
           __syncwarp();
           ub = ue;
           ue = ub + lbatch < u_end ? ub + lbatch : u_end;
-          stage_updates(ub, ue);
+          stage_updates(ub, ue, pnext);
+          row_positions(ft, ue, ue + lbatch < u_end ? ue + lbatch : u_end, lane, pnext);
           cp_async_wait_all();
           __syncwarp();
         }
@@ -163,7 +217,16 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
       dinv[(long long)k * batch + b] = 1.0f / dk;
     }
     __syncwarp();  // the warp-shared tables are restaged by the next row
+    ca = na;
+    cb = nb;
+    na = nna;
+    nb = nnb;
+    wc = wn;
+    float* t = kst;
+    kst = kst_next;
+    kst_next = t;
   }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -246,7 +309,7 @@ int launch_factor_plan(const wmpc_plan& plan, const float* values, long long ldv
     if (smem <= (size_t)kMaxSmemBytes) {
       WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       const FactorTables ft{plan.fac_init_slot, plan.fac_upd_ptr, plan.fac_upd_slot, plan.fac_upd_lidx,
-                            plan.fac_max_row, plan.fac_max_kv};
+                            plan.fac_row_info, plan.fac_kin_slot, plan.fac_max_row, plan.fac_max_kv};
       profile_mark_begin(stream, kProfileFactor);
       factor_rows_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, stream>>>(pat, ft, values, ldv, bstride, lx, d,
                                                                                dinv, batch, n_tiles, lbatch, only);

@@ -106,6 +106,10 @@ struct StreamPlan {
   // frontier form with termination checks: the unscale factor of each
   // permuted KKT index (the plain form's records carry it in their last word)
   const float* unscale_perm;  // [n]
+  // factorization rows read ahead: per row {p0, p1, i0, i1} (program steps,
+  // initial entries), {ub, uend, doff, kin base} (updates, D^-1 offset,
+  // first KKT input descriptor of the row in Osqp::kin_desc)
+  const int4* row_info;  // [2 n]
 };
 
 // ---- PTX helpers -----------------------------------------------------------
@@ -214,6 +218,14 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
 }
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// wait until at most N of this thread's committed cp.async groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
