@@ -1,6 +1,7 @@
-"""rho adaptation on the GPU (per instance, plain mode) against the oracle's
-restatement of the same rule: iterates bit for bit, the same final rho and
-the same number of rho changes (refactorizations) per instance.  The
+"""rho adaptation on the GPU (per instance; the per-call kernels and the
+streaming persistent path) against the oracle's restatement of the same
+rule: iterates bit for bit, the same final rho and the same number of rho
+changes (refactorizations) per instance.  The
 reference has no rho adaptation (solver.py:587-588 rejects adaptive_rho);
 the rule is OSQP's residual balancing (Stellato et al. 2020, sec. 5.2)."""
 
@@ -14,16 +15,17 @@ from warpmpc_b200.jax_osqp import OSQPSettings, compile_osqp
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("mode", ["plain", "persistent"])
 @pytest.mark.parametrize("cls", [problems.SMALL, problems.QUADROTOR], ids=lambda c: c.name)
-def test_adaptive_rho_matches_oracle(cuda_device, cls):
+def test_adaptive_rho_matches_oracle(cuda_device, cls, mode):
     import torch
 
     b = problems.make_batch(cls, 48, seed=17)
     settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 60, "adaptive_rho": True,
                                "adaptive_rho_interval": 10})
     plan = problems.make_plan(b, settings)
-    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
-    assert comp.engine.mode == "plain"
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode=mode)
+    assert comp.engine.mode == mode
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
     got = [o.cpu().numpy() for o in comp.solve(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u))]
     rho = comp.engine.last_rho.cpu().numpy()
@@ -56,3 +58,41 @@ def test_adaptive_rho_shared_matrices_and_warm_start(cuda_device):
     for name, g, r in zip(("x", "z", "y"), got[:3], ref[:3]):
         np.testing.assert_array_equal(g, r, err_msg=name)
     np.testing.assert_array_equal(comp.engine.last_rho_updates.cpu().numpy(), ref[7])
+
+
+@pytest.mark.parametrize("frontier", ["0", "1"])
+def test_adaptive_rho_persistent_many_tiles(cuda_device, monkeypatch, frontier):
+    """The streaming path over more tiles than SMs (several tiles per CTA, the
+    tiles whose instances keep their rho skip the refactorization), both
+    schedule forms, warm-started, against the per-call kernels: the same
+    bits, rho and refactor counts."""
+    import torch
+
+    from warpmpc_b200 import native
+
+    monkeypatch.setenv("WMPC_STREAM_FRONTIER", frontier)
+    cls = problems.CARTPOLE
+    n = 400 * 32 + 7
+    b = problems.make_batch(cls, n, seed=37)
+    settings = OSQPSettings(**{**problems.DEFAULT_SETTINGS, "max_iter": 30, "adaptive_rho": True,
+                               "adaptive_rho_interval": 8, "adaptive_rho_tolerance": 3.0})
+    plan = problems.make_plan(b, settings)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    rng = np.random.default_rng(5)
+    warm = [t(rng.standard_normal((n, k)).astype(np.float32) * 0.05) for k in (plan.n, plan.m, plan.m)]
+    out = {}
+    for mode in ("plain", "persistent"):
+        comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode=mode)
+        assert comp.engine.mode == mode
+        got = comp.solve_warm_start(t(b.p_values), t(b.a_values), t(b.q), t(b.l), t(b.u), *warm)
+        torch.cuda.synchronize()
+        if mode == "persistent":
+            assert native.stream_last_launch()["form"] == ("frontier" if frontier == "1" else "plain")
+        out[mode] = ([o.cpu().numpy() for o in got[:3]], comp.engine.last_rho.cpu().numpy(),
+                     comp.engine.last_rho_updates.cpu().numpy())
+    (xp, rp, up), (xs, rs, us) = out["plain"], out["persistent"]
+    for name, g, r in zip(("x", "z", "y"), xs, xp):
+        np.testing.assert_array_equal(g, r, err_msg=name)
+    np.testing.assert_array_equal(rs, rp)
+    np.testing.assert_array_equal(us, up)
+    assert 0 < (up > 0).sum() < n  # some instances changed rho, some kept it

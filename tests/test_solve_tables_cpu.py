@@ -11,7 +11,7 @@ from oracle import qdldl_ref
 from warpmpc_b200 import problems, schedule
 
 # the kernel's constants (solve_stream.cu)
-BOX, CHUNK_ENTRIES, CHUNK_COLS, RHS_ROWS, TABLE_BYTES = 32, 64, 32, 96, 512
+BOX, CHUNK_ENTRIES, CHUNK_COLS, RHS_ROWS, TABLE_BYTES, STEP = 32, 64, 32, 96, 512, 8
 DATA_ROWS = CHUNK_ENTRIES + CHUNK_COLS
 
 
@@ -20,7 +20,9 @@ def replay(qp, tab, lx, dinv, rhs):
     n, nnz_l = qp.n, qp.nnz_l
     T, D = tab["tables"], tab["desc"]
     f32 = np.float32
-    X = np.zeros(n, dtype=f32)
+    # rows, the trash row (n: padded forward slots write it) and the zero row (n + 1)
+    X = np.zeros(n + 2, dtype=f32)
+    X[n] = np.nan  # never read by a real entry
     # rhs items: boxes of 32 rows inside the data area, rows past n zero-filled
     for k in range((n + RHS_ROWS - 1) // RHS_ROWS):
         r0 = k * RHS_ROWS
@@ -42,7 +44,10 @@ def replay(qp, tab, lx, dinv, rhs):
         roff = t[4 + C : 4 + C + E]
         assert np.all(roff % 128 == 0) and np.all(roff // 128 < n) and np.all(roff >= 0)
         assert np.all(np.diff(np.concatenate([[0], cend])) >= 0) and (C == 0 or cend[-1] == E)
-        L = np.zeros(((E + BOX - 1) // BOX) * BOX, dtype=f32)
+        # a step reads up to STEP - 1 table words and L rows past the chunk's
+        # last entry: still inside the table area and the stage's data rows
+        assert (4 + C + E + STEP - 1) * 4 <= TABLE_BYTES and E + STEP - 1 <= DATA_ROWS
+        L = np.full(DATA_ROWS, np.nan, dtype=f32)  # stale stage contents past the copied rows
         L[:E] = lx[e0 : e0 + E]  # rows past nnz_l would be zero-filled by the copy
         return c0, C, cend, roff // 128, L
 
@@ -50,21 +55,30 @@ def replay(qp, tab, lx, dinv, rhs):
     for k in range(nch):
         c0, C, cend, rows, L = chunk(k, False)
         b = 0
-        for j in range(C):
-            e = int(cend[j])
-            if e > b:
-                val = X[c0 + j]
-                for q in range(b, e):
-                    X[rows[q]] = f32(X[rows[q]] - f32(L[q] * val))
-            b = e
+        with np.errstate(invalid="ignore"):
+            for j in range(C):
+                e = int(cend[j])
+                if e > b:
+                    val = X[c0 + j]
+                    for q in range(b, e, STEP):
+                        o = [int(rows[q + i]) if q + i < e else n for i in range(STEP)]
+                        w = [X[o[i]] for i in range(STEP)]
+                        for i in range(STEP):
+                            X[o[i]] = f32(w[i] - f32(L[q + i] * val))
+                b = e
+    assert X[n + 1] == 0.0
     for k in range(nch - 1, -1, -1):
         c0, C, cend, rows, L = chunk(k, True)
         for j in range(C - 1, -1, -1):
             b = int(cend[j - 1]) if j > 0 else 0
             e = int(cend[j])
             corr = f32(0.0)
-            for q in range(b, e):
-                corr = f32(corr + f32(L[q] * X[rows[q]]))
+            for q in range(b, e, STEP):
+                for i in range(STEP):
+                    if q + i < e:
+                        corr = f32(corr + f32(L[q + i] * X[rows[q + i]]))
+                    else:  # L = 0 times the zero row
+                        corr = f32(corr + f32(f32(0.0) * X[n + 1]))
             X[c0 + j] = f32(f32(X[c0 + j] * dinv[c0 + j]) - corr)
     # chunks cover every column exactly once, in order
     assert np.array_equal(np.concatenate([np.arange(d[3], d[3] + d[5]) for d in D]), np.arange(n))

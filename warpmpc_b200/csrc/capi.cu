@@ -211,7 +211,17 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
   }
   std::vector<float> unscale_perm(hp.n, 1.0f);
   for (int i = 0; i < hp.n; ++i) unscale_perm[i] = unscale[hp.p[i]];
+  // rho class of each U index's constraint (per-instance rho)
+  std::vector<int> u_cls;
+  if (desc->rho_type) {
+    u_cls.assign(hp.n, 0);
+    for (int u = 0; u < hp.n; ++u) {
+      const int orig = hs.u_orig[u];
+      if (orig >= desc->n) u_cls[u] = desc->rho_type[orig - desc->n];
+    }
+  }
   Packer sk;
+  if (!u_cls.empty()) sk.add(u_cls.data(), u_cls.size(), &sp.u_cls);
   sk.addf(unscale_perm.data(), unscale_perm.size(), &sp.unscale_perm);
   sk.add(hs.chunk_off.data(), hs.chunk_off.size(), &sp.chunk_off);
   sk.add(hs.chunk_units.data(), hs.chunk_units.size(), &sp.chunk_units);
@@ -745,6 +755,42 @@ int wmpc_osqp_create(const wmpc_osqp_desc* desc, const wmpc_plan* kkt_plan, wmpc
     pk.add(desc->rho_type, m, &o.rho_type);
     pk.add(kkt_rho_row.data(), nk, &o.kkt_rho_row);
     o.rho0 = desc->rho;
+    // the factorization rows' inputs with every -1/rho slot read from the
+    // instance's 1/rho row (constraint r: source nnz_p + nnz_a + r, kind 3)
+    const wmpc_plan& kp = *kkt_plan;
+    std::vector<int32_t> kin;
+    kin.reserve(4 * ((size_t)(n + m) + kp.h_init_pos.size()));
+    auto put = [&](int slot) {
+      const int idx = kp.h_perm_to_orig[slot];
+      const int r = kkt_rho_row[idx];
+      const int src = kkt_src[idx];
+      float scale = 0.0f, add = 0.0f;
+      int kind = 0, s = -1;
+      if (r >= 0) {
+        kind = 3;
+        s = np + na + r;
+      } else if (src < 0) {
+        add = desc->kkt_base[idx];
+      } else if (src < np) {
+        kind = 1;
+        s = src;
+        scale = desc->p_scale[src];
+        add = desc->p_diag_sigma[src];
+      } else {
+        kind = 2;
+        s = src;
+        scale = desc->a_scale[src - np];
+      }
+      int32_t sb, ab;
+      std::memcpy(&sb, &scale, 4);
+      std::memcpy(&ab, &add, 4);
+      kin.insert(kin.end(), {s, kind, sb, ab});
+    };
+    for (int k = 0; k < n + m; ++k) {
+      put(kp.h_diag_pos[k]);
+      for (int e = kp.h_init_ptr[k]; e < kp.h_init_ptr[k + 1]; ++e) put(kp.h_init_pos[e]);
+    }
+    pk.add(kin.data(), kin.size(), reinterpret_cast<const int**>(&o.kin_desc_rho));
   }
   int* block = nullptr;
   int rc = pk.upload(&block);

@@ -635,6 +635,13 @@ Layout carve(const Osqp& o, const Pattern& pat, int batch, int pb, int ab, int m
                                   q->has_frontier ? stream_workspace_floats(q->spf, batch) : (size_t)0));
     L.stream_status = reinterpret_cast<int*>(c.take((size_t)((batch + 31) / 32) * 32));
     L.error_word = reinterpret_cast<int*>(c.take(4));
+    if (o.rho_type) {  // per-instance rho (adaptation)
+      L.rho_row = c.take((size_t)o.m * batch);
+      L.rinv_row = c.take((size_t)o.m * batch);
+      L.rho_b = c.take((size_t)batch);
+      L.rho_changed = reinterpret_cast<int*>(c.take((size_t)batch));
+      L.rho_count = reinterpret_cast<int*>(c.take((size_t)batch));
+    }
     *total = c.used;
     return L;
   }
@@ -695,7 +702,8 @@ int assemble_and_factor(const Osqp& o, const wmpc_plan& plan, const float* pT, i
 int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
                  const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
                  const float* qs, const float* ls, const float* us, bool warm, bool track, float* work,
-                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s);
+                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s,
+                 const float* rinv_rows = nullptr, const int* only = nullptr);
 int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, cudaStream_t s);
 int stream_end(const StreamPlan& sp, const Osqp& o, const StreamJobDesc& job, float* x, float* z, float* y,
                cudaStream_t s);
@@ -820,6 +828,62 @@ int stream_solve_begin(const wmpc_osqp& q, const wmpc_osqp_options& opt, const w
   return WMPC_OK;
 }
 
+// Streaming solve with per-instance rho adaptation (fixed iterations): the
+// iterations run in launches of adaptive_rho_interval; between two, the state
+// comes back, each instance estimates its rho (rho_update_kernel, the plain
+// path's rule and sums), the tiles holding an instance whose rho changed
+// refactor with their instances' own -1/rho, and the next launch continues
+// from the state with each lane's rho by row class (admm_stream_kernel's
+// per-instance-rho form).  Same iterates, rho and refactor counts as the
+// plain path.
+int stream_solve_adaptive(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d,
+                          const Layout& L, StreamJobDesc* job, cudaStream_t s) {
+  const Osqp& o = q.dev;
+  const int B = d.batch, pb = d.p_batch, ab = d.a_batch;
+  const int sbp = pb > 1 ? 1 : 0, sba = ab > 1 ? 1 : 0;
+  const bool frontier = frontier_for(q, false, (B + 31) / 32);
+  const StreamPlan& sp = frontier ? q.spf : q.sp;
+  int rc;
+  if ((rc = stage_inputs(o, opt, d, L, s))) return rc;
+  WMPC_CUDA_TRY(cudaMemsetAsync(L.error_word, 0, sizeof(int), s));
+  dim3 rgrid(ceil_div(B, 128), o.m > 0 ? (o.m < 2048 ? o.m : 2048) : 1);
+  rho_init_kernel<<<rgrid, 128, 0, s>>>(o, L.rho_row, L.rinv_row, L.rho_b, L.rho_count, B);
+  WMPC_LAUNCH_CHECK();
+  State st{L.x, L.z, L.y, L.qs, L.ls, L.us, B};
+  auto begin = [&](bool warm, const int* only) -> int {
+    int r = stream_begin(q.kkt_plan->pat, sp, o, L.pT, pb, sbp, L.aT, ab, sba, L.x, L.z, L.y, L.qs, L.ls, L.us, warm,
+                         false, L.stream_ws, L.stream_status, B, q.num_sms, false, job, s, L.rinv_row, only);
+    job->check_every = 0;
+    job->ctas_limit = q.ctas_limit;
+    job->chg_eps = opt.eps_abs;
+    job->iters = nullptr;
+    job->rho_b = L.rho_b;
+    job->rho_count = L.rho_count;
+    return r;
+  };
+  if ((rc = begin(opt.warm_start != 0, nullptr))) return rc;
+  const int interval = opt.adaptive_rho_interval;
+  for (int it = 0; it < opt.max_iter;) {
+    const int seg = opt.max_iter - it < interval ? opt.max_iter - it : interval;
+    job->max_iter = seg;
+    if ((rc = stream_run(job, 1, L.error_word, q.num_sms, s))) return rc;
+    it += seg;
+    if (it < opt.max_iter) {
+      if ((rc = stream_end(sp, o, *job, L.x, L.z, L.y, s))) return rc;
+      rho_update_kernel<<<ceil_div(B, 128), 128, 0, s>>>(o, L.pT, pb, sbp, L.aT, ab, sba, st, L.rho_row, L.rinv_row,
+                                                         L.rho_b, L.rho_changed, L.rho_count,
+                                                         opt.adaptive_rho_tolerance, B);
+      WMPC_LAUNCH_CHECK();
+      if ((rc = begin(true, L.rho_changed))) return rc;
+    }
+  }
+  if (d.rho || d.rho_updates) {
+    rho_report_kernel<<<ceil_div(B, 256), 256, 0, s>>>(L.rho_b, L.rho_count, o.rho0, d.rho, d.rho_updates, B);
+    WMPC_LAUNCH_CHECK();
+  }
+  return WMPC_OK;
+}
+
 // Streaming solve, second half: state back, exact residuals and status, outputs.
 int stream_solve_end(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp_batch& d, const Layout& L,
                      const StreamJobDesc& job, const int* error_word, cudaStream_t s) {
@@ -862,7 +926,10 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
     return fail(WMPC_ERR_INVALID_ARGUMENT, "prim_res, dual_res and obj go together (and with termination checks)");
   const bool adaptive = opt.adaptive_rho_interval > 0;
   if (adaptive) {
-    if (mode != WMPC_OSQP_PLAIN) return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation runs in plain mode");
+    if (mode != WMPC_OSQP_PLAIN && !(mode == WMPC_OSQP_PERSISTENT && stream_eligible(q, &opt)))
+      return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation runs in plain mode or on the streaming persistent path");
+    if (mode == WMPC_OSQP_PERSISTENT && opt.check_termination > 0)
+      return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation on the persistent path runs fixed iterations");
     if (external || opt.reuse_factor)
       return fail(WMPC_ERR_UNSUPPORTED, "rho adaptation refactors: it cannot start from a given factorization");
     if (!o.rho_type || !o.kkt_rho_row)
@@ -876,6 +943,11 @@ int osqp_solve(const wmpc_osqp& q, const wmpc_osqp_options& opt, const wmpc_osqp
   if (ws == nullptr || ws_bytes < need)
     return fail(WMPC_ERR_WORKSPACE, "OSQP solve needs %zu workspace bytes, got %zu", need, ws_bytes);
   int rc;
+  if (L.streaming && adaptive) {
+    StreamJobDesc job;
+    if ((rc = stream_solve_adaptive(q, opt, d, L, &job, s))) return rc;
+    return stream_solve_end(q, opt, d, L, job, L.error_word, s);
+  }
   if (L.streaming) {
     StreamJobDesc job;
     const bool frontier = frontier_for(q, opt.check_termination > 0, (B + 31) / 32);

@@ -19,6 +19,7 @@ struct Osqp {
   // 1 P entry, 2 A entry), scale bits, add bits} -- the row's inputs of
   // kkt_base / kkt_src / p_scale / p_diag_sigma / a_scale resolved
   const int4* kin_desc;       // [n + m + initial entries]
+  const int4* kin_desc_rho;   // the same with each -1/rho input taken from the instance's 1/rho row (kind 3)
   const float* p_scale;       // [nnz_p]
   const float* p_diag_sigma;  // [nnz_p]
   const float* a_scale;       // [nnz_a]

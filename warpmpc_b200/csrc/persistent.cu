@@ -28,6 +28,8 @@ namespace wmpc {
 struct OsqpInputs {
   const float* pT; long long ldp; int sbp;
   const float* aT; long long lda; int sba;
+  // per-instance 1/rho rows [m][batch] (rho adaptation; null: the plan's -1/rho values)
+  const float* rT = nullptr; long long ldr = 0;
   __device__ __forceinline__ float p(int j, int b) const { return pT[(long long)j * ldp + (long long)b * sbp]; }
   __device__ __forceinline__ float a(int j, int b) const { return aT[(long long)j * lda + (long long)b * sba]; }
 };
@@ -65,6 +67,7 @@ __host__ __device__ inline int factor_warp_words(const StreamPlan& sp, int lbatc
 // time) and broadcast with shuffles.
 constexpr unsigned kFullMask = 0xffffffffu;
 constexpr int kPosRegs = 4;  // L re-read positions per lane: 32 x kPosRegs >= lbatch (at most 128)
+constexpr int kFacStep = 8;  // updates of one step loaded before their arithmetic
 
 struct PosBatch {
   int v[kPosRegs];
@@ -96,29 +99,34 @@ __device__ __forceinline__ void stage_updates(const StreamPlan& sp, const float*
 
 // How KKT input j of a row is formed from its staged raw input
 // (solver.py:764-776), one descriptor per input in row-program order (the
-// diagonal, then the row's initial entries): x the P/A entry (-1: none),
-// y kind (0 the base value `add`, 1 a P entry raw * p_scale +
-// sigma-on-the-diagonal `add`, 2 an A entry raw * a_scale), z scale bits,
+// diagonal, then the row's initial entries): x the P/A entry (-1: none;
+// nnz_p + nnz_a + r: constraint r's 1/rho row), y kind (0 the base value
+// `add`, 1 a P entry raw * p_scale + sigma-on-the-diagonal `add`, 2 an A
+// entry raw * a_scale, 3 -raw: the instance's own -1/rho), z scale bits,
 // w add bits.
 __device__ __forceinline__ float kkt_input_value(int kind, float scale, float add, float raw) {
   if (kind == 0) return add;
   if (kind == 1) return raw * scale + add;
+  if (kind == 3) return -raw;
   return raw * scale;
 }
 
-__device__ __forceinline__ int4 kin_desc_of(const Osqp& o, int base, int j, int nkv) {
-  return j < nkv ? __ldg(o.kin_desc + base + j) : make_int4(-1, 0, 0, 0);
+__device__ __forceinline__ int4 kin_desc_of(const int4* kin, int base, int j, int nkv) {
+  return j < nkv ? __ldg(kin + base + j) : make_int4(-1, 0, 0, 0);
 }
 
 // the raw KKT inputs [first, nkv) of a row (descriptor of input first + lane in d)
 __device__ __forceinline__ void copy_kkt_inputs(const Osqp& o, const OsqpInputs& in, const float* pin,
-                                                const float* ain, float* kst, int first, int nkv, int4 d) {
+                                                const float* ain, const float* rin, float* kst, int first, int nkv,
+                                                int4 d) {
   const int cnt = nkv - first < 32 ? nkv - first : 32;
   for (int j = 0; j < cnt; ++j) {
     const int src = __shfl_sync(kFullMask, d.x, j);
     if (src >= 0)
       cp_async4(kst + (first + j) * 32,
-                src < o.nnz_p ? pin + (long long)src * in.ldp : ain + (long long)(src - o.nnz_p) * in.lda);
+                src < o.nnz_p ? pin + (long long)src * in.ldp
+                : src < o.nnz_p + o.nnz_a ? ain + (long long)(src - o.nnz_p) * in.lda
+                                          : rin + (long long)(src - o.nnz_p - o.nnz_a) * in.ldr);
   }
 }
 
@@ -143,25 +151,31 @@ __device__ __forceinline__ FacRow load_fac_row(const StreamPlan& sp, int k) {
   return r;
 }
 
-__device__ __forceinline__ void load_row_words(const Osqp& o, const StreamPlan& sp, const FacRow& r, int lbatch,
+__device__ __forceinline__ void load_row_words(const int4* kin, const StreamPlan& sp, const FacRow& r, int lbatch,
                                                int lane, FacRowWords& w) {
   const int p0 = r.a.x, p1 = r.a.y, nkv = 1 + r.a.w - r.a.z;
-  w.kin = kin_desc_of(o, r.b.w, lane, nkv);
+  w.kin = kin_desc_of(kin, r.b.w, lane, nkv);
   w.sdoff = p0 + lane < p1 ? __ldg(sp.step_doff + p0 + lane) : 0;
   const int ub = r.b.x, uend = r.b.y;
   load_positions(sp, ub, ub + lbatch < uend ? ub + lbatch : uend, lane, w.pos);
 }
 
+// With per-instance 1/rho rows (in.rT) the rows' -1/rho inputs come from
+// them (kin_desc_rho); with `only`, a tile none of whose instances is marked
+// keeps its factorization (a marked tile's unmarked lanes recompute theirs
+// from unchanged inputs: the same bits).
 __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, StreamPlan sp, Osqp o, OsqpInputs in,
                                                             float* __restrict__ bstream, float* __restrict__ fstream,
                                                             int* __restrict__ status, int n_tiles, int batch,
-                                                            int lbatch) {
+                                                            int lbatch, const int* __restrict__ only) {
   extern __shared__ float fsm[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int tile = blockIdx.x * (blockDim.x >> 5) + warp;
   if (tile >= n_tiles) return;
   const int b = tile * 32 + lane;
+  if (only != nullptr && !__any_sync(kFullMask, b < batch && only[b] != 0)) return;
+  const int4* kin = in.rT ? o.kin_desc_rho : o.kin_desc;
   const int bb = b < batch ? b : batch - 1;  // padding lanes factor a copy of the last instance
   const int rmax = sp.max_row_nnz > 0 ? sp.max_row_nnz : 1;
   const int kvmax = sp.max_row_kv;
@@ -181,14 +195,15 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
   float* Ld = Lb + lane;      // D^-1 rows: lane stride 1
   const float* pin = in.pT + (long long)bb * in.sbp;
   const float* ain = in.aT + (long long)bb * in.sba;
+  const float* rin = in.rT ? in.rT + bb : nullptr;
   const int n = pat.n;
   bool bad = false;
   // row 0's ranges and words, row 1's ranges, row 0's raw inputs
   FacRow cur = load_fac_row(sp, 0);
   FacRow nxt = n > 1 ? load_fac_row(sp, 1) : cur;
   FacRowWords wc;
-  load_row_words(o, sp, cur, lbatch, lane, wc);
-  copy_kkt_inputs(o, in, pin, ain, kst, 0, 1 + cur.a.w - cur.a.z, wc.kin);
+  load_row_words(kin, sp, cur, lbatch, lane, wc);
+  copy_kkt_inputs(o, in, pin, ain, rin, kst, 0, 1 + cur.a.w - cur.a.z, wc.kin);
   cp_async_commit();
   for (int k = 0; k < n; ++k) {
     const int p0 = cur.a.x, p1 = cur.a.y, i0 = cur.a.z, i1 = cur.a.w;
@@ -200,11 +215,11 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     FacRow nn = nxt;
     if (k + 2 < n) nn = load_fac_row(sp, k + 2);
     FacRowWords wn = wc;
-    if (k + 1 < n) load_row_words(o, sp, nxt, lbatch, lane, wn);
+    if (k + 1 < n) load_row_words(kin, sp, nxt, lbatch, lane, wn);
     // stage this row's reads: raw inputs past the first 32, D^-1 of its
     // steps, step tables, the first batch of L re-reads
     for (int base = 32; base < nkv; base += 32)
-      copy_kkt_inputs(o, in, pin, ain, kst, base, nkv, kin_desc_of(o, kbase, base + lane, nkv));
+      copy_kkt_inputs(o, in, pin, ain, rin, kst, base, nkv, kin_desc_of(kin, kbase, base + lane, nkv));
     for (int base = p0; base < p1; base += 32) {
       const int e = base + lane;
       const int doff = base == p0 ? wc.sdoff : (e < p1 ? __ldg(sp.step_doff + e) : 0);
@@ -222,7 +237,7 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     PosBatch pnext;
     load_positions(sp, ue, ue + lbatch < u_end ? ue + lbatch : u_end, lane, pnext);
     // the next row's raw inputs into the other buffer (they depend on no factor value)
-    if (k + 1 < n) copy_kkt_inputs(o, in, pin, ain, kst_next, 0, 1 + nxt.a.w - nxt.a.z, wn.kin);
+    if (k + 1 < n) copy_kkt_inputs(o, in, pin, ain, rin, kst_next, 0, 1 + nxt.a.w - nxt.a.z, wn.kin);
     cp_async_commit();
     cp_async_wait_group<1>();  // everything but the next row's inputs
     __syncwarp();
@@ -231,7 +246,7 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     for (int s = 0; s < p1 - p0; ++s) ys[s * 32] = 0.0f;
     float dk = 0.0f;
     for (int base = 0; base < nkv; base += 32) {
-      const int4 kc = base == 0 ? wc.kin : kin_desc_of(o, kbase, base + lane, nkv);
+      const int4 kc = base == 0 ? wc.kin : kin_desc_of(kin, kbase, base + lane, nkv);
       const int jl = base + lane;
       const int islot = (jl > 0 && jl < nkv) ? __ldg(sp.init_slot + i0 + jl - 1) : 0;
       const int cnt = nkv - base < 32 ? nkv - base : 32;
@@ -251,7 +266,9 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
     for (int e = 0; e < p1 - p0; ++e) {
       const int off = off_w[e];
       const float val = ys[e * 32];
-      for (int q = 0; q < off; ++q, ++u) {
+      // a step's updates target distinct slots (the rows of one column):
+      // kFacStep of them at a time, every load issued before the stores
+      for (int q = 0; q < off;) {
         if (u == ue) {  // next batch of this row's L re-reads
           __syncwarp();
           ub = ue;
@@ -261,8 +278,22 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
           cp_async_wait_all();
           __syncwarp();
         }
-        const int su = slot_w[u - ub];
-        ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
+        int cnt = off - q < ue - u ? off - q : ue - u;
+        cnt = cnt < kFacStep ? cnt : kFacStep;
+        int su[kFacStep];
+        float yv[kFacStep], lv[kFacStep];
+#pragma unroll
+        for (int i = 0; i < kFacStep; ++i)
+          if (i < cnt) {
+            su[i] = slot_w[u - ub + i];
+            lv[i] = lst[(u - ub + i) * 32];
+            yv[i] = ys[su[i] * 32];
+          }
+#pragma unroll
+        for (int i = 0; i < kFacStep; ++i)
+          if (i < cnt) ys[su[i] * 32] = yv[i] - lv[i] * val;
+        q += cnt;
+        u += cnt;
       }
       const float lval = val * dst[e * 32];
       Lu[boff_w[e]] = lval;
@@ -368,6 +399,8 @@ struct StreamJob {
   int check_every;  // > 0: stop a tile once every lane's largest unscaled iterate change <= chg_eps
   float chg_eps;
   float sigma, alpha, one_minus_alpha;
+  const float* rho_b;    // per-instance rho (admm_stream_kernel<.., true>), see StreamJobDesc
+  const int* rho_count;
 };
 
 constexpr int kMaxStreamJobs = 6;
@@ -563,20 +596,58 @@ struct RelGroup {
   float4 st[kRelGroup];
 };
 
+// This lane's instance's rho by row class, when its rho adapted (on): the
+// rule of the rho update (loose rows 1e-6, inequality rows rho_b, equality
+// rows 1e3 rho_b; 1/rho one division each), else the records' (the plan's)
+// rho vector.
+struct RhoLane {
+  bool on;
+  float r_loose, r_ineq, r_eq, i_loose, i_ineq, i_eq;
+};
+
+__device__ __forceinline__ RhoLane rho_lane(const float* rho_b, const int* rho_count, int b) {
+  RhoLane l;
+  l.on = rho_count[b] > 0;
+  const float est = rho_b[b];
+  l.r_loose = 1e-6f;
+  l.r_ineq = est;
+  l.r_eq = 1e3f * est;
+  l.i_loose = 1.0f / l.r_loose;
+  l.i_ineq = 1.0f / l.r_ineq;
+  l.i_eq = 1.0f / l.r_eq;
+  return l;
+}
+
+// rho, 1/rho of a release of class cls (record values unless the lane's rho adapted)
+__device__ __forceinline__ void rho_of(const RhoLane& l, int cls, int4 r, float& rho, float& rinv) {
+  rho = __int_as_float(r.y);
+  rinv = __int_as_float(r.z);
+  if (l.on) {
+    rho = cls < 0 ? l.r_loose : (cls > 0 ? l.r_eq : l.r_ineq);
+    rinv = cls < 0 ? l.i_loose : (cls > 0 ? l.i_eq : l.i_ineq);
+  }
+}
+
 // A record's last word: the released index's unscale factor (plain form) or
 // the index itself (frontier form, whose unscale factors come from
-// unscale_perm when termination is checked).
-template <bool kTrack, bool kFrontier>
+// unscale_perm when termination is checked).  kRho: per-instance rho by the
+// release's class (ucls: the classes of the chunk's releases).
+template <bool kTrack, bool kFrontier, bool kRho>
 __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
-                                               const unsigned char* xb, const float* unscale_perm, RelGroup& g) {
+                                               const unsigned char* xb, const float* unscale_perm, const int* ucls,
+                                               const RhoLane& rl, RelGroup& g) {
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
     const int kk = (k + j < end) ? k + j : k;
     const int4 r = rel[kk];
     g.kk[j] = kk;
     g.o[j] = r.x;
-    g.rho[j] = __int_as_float(r.y);
-    g.rinv[j] = __int_as_float(r.z);
+    if constexpr (kRho) {
+      rho_of(rl, __ldg(ucls + kk), r, g.rho[j], g.rinv[j]);
+    } else {
+      g.rho[j] = __int_as_float(r.y);
+      g.rinv[j] = __int_as_float(r.z);
+    }
     if constexpr (kFrontier) {
       g.ix[j] = r.w;
       g.f[j] = kTrack ? __ldg(unscale_perm + r.w) : 1.0f;
@@ -643,22 +714,22 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
   }
 }
 
-template <bool kCons, bool kTrack, bool kFrontier>
+template <bool kCons, bool kTrack, bool kFrontier, bool kRho>
 __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
                                              const RelParams& rp, unsigned char* xb, float* rt, float4* stu,
                                              float* peu, float& chg, float& pres, bool frozen,
-                                             const float* unscale_perm) {
+                                             const float* unscale_perm, const int* ucls, const RhoLane& rl) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kTrack, kFrontier>(rel, begin, end, S, SE, xb, unscale_perm, a);
+  load_rel_group<kTrack, kFrontier, kRho>(rel, begin, end, S, SE, xb, unscale_perm, ucls, rl, a);
   for (int k = begin;; k += 2 * kRelGroup) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + kRelGroup < end ? k + kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier>(rel, kb, end, S, SE, xb, unscale_perm, b);
+    load_rel_group<kTrack, kFrontier, kRho>(rel, kb, end, S, SE, xb, unscale_perm, ucls, rl, b);
     update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + kRelGroup >= end) break;
     const int ka = k + 2 * kRelGroup < end ? k + 2 * kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier>(rel, ka, end, S, SE, xb, unscale_perm, a);
+    load_rel_group<kTrack, kFrontier, kRho>(rel, ka, end, S, SE, xb, unscale_perm, ucls, rl, a);
     update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + 2 * kRelGroup >= end) break;
   }
@@ -690,7 +761,10 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // (y_done).  The copies into stages wait for the writes: a sweep's first
 // forward chunk until every earlier item is released, its first backward
 // chunk until every earlier forward block is in fwd.
-template <bool kTrack, bool kFrontier>
+// kRho: per-instance rho (adaptation, fixed iterations): a lane whose rho
+// changed takes its constraints' rho and 1/rho from its instance's scalar
+// rho by row class (RhoLane), in the first right-hand side and the updates.
+template <bool kTrack, bool kFrontier, bool kRho = false>
 __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_constant__ StreamArgs a) {
   constexpr bool kSplit = !kTrack;  // the second releaser takes half of the releases (fixed iterations)
   extern __shared__ __align__(128) unsigned char smem[];
@@ -937,6 +1011,11 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
       }
       float4* stt = J.state + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
+      RhoLane rl{};
+      if constexpr (kRho) {
+        const int bl = tile * 32 + lane;
+        rl = rho_lane(J.rho_b, J.rho_count, bl < J.batch ? bl : J.batch - 1);
+      }
       float pres = 0.0f;  // this lane's largest unscaled primal residual in the current iteration
       float chg = 0.0f;  // this lane's largest unscaled iterate change in the current iteration
       int iters_run = 0, frozen_at = 0;
@@ -1003,7 +1082,12 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             for (int k = cb; k < ce; ++k) {
               const int4 r = rel[k];
               const float4 st = S[k * 32];
-              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = st.x - __int_as_float(r.z) * st.y;
+              float rinv = __int_as_float(r.z);
+              if constexpr (kRho) {
+                float rho;
+                rho_of(rl, __ldg(sp.u_cls + u0 + k), r, rho, rinv);
+              }
+              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = st.x - rinv * st.y;
             }
             // read back by bulk copies once rel_done covers the pass's last chunk
             if (kFrontier && ch == 0) fence_proxy_async_global();
@@ -1011,10 +1095,11 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             float4* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
-            run_releases<false, kTrack, kFrontier>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
-                                                   sp.unscale_perm);
-            run_releases<true, kTrack, kFrontier>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
-                                                  sp.unscale_perm);
+            const int* ucls = kRho ? sp.u_cls + u0 : nullptr;
+            run_releases<false, kTrack, kFrontier, false>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+                                                          sp.unscale_perm, ucls, rl);
+            run_releases<true, kTrack, kFrontier, kRho>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+                                                        sp.unscale_perm, ucls, rl);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
             fence_proxy_async_global();
@@ -1245,7 +1330,8 @@ size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
 int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const float* pT, long long ldp, int sbp,
                  const float* aT, long long lda, int sba, const float* x, const float* z, const float* y,
                  const float* qs, const float* ls, const float* us, bool warm, bool track, float* work,
-                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s) {
+                 int* status, int batch, int num_sms, bool reuse_factor, StreamJobDesc* job, cudaStream_t s,
+                 const float* rinv_rows, const int* only) {
   StreamLaunch cfg;
   if (!stream_launch_config(sp, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "pattern too large for the streaming kernel");
   const int n_tiles = (batch + 31) / 32;
@@ -1256,7 +1342,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   float* pres = reinterpret_cast<float*>(state + tl * sp.n);
   float* rhs = sp.frontier_slots > 0 ? pres + tl * sp.n : nullptr;
   float* fwd = sp.frontier_slots > 0 ? rhs + tl * sp.n : nullptr;
-  OsqpInputs in{pT, ldp, sbp, aT, lda, sba};
+  OsqpInputs in{pT, ldp, sbp, aT, lda, sba, rinv_rows, rinv_rows ? (long long)batch : 0};
+  if (rinv_rows && !o.kin_desc_rho) return fail(WMPC_ERR_UNSUPPORTED, "the problem has no per-instance rho inputs");
   if (!reuse_factor) {
     // L-batch sized so that every tile's warp is resident at once (all of a
     // launch's rows then wait out their round trips together)
@@ -1270,7 +1357,7 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
     WMPC_CUDA_TRY(cudaFuncSetAttribute(factor_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     profile_mark_begin(s, kProfileFactor);
     factor_stream_kernel<<<ceil_div(n_tiles, warps), warps * 32, smem, s>>>(pat, sp, o, in, bstream, fstream, status,
-                                                                            n_tiles, batch, lbatch);
+                                                                            n_tiles, batch, lbatch, only);
     profile_mark_end(s, kProfileFactor);
     WMPC_LAUNCH_CHECK();
   }
@@ -1307,8 +1394,13 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   RingSizes r{0, 0, 0, 0, 0, 12, 6};
   int order[kMaxStreamJobs];
   double cost[kMaxStreamJobs];
-  bool track = false;
+  bool track = false, rho = false;
   for (int i = 0; i < n_jobs; ++i) track = track || jobs[i].check_every > 0;
+  for (int i = 0; i < n_jobs; ++i) rho = rho || jobs[i].rho_b != nullptr;
+  if (rho && (track || n_jobs > 1))
+    return fail(WMPC_ERR_UNSUPPORTED, "per-instance rho runs one class with fixed iterations");
+  if (rho && (!jobs[0].rho_count || !jobs[0].sp.u_cls))
+    return fail(WMPC_ERR_UNSUPPORTED, "per-instance rho needs the rho counts and the schedule's row classes");
   const bool frontier = jobs[0].sp.frontier_slots > 0;
   for (int i = 0; i < n_jobs; ++i)
     if ((jobs[i].sp.frontier_slots > 0) != frontier)
@@ -1360,6 +1452,8 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     J.rhs = d.rhs;
     J.fwd = d.fwd;
     J.iters = d.iters;
+    J.rho_b = d.rho_b;
+    J.rho_count = d.rho_count;
     J.n_tiles = d.n_tiles;
     J.max_iter = d.max_iter;
     J.batch = d.batch;
@@ -1388,6 +1482,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   }
   const int grid = total < ctas_per_sm * num_sms ? total : ctas_per_sm * num_sms;
   auto kernel = track ? (frontier ? admm_stream_kernel<true, true> : admm_stream_kernel<true, false>)
+                : rho ? (frontier ? admm_stream_kernel<false, true, true> : admm_stream_kernel<false, false, true>)
                       : (frontier ? admm_stream_kernel<false, true> : admm_stream_kernel<false, false>);
   WMPC_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
   // all of the SM's unified memory as shared memory, so that two CTAs fit

@@ -72,6 +72,7 @@ __host__ __device__ inline int factor_rows_words(int max_row, int max_kv, int lb
 
 constexpr unsigned kLanes = 0xffffffffu;
 constexpr int kRowPosRegs = 4;  // L re-read positions per lane: 32 x kRowPosRegs >= lbatch (at most 128)
+constexpr int kRowStep = 8;     // updates of one step loaded before their arithmetic
 
 struct RowPos {
   int v[kRowPosRegs];
@@ -195,7 +196,9 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
     for (int e = 0; e < p1 - p0; ++e) {
       const int off = off_w[e];
       const float val = ys[e * 32];
-      for (int q = 0; q < off; ++q, ++u) {
+      // a step's updates target distinct slots (the rows of one column):
+      // kRowStep of them at a time, every load issued before the stores
+      for (int q = 0; q < off;) {
         if (u == ue) {  // next batch of this row's L re-reads
           __syncwarp();
           ub = ue;
@@ -205,8 +208,22 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
           cp_async_wait_all();
           __syncwarp();
         }
-        const int su = slot_w[u - ub];
-        ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
+        int cnt = off - q < ue - u ? off - q : ue - u;
+        cnt = cnt < kRowStep ? cnt : kRowStep;
+        int su[kRowStep];
+        float yv[kRowStep], lv[kRowStep];
+#pragma unroll
+        for (int i = 0; i < kRowStep; ++i)
+          if (i < cnt) {
+            su[i] = slot_w[u - ub + i];
+            lv[i] = lst[(u - ub + i) * 32];
+            yv[i] = ys[su[i] * 32];
+          }
+#pragma unroll
+        for (int i = 0; i < kRowStep; ++i)
+          if (i < cnt) ys[su[i] * 32] = yv[i] - lv[i] * val;
+        q += cnt;
+        u += cnt;
       }
       const float lval = val * dst[e * 32];
       if (keep) lx[(long long)lid_w[e] * batch + b] = lval;

@@ -14,8 +14,13 @@
 //   backward chunks the same runs in reverse, with D^-1 of their columns:
 //                  x_c = x_c D^-1_c - sum_r L_rc x_r (gather, ascending r);
 // then the tile's result rows are stored, unpermuted, to out.  X ([row][lane],
-// conflict-free) stays in shared memory for the whole tile.  Chunks end on
-// column boundaries, so every column's entries sit in one stage.
+// conflict-free, plus a trash row and a zero row) stays in shared memory for
+// the whole tile.  Chunks end on column boundaries, so every column's entries
+// sit in one stage.  A column is worked kStep entries at a time: the step's
+// index words, L values and work-vector reads are all issued before its
+// arithmetic (padding slots write the trash row, or read L = 0 times the
+// zero row), so one shared-memory round trip per step is on the sweep's
+// critical path instead of one per entry.
 //
 // Operation order is the reference's serial solve (warpmpc/jax_qdldl/
 // warp_backend.py:193-218: column-scatter forward substitution, D^-1, then
@@ -46,9 +51,13 @@ constexpr int kTableBytes = 512;                         // index table area of 
 constexpr int kDataBytes = (kChunkEntries + kChunkCols) * 128;  // L rows, then D^-1 rows
 constexpr int kStageBytes = kTableBytes + kDataBytes;    // 12800 (a multiple of 128)
 constexpr int kMaxStages = 8;
+constexpr int kStep = 8;  // L entries of one column a sweeper step loads before its arithmetic
 constexpr uint64_t kSolveWaitNs = 2000000000ull;          // 2 s: a healthy wait is microseconds
 static_assert(kRhsRows * 128 <= kDataBytes, "an rhs item must fit the data area");
 static_assert((4 + kChunkCols + kChunkEntries) * 4 <= kTableBytes, "a chunk table must fit its area");
+// a step may read kStep - 1 table words and L rows past a chunk's last entry
+static_assert((4 + kChunkCols + kChunkEntries + kStep - 1) * 4 <= kTableBytes, "step reads past the table area");
+static_assert(kChunkEntries + kStep - 1 <= kChunkEntries + kChunkCols, "step reads past the stage's L rows");
 
 enum : int { kSolveRhs = 0, kSolveFwd = 1, kSolveBwd = 2 };
 
@@ -90,8 +99,8 @@ __global__ void __launch_bounds__(64, 1) solve_stream_kernel(const __grid_consta
   extern __shared__ __align__(1024) unsigned char smem[];
   const int n = a.n;
   const int S = a.stages;
-  float* X = reinterpret_cast<float*>(smem);                                      // [n][32]
-  unsigned char* ring = smem + (((size_t)n * 128 + 1023) / 1024) * 1024;          // S stages
+  float* X = reinterpret_cast<float*>(smem);  // [n + 2][32]: rows, a trash row, a zero row
+  unsigned char* ring = smem + (((size_t)(n + 2) * 128 + 1023) / 1024) * 1024;  // S stages
   uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)S * kStageBytes);
   uint64_t* empty = full + S;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + S);
@@ -155,6 +164,8 @@ __global__ void __launch_bounds__(64, 1) solve_stream_kernel(const __grid_consta
     uint32_t stage = 0, phase = 0;
     bool ok = true;
     unsigned char* xb = smem + lane * 4;  // this lane's column of X (row r at xb + 128 r)
+    const int trash_off = n * 128, zero_off = (n + 1) * 128;
+    X[(n + 1) * 32 + lane] = 0.0f;
     int tile = blockIdx.x;
     for (; tile < a.n_tiles && ok; tile += gridDim.x) {
       for (int i = 0; i < per_tile; ++i) {
@@ -186,55 +197,52 @@ __global__ void __launch_bounds__(64, 1) solve_stream_kernel(const __grid_consta
           const int* cend = tb + 4;
           const int* roff = tb + 4 + C;  // byte offsets (row * 128) into X
           if (kind == kSolveFwd) {
-            // x_r -= L_rc x_c over column c's rows (distinct rows: independent)
+            // x_r -= L_rc x_c over column c's rows (distinct rows: independent),
+            // kStep entries at a time with all their loads issued before the
+            // arithmetic; slots past the column's end update the trash row
             int b = 0;
             for (int j = 0; j < C; ++j) {
               const int e = cend[j];
               if (e > b) {
                 const float val = X[(c0 + j) * 32 + lane];
-                int q = b;
-                for (; q + 4 <= e; q += 4) {
-                  const int o0 = roff[q], o1 = roff[q + 1], o2 = roff[q + 2], o3 = roff[q + 3];
-                  const float l0 = data[q * 32], l1 = data[(q + 1) * 32], l2 = data[(q + 2) * 32],
-                              l3 = data[(q + 3) * 32];
-                  float* y0 = reinterpret_cast<float*>(xb + o0);
-                  float* y1 = reinterpret_cast<float*>(xb + o1);
-                  float* y2 = reinterpret_cast<float*>(xb + o2);
-                  float* y3 = reinterpret_cast<float*>(xb + o3);
-                  const float w0 = *y0, w1 = *y1, w2 = *y2, w3 = *y3;
-                  *y0 = w0 - l0 * val;
-                  *y1 = w1 - l1 * val;
-                  *y2 = w2 - l2 * val;
-                  *y3 = w3 - l3 * val;
-                }
-                for (; q < e; ++q) {
-                  float* y0 = reinterpret_cast<float*>(xb + roff[q]);
-                  *y0 = *y0 - data[q * 32] * val;
+                for (int q = b; q < e; q += kStep) {
+                  int o[kStep];
+                  float l[kStep], w[kStep];
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) {
+                    o[i] = q + i < e ? roff[q + i] : trash_off;
+                    l[i] = data[(q + i) * 32];
+                  }
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) *reinterpret_cast<float*>(xb + o[i]) = w[i] - l[i] * val;
                 }
               }
               b = e;
             }
           } else {
-            // x_c = x_c D^-1_c - sum_r L_rc x_r (rows ascending), columns descending
+            // x_c = x_c D^-1_c - sum_r L_rc x_r (rows ascending), columns descending;
+            // slots past the column's end add L = 0 times the zero row (+0: the
+            // sum keeps its bits)
             const float* dv = data + kChunkEntries * 32;
             for (int j = C - 1; j >= 0; --j) {
               const int b = j > 0 ? cend[j - 1] : 0, e = cend[j];
               float corr = 0.0f;
-              int q = b;
-              for (; q + 4 <= e; q += 4) {
-                const int o0 = roff[q], o1 = roff[q + 1], o2 = roff[q + 2], o3 = roff[q + 3];
-                const float l0 = data[q * 32], l1 = data[(q + 1) * 32], l2 = data[(q + 2) * 32],
-                            l3 = data[(q + 3) * 32];
-                const float w0 = *reinterpret_cast<const float*>(xb + o0);
-                const float w1 = *reinterpret_cast<const float*>(xb + o1);
-                const float w2 = *reinterpret_cast<const float*>(xb + o2);
-                const float w3 = *reinterpret_cast<const float*>(xb + o3);
-                corr = corr + l0 * w0;
-                corr = corr + l1 * w1;
-                corr = corr + l2 * w2;
-                corr = corr + l3 * w3;
+              for (int q = b; q < e; q += kStep) {
+                int o[kStep];
+                float l[kStep], w[kStep];
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) {
+                  const bool v = q + i < e;
+                  o[i] = v ? roff[q + i] : zero_off;
+                  l[i] = v ? data[(q + i) * 32] : 0.0f;
+                }
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) corr = corr + l[i] * w[i];
               }
-              for (; q < e; ++q) corr = corr + data[q * 32] * *reinterpret_cast<const float*>(xb + roff[q]);
               float* xc = X + (c0 + j) * 32 + lane;
               *xc = *xc * dv[j * 32] - corr;
             }
@@ -316,7 +324,7 @@ bool encode_rows(CUtensorMap* map, const float* base, int rows, int batch) {
 }
 
 size_t solve_smem_bytes(int n, int stages) {
-  return (((size_t)n * 128 + 1023) / 1024) * 1024 + (size_t)stages * kStageBytes + 16 * (size_t)stages + 16;
+  return (((size_t)(n + 2) * 128 + 1023) / 1024) * 1024 + (size_t)stages * kStageBytes + 16 * (size_t)stages + 16;
 }
 
 }  // namespace

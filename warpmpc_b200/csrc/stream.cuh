@@ -110,6 +110,9 @@ struct StreamPlan {
   // initial entries), {ub, uend, doff, kin base} (updates, D^-1 offset,
   // first KKT input descriptor of the row in Osqp::kin_desc)
   const int4* row_info;  // [2 n]
+  // rho class of each U index's constraint (-1 loose, 0 inequality, 1
+  // equality; 0 for primal indices): per-instance rho, when it adapts
+  const int* u_cls;  // [n] (null: the problem has no rho classes)
 };
 
 // ---- PTX helpers -----------------------------------------------------------
@@ -313,6 +316,11 @@ struct StreamJobDesc {
   int n_tiles = 0, max_iter = 0, batch = 0, check_every = 0;
   float chg_eps = 0.0f, sigma = 0.0f, alpha = 0.0f, one_minus_alpha = 0.0f;
   int ctas_limit = 2;  // most CTAs per SM this class's problem allows (a launch takes the smallest)
+  // per-instance rho (adaptation): an instance whose rho changed (count > 0)
+  // takes its rows' rho from its scalar rho_b by the rows' classes; null: the
+  // schedule's rho vector for every instance
+  const float* rho_b = nullptr;
+  const int* rho_count = nullptr;
 };
 
 }  // namespace wmpc

@@ -114,21 +114,36 @@ _MODES = {"plain": native.WMPC_OSQP_PLAIN, "persistent": native.WMPC_OSQP_PERSIS
 class OSQPEngine:
     """Host-side driver of ``wmpc_osqp_factor`` / ``wmpc_osqp_solve``.
 
-    A plan with ``settings.adaptive_rho`` runs the per-call ("plain")
-    kernels whatever ``mode`` asks: the persistent kernels keep one rho
-    vector per pattern, rho adaptation needs one per instance."""
+    A plan with ``settings.adaptive_rho`` runs either the per-call ("plain")
+    kernels or, in "persistent" mode where the pattern has the streaming
+    schedule, the streaming kernels in launches of ``adaptive_rho_interval``
+    iterations with a per-instance rho (the same iterates, rho and refactor
+    counts); other modes fall back to "plain".  Rho adaptation runs fixed
+    iterations on the persistent path (``check_termination`` 0)."""
 
     def __init__(self, plan: FixedOSQPPlan, device=None, mode: str = "persistent", kkt_plan: DevicePlan | None = None):
         if mode not in _MODES:
             raise ValueError(f"unknown mode {mode!r}; expected one of {sorted(_MODES)}")
         self.plan = plan
-        self.mode = "plain" if plan.settings.adaptive_rho else mode
         self.dev = DeviceOSQP(plan, device, kkt_plan=kkt_plan)
+        self.mode = mode
+        if plan.settings.adaptive_rho and not (mode == "persistent" and self.stream_info()["streaming"]
+                                               and not plan.settings.check_termination):
+            self.mode = "plain"
         self.device = self.dev.torch_device
         self.last_iters = None
         self.last_status = None
         self.last_rho = None
         self.last_rho_updates = None
+
+    def workspace_bytes(self, batch: int, keep_factor: bool = False) -> int:
+        """Device workspace bytes of a solve of ``batch`` instances (factoring;
+        ``keep_factor``: enough for the adjoint on the kept factorization)."""
+        lib = native.lib()
+        mode_id = _MODES[self.mode]
+        if keep_factor:
+            return int(lib.wmpc_osqp_adjoint_workspace_bytes(self.dev.handle, batch, mode_id))
+        return int(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, 0))
 
     def stream_info(self) -> dict:
         """The streaming schedule this problem carries: ``streaming`` (persistent
@@ -235,13 +250,18 @@ class OSQPEngine:
         return data, opts, keep, (x, z, y, prim, dual, obj, iters, status), batch
 
     def solve(self, p_values, a_values, q, l, u, warm=None, factor=None, max_iter=None, check_termination=None,
-              mode=None, out=None, keep_factor=False):
+              mode=None, out=None, keep_factor=False, workspace=None):
         """Batched solve; returns ``(x, z, y, prim_res, dual_res, obj_val)``.
 
         ``out`` optionally supplies those six output tensors (plus ``iters``,
         ``status`` int32) to write into; warm-start inputs may alias ``out``
         (they are consumed before the outputs are written), which lets a CUDA
-        graph chain solves without copies.
+        graph chain solves without copies.  ``workspace`` optionally supplies
+        the device workspace (a uint8 tensor of at least ``workspace_bytes``,
+        or ``adjoint_workspace_bytes`` with ``keep_factor``) instead of a new
+        allocation per call: a caller that chains solves (an SQP loop, a CUDA
+        graph) keeps one; a kept factorization lives in it until the next
+        solve that is given the same workspace.
         """
         pl = self.plan
         dev = self.device
@@ -265,9 +285,15 @@ class OSQPEngine:
         if keep_factor:
             if factor is not None:
                 raise ValueError("keep_factor needs the solve to factor (no external factor)")
-            ws, wsb = _workspace(lib.wmpc_osqp_adjoint_workspace_bytes(self.dev.handle, batch, mode_id), dev)
+            need = lib.wmpc_osqp_adjoint_workspace_bytes(self.dev.handle, batch, mode_id)
         else:
-            ws, wsb = _workspace(lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext), dev)
+            need = lib.wmpc_osqp_workspace_bytes(self.dev.handle, batch, mode_id, ext)
+        if workspace is not None:
+            if workspace.device != dev or workspace.numel() * workspace.element_size() < need:
+                raise ValueError(f"workspace must be a device tensor of at least {need} bytes on {dev}")
+            ws, wsb = workspace, int(workspace.numel() * workspace.element_size())
+        else:
+            ws, wsb = _workspace(need, dev)
         if pl.settings.adaptive_rho:
             # each instance's final rho and number of rho changes (refactorizations)
             import torch

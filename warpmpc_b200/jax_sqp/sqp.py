@@ -68,6 +68,7 @@ class SparseMPCSQP:
         self.values = QPAssembler(plan, problem, self.device, values_only=True)
         self.qp = compile_osqp(plan.osqp_plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode=mode,
                                device=self.device)
+        self._qp_ws = None  # one QP workspace for every solve of a batch size (sized for a kept factorization)
 
     def linearize(self, z, params) -> SQPLinearization:
         """_linearize_jit (sparse_mpc.py:855-901)."""
@@ -81,9 +82,17 @@ class SparseMPCSQP:
     def solve_qp(self, z, params, warm, keep_factor: bool = False) -> SQPSolveResult:
         """_solve_qp_with_state_jit (sparse_mpc.py:954-976): the QP at z, warm-started.
         keep_factor: the QP engine keeps the factorization for an adjoint."""
+        import torch
+
         lin = self.linearize(z, params)
-        x, qz, qy, prim, dual, obj = self.qp.engine.solve(lin.p_values, lin.a_values, lin.q, lin.l, lin.u,
-                                                          warm=warm, keep_factor=keep_factor)
+        eng = self.qp.engine
+        batch = int(lin.q.shape[0])
+        need = eng.workspace_bytes(batch, keep_factor=True)
+        if self._qp_ws is None or self._qp_ws.numel() < need:
+            self._qp_ws = None
+            self._qp_ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        x, qz, qy, prim, dual, obj = eng.solve(lin.p_values, lin.a_values, lin.q, lin.l, lin.u, warm=warm,
+                                               keep_factor=keep_factor, workspace=self._qp_ws)
         return SQPSolveResult(x, qz, qy, prim, dual, obj, lin)
 
     def line_search_step(self, z, params, warm, keep_factor: bool = False) -> SQPLineSearchStepResult:
