@@ -156,3 +156,32 @@ def test_gradient_through_last_qp_matches_finite_differences(cuda_device):
         fd = (loss(pp, qp_, l0, u0) - loss(pm, qm, l0, u0)) / (2 * h)
         worst = max(worst, float(np.max(np.abs(gq[:, j] - fd) / np.maximum(1e-3, np.abs(fd)))))
     assert worst < 2e-2, worst
+
+
+def test_solve_and_gradient_graph_replay(cuda_device):
+    """The bench's nonlinear leg: the SQP iterations (last QP keeping its
+    factorization) followed by the gradient, captured in one CUDA graph with
+    the driver's one QP workspace, replay the eager results bit for bit."""
+    import torch
+
+    batch = 64
+    w, _ = _setup(batch, 10, 3)
+    ut = torch.full((batch, qs.NU), qs.U_HOVER * 1.1, device=cuda_device)
+    z, r = w.solve(keep_factor=True)
+    eager = [t.clone() for t in (z, *w.gradient(z, r, ut))]
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        zz, rr = w.solve(keep_factor=True)
+        w.gradient(zz, rr, ut)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        zg, rg = w.solve(keep_factor=True)
+        grads = w.gradient(zg, rg, ut)
+    g.replay()
+    torch.cuda.synchronize()
+    for got, want in zip((zg, *grads), eager):
+        np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy())
+    del g

@@ -72,7 +72,6 @@ __host__ __device__ inline int factor_rows_words(int max_row, int max_kv, int lb
 
 constexpr unsigned kLanes = 0xffffffffu;
 constexpr int kRowPosRegs = 4;  // L re-read positions per lane: 32 x kRowPosRegs >= lbatch (at most 128)
-constexpr int kRowStep = 8;     // updates of one step loaded before their arithmetic
 
 struct RowPos {
   int v[kRowPosRegs];
@@ -196,9 +195,7 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
     for (int e = 0; e < p1 - p0; ++e) {
       const int off = off_w[e];
       const float val = ys[e * 32];
-      // a step's updates target distinct slots (the rows of one column):
-      // kRowStep of them at a time, every load issued before the stores
-      for (int q = 0; q < off;) {
+      for (int q = 0; q < off; ++q, ++u) {
         if (u == ue) {  // next batch of this row's L re-reads
           __syncwarp();
           ub = ue;
@@ -208,22 +205,8 @@ __global__ void __launch_bounds__(64) factor_rows_kernel(Pattern pat, FactorTabl
           cp_async_wait_all();
           __syncwarp();
         }
-        int cnt = off - q < ue - u ? off - q : ue - u;
-        cnt = cnt < kRowStep ? cnt : kRowStep;
-        int su[kRowStep];
-        float yv[kRowStep], lv[kRowStep];
-#pragma unroll
-        for (int i = 0; i < kRowStep; ++i)
-          if (i < cnt) {
-            su[i] = slot_w[u - ub + i];
-            lv[i] = lst[(u - ub + i) * 32];
-            yv[i] = ys[su[i] * 32];
-          }
-#pragma unroll
-        for (int i = 0; i < kRowStep; ++i)
-          if (i < cnt) ys[su[i] * 32] = yv[i] - lv[i] * val;
-        q += cnt;
-        u += cnt;
+        const int su = slot_w[u - ub];
+        ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
       }
       const float lval = val * dst[e * 32];
       if (keep) lx[(long long)lid_w[e] * batch + b] = lval;

@@ -243,16 +243,19 @@ class ClosedLoop:
         u[:, :nx] = -self.x0
 
     def advance_host(self, x, l, u):
-        """NumPy (or host tensor) version of ``advance``."""
+        """Host version of ``advance`` on NumPy arrays or host tensors (updated
+        in place): the same torch operations on CPU (batched matrix products
+        on the host's threads, through zero-copy views)."""
+        import torch
+
         nx, nu = self.cls.nx, self.cls.nu
-        x = np.asarray(x)
-        u0 = x[:, self.ui : self.ui + nu]
-        nxt = np.einsum("bij,bj->bi", self.a_np, self.x0_np) + np.einsum("bij,bj->bi", self.b_np, u0)
-        self.x0_np[:] = np.clip(nxt, -self.bound, self.bound)
-        l = np.asarray(l)
-        u = np.asarray(u)
-        l[:, :nx] = -self.x0_np
-        u[:, :nx] = -self.x0_np
+        xt = torch.from_numpy(np.asarray(x, dtype=np.float32))
+        a, b, x0 = (torch.from_numpy(v) for v in (self.a_np, self.b_np, self.x0_np))
+        u0 = xt[:, self.ui : self.ui + nu]
+        nxt = torch.bmm(a, x0[:, :, None])[:, :, 0] + torch.bmm(b, u0[:, :, None])[:, :, 0]
+        x0.copy_(nxt.clamp_(-float(self.bound), float(self.bound)))
+        for t in (l, u):
+            torch.from_numpy(np.asarray(t))[:, :nx] = -x0
 
 
 def make_batch(cls: MPCClass, batch: int, seed: int = 0, dtype=np.float32) -> MPCBatch:

@@ -312,6 +312,9 @@ class QuadrotorSQP:
         self.sqp = SparseMPCSQP(self.problem, self.plan, self.evaluator, device=self.device)
         self.q_cols = [np.asarray(a.q_cols, dtype=np.int64) for a in self.plan.assemblies]
         self.p_pos = [np.asarray(a.p_pos, dtype=np.int64) for a in self.plan.assemblies]
+        # the same indices on the device, states and inputs apart (gradient's gathers, graph-capturable)
+        ix = lambda a: torch.as_tensor(a, dtype=torch.int64, device=self.device)  # noqa: E731
+        self._grad_index = [(ix(c[:NX]), ix(p[:NX]), ix(c[NX:]), ix(p[NX:])) for c, p in zip(self.q_cols, self.p_pos)]
 
     def solve(self, keep_factor: bool = False):
         """The SQP iterations; returns (z, last step result).  With
@@ -344,9 +347,9 @@ class QuadrotorSQP:
         g_r = torch.zeros_like(self.evaluator.r)
         for k, st in enumerate(self.problem.stages):
             off = NX_NU * k
-            cols, pos = self.q_cols[k], self.p_pos[k]
+            cx, px, cu, pu = self._grad_index[k]
             # P's diagonal entry of a variable is its weight; q's entry the weight times its offset
-            g_q += dp[:, pos[:NX]] + dq[:, cols[:NX]] * z_lin[:, off : off + NX]
+            g_q += dp[:, px] + dq[:, cx] * z_lin[:, off : off + NX]
             if not st.terminal:
-                g_r += dp[:, pos[NX:]] + dq[:, cols[NX:]] * (z_lin[:, off + NX : off + NX_NU] - U_HOVER)
+                g_r += dp[:, pu] + dq[:, cu] * (z_lin[:, off + NX : off + NX_NU] - U_HOVER)
         return g_x0, g_q, g_r
