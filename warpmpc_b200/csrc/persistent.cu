@@ -322,16 +322,20 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
 // state layout conversions: symbolic-major (KKT row, instance) <-> tile-major U order
 // ---------------------------------------------------------------------------
 
-// ADMM state per tile in release order U, one 16-byte record per (index, lane):
-// (x, 0, sigma-scaled q, 0) for a primal index, (z, y, l, u) for a constraint;
+// ADMM state per tile in release order U, two 8-byte records per (index,
+// lane): the iterate (x, 0) for a primal index, (z, y) for a constraint --
+// rewritten every iteration -- and the parameters (sigma-scaled q, 0) or
+// (l, u) -- only read --, in two arrays of the same layout (the iterates
+// first, then the parameters);
 // and the scaled primal residual (A x - z)_r of a constraint (0 for a primal
 // index), formed when `form` (a warm start whose termination is checked; a
 // cold start's x = z = 0 gives 0; without checks nothing reads it).
 __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, bool form, const float* __restrict__ x,
                                        const float* __restrict__ z, const float* __restrict__ y,
                                        const float* __restrict__ qs, const float* __restrict__ ls,
-                                       const float* __restrict__ us, float4* __restrict__ state,
-                                       float* __restrict__ pres, int batch, int n_tiles) {
+                                       const float* __restrict__ us, float2* __restrict__ state,
+                                       float2* __restrict__ param, float* __restrict__ pres, int batch,
+                                       int n_tiles) {
   const int n_primal = o.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n_tiles * 32) return;
@@ -341,12 +345,14 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
     const int k = __ldg(sp.u_orig + u);
     const size_t dst = ((size_t)tile * sp.n + u) * 32 + lane;
     if (k < n_primal) {
-      state[dst] = make_float4(x[(size_t)k * batch + bb], 0.0f, qs[(size_t)k * batch + bb], 0.0f);
+      state[dst] = make_float2(x[(size_t)k * batch + bb], 0.0f);
+      param[dst] = make_float2(qs[(size_t)k * batch + bb], 0.0f);
       pres[dst] = 0.0f;
     } else {
       const int r = k - n_primal;
       const float zr = z[(size_t)r * batch + bb];
-      state[dst] = make_float4(zr, y[(size_t)r * batch + bb], ls[(size_t)r * batch + bb], us[(size_t)r * batch + bb]);
+      state[dst] = make_float2(zr, y[(size_t)r * batch + bb]);
+      param[dst] = make_float2(ls[(size_t)r * batch + bb], us[(size_t)r * batch + bb]);
       float e = 0.0f;
       if (form) {
         float ax = 0.0f;
@@ -362,7 +368,7 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
   }
 }
 
-__global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float4* __restrict__ state,
+__global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float2* __restrict__ state,
                                        float* __restrict__ x, float* __restrict__ z, float* __restrict__ y,
                                        int batch) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -370,7 +376,7 @@ __global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float4
   const int tile = b >> 5, lane = b & 31;
   for (int u = blockIdx.y; u < sp.n; u += gridDim.y) {
     const int o = __ldg(sp.u_orig + u);
-    const float4 v = state[((size_t)tile * sp.n + u) * 32 + lane];
+    const float2 v = state[((size_t)tile * sp.n + u) * 32 + lane];
     if (o < n_primal) {
       x[(size_t)o * batch + b] = v.x;
     } else {
@@ -390,7 +396,8 @@ struct StreamJob {
   StreamPlan sp;
   const float* bstream;
   const float* fstream;
-  float4* state;  // [tile][U][lane] ADMM state records
+  float2* state;  // [tile][U][lane] ADMM iterate records (x, 0) / (z, y)
+  const float2* param;  // [tile][U][lane] parameter records (q, 0) / (l, u)
   float* pres;    // [tile][U][lane] scaled primal residual of each constraint
   float* rhs;     // frontier form: [tile][n][lane] right-hand sides (release -> forward stage)
   float* fwd;     // frontier form: [tile][n][lane] forward results (sweep -> backward stage)
@@ -417,8 +424,9 @@ struct StreamArgs {
   int lstages, sstages;
   int meta_bytes;   // per L stage, 128-byte multiple
   int lbytes;       // per L stage L area
-  int sbytes;       // per S stage: max_rel x 32 lanes x 16 bytes of records (+ 4 of residuals)
-  int pres_off;     // byte offset of the residuals in an S stage (end of the records)
+  int sbytes;       // per S stage: max_rel x 32 lanes x (8 iterate + 8 parameter) bytes (+ 4 of residuals)
+  int pres_off;     // byte offset of the residuals in an S stage (end of the records; the
+                    // parameter records start at pres_off / 2)
   unsigned long long wait_limit_ns;  // give-up time of every handshake wait (the drain keeps kWaitLimitNs)
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
@@ -587,7 +595,8 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 // `end` repeats the group's first index: it loads the same operands, computes
 // the same values and stores them to the same places again.
 //   rel: per release (row byte offset, rho bits, rho^-1 bits, 0)
-//   S:   this lane's state record of release 0 in the stage (k-th at S[32 k])
+//   S, SP: this lane's iterate and parameter records of release 0 in the
+//          stage (k-th at S[32 k], SP[32 k])
 constexpr int kRelGroup = 2;  // releases per group (groups of 4 measured 3.5 % slower: register pressure)
 
 struct RelGroup {
@@ -633,7 +642,8 @@ __device__ __forceinline__ void rho_of(const RhoLane& l, int cls, int4 r, float&
 // unscale_perm when termination is checked).  kRho: per-instance rho by the
 // release's class (ucls: the classes of the chunk's releases).
 template <bool kTrack, bool kFrontier, bool kRho>
-__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float4* S, const float* SE,
+__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float2* S, const float2* SP,
+                                               const float* SE,
                                                const unsigned char* xb, const float* unscale_perm, const int* ucls,
                                                const RhoLane& rl, RelGroup& g) {
 #pragma unroll
@@ -656,7 +666,8 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
       g.f[j] = __int_as_float(r.w);
     }
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
-    g.st[j] = S[kk * 32];
+    const float2 it = S[kk * 32], pa = SP[kk * 32];
+    g.st[j] = make_float4(it.x, it.y, pa.x, pa.y);
     if constexpr (kTrack) g.e[j] = SE[kk * 32];
   }
 }
@@ -679,12 +690,12 @@ struct RelParams {
 // not back into the work vector.
 template <bool kCons, bool kTrack, bool kFrontier>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb, float* rt,
-                                                 float4* stu, float* peu, float& chg, float& pres, bool frozen_in) {
+                                                 float2* stu, float* peu, float& chg, float& pres, bool frozen_in) {
   const bool frozen = kTrack && frozen_in;
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
     float* xi = kFrontier ? rt + g.ix[j] * 32 : reinterpret_cast<float*>(xb + g.o[j]);
-    float2* out = reinterpret_cast<float2*>(stu + g.kk[j] * 32);
+    float2* out = stu + g.kk[j] * 32;
     if (!kCons) {
       const float xa = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
       const float xn = frozen ? g.st[j].x : xa;
@@ -715,21 +726,22 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
 }
 
 template <bool kCons, bool kTrack, bool kFrontier, bool kRho>
-__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float4* S, const float* SE,
-                                             const RelParams& rp, unsigned char* xb, float* rt, float4* stu,
+__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float2* S, const float2* SP,
+                                             const float* SE, const RelParams& rp, unsigned char* xb, float* rt,
+                                             float2* stu,
                                              float* peu, float& chg, float& pres, bool frozen,
                                              const float* unscale_perm, const int* ucls, const RhoLane& rl) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kTrack, kFrontier, kRho>(rel, begin, end, S, SE, xb, unscale_perm, ucls, rl, a);
+  load_rel_group<kTrack, kFrontier, kRho>(rel, begin, end, S, SP, SE, xb, unscale_perm, ucls, rl, a);
   for (int k = begin;; k += 2 * kRelGroup) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + kRelGroup < end ? k + kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier, kRho>(rel, kb, end, S, SE, xb, unscale_perm, ucls, rl, b);
+    load_rel_group<kTrack, kFrontier, kRho>(rel, kb, end, S, SP, SE, xb, unscale_perm, ucls, rl, b);
     update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + kRelGroup >= end) break;
     const int ka = k + 2 * kRelGroup < end ? k + 2 * kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier, kRho>(rel, ka, end, S, SE, xb, unscale_perm, ucls, rl, a);
+    load_rel_group<kTrack, kFrontier, kRho>(rel, ka, end, S, SP, SE, xb, unscale_perm, ucls, rl, a);
     update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, peu, chg, pres, frozen);
     if (k + 2 * kRelGroup >= end) break;
   }
@@ -909,7 +921,8 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             mbar_arrive_expect_tx(sfull + sr.stage, nrel * (kTrack ? 640u : 512u));
             if (nrel) {
               const size_t u = soff + (size_t)d.u0 * 32;
-              bulk_g2s(ss, J.state + u, nrel * 512u, sfull + sr.stage);
+              bulk_g2s(ss, J.state + u, nrel * 256u, sfull + sr.stage);
+              bulk_g2s(ss + a.pres_off / 2, J.param + u, nrel * 256u, sfull + sr.stage);
               if constexpr (kTrack) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
             }
             sr.advance(a.sstages);
@@ -1009,7 +1022,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         rt = J.rhs + (size_t)tile * n * 32 + lane;
         yt = J.fwd + (size_t)tile * n * 32 + lane;
       }
-      float4* stt = J.state + (size_t)tile * n * 32 + lane;
+      float2* stt = J.state + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
       RhoLane rl{};
       if constexpr (kRho) {
@@ -1069,19 +1082,19 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           // leaf columns (read by no other column): solved here, just before their release
           if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, a.wait_limit_ns)) return false;
-          const float4* S = reinterpret_cast<const float4*>(sring + (size_t)sr.stage * a.sbytes) + lane;
+          const float2* S = reinterpret_cast<const float2*>(sring + (size_t)sr.stage * a.sbytes) + lane;
+          const float2* SP = reinterpret_cast<const float2*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off / 2) + lane;
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
             // (frontier form: into rhs at the record's index)
             for (int k = pb; k < pe; ++k) {
               const int4 r = rel[k];
-              const float4 st = S[k * 32];
-              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = sigma * st.x - st.z;
+              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = sigma * S[k * 32].x - SP[k * 32].x;
             }
             for (int k = cb; k < ce; ++k) {
               const int4 r = rel[k];
-              const float4 st = S[k * 32];
+              const float2 st = S[k * 32];
               float rinv = __int_as_float(r.z);
               if constexpr (kRho) {
                 float rho;
@@ -1092,13 +1105,13 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             // read back by bulk copies once rel_done covers the pass's last chunk
             if (kFrontier && ch == 0) fence_proxy_async_global();
           } else {
-            float4* stu = stt + (size_t)u0 * 32;
+            float2* stu = stt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
             const int* ucls = kRho ? sp.u_cls + u0 : nullptr;
-            run_releases<false, kTrack, kFrontier, false>(rel, pb, pe, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+            run_releases<false, kTrack, kFrontier, false>(rel, pb, pe, S, SP, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
                                                           sp.unscale_perm, ucls, rl);
-            run_releases<true, kTrack, kFrontier, kRho>(rel, cb, ce, S, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+            run_releases<true, kTrack, kFrontier, kRho>(rel, cb, ce, S, SP, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
                                                         sp.unscale_perm, ucls, rl);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
@@ -1338,8 +1351,9 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   const size_t tl = (size_t)n_tiles * 32;
   float* bstream = work;
   float* fstream = bstream + (size_t)n_tiles * sp.blen;
-  float4* state = reinterpret_cast<float4*>(fstream + (size_t)n_tiles * sp.flen);
-  float* pres = reinterpret_cast<float*>(state + tl * sp.n);
+  float2* state = reinterpret_cast<float2*>(fstream + (size_t)n_tiles * sp.flen);
+  float2* param = state + tl * sp.n;
+  float* pres = reinterpret_cast<float*>(param + tl * sp.n);
   float* rhs = sp.frontier_slots > 0 ? pres + tl * sp.n : nullptr;
   float* fwd = sp.frontier_slots > 0 ? rhs + tl * sp.n : nullptr;
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba, rinv_rows, rinv_rows ? (long long)batch : 0};
@@ -1363,14 +1377,15 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   }
   {
     dim3 grid(ceil_div(tl, 128), sp.n < 1024 ? sp.n : 1024);
-    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm && track, x, z, y, qs, ls, us, state, pres, batch,
-                                                 n_tiles);
+    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm && track, x, z, y, qs, ls, us, state, param, pres,
+                                                 batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
   job->sp = sp;
   job->bstream = bstream;
   job->fstream = fstream;
   job->state = state;
+  job->param = param;
   job->pres = pres;
   job->rhs = rhs;
   job->fwd = fwd;
@@ -1448,6 +1463,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     J.bstream = d.bstream;
     J.fstream = d.fstream;
     J.state = d.state;
+    J.param = d.param;
     J.pres = d.pres;
     J.rhs = d.rhs;
     J.fwd = d.fwd;

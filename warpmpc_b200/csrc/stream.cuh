@@ -8,8 +8,10 @@
 // the chunk's columns).  Both are cut into chunks; every chunk is one
 // contiguous bulk copy (cp.async.bulk) into a shared-memory ring stage.
 //
-// ADMM state (x or z, y) and parameters (q or l, u) are stored per tile as one
-// 16-byte record per (index, lane), in "release order" U: the order in which
+// ADMM state (x or z, y) and parameters (q or l, u) are stored per tile as
+// two 8-byte records per (index, lane) in two arrays -- the iterates, written
+// every iteration, and the parameters, only read -- in "release order" U: the
+// order in which
 // the backward sweep finishes with a KKT index (after the smallest column
 // whose correction reads it), so each chunk of the backward sweep updates one
 // contiguous U range.
@@ -308,7 +310,8 @@ struct StreamJobDesc {
   StreamPlan sp;
   const float* bstream = nullptr;
   const float* fstream = nullptr;
-  float4* state = nullptr;
+  float2* state = nullptr;        // [tile][U][lane] iterate records
+  const float2* param = nullptr;  // [tile][U][lane] parameter records
   float* pres = nullptr;
   float* rhs = nullptr;   // frontier form: [tile][n][lane] right-hand sides
   float* fwd = nullptr;   // frontier form: [tile][n][lane] forward results
