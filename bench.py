@@ -739,10 +739,14 @@ def mixed_timing(args, dev, world):
 
 # schedule candidates the bench's tuner times for each problem (the library
 # defaults first); every candidate must reproduce the first one's iterates
-TUNE_CANDIDATES = ({}, {"frontier_copies": 1}, {"max_ctas": 3}, {"units": 12, "cols": 12, "rel": 10, "funits": 12})
+# schedules the bench's tuner times (all give the same bits; measured on the quadrotor pattern at 65,536
+# instances: 24-unit chunks 59.8 ms per ADMM launch against 62.9 ms for the library's 16)
+TUNE_CANDIDATES = ({}, {"units": 24, "cols": 24, "rel": 16, "funits": 24},
+                   {"units": 24, "cols": 24, "rel": 16, "funits": 24, "frontier_copies": 1},
+                   {"frontier_copies": 1})
 
 
-def tuned_schedule(args, plan, batch_np, dev, max_instances=32768):
+def tuned_schedule(args, plan, batch_np, dev, max_instances=65536):
     """The fastest schedule of this pattern on this device (autotune_stream,
     timed on up to max_instances of the workload's instances, cached per
     pattern and device for the process), or {} with --no-tune."""
@@ -753,7 +757,7 @@ def tuned_schedule(args, plan, batch_np, dev, max_instances=32768):
     sl = slice(0, min(batch_np.batch, max_instances))
     try:
         r = autotune_stream(plan, batch_np.p_values[sl], batch_np.a_values[sl], batch_np.q[sl], batch_np.l[sl],
-                            batch_np.u[sl], candidates=TUNE_CANDIDATES, repeats=2, device=dev,
+                            batch_np.u[sl], candidates=TUNE_CANDIDATES, repeats=3, device=dev,
                             cache_path=os.path.join("/tmp", "wmpc_bench_tune.json"))
     except Exception as exc:  # report, do not hide: the defaults run instead
         print(f"[bench] schedule tuning failed, library defaults used: {exc!r}", file=sys.stderr)
