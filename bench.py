@@ -740,10 +740,9 @@ def mixed_timing(args, dev, world):
 # schedule candidates the bench's tuner times for each problem (the library
 # defaults first); every candidate must reproduce the first one's iterates
 # schedules the bench's tuner times (all give the same bits; measured on the quadrotor pattern at 65,536
-# instances: 24-unit chunks 59.8 ms per ADMM launch against 62.9 ms for the library's 16)
-TUNE_CANDIDATES = ({}, {"units": 24, "cols": 24, "rel": 16, "funits": 24},
-                   {"units": 24, "cols": 24, "rel": 16, "funits": 24, "frontier_copies": 1},
-                   {"frontier_copies": 1})
+# instances: the library's 24-unit chunks 59.8 ms per ADMM launch against 62.9 ms with 16)
+TUNE_CANDIDATES = ({}, {"frontier_copies": 1}, {"units": 16, "cols": 16, "rel": 12, "funits": 16},
+                   {"units": 16, "cols": 16, "rel": 12, "funits": 16, "frontier_copies": 1})
 
 
 def tuned_schedule(args, plan, batch_np, dev, max_instances=65536):

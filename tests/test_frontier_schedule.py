@@ -24,16 +24,18 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import stream_sim  # noqa: E402
 
 FRONTIER = (16, 16, 12, 16, 4)
+FRONTIER_24 = (24, 24, 16, 24, 4)  # the library's default chunk targets
 
 
 @pytest.mark.parametrize("cls,iters", [(problems.SMALL, 4), (problems.CARTPOLE, 3),
                                        (problems.MPCClass("q5", 12, 4, 5, 10.0, 2.0, 1.0, "quadrotor"), 3)],
                          ids=["small", "cartpole", "quadrotor_n5"])
 @pytest.mark.parametrize("lag", [None, 1])
-def test_frontier_replay_bitexact(cls, iters, lag):
+@pytest.mark.parametrize("targets", [FRONTIER, FRONTIER_24], ids=["chunks16", "chunks24"])
+def test_frontier_replay_bitexact(cls, iters, lag, targets):
     b = problems.make_batch(cls, 6, seed=31)
     plan = problems.make_plan(b)
-    sched = stream_schedule(plan, targets=FRONTIER)
+    sched = stream_schedule(plan, targets=targets)
     assert 0 < sched["frontier_slots"] < plan.qdldl_plan.n and sched["frontier_lag"] == 4
     got = stream_sim.replay(plan, sched, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters, lag=lag)
     ref = osqp_ref.solve(plan, b.p_values, b.a_values, b.q, b.l, b.u, max_iter=iters)

@@ -249,8 +249,12 @@ struct HostPattern {
 };
 
 struct StreamTargets {
-  int units = 16, cols = 16, rel = 12;  // backward chunks
-  int funits = 16;                      // forward chunks
+  // chunk targets: 24-unit chunks are the largest whose ring still lets two
+  // frontier-form CTAs share an SM on the quadrotor pattern, and measured
+  // fastest there (59.8 ms per ADMM launch at 65,536 instances against 62.9
+  // with 16) and chosen by the tuner for every benchmarked class
+  int units = 24, cols = 24, rel = 16;  // backward chunks
+  int funits = 24;                      // forward chunks
   int offload = 0;                      // also give the releaser warp: 1 leaf columns, 2 pre rows (bits)
   int frontier = 0;                     // frontier slots (see build_frontier_slots); needs offload 0
   int frontier_lag = 4;                 // chunks a release may trail the sweep (bounds the L ring depth)

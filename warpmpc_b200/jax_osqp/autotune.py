@@ -50,10 +50,11 @@ KNOBS = {
 }
 
 DEFAULT_CANDIDATES = (
-    {},  # the library defaults
+    {},  # the library defaults (24-unit chunks)
+    {"units": 16, "cols": 16, "rel": 12, "funits": 16},
     {"units": 12, "cols": 12, "rel": 10, "funits": 12},
-    {"units": 24, "cols": 24, "rel": 16, "funits": 24},
     {"units": 16, "cols": 16, "rel": 12, "funits": 16, "offload": 1},
+    {"frontier_copies": 1},
     {"ctas": 1},
 )
 

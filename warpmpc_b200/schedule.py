@@ -15,7 +15,7 @@ import numpy as np
 from . import native
 from .jax_qdldl.planning import plan_ragged_program
 
-DEFAULT_TARGETS = (16, 16, 12, 16, 0)  # backward units, columns, releases; forward units; offload bits
+DEFAULT_TARGETS = (24, 24, 16, 24, 0)  # backward units, columns, releases; forward units; offload bits (the library's)
 
 
 def _pattern_desc(qp):
