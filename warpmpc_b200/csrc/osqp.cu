@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(32 * kResParts) residual_kernel(
     for (int row = part; row < o.m; row += kResParts) {
       float ax = 0.0f;
       const int e0 = __ldg(o.a_row_ptr + row), e1 = __ldg(o.a_row_ptr + row + 1);
+#pragma unroll 4
       for (int t = e0; t < e1; ++t) {
         const int e = __ldg(o.a_row_ent + t);
         ax = ax + in.a(e) * xu(__ldg(o.a_cols + e));
@@ -421,9 +422,11 @@ __global__ void __launch_bounds__(32 * kResParts) residual_kernel(
     for (int j = part; j < o.n; j += kResParts) {
       float px = 0.0f;
       const int f0 = __ldg(o.pf_row_ptr + j), f1 = __ldg(o.pf_row_ptr + j + 1);
+#pragma unroll 4
       for (int t = f0; t < f1; ++t) px = px + in.p(__ldg(o.pf_val + t)) * xu(__ldg(o.pf_col + t));
       float aty = 0.0f;
       const int c0 = __ldg(o.a_col_ptr + j), c1 = __ldg(o.a_col_ptr + j + 1);
+#pragma unroll 4
       for (int e = c0; e < c1; ++e) {
         const int row = __ldg(o.a_rows + e);
         aty = aty + in.a(e) * (st.y[(long long)row * st.ld + b] * __ldg(o.y_unscale + row));

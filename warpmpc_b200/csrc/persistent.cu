@@ -1365,6 +1365,9 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
     const int per_sm = ceil_div(n_tiles, num_sms > 0 ? num_sms : 1);
     const int budget_floats = (200 * 1024 / 4) / (per_sm > 0 ? per_sm : 1);
     int lbatch = (budget_floats - factor_warp_words(sp, 0)) / 33;
+    // WMPC_FACTOR_LBATCH fixes the batch instead (tuning: fewer resident
+    // warps, fewer round trips per row)
+    if (const char* v = getenv("WMPC_FACTOR_LBATCH")) lbatch = atoi(v);
     lbatch = lbatch < 8 ? 8 : (lbatch > 128 ? 128 : lbatch);
     const size_t smem = (size_t)warps * factor_warp_words(sp, lbatch) * sizeof(float);
     if (smem > (size_t)kMaxSmemBytes) return fail(WMPC_ERR_UNSUPPORTED, "factor rows too long for shared memory");
