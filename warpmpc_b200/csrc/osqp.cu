@@ -313,7 +313,7 @@ struct Residuals {
 // The objective's sums run in kResParts interleaved partial sums (column j
 // into part j % kResParts), added in part order: the split residual_kernel
 // and this one-thread form give the same bits.
-constexpr int kResParts = 4;
+constexpr int kResParts = 8;  // threads per instance in residual_kernel
 
 // q is the unscaled linear term: q[j * ldq]
 __device__ Residuals residuals(const Osqp& o, const InstanceData& in, const State& st, int b,
@@ -391,7 +391,7 @@ __device__ __forceinline__ bool finite_res(const Residuals& r) {
 // part p takes A's rows and the columns j = p, p + kResParts, ...; every
 // row's and column's sum is still formed by one thread in the reference's
 // order, so prim, dual and the norms (maxima) equal residuals()' exactly; the
-// objective's two sums are added part by part.  Four times the warps in
+// objective's two sums are added part by part.  Eight times the warps in
 // flight for a latency-bound loop of dependent index and value loads.
 __global__ void __launch_bounds__(32 * kResParts) residual_kernel(
     Osqp o, const float* __restrict__ pT, long long ldp, int sbp, const float* __restrict__ aT, long long lda,

@@ -1367,6 +1367,10 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
     int lbatch = (budget_floats - factor_warp_words(sp, 0)) / 33;
     // WMPC_FACTOR_LBATCH fixes the batch instead (tuning: fewer resident
     // warps, fewer round trips per row)
+    // with many tiles per SM a short batch measured faster (16: 8.98 ms against 9.23 for the budget's
+    // 24 on 65,536 quadrotor instances; 32 to 128: 11.9 to 16.5 ms): the smaller shared-memory
+    // request leaves more of the SM's unified memory to L1, which serves the index tables
+    if (per_sm >= 8 && lbatch > 16) lbatch = 16;
     if (const char* v = getenv("WMPC_FACTOR_LBATCH")) lbatch = atoi(v);
     lbatch = lbatch < 8 ? 8 : (lbatch > 128 ? 128 : lbatch);
     const size_t smem = (size_t)warps * factor_warp_words(sp, lbatch) * sizeof(float);
