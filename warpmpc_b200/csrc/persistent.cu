@@ -428,7 +428,6 @@ struct StreamArgs {
   int pres_off;     // byte offset of the residuals in an S stage (end of the records; the
                     // parameter records start at pres_off / 2)
   unsigned long long wait_limit_ns;  // give-up time of every handshake wait (the drain keeps kWaitLimitNs)
-  int role_rotate;  // 1: rotate the warps' roles by the CTA's hardware warp-slot group (see the kernel)
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
 
@@ -488,7 +487,7 @@ __device__ __forceinline__ bool check_point(int check_every, int it) { return ch
 __host__ __device__ inline size_t stream_smem_bytes(int n, int lstages, int sstages, int lstage_bytes,
                                                     int sstage_bytes) {
   return (size_t)(n + 2) * 128 + (size_t)lstages * lstage_bytes + (size_t)sstages * sstage_bytes +
-         16 * (size_t)(lstages + sstages) + 32;  // barriers; abort flag, counters, the stop item, role rotation
+         16 * (size_t)(lstages + sstages) + 32;  // barriers; abort flag, three counters, the stop item
 }
 
 // One unit's operands, loaded ahead of its arithmetic.
@@ -796,7 +795,6 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
   volatile unsigned* stop_at = rel_done + 1;  // item index where a converged tile's items end
   unsigned* rel_done1 = rel_done + 2;         // items the second releaser finished (kSplit)
   unsigned* y_done = rel_done + 3;            // frontier form: forward items whose results are in fwd
-  unsigned* role_rot = rel_done + 4;          // the CTA's role rotation
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.lstages; ++s) {
@@ -813,27 +811,13 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
     *stop_at = 0xffffffffu;
     *rel_done1 = 0;
     *y_done = 0;
-    // Roles (0 sweeper, 1 producer, 2 and 3 releasers) rotate by the warp-slot
-    // group this CTA got on its SM, so that two co-resident 4-warp CTAs put
-    // their sweepers (the busiest warps) on different SM sub-partitions
-    // (warp slot modulo 4) instead of the same one.  Any rotation is correct:
-    // the warps only need to agree on it.
-    unsigned rot = 0;
-    if (a.role_rotate && blockDim.x == 128) {
-      unsigned wid;
-      asm volatile("mov.u32 %0, %%warpid;" : "=r"(wid));
-      rot = (wid >> 2) & 3u;
-    }
-    *role_rot = rot;
     fence_mbarrier_init();
   }
   __syncthreads();
-  const int nwarps = blockDim.x >> 5;
-  const int role = (warp - (int)*role_rot + nwarps) % nwarps;
 
   uint32_t issued_l = 0, issued_s = 0;  // producer: copies issued per ring
 
-  if (role == 1) {
+  if (warp == 1) {
     // ------------------------------ producer ------------------------------
     if (lane == 0) {
       Ring lr{0, 0}, sr{0, 0};
@@ -958,7 +942,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         }
       }
     }
-  } else if (role == 0) {
+  } else if (warp == 0) {
     // ------------------------------ sweeper ------------------------------
     Ring lr{0, 0};
     unsigned t = 0;  // item index (all tiles)
@@ -1018,7 +1002,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
     if (!ok && lane == 0) *abort_flag = 1;
   } else {
     // ------------------------------ releaser ------------------------------
-    const int rw = role - 2;  // releaser 0, or (kSplit) releaser 1
+    const int rw = warp - 2;  // releaser 0, or (kSplit) releaser 1
     Ring lr{0, 0}, sr{0, 0};
     unsigned t = 0;
     unsigned char* xb = smem + lane * 4;
@@ -1192,7 +1176,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
   }
   __syncthreads();
   if (*abort_flag) {
-    if (role == 1 && lane == 0) {  // the producer's issuing lane
+    if (threadIdx.x == 32) {
       // drain: wait (bounded) for the last bulk copy issued into every stage
       // (earlier ones completed before their stage was reused)
       for (uint32_t s = 0; s < (uint32_t)a.lstages && s < issued_l; ++s) {
@@ -1515,7 +1499,6 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.sbytes = cfg.sbytes;
   a.pres_off = cfg.pres_off;
   a.wait_limit_ns = kWaitLimitNs;
-  a.role_rotate = env_disabled("WMPC_STREAM_ROLE_ROTATE_OFF") ? 0 : 1;
   if (const char* v = getenv("WMPC_STREAM_WAIT_LIMIT_NS")) {
     const long long ns = atoll(v);
     if (ns > 0) a.wait_limit_ns = (unsigned long long)ns;
