@@ -11,12 +11,7 @@ from oracle import qdldl_ref
 from warpmpc_b200 import problems, schedule
 
 # the kernel's constants (solve_stream.cu)
-BOX, CHUNK_ENTRIES, CHUNK_COLS, RHS_ROWS, TABLE_BYTES, STEP = 32, 64, 32, 96, 512, 16
-
-
-def step_width(cnt):
-    """The kernel's step for a column of cnt entries (1, 4, 8, else 16 per step)."""
-    return 1 if cnt == 1 else 4 if cnt <= 4 else 8 if cnt <= 8 else 16
+BOX, CHUNK_ENTRIES, CHUNK_COLS, RHS_ROWS, TABLE_BYTES, STEP = 32, 64, 32, 96, 512, 8
 DATA_ROWS = CHUNK_ENTRIES + CHUNK_COLS
 
 
@@ -65,11 +60,10 @@ def replay(qp, tab, lx, dinv, rhs):
                 e = int(cend[j])
                 if e > b:
                     val = X[c0 + j]
-                    W = step_width(e - b)
-                    for q in range(b, e, W):
-                        o = [int(rows[q + i]) if q + i < e else n for i in range(W)]
-                        w = [X[o[i]] for i in range(W)]
-                        for i in range(W):
+                    for q in range(b, e, STEP):
+                        o = [int(rows[q + i]) if q + i < e else n for i in range(STEP)]
+                        w = [X[o[i]] for i in range(STEP)]
+                        for i in range(STEP):
                             X[o[i]] = f32(w[i] - f32(L[q + i] * val))
                 b = e
     assert X[n + 1] == 0.0
@@ -79,9 +73,8 @@ def replay(qp, tab, lx, dinv, rhs):
             b = int(cend[j - 1]) if j > 0 else 0
             e = int(cend[j])
             corr = f32(0.0)
-            W = step_width(e - b) if e > b else 1
-            for q in range(b, e, W):
-                for i in range(W):
+            for q in range(b, e, STEP):
+                for i in range(STEP):
                     if q + i < e:
                         corr = f32(corr + f32(L[q + i] * X[rows[q + i]]))
                     else:  # L = 0 times the zero row

@@ -130,6 +130,23 @@ __device__ __forceinline__ void copy_kkt_inputs(const Osqp& o, const OsqpInputs&
   }
 }
 
+// cnt (<= W) updates of one step, to distinct slots: every load, then every store.
+template <int W>
+__device__ __forceinline__ void update_batch(const int* slot, const float* lv, float* ys, float val, int cnt) {
+  int su[W];
+  float yv[W], l[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    if (i < cnt) {
+      su[i] = slot[i];
+      l[i] = lv[i * 32];
+      yv[i] = ys[su[i] * 32];
+    }
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    if (i < cnt) ys[su[i] * 32] = yv[i] - l[i] * val;
+}
+
 // A row's ranges: a = {p0, p1, i0, i1} (program steps, initial entries),
 // b = {ub, uend, doff, kin base} (updates, D^-1 offset of the row, first
 // KKT input descriptor).
@@ -280,18 +297,15 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
         }
         int cnt = off - q < ue - u ? off - q : ue - u;
         cnt = cnt < kFacStep ? cnt : kFacStep;
-        int su[kFacStep];
-        float yv[kFacStep], lv[kFacStep];
-#pragma unroll
-        for (int i = 0; i < kFacStep; ++i)
-          if (i < cnt) {
-            su[i] = slot_w[u - ub + i];
-            lv[i] = lst[(u - ub + i) * 32];
-            yv[i] = ys[su[i] * 32];
-          }
-#pragma unroll
-        for (int i = 0; i < kFacStep; ++i)
-          if (i < cnt) ys[su[i] * 32] = yv[i] - lv[i] * val;
+        // the batch width by the count (predicated-off slots still issue)
+        if (cnt == 1) {
+          const int su = slot_w[u - ub];
+          ys[su * 32] = ys[su * 32] - lst[(u - ub) * 32] * val;
+        } else if (cnt <= 4) {
+          update_batch<4>(slot_w + (u - ub), lst + (u - ub) * 32, ys, val, cnt);
+        } else {
+          update_batch<kFacStep>(slot_w + (u - ub), lst + (u - ub) * 32, ys, val, cnt);
+        }
         q += cnt;
         u += cnt;
       }

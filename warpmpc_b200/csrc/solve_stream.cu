@@ -16,8 +16,7 @@
 // then the tile's result rows are stored, unpermuted, to out.  X ([row][lane],
 // conflict-free, plus a trash row and a zero row) stays in shared memory for
 // the whole tile.  Chunks end on column boundaries, so every column's entries
-// sit in one stage.  A column is worked in steps of 1, 4, 8 or 16 entries (by
-// its length; at most kStep): the step's
+// sit in one stage.  A column is worked kStep entries at a time: the step's
 // index words, L values and work-vector reads are all issued before its
 // arithmetic (padding slots write the trash row, or read L = 0 times the
 // zero row), so one shared-memory round trip per step is on the sweep's
@@ -52,7 +51,7 @@ constexpr int kTableBytes = 512;                         // index table area of 
 constexpr int kDataBytes = (kChunkEntries + kChunkCols) * 128;  // L rows, then D^-1 rows
 constexpr int kStageBytes = kTableBytes + kDataBytes;    // 12800 (a multiple of 128)
 constexpr int kMaxStages = 8;
-constexpr int kStep = 16;  // most L entries of one column a sweeper step loads before its arithmetic
+constexpr int kStep = 8;  // L entries of one column a sweeper step loads before its arithmetic
 constexpr uint64_t kSolveWaitNs = 2000000000ull;          // 2 s: a healthy wait is microseconds
 static_assert(kRhsRows * 128 <= kDataBytes, "an rhs item must fit the data area");
 static_assert((4 + kChunkCols + kChunkEntries) * 4 <= kTableBytes, "a chunk table must fit its area");
@@ -80,44 +79,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
           smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
-}
-
-// One forward step: entries [q, q + W) of a column (those past e update the
-// trash row), every load before the arithmetic.
-template <int W>
-__device__ __forceinline__ void fwd_step(int q, int e, const int* roff, const float* data, unsigned char* xb,
-                                         float val, int trash_off) {
-  int o[W];
-  float l[W], w[W];
-#pragma unroll
-  for (int i = 0; i < W; ++i) {
-    o[i] = q + i < e ? roff[q + i] : trash_off;
-    l[i] = data[(q + i) * 32];
-  }
-#pragma unroll
-  for (int i = 0; i < W; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
-#pragma unroll
-  for (int i = 0; i < W; ++i) *reinterpret_cast<float*>(xb + o[i]) = w[i] - l[i] * val;
-}
-
-// One backward step: corr + L_r x_r over entries [q, q + W) in order (those
-// past e add L = 0 times the zero row, +0).
-template <int W>
-__device__ __forceinline__ float bwd_step(int q, int e, const int* roff, const float* data, const unsigned char* xb,
-                                          int zero_off, float corr) {
-  int o[W];
-  float l[W], w[W];
-#pragma unroll
-  for (int i = 0; i < W; ++i) {
-    const bool v = q + i < e;
-    o[i] = v ? roff[q + i] : zero_off;
-    l[i] = v ? data[(q + i) * 32] : 0.0f;
-  }
-#pragma unroll
-  for (int i = 0; i < W; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
-#pragma unroll
-  for (int i = 0; i < W; ++i) corr = corr + l[i] * w[i];
-  return corr;
 }
 
 // Items of one tile: rhs blocks, forward chunks ascending, backward chunks descending.
@@ -237,24 +198,25 @@ __global__ void __launch_bounds__(64, 1) solve_stream_kernel(const __grid_consta
           const int* roff = tb + 4 + C;  // byte offsets (row * 128) into X
           if (kind == kSolveFwd) {
             // x_r -= L_rc x_c over column c's rows (distinct rows: independent),
-            // in steps of W entries (1, 4, 8 or 16 by the column's length) with
-            // all of a step's loads issued before its arithmetic; slots past the
-            // column's end update the trash row
+            // kStep entries at a time with all their loads issued before the
+            // arithmetic; slots past the column's end update the trash row
             int b = 0;
             for (int j = 0; j < C; ++j) {
               const int e = cend[j];
-              const int cnt = e - b;
-              if (cnt > 0) {
+              if (e > b) {
                 const float val = X[(c0 + j) * 32 + lane];
-                if (cnt == 1) {
-                  float* y = reinterpret_cast<float*>(xb + roff[b]);
-                  *y = *y - data[b * 32] * val;
-                } else if (cnt <= 4) {
-                  fwd_step<4>(b, e, roff, data, xb, val, trash_off);
-                } else if (cnt <= 8) {
-                  fwd_step<8>(b, e, roff, data, xb, val, trash_off);
-                } else {
-                  for (int q = b; q < e; q += 16) fwd_step<16>(q, e, roff, data, xb, val, trash_off);
+                for (int q = b; q < e; q += kStep) {
+                  int o[kStep];
+                  float l[kStep], w[kStep];
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) {
+                    o[i] = q + i < e ? roff[q + i] : trash_off;
+                    l[i] = data[(q + i) * 32];
+                  }
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
+#pragma unroll
+                  for (int i = 0; i < kStep; ++i) *reinterpret_cast<float*>(xb + o[i]) = w[i] - l[i] * val;
                 }
               }
               b = e;
@@ -266,16 +228,20 @@ __global__ void __launch_bounds__(64, 1) solve_stream_kernel(const __grid_consta
             const float* dv = data + kChunkEntries * 32;
             for (int j = C - 1; j >= 0; --j) {
               const int b = j > 0 ? cend[j - 1] : 0, e = cend[j];
-              const int cnt = e - b;
               float corr = 0.0f;
-              if (cnt == 1) {
-                corr = corr + data[b * 32] * *reinterpret_cast<const float*>(xb + roff[b]);
-              } else if (cnt > 1 && cnt <= 4) {
-                corr = bwd_step<4>(b, e, roff, data, xb, zero_off, corr);
-              } else if (cnt > 4 && cnt <= 8) {
-                corr = bwd_step<8>(b, e, roff, data, xb, zero_off, corr);
-              } else if (cnt > 8) {
-                for (int q = b; q < e; q += 16) corr = bwd_step<16>(q, e, roff, data, xb, zero_off, corr);
+              for (int q = b; q < e; q += kStep) {
+                int o[kStep];
+                float l[kStep], w[kStep];
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) {
+                  const bool v = q + i < e;
+                  o[i] = v ? roff[q + i] : zero_off;
+                  l[i] = v ? data[(q + i) * 32] : 0.0f;
+                }
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) w[i] = *reinterpret_cast<const float*>(xb + o[i]);
+#pragma unroll
+                for (int i = 0; i < kStep; ++i) corr = corr + l[i] * w[i];
               }
               float* xc = X + (c0 + j) * 32 + lane;
               *xc = *xc * dv[j * 32] - corr;
