@@ -231,6 +231,10 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
   sk.add(hs.frow0.data(), hs.frow0.size(), &sp.frow0);
   sk.add(hs.frows.data(), hs.frows.size(), &sp.frows);
   sk.add(hs.chunk_nrel.data(), hs.chunk_nrel.size(), &sp.chunk_nrel);
+  // primal releases per backward chunk (chunk header word 5)
+  std::vector<int> chunk_nprim(hs.n_chunks, 0);
+  for (int c = 0; c < hs.n_chunks; ++c) chunk_nprim[c] = hs.meta[hs.meta_off[c] + 5];
+  sk.add(chunk_nprim.data(), chunk_nprim.size(), &sp.chunk_nprim);
   sk.add(hs.chunk_pre_u0.data(), hs.chunk_pre_u0.size(), &sp.chunk_pre_u0);
   sk.add(hs.chunk_pre_units.data(), hs.chunk_pre_units.size(), &sp.chunk_pre_units);
   sk.add(hs.meta_off.data(), hs.meta_off.size(), &sp.meta_off);

@@ -336,11 +336,11 @@ __global__ void __launch_bounds__(64, 1) factor_stream_kernel(Pattern pat, Strea
 // state layout conversions: symbolic-major (KKT row, instance) <-> tile-major U order
 // ---------------------------------------------------------------------------
 
-// ADMM state per tile in release order U, two 8-byte records per (index,
-// lane): the iterate (x, 0) for a primal index, (z, y) for a constraint --
-// rewritten every iteration -- and the parameters (sigma-scaled q, 0) or
-// (l, u) -- only read --, in two arrays of the same layout (the iterates
-// first, then the parameters);
+// ADMM state per tile in release order U, per (index, lane) an iterate --
+// rewritten every iteration -- and parameters -- only read --, each in
+// arrays of the layout [tile][U][lane]: a primal index's x and sigma-scaled
+// q as 4-byte records (state_p, param_p), a constraint's (z, y) and (l, u)
+// as 8-byte records (state, param);
 // and the scaled primal residual (A x - z)_r of a constraint (0 for a primal
 // index), formed when `form` (a warm start whose termination is checked; a
 // cold start's x = z = 0 gives 0; without checks nothing reads it).
@@ -348,7 +348,8 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
                                        const float* __restrict__ z, const float* __restrict__ y,
                                        const float* __restrict__ qs, const float* __restrict__ ls,
                                        const float* __restrict__ us, float2* __restrict__ state,
-                                       float2* __restrict__ param, float* __restrict__ pres, int batch,
+                                       float2* __restrict__ param, float* __restrict__ state_p,
+                                       float* __restrict__ param_p, float* __restrict__ pres, int batch,
                                        int n_tiles) {
   const int n_primal = o.n;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -359,8 +360,8 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
     const int k = __ldg(sp.u_orig + u);
     const size_t dst = ((size_t)tile * sp.n + u) * 32 + lane;
     if (k < n_primal) {
-      state[dst] = make_float2(x[(size_t)k * batch + bb], 0.0f);
-      param[dst] = make_float2(qs[(size_t)k * batch + bb], 0.0f);
+      state_p[dst] = x[(size_t)k * batch + bb];
+      param_p[dst] = qs[(size_t)k * batch + bb];
       pres[dst] = 0.0f;
     } else {
       const int r = k - n_primal;
@@ -383,6 +384,7 @@ __global__ void state_to_stream_kernel(StreamPlan sp, Osqp o, OsqpInputs in, boo
 }
 
 __global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float2* __restrict__ state,
+                                       const float* __restrict__ state_p,
                                        float* __restrict__ x, float* __restrict__ z, float* __restrict__ y,
                                        int batch) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -390,10 +392,11 @@ __global__ void stream_to_state_kernel(StreamPlan sp, int n_primal, const float2
   const int tile = b >> 5, lane = b & 31;
   for (int u = blockIdx.y; u < sp.n; u += gridDim.y) {
     const int o = __ldg(sp.u_orig + u);
-    const float2 v = state[((size_t)tile * sp.n + u) * 32 + lane];
+    const size_t at = ((size_t)tile * sp.n + u) * 32 + lane;
     if (o < n_primal) {
-      x[(size_t)o * batch + b] = v.x;
+      x[(size_t)o * batch + b] = state_p[at];
     } else {
+      const float2 v = state[at];
       const int r = o - n_primal;
       z[(size_t)r * batch + b] = v.x;
       y[(size_t)r * batch + b] = v.y;
@@ -410,8 +413,10 @@ struct StreamJob {
   StreamPlan sp;
   const float* bstream;
   const float* fstream;
-  float2* state;  // [tile][U][lane] ADMM iterate records (x, 0) / (z, y)
-  const float2* param;  // [tile][U][lane] parameter records (q, 0) / (l, u)
+  float2* state;  // [tile][U][lane] constraint iterate records (z, y)
+  const float2* param;  // [tile][U][lane] constraint parameter records (l, u)
+  float* state_p;  // [tile][U][lane] primal iterate records x
+  const float* param_p;  // [tile][U][lane] primal parameter records (sigma-scaled q)
   float* pres;    // [tile][U][lane] scaled primal residual of each constraint
   float* rhs;     // frontier form: [tile][n][lane] right-hand sides (release -> forward stage)
   float* fwd;     // frontier form: [tile][n][lane] forward results (sweep -> backward stage)
@@ -609,8 +614,8 @@ __device__ __forceinline__ void run_units(const int4* __restrict__ mu, const uns
 // `end` repeats the group's first index: it loads the same operands, computes
 // the same values and stores them to the same places again.
 //   rel: per release (row byte offset, rho bits, rho^-1 bits, 0)
-//   S, SP: this lane's iterate and parameter records of release 0 in the
-//          stage (k-th at S[32 k], SP[32 k])
+//   Recs: this lane's records of the chunk's releases in the stage (the
+//         primal ones first, 4 bytes each, then the constraints', 8 bytes)
 constexpr int kRelGroup = 2;  // releases per group (groups of 4 measured 3.5 % slower: register pressure)
 
 struct RelGroup {
@@ -651,13 +656,23 @@ __device__ __forceinline__ void rho_of(const RhoLane& l, int cls, int4 r, float&
   }
 }
 
+// This lane's records of a backward chunk's releases in an S stage: release
+// k < nprim (primal) at ip[32 k] (iterate x) and pp[32 k] (q), a constraint
+// release k at ic[32 (k - nprim)] ((z, y)) and pc[...] ((l, u)).
+struct StageRecs {
+  const float* ip;
+  const float* pp;
+  const float2* ic;
+  const float2* pc;
+  int nprim;
+};
+
 // A record's last word: the released index's unscale factor (plain form) or
 // the index itself (frontier form, whose unscale factors come from
 // unscale_perm when termination is checked).  kRho: per-instance rho by the
 // release's class (ucls: the classes of the chunk's releases).
-template <bool kTrack, bool kFrontier, bool kRho>
-__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const float2* S, const float2* SP,
-                                               const float* SE,
+template <bool kCons, bool kTrack, bool kFrontier, bool kRho>
+__device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, const StageRecs& S, const float* SE,
                                                const unsigned char* xb, const float* unscale_perm, const int* ucls,
                                                const RhoLane& rl, RelGroup& g) {
 #pragma unroll
@@ -680,8 +695,12 @@ __device__ __forceinline__ void load_rel_group(const int4* rel, int k, int end, 
       g.f[j] = __int_as_float(r.w);
     }
     g.x[j] = *reinterpret_cast<const float*>(xb + r.x);
-    const float2 it = S[kk * 32], pa = SP[kk * 32];
-    g.st[j] = make_float4(it.x, it.y, pa.x, pa.y);
+    if constexpr (kCons) {
+      const float2 it = S.ic[(kk - S.nprim) * 32], pa = S.pc[(kk - S.nprim) * 32];
+      g.st[j] = make_float4(it.x, it.y, pa.x, pa.y);
+    } else {
+      g.st[j] = make_float4(S.ip[kk * 32], 0.0f, S.pp[kk * 32], 0.0f);
+    }
     if constexpr (kTrack) g.e[j] = SE[kk * 32];
   }
 }
@@ -702,9 +721,12 @@ struct RelParams {
 // kFrontier: the next right-hand side goes to rt (this lane's column of the
 // right-hand-side vector) at the index the record carries in its last word,
 // not back into the work vector.
+// stu / stp: this lane's constraint / primal iterate records of the chunk's
+// first release in HBM (release k at [32 k]).
 template <bool kCons, bool kTrack, bool kFrontier>
 __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelParams& rp, unsigned char* xb, float* rt,
-                                                 float2* stu, float* peu, float& chg, float& pres, bool frozen_in) {
+                                                 float2* stu, float* stp, float* peu, float& chg, float& pres,
+                                                 bool frozen_in) {
   const bool frozen = kTrack && frozen_in;
 #pragma unroll
   for (int j = 0; j < kRelGroup; ++j) {
@@ -713,7 +735,7 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
     if (!kCons) {
       const float xa = rp.alpha * g.x[j] + rp.oma * g.st[j].x;
       const float xn = frozen ? g.st[j].x : xa;
-      *out = make_float2(xn, g.st[j].y);
+      stp[g.kk[j] * 32] = xn;
       *xi = rp.sigma * xn - g.st[j].z;
       if constexpr (kTrack) chg = fmaxf(chg, fabsf(xn - g.st[j].x) * g.f[j]);
     } else {
@@ -740,23 +762,23 @@ __device__ __forceinline__ void update_rel_group(const RelGroup& g, const RelPar
 }
 
 template <bool kCons, bool kTrack, bool kFrontier, bool kRho>
-__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const float2* S, const float2* SP,
+__device__ __forceinline__ void run_releases(const int4* rel, int begin, int end, const StageRecs& S,
                                              const float* SE, const RelParams& rp, unsigned char* xb, float* rt,
-                                             float2* stu,
+                                             float2* stu, float* stp,
                                              float* peu, float& chg, float& pres, bool frozen,
                                              const float* unscale_perm, const int* ucls, const RhoLane& rl) {
   if (begin >= end) return;
   RelGroup a, b;
-  load_rel_group<kTrack, kFrontier, kRho>(rel, begin, end, S, SP, SE, xb, unscale_perm, ucls, rl, a);
+  load_rel_group<kCons, kTrack, kFrontier, kRho>(rel, begin, end, S, SE, xb, unscale_perm, ucls, rl, a);
   for (int k = begin;; k += 2 * kRelGroup) {
     // a group starting at or past `end` clamps to end - 1 (loads only)
     const int kb = k + kRelGroup < end ? k + kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier, kRho>(rel, kb, end, S, SP, SE, xb, unscale_perm, ucls, rl, b);
-    update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, peu, chg, pres, frozen);
+    load_rel_group<kCons, kTrack, kFrontier, kRho>(rel, kb, end, S, SE, xb, unscale_perm, ucls, rl, b);
+    update_rel_group<kCons, kTrack, kFrontier>(a, rp, xb, rt, stu, stp, peu, chg, pres, frozen);
     if (k + kRelGroup >= end) break;
     const int ka = k + 2 * kRelGroup < end ? k + 2 * kRelGroup : end - 1;
-    load_rel_group<kTrack, kFrontier, kRho>(rel, ka, end, S, SP, SE, xb, unscale_perm, ucls, rl, a);
-    update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, peu, chg, pres, frozen);
+    load_rel_group<kCons, kTrack, kFrontier, kRho>(rel, ka, end, S, SE, xb, unscale_perm, ucls, rl, a);
+    update_rel_group<kCons, kTrack, kFrontier>(b, rp, xb, rt, stu, stp, peu, chg, pres, frozen);
     if (k + 2 * kRelGroup >= end) break;
   }
 }
@@ -849,7 +871,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         // sides (forward) or the columns' forward results (backward) behind
         // the L data; backward and first-rhs items also the state records.
         struct Copies {
-          int moff, mwords, loff, nrel, u0;
+          int moff, mwords, loff, nrel, u0, nprim;
           uint32_t lbytes, pre_at, xrow, xbytes;
         };
         auto describe = [&](int kind, int ch) {
@@ -860,6 +882,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           d.loff = __ldg((fwd ? sp.fchunk_off : sp.chunk_off) + ch);
           d.nrel = 0;
           d.u0 = 0;
+          d.nprim = 0;
           d.pre_at = 0;
           d.xrow = 0;
           d.xbytes = 0;
@@ -872,6 +895,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           } else {
             d.nrel = __ldg(sp.chunk_nrel + ch);
             d.u0 = __ldg(sp.chunk_u0 + ch);
+            d.nprim = __ldg(sp.chunk_nprim + ch);
             if (kind == kItemBwd) {
               const uint32_t cols = (uint32_t)__ldg(sp.chunk_cols + ch);
               d.lbytes = (uint32_t)__ldg(sp.chunk_units + ch) * 512u + cols * 128u;
@@ -931,14 +955,21 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
                 !mbar_wait_bounded(sempty + sr.stage, sr.phase ^ 1u, abort_flag, a.wait_limit_ns))
               return false;
             unsigned char* ss = sring + (size_t)sr.stage * a.sbytes;
-            const uint32_t nrel = (uint32_t)d.nrel;
-            mbar_arrive_expect_tx(sfull + sr.stage, nrel * (kTrack ? 640u : 512u));
-            if (nrel) {
-              const size_t u = soff + (size_t)d.u0 * 32;
-              bulk_g2s(ss, J.state + u, nrel * 256u, sfull + sr.stage);
-              bulk_g2s(ss + a.pres_off / 2, J.param + u, nrel * 256u, sfull + sr.stage);
-              if constexpr (kTrack) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
+            const uint32_t nrel = (uint32_t)d.nrel, np = (uint32_t)d.nprim, nc = nrel - np;
+            // per region (iterates at 0, parameters at pres_off / 2): the primal
+            // records (4 bytes), then the constraints' (8 bytes)
+            mbar_arrive_expect_tx(sfull + sr.stage, 2u * (np * 128u + nc * 256u) + (kTrack ? nrel * 128u : 0u));
+            const size_t u = soff + (size_t)d.u0 * 32;
+            if (np) {
+              bulk_g2s(ss, J.state_p + u, np * 128u, sfull + sr.stage);
+              bulk_g2s(ss + a.pres_off / 2, J.param_p + u, np * 128u, sfull + sr.stage);
             }
+            if (nc) {
+              const size_t uc = u + (size_t)np * 32;
+              bulk_g2s(ss + np * 128u, J.state + uc, nc * 256u, sfull + sr.stage);
+              bulk_g2s(ss + a.pres_off / 2 + np * 128u, J.param + uc, nc * 256u, sfull + sr.stage);
+            }
+            if (kTrack && nrel) bulk_g2s(ss + a.pres_off, J.pres + u, nrel * 128u, sfull + sr.stage);
             sr.advance(a.sstages);
             ++issued_s;
           }
@@ -1037,6 +1068,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
         yt = J.fwd + (size_t)tile * n * 32 + lane;
       }
       float2* stt = J.state + (size_t)tile * n * 32 + lane;
+      float* stpt = J.state_p + (size_t)tile * n * 32 + lane;
       float* pet = J.pres + (size_t)tile * n * 32 + lane;
       RhoLane rl{};
       if constexpr (kRho) {
@@ -1096,19 +1128,22 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           // leaf columns (read by no other column): solved here, just before their release
           if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
           if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, a.wait_limit_ns)) return false;
-          const float2* S = reinterpret_cast<const float2*>(sring + (size_t)sr.stage * a.sbytes) + lane;
-          const float2* SP = reinterpret_cast<const float2*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off / 2) + lane;
+          const unsigned char* sst = sring + (size_t)sr.stage * a.sbytes;
+          const StageRecs S{reinterpret_cast<const float*>(sst) + lane,
+                            reinterpret_cast<const float*>(sst + a.pres_off / 2) + lane,
+                            reinterpret_cast<const float2*>(sst + nprim * 128) + lane,
+                            reinterpret_cast<const float2*>(sst + a.pres_off / 2 + nprim * 128) + lane, nprim};
           const float* SE = reinterpret_cast<const float*>(sring + (size_t)sr.stage * a.sbytes + a.pres_off) + lane;
           if (kind == kItemRel) {
             // first right-hand side: sigma x - q (primal), z - rho^-1 y (constraint)
             // (frontier form: into rhs at the record's index)
             for (int k = pb; k < pe; ++k) {
               const int4 r = rel[k];
-              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = sigma * S[k * 32].x - SP[k * 32].x;
+              *(kFrontier ? rt + r.w * 32 : reinterpret_cast<float*>(xb + r.x)) = sigma * S.ip[k * 32] - S.pp[k * 32];
             }
             for (int k = cb; k < ce; ++k) {
               const int4 r = rel[k];
-              const float2 st = S[k * 32];
+              const float2 st = S.ic[(k - nprim) * 32];
               float rinv = __int_as_float(r.z);
               if constexpr (kRho) {
                 float rho;
@@ -1120,12 +1155,13 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             if (kFrontier && ch == 0) fence_proxy_async_global();
           } else {
             float2* stu = stt + (size_t)u0 * 32;
+            float* stp = stpt + (size_t)u0 * 32;
             float* peu = pet + (size_t)u0 * 32;
             const RelParams rp{sigma, alpha, oma};
             const int* ucls = kRho ? sp.u_cls + u0 : nullptr;
-            run_releases<false, kTrack, kFrontier, false>(rel, pb, pe, S, SP, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+            run_releases<false, kTrack, kFrontier, false>(rel, pb, pe, S, SE, rp, xb, rt, stu, stp, peu, chg, pres, frozen,
                                                           sp.unscale_perm, ucls, rl);
-            run_releases<true, kTrack, kFrontier, kRho>(rel, cb, ce, S, SP, SE, rp, xb, rt, stu, peu, chg, pres, frozen,
+            run_releases<true, kTrack, kFrontier, kRho>(rel, cb, ce, S, SE, rp, xb, rt, stu, stp, peu, chg, pres, frozen,
                                                         sp.unscale_perm, ucls, rl);
             // order these generic-proxy state writes before the bulk copies
             // that read them back in the next pass
@@ -1349,7 +1385,7 @@ int stream_ctas_for(const StreamPlan& sp, int device, int tiles, int num_sms, in
 // streams, state records, residuals (+ frontier form: right-hand sides and forward results)
 size_t stream_workspace_floats(const StreamPlan& sp, int batch) {
   const size_t tiles = (size_t)(batch + 31) / 32;
-  const size_t vectors = sp.frontier_slots > 0 ? 7 : 5;
+  const size_t vectors = sp.frontier_slots > 0 ? 9 : 7;  // state 2 + 2 (+ 1 + 1 primal), pres (+ rhs, fwd)
   return tiles * ((size_t)sp.blen + (size_t)sp.flen + vectors * 32 * (size_t)sp.n) + 64;
 }
 
@@ -1367,7 +1403,9 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   float* fstream = bstream + (size_t)n_tiles * sp.blen;
   float2* state = reinterpret_cast<float2*>(fstream + (size_t)n_tiles * sp.flen);
   float2* param = state + tl * sp.n;
-  float* pres = reinterpret_cast<float*>(param + tl * sp.n);
+  float* state_p = reinterpret_cast<float*>(param + tl * sp.n);
+  float* param_p = state_p + tl * sp.n;
+  float* pres = param_p + tl * sp.n;
   float* rhs = sp.frontier_slots > 0 ? pres + tl * sp.n : nullptr;
   float* fwd = sp.frontier_slots > 0 ? rhs + tl * sp.n : nullptr;
   OsqpInputs in{pT, ldp, sbp, aT, lda, sba, rinv_rows, rinv_rows ? (long long)batch : 0};
@@ -1398,8 +1436,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   }
   {
     dim3 grid(ceil_div(tl, 128), sp.n < 1024 ? sp.n : 1024);
-    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm && track, x, z, y, qs, ls, us, state, param, pres,
-                                                 batch, n_tiles);
+    state_to_stream_kernel<<<grid, 128, 0, s>>>(sp, o, in, warm && track, x, z, y, qs, ls, us, state, param, state_p,
+                                                 param_p, pres, batch, n_tiles);
     WMPC_LAUNCH_CHECK();
   }
   job->sp = sp;
@@ -1407,6 +1445,8 @@ int stream_begin(const Pattern& pat, const StreamPlan& sp, const Osqp& o, const 
   job->fstream = fstream;
   job->state = state;
   job->param = param;
+  job->state_p = state_p;
+  job->param_p = param_p;
   job->pres = pres;
   job->rhs = rhs;
   job->fwd = fwd;
@@ -1485,6 +1525,8 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
     J.fstream = d.fstream;
     J.state = d.state;
     J.param = d.param;
+    J.state_p = d.state_p;
+    J.param_p = d.param_p;
     J.pres = d.pres;
     J.rhs = d.rhs;
     J.fwd = d.fwd;
@@ -1537,7 +1579,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
 int stream_end(const StreamPlan& sp, const Osqp& o, const StreamJobDesc& job, float* x, float* z, float* y,
                cudaStream_t s) {
   dim3 grid2(ceil_div(job.batch, 128), sp.n < 1024 ? sp.n : 1024);
-  stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, job.state, x, z, y, job.batch);
+  stream_to_state_kernel<<<grid2, 128, 0, s>>>(sp, o.n, job.state, job.state_p, x, z, y, job.batch);
   WMPC_LAUNCH_CHECK();
   return WMPC_OK;
 }

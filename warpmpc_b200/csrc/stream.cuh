@@ -9,9 +9,9 @@
 // contiguous bulk copy (cp.async.bulk) into a shared-memory ring stage.
 //
 // ADMM state (x or z, y) and parameters (q or l, u) are stored per tile as
-// two 8-byte records per (index, lane) in two arrays -- the iterates, written
-// every iteration, and the parameters, only read -- in "release order" U: the
-// order in which
+// records per (index, lane) -- the iterates, written every iteration, and the
+// parameters, only read; 4 bytes for a primal index, 8 for a constraint --
+// in "release order" U: the order in which
 // the backward sweep finishes with a KKT index (after the smallest column
 // whose correction reads it), so each chunk of the backward sweep updates one
 // contiguous U range.
@@ -75,6 +75,7 @@ struct StreamPlan {
   const int* chunk_cols;    // [n_chunks]
   const int* chunk_u0;      // [n_chunks] first U index released
   const int* chunk_nrel;    // [n_chunks]
+  const int* chunk_nprim;   // [n_chunks] primal releases (the chunk's first)
   const int* chunk_pre_u0;     // [n_chunks] stage position of the releaser's forward units
   const int* chunk_pre_units;  // [n_chunks] their count (copied in the first-right-hand-side pass too)
   const int* meta_off;      // [n_chunks]
@@ -314,8 +315,10 @@ struct StreamJobDesc {
   StreamPlan sp;
   const float* bstream = nullptr;
   const float* fstream = nullptr;
-  float2* state = nullptr;        // [tile][U][lane] iterate records
-  const float2* param = nullptr;  // [tile][U][lane] parameter records
+  float2* state = nullptr;        // [tile][U][lane] constraint iterate records (z, y)
+  const float2* param = nullptr;  // [tile][U][lane] constraint parameter records (l, u)
+  float* state_p = nullptr;       // [tile][U][lane] primal iterate records x
+  const float* param_p = nullptr; // [tile][U][lane] primal parameter records (sigma-scaled q)
   float* pres = nullptr;
   float* rhs = nullptr;   // frontier form: [tile][n][lane] right-hand sides
   float* fwd = nullptr;   // frontier form: [tile][n][lane] forward results
