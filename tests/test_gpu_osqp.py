@@ -229,3 +229,31 @@ def test_autotune_stream_candidates_agree(cuda_device, tmp_path):
     assert r.best in [dict(c) for c in cands] and len(r.timings_ms) == len(cands) and not r.cached
     again = autotune_stream(plan, b.p_values, b.a_values, b.q, b.l, b.u, candidates=cands, cache_path=cache)
     assert again.cached and again.best == r.best
+
+
+def test_solve_host_default_slicing_and_caller_workspace(cuda_device):
+    """The host-buffer solve with its default slicing (four wave-aligned
+    slices) over several waves, and a device solve given the caller's
+    workspace: both bit-identical to a plain device solve; a workspace that is
+    too small is refused."""
+    import torch
+
+    b = problems.make_batch(problems.SMALL, 4 * 32 * 148 + 77, seed=97)
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    eng = comp.engine
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()  # noqa: E731
+    args = [pin(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u)]
+    dev_args = [a.cuda() for a in args]
+    want = [t.cpu().numpy() for t in eng.solve(*dev_args)]
+    got = eng.solve_host(*args)
+    for g, r in zip(got, want):
+        np.testing.assert_array_equal(g.numpy(), r)
+    batch = b.batch
+    ws = torch.empty(eng.workspace_bytes(batch, keep_factor=True), dtype=torch.uint8, device=cuda_device)
+    got2 = [t.cpu().numpy() for t in eng.solve(*dev_args, workspace=ws)]
+    for g, r in zip(got2, want):
+        np.testing.assert_array_equal(g, r)
+    small = torch.empty(16, dtype=torch.uint8, device=cuda_device)
+    with pytest.raises(ValueError):
+        eng.solve(*dev_args, workspace=small)
