@@ -181,6 +181,7 @@ bool build_stream_plan(const HostPattern& hp, const StreamTargets& targets, cons
   sp.max_cols = hs.max_cols;
   sp.max_rel = hs.max_rel;
   sp.max_meta_words = hs.max_meta_words;
+  sp.max_meta_lead = hs.max_meta_lead;
   sp.max_row_nnz = max_row;
   sp.n_fchunks = hs.n_fchunks;
   sp.flen = hs.flen;

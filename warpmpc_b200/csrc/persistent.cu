@@ -446,6 +446,8 @@ struct StreamArgs {
   int sbytes;       // per S stage: max_rel x 32 lanes x (8 iterate + 8 parameter) bytes (+ 4 of residuals)
   int pres_off;     // byte offset of the residuals in an S stage (end of the records; the
                     // parameter records start at pres_off / 2)
+  int rec_off;      // frontier form: byte offset in an S stage of the releases' header
+                    // {nrel, u0, nprim, 0} and, after it, their 16-byte records
   unsigned long long wait_limit_ns;  // give-up time of every handshake wait (the drain keeps kWaitLimitNs)
 };
 static_assert(sizeof(StreamArgs) <= 4000, "launch arguments exceed the kernel parameter space");
@@ -942,8 +944,11 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
               xsrc = J.fwd + soff + (size_t)d.xrow * 32;
             }
           }
-          mbar_arrive_expect_tx(lfull + lr.stage, (uint32_t)d.mwords * 4u + d.lbytes + d.xbytes);
-          bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + d.moff, (uint32_t)d.mwords * 4u, lfull + lr.stage);
+          // (frontier form: a release item's records, the last 4 nrel words of
+          // its meta block, go to its S stage)
+          const uint32_t mwords_l = (uint32_t)d.mwords - (kFrontier ? 4u * (uint32_t)d.nrel : 0u);
+          mbar_arrive_expect_tx(lfull + lr.stage, mwords_l * 4u + d.lbytes + d.xbytes);
+          bulk_g2s(st, (fwd ? sp.fmeta : sp.meta) + d.moff, mwords_l * 4u, lfull + lr.stage);
           if (d.lbytes)
             bulk_g2s(st + a.meta_bytes + d.pre_at * 512u, (fwd ? ft : bt) + d.loff + d.pre_at * 128u, d.lbytes,
                      lfull + lr.stage);
@@ -958,7 +963,12 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             const uint32_t nrel = (uint32_t)d.nrel, np = (uint32_t)d.nprim, nc = nrel - np;
             // per region (iterates at 0, parameters at pres_off / 2): the primal
             // records (4 bytes), then the constraints' (8 bytes)
-            mbar_arrive_expect_tx(sfull + sr.stage, 2u * (np * 128u + nc * 256u) + (kTrack ? nrel * 128u : 0u));
+            if constexpr (kFrontier)  // the releases' header, then (bulk) their records
+              *reinterpret_cast<int4*>(ss + a.rec_off) = make_int4(d.nrel, d.u0, d.nprim, 0);
+            mbar_arrive_expect_tx(sfull + sr.stage, 2u * (np * 128u + nc * 256u) + (kTrack ? nrel * 128u : 0u) +
+                                                        (kFrontier ? nrel * 16u : 0u));
+            if (kFrontier && nrel)
+              bulk_g2s(ss + a.rec_off + 16, sp.meta + d.moff + d.mwords - 4 * (int)nrel, nrel * 16u, sfull + sr.stage);
             const size_t u = soff + (size_t)d.u0 * 32;
             if (np) {
               bulk_g2s(ss, J.state_p + u, np * 128u, sfull + sr.stage);
@@ -1001,6 +1011,12 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           // a forward sweep needs every right-hand side of the previous pass
           if (kind == kItemFwd && ch == 0 && !wait_counter_bounded(rel_done, t, abort_flag, a.wait_limit_ns))
             return false;
+          // frontier form: the slots assume that a backward chunk's releases
+          // are done before the sweep is frontier_lag chunks further (the
+          // sweeper frees backward stages itself, so the ring does not pace it)
+          if (kFrontier && kind == kItemBwd && t + 1 >= (unsigned)sp.frontier_lag &&
+              !wait_counter_bounded(rel_done, t + 1 - (unsigned)sp.frontier_lag, abort_flag, a.wait_limit_ns))
+            return false;
           if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, a.wait_limit_ns)) return false;
           const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
           const int* meta = reinterpret_cast<const int*>(stage);
@@ -1028,7 +1044,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           if (lane == 0) {
             // (frontier form: the second releaser frees a forward stage once it
             // has copied the stage's forward results out)
-            if (!kFrontier && kind == kItemFwd) mbar_arrive(lempty + lr.stage);
+            if (kFrontier ? kind == kItemBwd : kind == kItemFwd) mbar_arrive(lempty + lr.stage);
             st_release_cta(sweep_done, t + 1);
           }
           __syncwarp();
@@ -1106,13 +1122,38 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           } else if (!mbar_wait_bounded(lfull + lr.stage, lr.phase, abort_flag, a.wait_limit_ns)) {
             return false;
           }
-          const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
-          const int* meta = reinterpret_cast<const int*>(stage);
-          const unsigned char* lst = stage + a.meta_bytes;
-          const int ns = meta[0], nrel = meta[2], u0 = meta[4], nprim = meta[5], nl = meta[6], np = meta[7];
-          const int4* mu_leaf = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + kUnitSentinels) * kUnitWords);
-          const int4* mu_pre = mu_leaf + (nl + kUnitSentinels) * (kUnitWords / 4);
-          const int4* rel = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + nl + np + 3 * kUnitSentinels) * kUnitWords);
+          // plain form: the releases' header and records are in the item's L
+          // stage (with the releaser's units); frontier form: in its S stage
+          // (the sweeper frees a backward L stage as soon as it is swept)
+          int nrel = 0, u0 = 0, nprim = 0, nl = 0, np = 0;
+          const int4* mu_pre = nullptr;
+          const int4* rel = nullptr;
+          const unsigned char* lst = nullptr;
+          if constexpr (!kFrontier) {
+            const unsigned char* stage = lring + (size_t)lr.stage * lstage_bytes;
+            const int* meta = reinterpret_cast<const int*>(stage);
+            lst = stage + a.meta_bytes;
+            const int ns = meta[0];
+            nrel = meta[2];
+            u0 = meta[4];
+            nprim = meta[5];
+            nl = meta[6];
+            np = meta[7];
+            const int4* mu_leaf = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + kUnitSentinels) * kUnitWords);
+            mu_pre = mu_leaf + (nl + kUnitSentinels) * (kUnitWords / 4);
+            rel = reinterpret_cast<const int4*>(meta + kChunkHeader + (ns + nl + np + 3 * kUnitSentinels) * kUnitWords);
+            // leaf columns (read by no other column): solved here, just before their release
+            if (rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
+          }
+          if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, a.wait_limit_ns)) return false;
+          const unsigned char* sst = sring + (size_t)sr.stage * a.sbytes;
+          if constexpr (kFrontier) {
+            const int4 h = *reinterpret_cast<const int4*>(sst + a.rec_off);
+            nrel = h.x;
+            u0 = h.y;
+            nprim = h.z;
+            rel = reinterpret_cast<const int4*>(sst + a.rec_off + 16);
+          }
           // this warp's share of the releases: halves of the primal and of the
           // constraint range (all of them, on releaser 0, when the chunk has
           // releaser units, which need every release of the chunk done first)
@@ -1125,10 +1166,6 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
           int pb, pe, cb, ce;
           share(0, nprim, pb, pe);
           share(nprim, nrel, cb, ce);
-          // leaf columns (read by no other column): solved here, just before their release
-          if (!kFrontier && rw == 0 && kind == kItemBwd && nl > 0) run_units<true>(mu_leaf, lst, xb, xb, lane, nl);
-          if (!mbar_wait_bounded(sfull + sr.stage, sr.phase, abort_flag, a.wait_limit_ns)) return false;
-          const unsigned char* sst = sring + (size_t)sr.stage * a.sbytes;
           const StageRecs S{reinterpret_cast<const float*>(sst) + lane,
                             reinterpret_cast<const float*>(sst + a.pres_off / 2) + lane,
                             reinterpret_cast<const float2*>(sst + nprim * 128) + lane,
@@ -1180,7 +1217,7 @@ __global__ void __launch_bounds__(128, 1) admm_stream_kernel(const __grid_consta
             if (kSplit && !wait_counter_bounded(rel_done1, t + 1, abort_flag, a.wait_limit_ns)) return false;
             if (lane == 0) {
               mbar_arrive(sempty + sr.stage);
-              mbar_arrive(lempty + lr.stage);
+              if (!kFrontier || kind != kItemBwd) mbar_arrive(lempty + lr.stage);
             }
           }
           sr.advance(a.sstages);
@@ -1256,7 +1293,10 @@ struct RingSizes {
 // track: the S stages also carry the primal residuals (termination checked)
 RingSizes ring_sizes(const StreamPlan& sp, bool track) {
   RingSizes r;
-  const int mw = sp.max_meta_words > sp.max_fmeta_words ? sp.max_meta_words : sp.max_fmeta_words;
+  const bool fr = sp.frontier_slots > 0;
+  // (frontier form: without a backward chunk's release records, which go to the S stage)
+  const int mwb = fr ? sp.max_meta_lead : sp.max_meta_words;
+  const int mw = mwb > sp.max_fmeta_words ? mwb : sp.max_fmeta_words;
   r.meta_bytes = ((mw * 4 + 127) / 128) * 128;
   // (frontier form: a backward stage also holds its columns' forward results,
   // a forward stage its rows' right-hand sides)
@@ -1266,6 +1306,7 @@ RingSizes ring_sizes(const StreamPlan& sp, bool track) {
   r.lbytes = ((bl > fl ? bl : fl) + 127) / 128 * 128;
   r.pres_off = (sp.max_rel > 0 ? sp.max_rel : 1) * 512;
   r.sbytes = r.pres_off + (track ? r.pres_off / 4 : 0);
+  if (fr) r.sbytes += 16 + 16 * (sp.max_rel > 0 ? sp.max_rel : 1);  // releases' header and records
   r.x_rows = (frontier ? sp.frontier_slots : sp.n) + 2;
   r.lmax = sp.max_lstages >= 2 ? sp.max_lstages : 12;
   r.smax = sp.max_sstages >= 2 ? sp.max_sstages : 6;
@@ -1554,6 +1595,7 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   a.lbytes = cfg.lbytes;
   a.sbytes = cfg.sbytes;
   a.pres_off = cfg.pres_off;
+  a.rec_off = cfg.pres_off + (track ? cfg.pres_off / 4 : 0);
   a.wait_limit_ns = kWaitLimitNs;
   if (const char* v = getenv("WMPC_STREAM_WAIT_LIMIT_NS")) {
     const long long ns = atoll(v);

@@ -635,6 +635,7 @@ bool build_stream_schedule(const HostPattern& hp, const StreamTargets& t, const 
       bwd_units.push_back(std::move(cu));
     }
     S.max_meta_words = std::max(S.max_meta_words, static_cast<int>(m.size()));
+    S.max_meta_lead = std::max(S.max_meta_lead, static_cast<int>(m.size()) - 4 * nrel);
     S.meta.insert(S.meta.end(), m.begin(), m.end());
     for (int li = 0; li < 3; ++li)
       for (int u = 0; u < static_cast<int>(lists[li].size()); ++u)

@@ -70,6 +70,7 @@ struct StreamPlan {
   const int* fmeta;
   // backward sweep (column form) + releases
   int n_chunks, blen, max_units, max_cols, max_rel, max_meta_words;
+  int max_meta_lead;        // backward meta words before the release records (the last 4 nrel words), at most
   const int* chunk_off;     // [n_chunks + 1] float offset (lane 0) in the backward stream
   const int* chunk_units;   // [n_chunks]
   const int* chunk_cols;    // [n_chunks]
@@ -265,6 +266,7 @@ struct StreamTargets {
 // Host result: every array of StreamPlan, to be uploaded by the plan.
 struct HostStream {
   int n_chunks = 0, blen = 0, max_units = 0, max_cols = 0, max_rel = 0, max_meta_words = 0;
+  int max_meta_lead = 0;  // backward meta words before the release records, at most
   std::vector<int> chunk_off, chunk_units, chunk_cols, chunk_u0, chunk_nrel, meta_off, meta_words, meta;
   std::vector<int> chunk_pre_u0, chunk_pre_units;
   int n_fchunks = 0, flen = 0, max_funits = 0, max_fmeta_words = 0;
