@@ -790,7 +790,9 @@ __device__ __forceinline__ void run_releases(const int4* rel, int begin, int end
 // 2 releases (first right-hand side, ADMM updates; with fixed iterations warp
 // 3 releases half of each chunk's indices alongside).  Every warp walks the same
 // item sequence; item t's L stage is freed by the warp that finishes with it
-// last (forward: sweeper; backward and first-rhs: releaser).  Two monotone
+// last (plain form: forward sweeper, backward and first-rhs releaser; frontier
+// form: forward the second releaser, backward the sweeper, first-rhs the
+// releaser -- its release records travel in the S stage).  Two monotone
 // counters order the consumers: sweep_done (items the sweeper finished: a
 // backward item's releases need its columns solved) and rel_done (items the
 // releaser finished: a forward sweep needs every right-hand side).
