@@ -985,8 +985,11 @@ def main():
         def e2e_step():
             # host in, host out: the engine copies slices in and out on two streams while it solves;
             # then the host applies u0 and writes the instances' next states into l and u
-            comp.engine.solve_host(hP, hA, hQ, hL, hU, warm=(hx, hz, hy), out=(hx, hz, hy, *hres))
-            hloop.advance_host(hx.numpy(), hL.numpy(), hU.numpy())
+            # (each slice's instances advance as soon as its results are on the host,
+            # while the later slices are still being solved)
+            comp.engine.solve_host(hP, hA, hQ, hL, hU, warm=(hx, hz, hy), out=(hx, hz, hy, *hres),
+                                   on_slice=lambda s0, s1: hloop.advance_host(hx.numpy(), hL.numpy(), hU.numpy(),
+                                                                              rows=(s0, s1)))
 
         e2e_step()
         torch.cuda.synchronize()

@@ -257,3 +257,34 @@ def test_solve_host_default_slicing_and_caller_workspace(cuda_device):
     small = torch.empty(16, dtype=torch.uint8, device=cuda_device)
     with pytest.raises(ValueError):
         eng.solve(*dev_args, workspace=small)
+
+
+@pytest.mark.gpu
+def test_solve_host_per_slice_callback(cuda_device):
+    """on_slice is called once per slice, in order, over contiguous ranges
+    covering the batch, each time with that slice's results already on the
+    host; the results stay bit-identical to a device solve."""
+    import torch
+
+    b = problems.make_batch(problems.SMALL, 3 * 32 * 148 + 5, seed=41)
+    plan = problems.make_plan(b)
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent")
+    eng = comp.engine
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()  # noqa: E731
+    args = [pin(v) for v in (b.p_values, b.a_values, b.q, b.l, b.u)]
+    want = [t.cpu().numpy() for t in eng.solve(*[a.cuda() for a in args])]
+    calls = []
+    out = tuple(torch.full(t.shape, float("nan"), dtype=torch.float32).pin_memory() for t in
+                (torch.empty(b.batch, plan.n), torch.empty(b.batch, plan.m), torch.empty(b.batch, plan.m),
+                 torch.empty(b.batch), torch.empty(b.batch), torch.empty(b.batch)))
+
+    def seen(s0, s1):
+        # this slice's x is already on the host
+        np.testing.assert_array_equal(out[0][s0:s1].numpy(), want[0][s0:s1])
+        calls.append((s0, s1))
+
+    got = eng.solve_host(*args, out=out, on_slice=seen)
+    assert len(calls) >= 2 and calls[0][0] == 0 and calls[-1][1] == b.batch
+    assert all(calls[i][1] == calls[i + 1][0] for i in range(len(calls) - 1))
+    for g, r in zip(got, want):
+        np.testing.assert_array_equal(g.numpy(), r)

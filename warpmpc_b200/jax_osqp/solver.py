@@ -310,7 +310,7 @@ class OSQPEngine:
         return x, z, y, prim, dual, obj
 
     def solve_host(self, p_values, a_values, q, l, u, warm=None, out=None, chunks=4, max_iter=None,
-                   check_termination=None, granule=None, first_fraction=0.15):
+                   check_termination=None, granule=None, first_fraction=0.15, on_slice=None):
         """Batched solve of host (CPU) tensors into host tensors, transfers overlapped with the solves.
 
         The batch is cut into ``chunks`` slices with boundaries on whole waves
@@ -332,7 +332,11 @@ class OSQPEngine:
         copied in before its results are copied out).  Returns them once the
         results are on the host (the
         call synchronizes the current stream); ``last_iters`` and
-        ``last_status`` are host tensors afterwards.
+        ``last_status`` are host tensors afterwards.  ``on_slice(s0, s1)``, if
+        given, is called for each slice in order as soon as its results are on
+        the host, while the later slices are still being solved (a closed loop
+        can advance those instances meanwhile); it may rewrite the host input
+        rows [s0, s1), whose copies are done, and no other rows.
         """
         import torch
 
@@ -435,6 +439,10 @@ class OSQPEngine:
             ev = torch.cuda.Event()
             ev.record(down)
             copied.append(ev)
+        if on_slice is not None:
+            for i in range(k):
+                copied[i].synchronize()
+                on_slice(bounds[i], bounds[i + 1])
         cur.wait_event(copied[-1])
         cur.wait_event(in_ready[-1])
         cur.synchronize()

@@ -242,20 +242,22 @@ class ClosedLoop:
         l[:, :nx] = -self.x0
         u[:, :nx] = -self.x0
 
-    def advance_host(self, x, l, u):
+    def advance_host(self, x, l, u, rows=None):
         """Host version of ``advance`` on NumPy arrays or host tensors (updated
         in place): the same torch operations on CPU (batched matrix products
-        on the host's threads, through zero-copy views)."""
+        on the host's threads, through zero-copy views).  ``rows=(s0, s1)``
+        advances only instances s0..s1-1 (x, l, u are still whole-batch arrays)."""
         import torch
 
         nx, nu = self.cls.nx, self.cls.nu
-        xt = torch.from_numpy(np.asarray(x, dtype=np.float32))
-        a, b, x0 = (torch.from_numpy(v) for v in (self.a_np, self.b_np, self.x0_np))
+        s0, s1 = (0, self.x0_np.shape[0]) if rows is None else rows
+        xt = torch.from_numpy(np.asarray(x, dtype=np.float32))[s0:s1]
+        a, b, x0 = (torch.from_numpy(v)[s0:s1] for v in (self.a_np, self.b_np, self.x0_np))
         u0 = xt[:, self.ui : self.ui + nu]
         nxt = torch.bmm(a, x0[:, :, None])[:, :, 0] + torch.bmm(b, u0[:, :, None])[:, :, 0]
         x0.copy_(nxt.clamp_(-float(self.bound), float(self.bound)))
         for t in (l, u):
-            torch.from_numpy(np.asarray(t))[:, :nx] = -x0
+            torch.from_numpy(np.asarray(t))[s0:s1, :nx] = -x0
 
 
 def make_batch(cls: MPCClass, batch: int, seed: int = 0, dtype=np.float32) -> MPCBatch:
