@@ -198,9 +198,46 @@ def barrier(world):
         multirank.barrier(_env(world))
 
 
-def cpu_baseline(plan, batch_np, args, cls, seed, cores=None):
+def accuracy_vs_fp64(plan, p, a, q, l, u, warm, dev, cores):
+    """The library's solve of a step's inputs (host arrays, float32) against a
+    float64 run of the C restatement from the same inputs and warm start (the
+    reference's JAX/Warp backends cannot run here): per instance the largest
+    deviation of x, z, y relative to the float64 solution's largest entry."""
+    import torch
+
+    from oracle.cpu_baseline import CpuOSQP
+    from warpmpc_b200.jax_osqp import compile_osqp
+
+    comp = compile_osqp(plan, np.float32, qdldl_backend="cuda", transpose_work=True, mode="persistent", device=dev)
+    t = lambda v: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)).to(dev)  # noqa: E731
+    got = comp.engine.solve(t(p), t(a), t(q), t(l), t(u), warm=tuple(t(w) for w in warm))
+    got = [g.cpu().numpy().astype(np.float64) for g in got[:3]]
+    f64 = lambda v: np.asarray(v, dtype=np.float64)  # noqa: E731
+    ref = CpuOSQP(plan, np.float64).solve(f64(p), f64(a), f64(q), f64(l), f64(u), warm=tuple(f64(w) for w in warm),
+                                         threads=cores)[:3]
+    f32 = lambda v: np.asarray(v, dtype=np.float32)  # noqa: E731
+    ref32 = CpuOSQP(plan, np.float32).solve(f32(p), f32(a), f32(q), f32(l), f32(u), warm=tuple(f32(w) for w in warm),
+                                           threads=cores)[:3]
+    out = {"instances": int(q.shape[0]), "iterations": int(plan.settings.max_iter),
+           "rule": "per instance max|v - v64| / max|v64| for v in x, z, y (same inputs and warm start)",
+           "fp32_restatement": {}}
+
+    def rel(g, r):
+        e = np.abs(g - r).max(1) / np.maximum(np.abs(r).max(1), 1e-30)
+        return {"median": float(np.median(e)), "max": float(e.max())}
+
+    for name, g, r, r32 in zip(("x", "z", "y"), got, ref, ref32):
+        out[name] = rel(g, r)
+        # the float32 C restatement's own error: what float32 arithmetic costs
+        out["fp32_restatement"][name] = rel(r32.astype(np.float64), r)
+    return out
+
+
+def cpu_baseline(plan, batch_np, args, cls, seed, cores=None, dev=None):
     """Oracle C restatement on the host cores: one closed-loop warm-started
-    step on a bounded sample (cold solve, state advanced by u0, timed warm solve)."""
+    step on a bounded sample (cold solve, state advanced by u0, timed warm solve).
+    With ``dev``, also the library's error on the first 256 instances of that
+    step against a float64 run of the restatement (``accuracy_vs_fp64``)."""
     from oracle.cpu_baseline import CpuOSQP
     from warpmpc_b200 import problems
 
@@ -226,7 +263,13 @@ def cpu_baseline(plan, batch_np, args, cls, seed, cores=None):
                                        threads=cores)
     dt = time.perf_counter() - t0
     ok = float(np.mean((prim <= RES_TOL) & (dual <= RES_TOL)))
+    acc = None
+    if dev is not None:
+        k = slice(0, min(256, sample))
+        acc = accuracy_vs_fp64(plan, b.p_values[k], b.a_values[k], b.q[k], lo[k], hi[k], (x[k], z[k], y[k]), dev,
+                               cores)
     return {
+        "accuracy_vs_fp64": acc,
         "value": sample * ok / dt,
         "unit": "solves/s",
         "cores": cpu.threads_used,
@@ -1057,7 +1100,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(plan, b, args, cls, seed)
+        cpu = cpu_baseline(plan, b, args, cls, seed, dev=dev)
 
     if rank == 0:
         line = {
@@ -1088,6 +1131,7 @@ def main():
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "accuracy_vs_fp64": cpu.pop("accuracy_vs_fp64") if cpu else None,
             "clocks": clocks.summary(),
             "gpu_launches": int(launches_step * args.steps),
             "algorithmic_bytes": {"per_instance": per_inst, "factor": fac_b, "iteration": it_b},
