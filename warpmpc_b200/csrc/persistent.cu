@@ -1539,9 +1539,9 @@ int stream_run(const StreamJobDesc* jobs, int n_jobs, int* error, int num_sms, c
   std::sort(order, order + n_jobs, [&](int x, int y) { return cost[x] > cost[y]; });
   StreamLaunch cfg;
   if (!ring_config(r, &cfg)) return fail(WMPC_ERR_UNSUPPORTED, "these classes do not fit one launch's shared memory");
-  // k CTAs (k sweepers) per SM when k fit with 4-stage L and 3-stage S rings
-  // (the ring depth does not limit the sweep; the sweeper's instruction stream
-  // does) and there are more tiles than k - 1 per SM: small patterns.
+  // k CTAs (k sweepers) per SM when k fit with rings of at most 4 L and 3 S
+  // stages (a sweeper per SM is worth more than ring depth beyond 2 stages)
+  // and there are more tiles than k - 1 per SM.
   int ctas_per_sm = 1;
   {
     const int tiles = total_tiles_of(jobs, n_jobs);
