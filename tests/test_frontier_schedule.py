@@ -147,3 +147,30 @@ def test_schedule_replay_random_patterns(bits):
         ref = osqp_ref.solve(plan, pv, av, q, lb, ub, max_iter=4)
         for name, g, r in zip("xzy", got, ref[:3]):
             np.testing.assert_array_equal(g, r, err_msg=f"trial {trial} ({n}x{m}): {name}")
+
+
+@pytest.mark.parametrize("cls", [problems.SMALL, problems.CARTPOLE, problems.QUADROTOR],
+                         ids=["small", "cartpole", "quadrotor"])
+@pytest.mark.parametrize("targets", [FRONTIER, FRONTIER_24, FRONTIER_COPIES], ids=["chunks16", "chunks24", "copies"])
+def test_frontier_release_records_close_each_backward_block(cls, targets):
+    """The frontier-form producer copies a backward chunk's release records
+    into its S stage as the last 4 nrel words of the chunk's meta block (one
+    16-byte-aligned bulk copy) and the rest of the block into the L stage:
+    the records must be exactly those words, in release order, each naming
+    its slot and its permuted KKT index, and the rest must stay 16-byte
+    aligned."""
+    plan = problems.make_plan(problems.make_batch(cls, 2, seed=0))
+    sched = stream_schedule(plan, targets=targets)
+    slots = int(sched["frontier_slots"])
+    assert slots > 0
+    meta, u_perm = np.asarray(sched["meta"]), np.asarray(sched["u_perm"])
+    for ch in range(int(sched["n_chunks"])):
+        off, words = int(sched["meta_off"][ch]), int(sched["meta_words"][ch])
+        m = meta[off : off + words]
+        nrel, u0 = int(sched["chunk_nrel"][ch]), int(sched["chunk_u0"][ch])
+        assert m[2] == nrel and m[4] == u0 and off % 4 == 0
+        lead = words - 4 * nrel
+        assert lead % 4 == 0 and lead >= 8
+        rec = m[lead:].reshape(nrel, 4)
+        np.testing.assert_array_equal(rec[:, 3], u_perm[u0 : u0 + nrel])
+        assert np.all(rec[:, 0] % 128 == 0) and np.all((rec[:, 0] >= 0) & (rec[:, 0] < slots * 128))
