@@ -322,8 +322,10 @@ class OSQPEngine:
         few slices; ``first_fraction`` sizes the first slice, whose copy in
         nothing hides; the rest are equal (None: all equal).  Measured on the
         quadrotor workload (65,536 instances, closed loop, host advance
-        included): 4 slices with a 0.15 first slice 109 ms per step, 3 with
-        0.15 113 ms, 2 with 0.3 127 ms, one 142 ms.  Each slice is an ordinary ``solve`` of its instances, so
+        included) when the solve itself took 83 ms: 4 slices with a 0.15 first
+        slice 109 ms per step, 3 with 0.15 113 ms, 2 with 0.3 127 ms, one 142
+        ms; with the current kernels the default takes 94.5 ms per step (the
+        host advance in ``on_slice``).  Each slice is an ordinary ``solve`` of its instances, so
         the results equal a one-shot ``solve`` of the whole batch bit for bit.
         Inputs should be in pinned memory (pageable tensors still work, without
         the overlap).  ``out`` optionally gives the six host output tensors
