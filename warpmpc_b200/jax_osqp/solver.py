@@ -322,7 +322,7 @@ class OSQPEngine:
         few slices; ``first_fraction`` sizes the first slice, whose copy in
         nothing hides; the rest are equal (None: all equal).  Measured on the
         quadrotor workload (65,536 instances, closed loop, host advance
-        included) when the solve itself took 83 ms: 4 slices with a 0.15 first
+        included) with earlier, slower kernels: 4 slices with a 0.15 first
         slice 109 ms per step, 3 with 0.15 113 ms, 2 with 0.3 127 ms, one 142
         ms; with the current kernels the default takes 94.5 ms per step (the
         host advance in ``on_slice``).  Each slice is an ordinary ``solve`` of its instances, so
